@@ -1,0 +1,491 @@
+#!/usr/bin/env python
+"""MPM particle-substeps/s of the B200-native MLS-MPM substep.
+
+Workload (N=1): the 500,000-particle mixed-material scene -- four seeded 50^3 jittered
+lattices (Liquid E=1e5 nu=0.2, Sand friction 45 deg, Snow yield 2.5e-2/7.5e-3,
+ElastoPlastic von Mises 1e4), v ~ N(0, 0.5 m/s), grid_density 128 (129^3 nodes),
+dt = 5e-5.  One bench step = one scene.step() of 100 substeps (the 2000-substep rollout
+is 20 steps).
+
+  value  particle-substeps/s with the state resident in HBM (CUDA events on the launch
+         stream, L2 flushed between timed steps)
+  e2e    the same through the public API (gs.Scene): every step uploads the full particle
+         state from pinned host memory, runs scene.step() and reads positions and
+         velocities back
+  roofline  the dominant kernel's algorithmic bytes / its measured duration, against the
+         measured HBM copy bandwidth
+  cpu_baseline  the C/OpenMP restatement of the reference algorithm on the host cores
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Under torchrun with N>1 every rank advances its own replica of the scene (the plain
+single-scene path has no exchange step): value = N x per-rank work / max rank time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MPM particle-substeps/s"
+UNIT = "particle-substeps/s"
+WORKLOAD = (
+    "mixed_500k: 4 x 125,000 particles (Liquid, Sand, Snow, ElastoPlastic), grid_density 128 (129^3 nodes), "
+    "dt 5e-5, 100 substeps per step"
+)
+# algorithmic bytes per particle / per active grid node, per kernel
+BYTES = {
+    "p2g": (148, 16),  # read x,v,C,F,Jp (100) + material idx & mass (8); write F,Jp (40); grid m+mom (16)
+    "grid_op": (0, 28),  # read m+mom (16), write v (12)
+    "g2p": (60, 12),  # write x,v,C (60); read grid v (12)  (x read counted in p2g)
+}
+SUBSTEP_BYTES = (208, 56)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--substeps-per-step", type=int, default=100)
+    ap.add_argument("--sort-interval", type=int, default=16)
+    ap.add_argument("--chunk", type=int, default=256)
+    ap.add_argument("--n-side", type=int, default=50, help="particles per box edge (50 -> 500k)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-run", action="store_true", help="short run for ncu launch lists")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            line = line.strip()
+            if line and not line.startswith("#") and "=" in line:
+                k, v = line.split("=", 1)
+                try:
+                    out[k.strip()] = float(v.split()[0])
+                except ValueError:
+                    pass
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def reduce_max(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ CPU (reference arm)
+def cpu_port_rate(desc, target_s=12.0, max_substeps=40):
+    """Time the C/OpenMP restatement on all host threads; returns (rate, threads, sample)."""
+    import numpy as np
+
+    from oracle import bridge, cref
+
+    threads = os.cpu_count() or 1
+    p, mats, st = bridge.from_desc(desc, np.float32)
+    t0 = time.perf_counter()
+    st1, _ = cref.substeps(p, mats, st, 1, n_threads=threads)
+    one = time.perf_counter() - t0
+    n = int(max(1, min(max_substeps, target_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    cref.substeps(p, mats, st1, n, n_threads=threads)
+    el = time.perf_counter() - t0
+    rate = desc.n_particles * n / el
+    return rate, threads, f"{desc.n_particles:,} particles x {n} substeps (after 1 warm-up substep), float32"
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    import numpy as np
+
+    from genesis_b200 import workloads as W
+    from oracle import bridge, cref
+
+    d = W.mixed_500k(n_side=args.n_side)
+    threads = os.cpu_count() or 1
+    p, mats, st = bridge.from_desc(d, np.float32)
+    sub = 2  # substeps per reference step: a bounded sample of the 100-substep step
+    for _ in range(max(0, min(args.warmup, 1))):
+        st, _ = cref.substeps(p, mats, st, 1, n_threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        st, _ = cref.substeps(p, mats, st, sub, n_threads=threads)
+        times.append(time.perf_counter() - t0)
+    el = sum(times)
+    value = d.n_particles * sub * args.steps / el
+    sample = f"{d.n_particles:,} particles x {sub} substeps per step, float32, {threads} threads"
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": d.n_particles, "grid": "129^3",
+                   "substeps_per_step": sub, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference = C/OpenMP restatement of Genesis's MPM substep (gstaichi, the reference's "
+                "runtime, is not installed on this image)",
+    }
+
+
+# ------------------------------------------------------------------ GPU (our arm)
+def kernel_breakdown(rt, n_substeps=20):
+    """Per-kernel CUDA-event durations (ms) over eager substeps on the launch stream."""
+    import torch
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    acc = {"sort": [], "p2g": [], "grid_op": [], "g2p": []}
+    K = max(rt.sort_interval, 1)
+    torch.cuda.synchronize()
+    # keep the GPU busy while the host enqueues, so events bracket kernels back to back
+    torch.cuda._sleep(int(2e8))
+    for _ in range(n_substeps):
+        if rt._count % K == 0:
+            a, b = ev(), ev()
+            a.record()
+            rt.sort()
+            b.record()
+            acc["sort"].append((a, b))
+        e = [ev() for _ in range(4)]
+        e[0].record()
+        rt.p2g()
+        e[1].record()
+        rt.grid_op()
+        e[2].record()
+        rt.g2p()
+        e[3].record()
+        rt._count += 1
+        acc["p2g"].append((e[0], e[1]))
+        acc["grid_op"].append((e[1], e[2]))
+        acc["g2p"].append((e[2], e[3]))
+    torch.cuda.synchronize()
+    return {k: (statistics.mean(a.elapsed_time(b) for a, b in v) if v else 0.0, len(v)) for k, v in acc.items()}
+
+
+def active_nodes(rt):
+    import torch
+
+    from genesis_b200.engine.runtime import F32_EPS
+
+    rt.ensure_sorted()
+    rt.p2g()
+    mm, _ = rt.grid_views()
+    n = int((mm[:, 3] > F32_EPS).sum().item())
+    rt.grid_op()
+    rt.g2p()
+    rt._count += 1
+    torch.cuda.synchronize()
+    return n
+
+
+def build_scene(d, S):
+    import genesis_b200 as gs
+
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=d.dt * S, substeps=S, gravity=d.gravity),
+        mpm_options=gs.options.MPMOptions(lower_bound=d.lower_bound, upper_bound=d.upper_bound,
+                                          grid_density=d.grid_density, particle_size=d.particle_size),
+        b200_options=gs.options.B200Options(sort_interval=16, check_nan="step"),
+    )
+    from genesis_b200 import workloads as W
+
+    mats = W.make_materials(d, gs.materials.MPM)
+    ents = []
+    for mi, m in enumerate(mats):
+        sel = d.mat_idx == mi
+        lo, hi = d.pos[sel].min(0) - 1e-4, d.pos[sel].max(0) + 1e-4
+        ents.append((scene.add_entity(gs.morphs.Box(lower=tuple(lo), upper=tuple(hi)), material=m), sel))
+    scene.build()
+    for ent, sel in ents:
+        n = ent.n_particles
+        if n != int(sel.sum()):
+            raise RuntimeError("entity sampling does not match the workload particle count")
+        ent.set_particles_pos(d.pos[sel])
+        ent.set_particles_vel(d.vel[sel])
+    return scene
+
+
+def run_e2e(d, S, K, W_):
+    """Through gs.Scene with host buffers: H2D state from pinned memory, scene.step(), D2H pos/vel."""
+    import torch
+
+    scene = build_scene(d, S)
+    st = scene.get_state()[0]
+    host = {k: getattr(st, k).cpu().pin_memory() for k in ("pos", "vel", "C", "F", "Jp", "active")}
+    from genesis_b200.engine.states import MPMSolverState
+
+    out_pos = torch.empty_like(host["pos"]).pin_memory()
+    out_vel = torch.empty_like(host["vel"]).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    d2h = out_pos.numel() * 4 + out_vel.numel() * 4
+
+    def one():
+        s = MPMSolverState(scene, host["pos"], host["vel"], host["C"], host["F"], host["Jp"], host["active"])
+        scene.reset(s)
+        scene.step()
+        cur = scene.get_state()[0]
+        out_pos.copy_(cur.pos)
+        out_vel.copy_(cur.vel)
+
+    for _ in range(W_):
+        one()
+    torch.cuda.synchronize()
+    t = []
+    for _ in range(K):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        one()
+        b.record()
+        torch.cuda.synchronize()
+        t.append(a.elapsed_time(b))
+    ms = sum(t) / K
+    return d.n_particles * S / (ms * 1e-3), ms, h2d, d2h
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from genesis_b200 import workloads as W
+    from genesis_b200.engine.runtime import runtime_from_descs
+
+    S = args.substeps_per_step
+    d = W.mixed_500k(n_side=args.n_side)
+    rt = runtime_from_descs([d], sort_interval=args.sort_interval, chunk_particles=args.chunk)
+    for _ in range(args.warmup):
+        rt.substeps(S)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    step_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)  # evict L2 between timed steps (not timed)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        rt.substeps(S)
+        b.record()
+        step_ms.append((a, b))
+    torch.cuda.synchronize()
+    barrier(world)
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    dev_ms = sum(a.elapsed_time(b) for a, b in step_ms)
+    dev_s = reduce_max(world, dev_ms * 1e-3)
+    status = rt.status()
+    units = d.n_particles * S * args.steps * world
+    value = units / dev_s
+
+    # per-kernel breakdown + roofline of the dominant kernel
+    n_act = active_nodes(rt)
+    kb = kernel_breakdown(rt, 3 * args.sort_interval)
+    hbm, src = peaks()
+    dom = max(("p2g", "grid_op", "g2p"), key=lambda k: kb[k][0])
+    bp, bc = BYTES[dom]
+    alg = bp * d.n_particles + bc * n_act
+    t_dom = kb[dom][0] * 1e-3
+    achieved = alg / t_dom / 1e9
+    tr = ncu_traffic()
+    traffic = tr.get(f"{dom}_dram_bytes_per_launch")
+    sub_ms = sum(kb[k][0] for k in ("p2g", "grid_op", "g2p")) + kb["sort"][0] / max(args.sort_interval, 1)
+    sub_alg = SUBSTEP_BYTES[0] * d.n_particles + SUBSTEP_BYTES[1] * n_act
+    launches_per_substep = 3
+    sorts = sum(1 for i in range(S * args.steps) if (rt._count + i) % args.sort_interval == 0)
+    gpu_launches = launches_per_substep * S * args.steps + 7 * sorts
+
+    res = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_s * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD,
+            "particles": d.n_particles,
+            "grid": "129^3",
+            "substeps_per_step": S,
+            "sort_interval": args.sort_interval,
+            "chunk_particles": args.chunk,
+            "l2": "flushed between timed steps (256 MB write, untimed)",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "wall_s": wall,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": dom,
+            "achieved": achieved,
+            "peak": hbm,
+            "unit": "GB/s",
+            "frac": achieved / hbm,
+            "peak_source": src,
+            "traffic": traffic,
+            "alg_bytes_per_launch": alg,
+            "active_nodes": n_act,
+            "kernel_ms": {k: round(v[0], 5) for k, v in kb.items()},
+            "substep_alg_GBs": sub_alg / (sub_ms * 1e-3) / 1e9,
+            "substep_frac": sub_alg / (sub_ms * 1e-3) / 1e9 / hbm,
+        },
+        "gpu_launches": gpu_launches,
+        "clocks": clk,
+        "status_word": status,
+    }
+    return res, d, rt
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    import torch
+
+    from genesis_b200 import build as B
+
+    B.build()
+    res, d, rt = run_ours(args, world, rank, local)
+    del rt
+    torch.cuda.empty_cache()
+    S = args.substeps_per_step
+    if not args.no_e2e:
+        rate, ms, h2d, d2h = run_e2e(d, S, args.steps, args.warmup)
+        rate = reduce_max(world, -rate) * -1 if world > 1 else rate
+        res["e2e"] = {"value": rate * (world if world > 1 else 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                      "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": "gs.Scene.reset(state)+step()+get_state()"}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, threads, sample = cpu_port_rate(d)
+        res["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(res))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

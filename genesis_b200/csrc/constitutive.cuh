@@ -1,0 +1,179 @@
+// Per-material return mapping and stress for the fused p2g kernel.
+//
+// Each branch restates one gs.materials.MPM class:
+//   Elastic        materials/MPM/elastic.py:62-83
+//   ElastoPlastic  materials/MPM/elasto_plastic.py:66-93 (stress: base.py:83-90)
+//   Liquid         materials/MPM/liquid.py:50-64
+//   Sand           materials/MPM/sand.py:51-89
+//   Snow           materials/MPM/snow.py:62-81
+// and the call protocol of p2g (mpm_solver.py:303-345): J is det(S) of F_tmp's SVD,
+// Snow's hardening uses the previous Jp, Sand's stress uses S_new, Liquid's uses F_tmp.
+#pragma once
+
+#include "../../include/genesis_b200_mpm.h"
+
+namespace gbm {
+
+// M = U diag(s) V^T
+__device__ __forceinline__ void usvt(const float* U, const float* s, const float* V, float* M) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            M[i * 3 + j] = U[i * 3 + 0] * s[0] * V[j * 3 + 0] + U[i * 3 + 1] * s[1] * V[j * 3 + 1] +
+                           U[i * 3 + 2] * s[2] * V[j * 3 + 2];
+}
+
+// R = U V^T
+__device__ __forceinline__ void uvt(const float* U, const float* V, float* R) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            R[i * 3 + j] = U[i * 3 + 0] * V[j * 3 + 0] + U[i * 3 + 1] * V[j * 3 + 1] + U[i * 3 + 2] * V[j * 3 + 2];
+}
+
+// out = 2 mu (F - R) F^T + lam J (J - 1) I   (corotated form, base.py:86-88)
+__device__ __forceinline__ void corotated(float mu, float lam, float J, const float* F, const float* R, float* out) {
+    const float two_mu = 2.f * mu;
+    const float diag = lam * J * (J - 1.f);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float acc = (F[i * 3 + 0] - R[i * 3 + 0]) * F[j * 3 + 0] + (F[i * 3 + 1] - R[i * 3 + 1]) * F[j * 3 + 1] +
+                        (F[i * 3 + 2] - R[i * 3 + 2]) * F[j * 3 + 2];
+            out[i * 3 + j] = two_mu * acc + (i == j ? diag : 0.f);
+        }
+}
+
+// Return mapping + stress for one particle.
+//   in : material m (mu/lam possibly overridden per particle), eps = gs.EPS,
+//        J = det(S), F_tmp, U, S, V, Jp (previous frame)
+//   out: F_new, Jp_new, stress (unscaled Kirchhoff-type stress of update_stress)
+__device__ __forceinline__ void constitutive(const mpm_material& m, float mu, float lam, float eps, float J,
+                                             const float* Ft, const float* U, const float* S, const float* V,
+                                             float Jp, float* F_new, float& Jp_new, float* stress) {
+    float R[9];
+    switch (m.kind) {
+        case MPM_MAT_ELASTIC: {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) F_new[k] = Ft[k];
+            Jp_new = Jp;
+            if (m.flags & MPM_MATF_NEOHOOKEAN) {
+                // mu F_tmp F_tmp^T + (lam log J - mu) I   (elastic.py:78-81)
+                const float d = lam * logf(J) - mu;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        float acc = Ft[i * 3 + 0] * Ft[j * 3 + 0] + Ft[i * 3 + 1] * Ft[j * 3 + 1] + Ft[i * 3 + 2] * Ft[j * 3 + 2];
+                        stress[i * 3 + j] = mu * acc + (i == j ? d : 0.f);
+                    }
+            } else {
+                uvt(U, V, R);
+                corotated(mu, lam, J, F_new, R, stress);
+            }
+            break;
+        }
+        case MPM_MAT_LIQUID: {
+            // F_new = J^(1/3) I (liquid.py:52); pow keeps the NaN of a negative J
+            const float c = powf(J, 1.f / 3.f);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) F_new[k] = (k % 4 == 0) ? c : 0.f;
+            Jp_new = Jp;
+            uvt(U, V, R);
+            corotated(mu, lam, J, Ft, R, stress);  // liquid.py:60 uses F_tmp
+            break;
+        }
+        case MPM_MAT_ELASTOPLASTIC: {
+            float Sn[3];
+            if (m.flags & MPM_MATF_VON_MISES) {
+                // elasto_plastic.py:71-84
+                float e[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) e[d] = logf(fmaxf(S[d], 0.05f));
+                const float mean = (e[0] + e[1] + e[2]) / 3.f;
+                float eh[3] = {e[0] - mean, e[1] - mean, e[2] - mean};
+                const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
+                const float dg = ehn - m.vm_threshold * (m.mu / mu);
+                if (dg > 0.f) {
+                    const float r = dg / ehn;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) Sn[d] = expf(e[d] - r * eh[d]);
+                    usvt(U, Sn, V, F_new);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) F_new[k] = Ft[k];
+                }
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Sn[d] = fminf(fmaxf(S[d], m.clamp_lo), m.clamp_hi);
+                usvt(U, Sn, V, F_new);
+            }
+            Jp_new = Jp;
+            uvt(U, V, R);
+            corotated(mu, lam, J, F_new, R, stress);
+            break;
+        }
+        case MPM_MAT_SNOW: {
+            float Sn[3];
+            float jp = Jp;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                Sn[d] = fminf(fmaxf(S[d], m.clamp_lo), m.clamp_hi);
+                jp = jp * (S[d] / Sn[d]);
+            }
+            Jp_new = jp;
+            usvt(U, Sn, V, F_new);
+            // snow.py:75-79: hardening from the previous Jp
+            const float h = expf(10.f * (1.f - Jp));
+            uvt(U, V, R);
+            corotated(mu * h, lam * h, J, F_new, R, stress);
+            break;
+        }
+        case MPM_MAT_SAND:
+        default: {
+            // sand.py:52-77
+            float e[3], Sn[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) e[d] = logf(fmaxf(fabsf(S[d]), 1e-4f));
+            const float tr = e[0] + e[1] + e[2] + Jp;
+            float eh[3] = {e[0] - tr / 3.f, e[1] - tr / 3.f, e[2] - tr / 3.f};
+            const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
+            if (tr >= 0.f) {
+                Jp_new = tr;
+                Sn[0] = Sn[1] = Sn[2] = 1.f;
+            } else {
+                Jp_new = 0.f;
+                const float c1 = (3.f * lam + 2.f * mu) / (2.f * mu);
+                const float dg = ehn + c1 * tr * m.sand_alpha;
+                const float r = fmaxf(0.f, dg) / ehn;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Sn[d] = expf(e[d] - r * eh[d]);
+            }
+            usvt(U, Sn, V, F_new);
+            // sand.py:80-88 with S = S_new
+            float center[3];
+            const float l0 = logf(Sn[0]), l1 = logf(Sn[1]), l2 = logf(Sn[2]);
+            const float lsum = l0 + l1 + l2;
+            const float ls[3] = {l0, l1, l2};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float inv = 1.f / Sn[d];
+                center[d] = 2.f * mu * ls[d] * inv + lam * lsum * inv;
+            }
+            float M[9];
+            usvt(U, center, V, M);  // U diag(center) V^T
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    stress[i * 3 + j] = M[i * 3 + 0] * F_new[j * 3 + 0] + M[i * 3 + 1] * F_new[j * 3 + 1] +
+                                        M[i * 3 + 2] * F_new[j * 3 + 2];
+            break;
+        }
+    }
+}
+
+}  // namespace gbm

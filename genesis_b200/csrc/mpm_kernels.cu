@@ -1,0 +1,1210 @@
+// B200-native MLS-MPM substep: counting sort by grid block, fused p2g, grid op, g2p.
+//
+// Reference path (Genesis, gstaichi kernels):
+//   reset_grid_and_grad  mpm_solver.py:540-550   -> folded into k_grid_op (clear after read)
+//   compute_F_tmp        mpm_solver.py:261-267   -> k_p2g, registers
+//   svd                  mpm_solver.py:269-275   -> k_p2g, registers (svd3.cuh)
+//   p2g                  mpm_solver.py:290-389   -> k_p2g (shared-memory tile + float4 red)
+//   mpm_grid_op          legacy_coupler.py:352-496 (MPM core) -> k_grid_op over active blocks
+//   g2p                  mpm_solver.py:391-449   -> k_g2p (shared-memory velocity tile)
+//   _is_state_valid      mpm_solver.py:451-457   -> status bit set in k_g2p, read lazily
+//   copy_frame           mpm_solver.py:519-528   -> not needed: state is updated in place
+//
+// Memory-system design (no tensor cores: MPM is a scatter/gather stencil):
+//   * particles live in planar SoA channels, sorted by 4x4x4 grid block every few
+//     substeps with a counting sort; each work item ("chunk") is up to P particles of one
+//     block, so a warp's loads of any channel are 128-byte coalesced;
+//   * p2g accumulates the chunk's 8x8x8-node neighbourhood (the block, its +2 stencil
+//     reach and a 1-node drift margin on each side) in shared memory with shared-memory
+//     atomics, then flushes only non-empty nodes to the block-major grid with one
+//     16-byte vector reduction each, and records which grid blocks became active;
+//   * grid op streams the active-block list only (the dense grid is never swept) and
+//     re-zeroes mass/momentum behind itself;
+//   * g2p stages the same 8x8x8 velocity neighbourhood in shared memory and gathers.
+//   Particles that drifted out of their chunk's tile since the last sort take a
+//   bounds-checked global-memory path, so stale binning costs speed, never correctness.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/genesis_b200_mpm.h"
+#include "constitutive.cuh"
+#include "svd3.cuh"
+
+namespace gbm {
+
+constexpr int BLK = MPM_BLOCK;         // grid block edge
+constexpr int BLK3 = BLK * BLK * BLK;  // nodes per block
+constexpr int MARGIN = 1;              // drift margin of the shared tile (nodes)
+constexpr int TILE = BLK + 2 + 2 * MARGIN;  // 8
+constexpr int TN = TILE * TILE * TILE;      // 512
+constexpr int SCAN_T = 1024;                // threads of the scan kernels
+constexpr int SCAN_ITEMS = 4;               // items per thread
+constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
+constexpr int MAX_SCAN_TILES = SCAN_T * SCAN_ITEMS;  // single-CTA scan of tile sums
+constexpr int64_t MAX_BLOCKS = (int64_t)SCAN_TILE * MAX_SCAN_TILES;
+
+enum Counter { CNT_ACTIVE = 0, CNT_CHUNKS = 1, CNT_STATUS = 2, CNT_SORTED = 3, CNT_FALLBACK = 4 /* u64 at 4,5 */ };
+constexpr int N_COUNTERS = 16;
+
+struct Ws {
+    float4* mm;          // grid momentum.xyz + mass, block-major
+    float4* gv;          // grid velocity (w unused)
+    uint32_t* flag;      // per grid block: 1 if active this substep
+    int2* active;        // active block list {instance, local block}
+    int* bin_count;      // sort histogram
+    int* bin_start;      // exclusive scan of bin_count
+    int* chunk_start;    // exclusive scan of chunks per bin
+    int* key;            // per particle bin (global block id)
+    int* rank;           // per particle rank within its bin
+    int4* tile_sums;     // scan scratch
+    int4* chunks;        // work items {instance, local block, first slot, end slot}
+    float* state_tmp;    // permutation scratch
+    uint8_t* mat_tmp;
+    uint8_t* pflags_tmp;
+    int* gid_tmp;
+    float* mu_tmp;
+    float* lam_tmp;
+    uint32_t* counters;
+    int64_t tmp_stride;
+};
+
+static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+struct Layout {
+    uint64_t off[18];
+    uint64_t total;
+};
+
+static Layout layout_of(const mpm_problem& p) {
+    Layout L{};
+    const uint64_t nb = (uint64_t)p.n_blocks;
+    const uint64_t n = (uint64_t)p.n_particles;
+    const uint64_t ntiles = (nb + SCAN_TILE - 1) / SCAN_TILE;
+    const uint64_t stride = align_up(n > 0 ? n : 1, 64);
+    uint64_t sizes[18] = {
+        nb * BLK3 * 16,            // mm
+        nb * BLK3 * 16,            // gv
+        nb * 4,                    // flag
+        nb * 8,                    // active
+        nb * 4,                    // bin_count
+        nb * 4,                    // bin_start
+        nb * 4,                    // chunk_start
+        n * 4,                     // key
+        n * 4,                     // rank
+        (ntiles + 1) * 16,         // tile_sums
+        (uint64_t)p.max_chunks * 16,  // chunks
+        stride * MPM_STATE_CH * 4,    // state_tmp
+        n,                         // mat_tmp
+        n,                         // pflags_tmp
+        n * 4,                     // gid_tmp
+        n * 4,                     // mu_tmp
+        n * 4,                     // lam_tmp
+        N_COUNTERS * 4,            // counters
+    };
+    uint64_t o = 0;
+    for (int i = 0; i < 18; ++i) {
+        L.off[i] = o;
+        o = align_up(o + (sizes[i] ? sizes[i] : 1), 256);
+    }
+    L.total = o;
+    return L;
+}
+
+static Ws ws_of(const mpm_problem& p, void* base) {
+    Layout L = layout_of(p);
+    char* b = (char*)base;
+    Ws w;
+    w.mm = (float4*)(b + L.off[0]);
+    w.gv = (float4*)(b + L.off[1]);
+    w.flag = (uint32_t*)(b + L.off[2]);
+    w.active = (int2*)(b + L.off[3]);
+    w.bin_count = (int*)(b + L.off[4]);
+    w.bin_start = (int*)(b + L.off[5]);
+    w.chunk_start = (int*)(b + L.off[6]);
+    w.key = (int*)(b + L.off[7]);
+    w.rank = (int*)(b + L.off[8]);
+    w.tile_sums = (int4*)(b + L.off[9]);
+    w.chunks = (int4*)(b + L.off[10]);
+    w.state_tmp = (float*)(b + L.off[11]);
+    w.mat_tmp = (uint8_t*)(b + L.off[12]);
+    w.pflags_tmp = (uint8_t*)(b + L.off[13]);
+    w.gid_tmp = (int*)(b + L.off[14]);
+    w.mu_tmp = (float*)(b + L.off[15]);
+    w.lam_tmp = (float*)(b + L.off[16]);
+    w.counters = (uint32_t*)(b + L.off[17]);
+    w.tmp_stride = (int64_t)align_up(p.n_particles > 0 ? p.n_particles : 1, 64);
+    return w;
+}
+
+// ---------------------------------------------------------------- helpers
+
+__device__ __forceinline__ int find_instance_by_particle(const mpm_instance* inst, int n_inst, int p) {
+    int lo = 0, hi = n_inst - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&inst[mid].p_begin) <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int find_instance_by_block(const mpm_instance* inst, int n_inst, int64_t b) {
+    int lo = 0, hi = n_inst - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&inst[mid].blk_base) <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void set_status(uint32_t* counters, uint32_t bit) {
+    atomicOr(&counters[CNT_STATUS], bit);
+}
+
+// quadratic B-spline weights (mpm_solver.py:350, 397)
+__device__ __forceinline__ void bspline(float fx, float* w) {
+    const float a = 1.5f - fx;
+    const float b = fx - 1.f;
+    const float c = fx - 0.5f;
+    w[0] = 0.5f * a * a;
+    w[1] = 0.75f - b * b;
+    w[2] = 0.5f * c * c;
+}
+
+// CubeBoundary.impose_pos_vel with restitution 0 (boundaries.py:23-33); velocity part
+__device__ __forceinline__ float bc_vel(float pos, float vel, float lo, float hi) {
+    if (pos >= hi && vel >= 0.f) return vel * -0.f;
+    if (pos <= lo && vel <= 0.f) return vel * -0.f;
+    return vel;
+}
+
+struct BlockCoord {
+    int bx, by, bz;
+};
+
+__device__ __forceinline__ BlockCoord block_coord(int lb, const mpm_instance& I) {
+    BlockCoord c;
+    c.bz = lb % I.nblk[2];
+    int t = lb / I.nblk[2];
+    c.by = t % I.nblk[1];
+    c.bx = t / I.nblk[1];
+    return c;
+}
+
+__device__ __forceinline__ int64_t node_addr(const mpm_instance& I, int gx, int gy, int gz) {
+    const int lb = ((gx >> 2) * I.nblk[1] + (gy >> 2)) * I.nblk[2] + (gz >> 2);
+    const int ln = ((gx & 3) * BLK + (gy & 3)) * BLK + (gz & 3);
+    return (I.blk_base + lb) * BLK3 + ln;
+}
+
+__device__ __forceinline__ void mark_block(Ws& w, int inst, const mpm_instance& I, int bx, int by, int bz) {
+    const int lb = (bx * I.nblk[1] + by) * I.nblk[2] + bz;
+    uint32_t* f = &w.flag[I.blk_base + lb];
+    if (*((volatile uint32_t*)f) == 0u && atomicExch(f, 1u) == 0u) {
+        const int i = (int)atomicAdd(&w.counters[CNT_ACTIVE], 1u);
+        w.active[i] = make_int2(inst, lb);
+    }
+}
+
+__device__ __forceinline__ bool finite3(float a, float b, float c) {
+    return isfinite(a) && isfinite(b) && isfinite(c);
+}
+
+// ---------------------------------------------------------------- sort
+
+__global__ void k_sort_keys(mpm_problem prob, const mpm_instance* __restrict__ inst, mpm_particles par, Ws w) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= prob.n_particles) return;
+    const int k = find_instance_by_particle(inst, prob.n_instances, p);
+    const mpm_instance& I = inst[k];
+    const int64_t s = par.state_stride;
+    const float x0 = par.state[MPM_CH_X * s + p], x1 = par.state[(MPM_CH_X + 1) * s + p],
+                x2 = par.state[(MPM_CH_X + 2) * s + p];
+    int b[3];
+    const float xs[3] = {x0, x1, x2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float f = floorf(xs[d] * I.inv_dx - 0.5f);
+        int c = isfinite(f) ? (int)fminf(fmaxf(f - (float)I.lower_cell[d], 0.f), (float)(I.res[d] - 1)) : 0;
+        b[d] = min(c >> 2, I.nblk[d] - 1);
+    }
+    const int lb = (b[0] * I.nblk[1] + b[1]) * I.nblk[2] + b[2];
+    const int key = (int)(I.blk_base + lb);
+    w.key[p] = key;
+    w.rank[p] = atomicAdd(&w.bin_count[key], 1);
+}
+
+// Scan of (count, ceil(count/P)) over bins: three phases.
+__global__ void k_scan_reduce(int64_t nb, int P, Ws w) {
+    __shared__ int s_a[SCAN_T / 32], s_b[SCAN_T / 32];
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+    int a = 0, c = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        int64_t j = base + (int64_t)i * SCAN_T + threadIdx.x;
+        if (j < nb) {
+            int cnt = w.bin_count[j];
+            a += cnt;
+            c += (cnt + P - 1) / P;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_a[threadIdx.x >> 5] = a;
+        s_b[threadIdx.x >> 5] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        a = s_a[threadIdx.x];
+        c = s_b[threadIdx.x];
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            c += __shfl_down_sync(0xffffffffu, c, o);
+        }
+        if (threadIdx.x == 0) w.tile_sums[blockIdx.x] = make_int4(a, c, 0, 0);
+    }
+}
+
+// block-wide exclusive scan of (a, c) pairs held one per thread; returns totals
+__device__ __forceinline__ int2 block_exscan2(int& a, int& c, int2* s_warp) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int ia = a, ic = c;
+    for (int o = 1; o < 32; o <<= 1) {
+        int ta = __shfl_up_sync(0xffffffffu, ia, o);
+        int tc = __shfl_up_sync(0xffffffffu, ic, o);
+        if (lane >= o) {
+            ia += ta;
+            ic += tc;
+        }
+    }
+    if (lane == 31) s_warp[wid] = make_int2(ia, ic);
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        int2 v = lane < nw ? s_warp[lane] : make_int2(0, 0);
+        int va = v.x, vc = v.y;
+        for (int o = 1; o < 32; o <<= 1) {
+            int ta = __shfl_up_sync(0xffffffffu, va, o);
+            int tc = __shfl_up_sync(0xffffffffu, vc, o);
+            if (lane >= o) {
+                va += ta;
+                vc += tc;
+            }
+        }
+        if (lane < nw) s_warp[lane] = make_int2(va, vc);
+    }
+    __syncthreads();
+    const int2 pre = wid > 0 ? s_warp[wid - 1] : make_int2(0, 0);
+    const int2 tot = s_warp[(blockDim.x >> 5) - 1];
+    a = pre.x + ia - a;
+    c = pre.y + ic - c;
+    __syncthreads();
+    return tot;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_tiles(int ntiles, Ws w) {
+    __shared__ int2 s_warp[32];
+    int va[SCAN_ITEMS], vc[SCAN_ITEMS];
+    int a = 0, c = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        int j = threadIdx.x * SCAN_ITEMS + i;
+        int4 t = j < ntiles ? w.tile_sums[j] : make_int4(0, 0, 0, 0);
+        va[i] = t.x;
+        vc[i] = t.y;
+        a += t.x;
+        c += t.y;
+    }
+    int2 tot = block_exscan2(a, c, s_warp);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        int j = threadIdx.x * SCAN_ITEMS + i;
+        if (j < ntiles) w.tile_sums[j] = make_int4(a, c, 0, 0);
+        a += va[i];
+        c += vc[i];
+    }
+    if (threadIdx.x == 0) {
+        w.counters[CNT_CHUNKS] = (uint32_t)tot.y;
+        w.counters[CNT_SORTED] = 1u;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_apply(int64_t nb, int P, Ws w) {
+    __shared__ int2 s_warp[32];
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int va[SCAN_ITEMS], vc[SCAN_ITEMS];
+    int a = 0, c = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        int64_t j = base + i;
+        int cnt = j < nb ? w.bin_count[j] : 0;
+        va[i] = cnt;
+        vc[i] = (cnt + P - 1) / P;
+        a += va[i];
+        c += vc[i];
+    }
+    block_exscan2(a, c, s_warp);
+    const int4 t = w.tile_sums[blockIdx.x];
+    a += t.x;
+    c += t.y;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        int64_t j = base + i;
+        if (j < nb) {
+            w.bin_start[j] = a;
+            w.chunk_start[j] = c;
+        }
+        a += va[i];
+        c += vc[i];
+    }
+}
+
+__global__ void k_sort_scatter(mpm_problem prob, mpm_particles par, Ws w) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= prob.n_particles) return;
+    const int dst = w.bin_start[w.key[p]] + w.rank[p];
+    const int64_t s = par.state_stride, t = w.tmp_stride;
+#pragma unroll 5
+    for (int ch = 0; ch < MPM_STATE_CH; ++ch) w.state_tmp[ch * t + dst] = par.state[ch * s + p];
+    w.mat_tmp[dst] = par.mat[p];
+    w.pflags_tmp[dst] = par.pflags[p];
+    const int g = par.gid[p];
+    w.gid_tmp[dst] = g;
+    par.slot[g] = dst;
+    if (par.mu_p) {
+        w.mu_tmp[dst] = par.mu_p[p];
+        w.lam_tmp[dst] = par.lam_p[p];
+    }
+}
+
+__global__ void k_sort_copyback(mpm_problem prob, mpm_particles par, Ws w) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= prob.n_particles) return;
+    const int64_t s = par.state_stride, t = w.tmp_stride;
+#pragma unroll 5
+    for (int ch = 0; ch < MPM_STATE_CH; ++ch) par.state[ch * s + p] = w.state_tmp[ch * t + p];
+    par.mat[p] = w.mat_tmp[p];
+    par.pflags[p] = w.pflags_tmp[p];
+    par.gid[p] = w.gid_tmp[p];
+    if (par.mu_p) {
+        par.mu_p[p] = w.mu_tmp[p];
+        par.lam_p[p] = w.lam_tmp[p];
+    }
+}
+
+__global__ void k_build_chunks(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= prob.n_blocks) return;
+    const int cnt = w.bin_count[b];
+    if (cnt == 0) return;
+    const int P = prob.chunk_particles;
+    const int k = find_instance_by_block(inst, prob.n_instances, b);
+    const int lb = (int)(b - inst[k].blk_base);
+    const int start = w.bin_start[b];
+    const int cs = w.chunk_start[b];
+    const int nch = (cnt + P - 1) / P;
+    for (int j = 0; j < nch; ++j) {
+        const int s0 = start + j * P;
+        w.chunks[cs + j] = make_int4(k, lb, s0, min(s0 + P, start + cnt));
+    }
+}
+
+// ---------------------------------------------------------------- p2g
+
+struct P2GArgs {
+    mpm_problem prob;
+    const mpm_instance* inst;
+    const mpm_material* mats;
+    mpm_particles par;
+    Ws w;
+};
+
+template <int P>
+__global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
+    __shared__ float s_m[TN], s_px[TN], s_py[TN], s_pz[TN];
+    __shared__ uint32_t s_mask;
+    Ws& w = a.w;
+    const int n_chunks = (int)w.counters[CNT_CHUNKS];
+    const int64_t st = a.par.state_stride;
+    float* __restrict__ S = a.par.state;
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        const int4 ch = w.chunks[ci];
+        const mpm_instance& I = a.inst[ch.x];
+        const BlockCoord bc = block_coord(ch.y, I);
+        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
+        for (int n = threadIdx.x; n < TN; n += P) {
+            s_m[n] = 0.f;
+            s_px[n] = 0.f;
+            s_py[n] = 0.f;
+            s_pz[n] = 0.f;
+        }
+        if (threadIdx.x == 0) s_mask = 0u;
+        __syncthreads();
+
+        const int p = ch.z + threadIdx.x;
+        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
+            float x[3], v[3], C[9], F[9];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x[d] = S[(MPM_CH_X + d) * st + p];
+                v[d] = S[(MPM_CH_V + d) * st + p];
+            }
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                C[k] = S[(MPM_CH_C + k) * st + p];
+                F[k] = S[(MPM_CH_F + k) * st + p];
+            }
+            const float Jp = S[MPM_CH_JP * st + p];
+            const mpm_material m = a.mats[I.mat_base + a.par.mat[p]];
+            float mu = m.mu, lam = m.lam;
+            if (a.par.mu_p) {
+                mu = a.par.mu_p[p];
+                lam = a.par.lam_p[p];
+            }
+            // compute_F_tmp: (I + dt C) F   (mpm_solver.py:264-266)
+            float Ft[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    float acc = F[i * 3 + j];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) acc += I.dt * C[i * 3 + k] * F[k * 3 + j];
+                    Ft[i * 3 + j] = acc;
+                }
+            float U[9], Sg[3], V[9];
+            svd3(Ft, U, Sg, V);
+            const float J = Sg[0] * (Sg[1] * Sg[2]);
+            float Fn[9], stress[9], Jpn;
+            constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, stress);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
+            S[MPM_CH_JP * st + p] = Jpn;
+            // affine = stress*scale + mass*C (mpm_solver.py:344-345)
+            const float mass = m.mass;
+            float A[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) A[k] = I.stress_scale * stress[k] + mass * C[k];
+            if (finite3(x[0], x[1], x[2])) {
+                float fx[3], wx[3], wy[3], wz[3];
+                int base[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const float xi = x[d] * I.inv_dx;
+                    const float bf = floorf(xi - 0.5f);
+                    base[d] = (int)fminf(fmaxf(bf, -1e8f), 1e8f) - I.lower_cell[d];
+                    fx[d] = xi - bf;
+                }
+                bspline(fx[0], wx);
+                bspline(fx[1], wy);
+                bspline(fx[2], wz);
+                // mass*v + affine @ dpos with dpos = (off - fx) * dx
+                const float dx = I.dx;
+                float q[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    q[i] = mass * v[i] - (A[i * 3 + 0] * fx[0] + A[i * 3 + 1] * fx[1] + A[i * 3 + 2] * fx[2]) * dx;
+                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+                const bool in_tile = lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3;
+                if (in_tile) {
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                const float wt = wx[i] * wy[j] * wz[k];
+                                const float ax = q[0] + dx * (A[0] * i + A[1] * j + A[2] * k);
+                                const float ay = q[1] + dx * (A[3] * i + A[4] * j + A[5] * k);
+                                const float az = q[2] + dx * (A[6] * i + A[7] * j + A[8] * k);
+                                const int n = ((lx + i) * TILE + (ly + j)) * TILE + (lz + k);
+                                atomicAdd(&s_m[n], wt * mass);
+                                atomicAdd(&s_px[n], wt * ax);
+                                atomicAdd(&s_py[n], wt * ay);
+                                atomicAdd(&s_pz[n], wt * az);
+                            }
+                } else {
+                    // drifted since the last sort: bounds-checked global path
+                    atomicAdd((unsigned long long*)&w.counters[CNT_FALLBACK], 1ull);
+#pragma unroll 1
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll 1
+                        for (int j = 0; j < 3; ++j)
+#pragma unroll 1
+                            for (int k = 0; k < 3; ++k) {
+                                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
+                                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                                    set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                                    continue;
+                                }
+                                const float wt = wx[i] * wy[j] * wz[k];
+                                const float ax = q[0] + dx * (A[0] * i + A[1] * j + A[2] * k);
+                                const float ay = q[1] + dx * (A[3] * i + A[4] * j + A[5] * k);
+                                const float az = q[2] + dx * (A[6] * i + A[7] * j + A[8] * k);
+                                atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(wt * ax, wt * ay, wt * az, wt * mass));
+                                mark_block(w, ch.x, I, gx >> 2, gy >> 2, gz >> 2);
+                            }
+                }
+            } else {
+                set_status(w.counters, MPM_STATUS_NAN);
+            }
+        }
+        __syncthreads();
+        // flush non-empty tile nodes: one 16-byte reduction per node
+        for (int n = threadIdx.x; n < TN; n += P) {
+            const float mval = s_m[n];
+            if (mval != 0.f) {
+                const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
+                const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
+                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                    set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                    continue;
+                }
+                atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(s_px[n], s_py[n], s_pz[n], mval));
+                const int bit = ((gx >> 2) - bc.bx + 1) * 9 + ((gy >> 2) - bc.by + 1) * 3 + ((gz >> 2) - bc.bz + 1);
+                atomicOr(&s_mask, 1u << bit);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 27 && ((s_mask >> threadIdx.x) & 1u)) {
+            const int t = threadIdx.x;
+            mark_block(w, ch.x, I, bc.bx + t / 9 - 1, bc.by + (t / 3) % 3 - 1, bc.bz + t % 3 - 1);
+        }
+        __syncthreads();
+    }
+}
+
+// non-free particles zero the momentum of their stencil (mpm_solver.py:388-389)
+__global__ void k_nonfree_zero(mpm_problem prob, const mpm_instance* __restrict__ inst, mpm_particles par, Ws w) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= prob.n_particles) return;
+    const uint8_t fl = par.pflags[p];
+    if (!(fl & MPM_PFLAG_ACTIVE) || (fl & MPM_PFLAG_FREE)) return;
+    const int k = find_instance_by_particle(inst, prob.n_instances, p);
+    const mpm_instance& I = inst[k];
+    const int64_t st = par.state_stride;
+    int base[3];
+    for (int d = 0; d < 3; ++d) {
+        const float x = par.state[(MPM_CH_X + d) * st + p];
+        if (!isfinite(x)) return;
+        base[d] = (int)fminf(fmaxf(floorf(x * I.inv_dx - 0.5f), -1e8f), 1e8f) - I.lower_cell[d];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int kk = 0; kk < 3; ++kk) {
+                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + kk;
+                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) continue;
+                float4* c = &w.mm[node_addr(I, gx, gy, gz)];
+                c->x = 0.f;
+                c->y = 0.f;
+                c->z = 0.f;
+            }
+}
+
+// ---------------------------------------------------------------- grid op
+
+__global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w) {
+    const int n_active = (int)w.counters[CNT_ACTIVE];
+    const int gpc = blockDim.x / BLK3;
+    const int grp = threadIdx.x / BLK3;
+    const int ln = threadIdx.x % BLK3;
+    const int lx = ln / (BLK * BLK), ly = (ln / BLK) % BLK, lz = ln % BLK;
+    for (int i = blockIdx.x * gpc + grp; i < n_active; i += gridDim.x * gpc) {
+        const int2 e = w.active[i];
+        const mpm_instance& I = inst[e.x];
+        const BlockCoord bc = block_coord(e.y, I);
+        const int64_t g = (I.blk_base + e.y) * BLK3 + ln;
+        const float4 mm = w.mm[g];
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+        if (mm.w > I.eps) {
+            const float inv = 1.f / mm.w;  // (1 / mass) * vel_in (legacy_coupler.py:369)
+            vx = inv * mm.x + I.dt * I.gravity[0];
+            vy = inv * mm.y + I.dt * I.gravity[1];
+            vz = inv * mm.z + I.dt * I.gravity[2];
+            // pos = (I + grid_offset) * dx (legacy_coupler.py:374)
+            const float px = (float)(bc.bx * BLK + lx + I.lower_cell[0]) * I.dx;
+            const float py = (float)(bc.by * BLK + ly + I.lower_cell[1]) * I.dx;
+            const float pz = (float)(bc.bz * BLK + lz + I.lower_cell[2]) * I.dx;
+            vx = bc_vel(px, vx, I.bnd_lo[0], I.bnd_hi[0]);
+            vy = bc_vel(py, vy, I.bnd_lo[1], I.bnd_hi[1]);
+            vz = bc_vel(pz, vz, I.bnd_lo[2], I.bnd_hi[2]);
+        }
+        w.gv[g] = make_float4(vx, vy, vz, 0.f);
+        w.mm[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ln == 0) w.flag[I.blk_base + e.y] = 0u;
+    }
+}
+
+// ---------------------------------------------------------------- g2p
+
+template <int P>
+__global__ void __launch_bounds__(P) k_g2p(P2GArgs a) {
+    __shared__ float4 s_v[TN];
+    Ws& w = a.w;
+    const int n_chunks = (int)w.counters[CNT_CHUNKS];
+    const int64_t st = a.par.state_stride;
+    float* __restrict__ S = a.par.state;
+    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[CNT_ACTIVE] = 0u;  // grid op is done with it
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        const int4 ch = w.chunks[ci];
+        const mpm_instance& I = a.inst[ch.x];
+        const BlockCoord bc = block_coord(ch.y, I);
+        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
+        for (int n = threadIdx.x; n < TN; n += P) {
+            const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
+            const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
+            float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gx >= 0 && gy >= 0 && gz >= 0 && gx < I.res[0] && gy < I.res[1] && gz < I.res[2])
+                val = w.gv[node_addr(I, gx, gy, gz)];
+            s_v[n] = val;
+        }
+        __syncthreads();
+        const int p = ch.z + threadIdx.x;
+        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
+            float x[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
+            if (finite3(x[0], x[1], x[2])) {
+                float fx[3], wx[3], wy[3], wz[3];
+                int base[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const float xi = x[d] * I.inv_dx;
+                    const float bf = floorf(xi - 0.5f);
+                    base[d] = (int)fminf(fmaxf(bf, -1e8f), 1e8f) - I.lower_cell[d];
+                    fx[d] = xi - bf;
+                }
+                bspline(fx[0], wx);
+                bspline(fx[1], wy);
+                bspline(fx[2], wz);
+                float nv[3] = {0.f, 0.f, 0.f};
+                float nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+                const bool in_tile = lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            float4 gvv;
+                            if (in_tile) {
+                                gvv = s_v[((lx + i) * TILE + (ly + j)) * TILE + (lz + k)];
+                            } else {
+                                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
+                                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                                    set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                                    continue;
+                                }
+                                gvv = w.gv[node_addr(I, gx, gy, gz)];
+                            }
+                            const float wt = wx[i] * wy[j] * wz[k];
+                            const float d0 = (float)i - fx[0], d1 = (float)j - fx[1], d2 = (float)k - fx[2];
+                            nv[0] += wt * gvv.x;
+                            nv[1] += wt * gvv.y;
+                            nv[2] += wt * gvv.z;
+                            const float cw = I.c_scale * wt;
+                            nC[0] += cw * gvv.x * d0;
+                            nC[1] += cw * gvv.x * d1;
+                            nC[2] += cw * gvv.x * d2;
+                            nC[3] += cw * gvv.y * d0;
+                            nC[4] += cw * gvv.y * d1;
+                            nC[5] += cw * gvv.y * d2;
+                            nC[6] += cw * gvv.z * d0;
+                            nC[7] += cw * gvv.z * d1;
+                            nC[8] += cw * gvv.z * d2;
+                        }
+                float nx[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    nx[d] = x[d] + I.dt * nv[d];
+                    nv[d] = bc_vel(nx[d], nv[d], I.bnd_lo[d], I.bnd_hi[d]);
+                    nx[d] = fmaxf(fminf(nx[d], I.bnd_hi[d]), I.bnd_lo[d]);
+                }
+                if (!finite3(nx[0], nx[1], nx[2])) set_status(w.counters, MPM_STATUS_NAN);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    S[(MPM_CH_X + d) * st + p] = nx[d];
+                    S[(MPM_CH_V + d) * st + p] = nv[d];
+                }
+#pragma unroll
+                for (int k = 0; k < 9; ++k) S[(MPM_CH_C + k) * st + p] = nC[k];
+            } else {
+                set_status(w.counters, MPM_STATUS_NAN);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- state I/O
+
+__global__ void k_get_state(mpm_problem prob, mpm_particles par, float* pos, float* vel, float* C, float* F, float* Jp,
+                            uint8_t* active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= prob.n_particles) return;
+    const int g = par.gid[s];
+    const int64_t st = par.state_stride;
+    for (int d = 0; d < 3; ++d) {
+        if (pos) pos[(int64_t)g * 3 + d] = par.state[(MPM_CH_X + d) * st + s];
+        if (vel) vel[(int64_t)g * 3 + d] = par.state[(MPM_CH_V + d) * st + s];
+    }
+    for (int k = 0; k < 9; ++k) {
+        if (C) C[(int64_t)g * 9 + k] = par.state[(MPM_CH_C + k) * st + s];
+        if (F) F[(int64_t)g * 9 + k] = par.state[(MPM_CH_F + k) * st + s];
+    }
+    if (Jp) Jp[g] = par.state[MPM_CH_JP * st + s];
+    if (active) active[g] = (par.pflags[s] & MPM_PFLAG_ACTIVE) ? 1 : 0;
+}
+
+__global__ void k_set_state(mpm_problem prob, mpm_particles par, const float* pos, const float* vel, const float* C,
+                            const float* F, const float* Jp, const uint8_t* active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= prob.n_particles) return;
+    const int g = par.gid[s];
+    const int64_t st = par.state_stride;
+    for (int d = 0; d < 3; ++d) {
+        if (pos) par.state[(MPM_CH_X + d) * st + s] = pos[(int64_t)g * 3 + d];
+        if (vel) par.state[(MPM_CH_V + d) * st + s] = vel[(int64_t)g * 3 + d];
+    }
+    for (int k = 0; k < 9; ++k) {
+        if (C) par.state[(MPM_CH_C + k) * st + s] = C[(int64_t)g * 9 + k];
+        if (F) par.state[(MPM_CH_F + k) * st + s] = F[(int64_t)g * 9 + k];
+    }
+    if (Jp) par.state[MPM_CH_JP * st + s] = Jp[g];
+    if (active) par.pflags[s] = (uint8_t)((par.pflags[s] & ~MPM_PFLAG_ACTIVE) | (active[g] ? MPM_PFLAG_ACTIVE : 0));
+}
+
+__global__ void k_set_pos(mpm_problem prob, const mpm_instance* __restrict__ inst, const mpm_material* __restrict__ mats,
+                          mpm_particles par, int n, const int* idx, const float* pos) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = idx[i];
+    if (g < 0 || g >= prob.n_particles) return;
+    const int s = par.slot[g];
+    const int64_t st = par.state_stride;
+    const int k = find_instance_by_particle(inst, prob.n_instances, s);
+    const float djp = mats[inst[k].mat_base + par.mat[s]].default_Jp;
+    for (int d = 0; d < 3; ++d) {
+        par.state[(MPM_CH_X + d) * st + s] = pos[(int64_t)i * 3 + d];
+        par.state[(MPM_CH_V + d) * st + s] = 0.f;
+    }
+    for (int kk = 0; kk < 9; ++kk) {
+        par.state[(MPM_CH_C + kk) * st + s] = 0.f;
+        par.state[(MPM_CH_F + kk) * st + s] = (kk % 4 == 0) ? 1.f : 0.f;
+    }
+    par.state[MPM_CH_JP * st + s] = djp;
+}
+
+__global__ void k_set_vel(mpm_problem prob, mpm_particles par, int n, const int* idx, const float* vel) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = idx[i];
+    if (g < 0 || g >= prob.n_particles) return;
+    const int s = par.slot[g];
+    for (int d = 0; d < 3; ++d) par.state[(MPM_CH_V + d) * par.state_stride + s] = vel[(int64_t)i * 3 + d];
+}
+
+__global__ void k_set_flag(mpm_problem prob, mpm_particles par, int n, const int* idx, const uint8_t* val, uint8_t bit) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = idx[i];
+    if (g < 0 || g >= prob.n_particles) return;
+    const int s = par.slot[g];
+    par.pflags[s] = (uint8_t)((par.pflags[s] & ~bit) | (val[i] ? bit : 0));
+}
+
+// ---------------------------------------------------------------- host side
+
+struct DevInfo {
+    int sms = 0;
+    int occ_p2g[3] = {0, 0, 0};
+    int occ_g2p[3] = {0, 0, 0};
+    int occ_grid = 0;
+};
+
+static std::mutex g_mu;
+static DevInfo g_dev[64];
+
+template <int P>
+static int occ_of(void (*k)(P2GArgs)) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, P, 0);
+    return n > 0 ? n : 1;
+}
+
+static const DevInfo* dev_info() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevInfo& d = g_dev[dev];
+    if (d.sms == 0) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        d.occ_p2g[0] = occ_of<128>(k_p2g<128>);
+        d.occ_p2g[1] = occ_of<256>(k_p2g<256>);
+        d.occ_p2g[2] = occ_of<512>(k_p2g<512>);
+        d.occ_g2p[0] = occ_of<128>(k_g2p<128>);
+        d.occ_g2p[1] = occ_of<256>(k_g2p<256>);
+        d.occ_g2p[2] = occ_of<512>(k_g2p<512>);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op, 256, 0);
+        d.occ_grid = n > 0 ? n : 1;
+        d.sms = sms > 0 ? sms : 1;
+    }
+    return &d;
+}
+
+static int p_index(int P) { return P == 128 ? 0 : (P == 256 ? 1 : (P == 512 ? 2 : -1)); }
+
+static int check_problem(const mpm_problem* p) {
+    if (!p) return MPM_E_INVALID;
+    if (p->n_instances <= 0 || p->n_particles < 0 || p->n_blocks <= 0 || p->n_materials <= 0) return MPM_E_INVALID;
+    if (p_index(p->chunk_particles) < 0) return MPM_E_INVALID;
+    if (p->n_blocks > MAX_BLOCKS || p->n_blocks > INT32_MAX) return MPM_E_CAPACITY;
+    int32_t need = 0;
+    mpm_max_chunks(p->n_particles, p->n_blocks, p->chunk_particles, &need);
+    if (p->max_chunks < need) return MPM_E_INVALID;
+    return MPM_OK;
+}
+
+static int check_par(const mpm_problem* p, const mpm_particles* par) {
+    if (!par || !par->state || !par->mat || !par->pflags || !par->gid || !par->slot) return MPM_E_INVALID;
+    if (par->state_stride < p->n_particles) return MPM_E_INVALID;
+    if ((par->mu_p == nullptr) != (par->lam_p == nullptr)) return MPM_E_INVALID;
+    return MPM_OK;
+}
+
+static inline int cuda_ok() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "genesis_b200_mpm: CUDA error %s\n", cudaGetErrorString(e));
+        return MPM_E_CUDA;
+    }
+    return MPM_OK;
+}
+
+static int launch_sort(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, cudaStream_t s) {
+    Ws w = ws_of(*prob, ws);
+    const int64_t nb = prob->n_blocks;
+    if (cudaMemsetAsync(w.bin_count, 0, nb * sizeof(int), s) != cudaSuccess) return MPM_E_CUDA;
+    const int n = prob->n_particles;
+    const int T = 256;
+    if (n > 0) k_sort_keys<<<(n + T - 1) / T, T, 0, s>>>(*prob, tab->instances, *par, w);
+    const int ntiles = (int)((nb + SCAN_TILE - 1) / SCAN_TILE);
+    k_scan_reduce<<<ntiles, SCAN_T, 0, s>>>(nb, prob->chunk_particles, w);
+    k_scan_tiles<<<1, SCAN_T, 0, s>>>(ntiles, w);
+    k_scan_apply<<<ntiles, SCAN_T, 0, s>>>(nb, prob->chunk_particles, w);
+    if (n > 0) {
+        k_sort_scatter<<<(n + T - 1) / T, T, 0, s>>>(*prob, *par, w);
+        k_sort_copyback<<<(n + T - 1) / T, T, 0, s>>>(*prob, *par, w);
+    }
+    k_build_chunks<<<(int)((nb + T - 1) / T), T, 0, s>>>(*prob, tab->instances, w);
+    return cuda_ok();
+}
+
+static int persistent_ctas(const mpm_problem* prob, int occ) {
+    const DevInfo* d = dev_info();
+    if (!d) return -1;
+    int ctas = prob->grid_ctas > 0 ? prob->grid_ctas : d->sms * occ;
+    if (ctas > prob->max_chunks) ctas = prob->max_chunks > 0 ? prob->max_chunks : 1;
+    return ctas;
+}
+
+static int launch_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, cudaStream_t s) {
+    const DevInfo* d = dev_info();
+    if (!d) return MPM_E_CUDA;
+    P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
+    const int pi = p_index(prob->chunk_particles);
+    const int ctas = persistent_ctas(prob, d->occ_p2g[pi]);
+    switch (prob->chunk_particles) {
+        case 128: k_p2g<128><<<ctas, 128, 0, s>>>(a); break;
+        case 256: k_p2g<256><<<ctas, 256, 0, s>>>(a); break;
+        case 512: k_p2g<512><<<ctas, 512, 0, s>>>(a); break;
+    }
+    if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
+        k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);
+    return cuda_ok();
+}
+
+static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* ws, cudaStream_t s) {
+    const DevInfo* d = dev_info();
+    if (!d) return MPM_E_CUDA;
+    int ctas = prob->grid_ctas > 0 ? prob->grid_ctas : d->sms * d->occ_grid;
+    const int64_t need = (prob->n_blocks + 3) / 4;
+    if (ctas > need) ctas = (int)need;
+    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws));
+    return cuda_ok();
+}
+
+static int launch_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, cudaStream_t s) {
+    const DevInfo* d = dev_info();
+    if (!d) return MPM_E_CUDA;
+    P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
+    const int pi = p_index(prob->chunk_particles);
+    const int ctas = persistent_ctas(prob, d->occ_g2p[pi]);
+    switch (prob->chunk_particles) {
+        case 128: k_g2p<128><<<ctas, 128, 0, s>>>(a); break;
+        case 256: k_g2p<256><<<ctas, 256, 0, s>>>(a); break;
+        case 512: k_g2p<512><<<ctas, 512, 0, s>>>(a); break;
+    }
+    return cuda_ok();
+}
+
+}  // namespace gbm
+
+using namespace gbm;
+
+extern "C" {
+
+int mpm_abi_version(void) { return MPM_ABI_VERSION; }
+
+int mpm_struct_sizes(int32_t* out4) {
+    if (!out4) return MPM_E_INVALID;
+    out4[0] = (int32_t)sizeof(mpm_instance);
+    out4[1] = (int32_t)sizeof(mpm_material);
+    out4[2] = (int32_t)sizeof(mpm_problem);
+    out4[3] = (int32_t)sizeof(mpm_particles);
+    return MPM_OK;
+}
+
+int mpm_max_chunks(int32_t n_particles, int64_t n_blocks, int32_t chunk_particles, int32_t* out) {
+    if (!out || chunk_particles <= 0 || n_particles < 0 || n_blocks < 0) return MPM_E_INVALID;
+    int64_t m = (int64_t)n_particles / chunk_particles + (n_particles < n_blocks ? n_particles : n_blocks) + 1;
+    if (m > INT32_MAX) return MPM_E_CAPACITY;
+    *out = (int32_t)m;
+    return MPM_OK;
+}
+
+int mpm_workspace_bytes(const mpm_problem* prob, uint64_t* out) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!out) return MPM_E_INVALID;
+    *out = layout_of(*prob).total;
+    return MPM_OK;
+}
+
+int mpm_grid_offsets(const mpm_problem* prob, uint64_t* mm_offset, uint64_t* vel_offset) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!mm_offset || !vel_offset) return MPM_E_INVALID;
+    Layout L = layout_of(*prob);
+    *mm_offset = L.off[0];
+    *vel_offset = L.off[1];
+    return MPM_OK;
+}
+
+int mpm_workspace_init(const mpm_problem* prob, void* workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!workspace) return MPM_E_INVALID;
+    if (cudaMemsetAsync(workspace, 0, layout_of(*prob).total, (cudaStream_t)stream) != cudaSuccess) return MPM_E_CUDA;
+    return MPM_OK;
+}
+
+int mpm_sort_particles(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                       void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !workspace) return MPM_E_INVALID;
+    return launch_sort(prob, tab, par, workspace, (cudaStream_t)stream);
+}
+
+int mpm_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !workspace) return MPM_E_INVALID;
+    return launch_p2g(prob, tab, par, workspace, (cudaStream_t)stream);
+}
+
+int mpm_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!tab || !tab->instances || !workspace) return MPM_E_INVALID;
+    return launch_grid_op(prob, tab, workspace, (cudaStream_t)stream);
+}
+
+int mpm_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !workspace) return MPM_E_INVALID;
+    return launch_g2p(prob, tab, par, workspace, (cudaStream_t)stream);
+}
+
+static int substeps_impl(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, int32_t n,
+                         int32_t sort_interval, int64_t first, cudaStream_t s) {
+    for (int32_t i = 0; i < n; ++i) {
+        int rc;
+        if (sort_interval > 0 && ((first + i) % sort_interval) == 0) {
+            if ((rc = launch_sort(prob, tab, par, ws, s))) return rc;
+        }
+        if ((rc = launch_p2g(prob, tab, par, ws, s))) return rc;
+        if ((rc = launch_grid_op(prob, tab, ws, s))) return rc;
+        if ((rc = launch_g2p(prob, tab, par, ws, s))) return rc;
+    }
+    return MPM_OK;
+}
+
+int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                 int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !workspace || n_substeps < 0) return MPM_E_INVALID;
+    return substeps_impl(prob, tab, par, workspace, n_substeps, sort_interval, first_substep, (cudaStream_t)stream);
+}
+
+int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!workspace || !out) return MPM_E_INVALID;
+    Ws w = ws_of(*prob, workspace);
+    cudaStream_t s = (cudaStream_t)stream;
+    uint32_t v = 0;
+    if (cudaMemcpyAsync(&v, &w.counters[CNT_STATUS], 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPM_E_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPM_E_CUDA;
+    if (clear && cudaMemsetAsync(&w.counters[CNT_STATUS], 0, 4, s) != cudaSuccess) return MPM_E_CUDA;
+    *out = v;
+    return MPM_OK;
+}
+
+int mpm_fallback_count(const mpm_problem* prob, void* workspace, int32_t clear, uint64_t* out, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!workspace || !out) return MPM_E_INVALID;
+    Ws w = ws_of(*prob, workspace);
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long v = 0;
+    if (cudaMemcpyAsync(&v, &w.counters[CNT_FALLBACK], 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPM_E_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPM_E_CUDA;
+    if (clear && cudaMemsetAsync(&w.counters[CNT_FALLBACK], 0, 8, s) != cudaSuccess) return MPM_E_CUDA;
+    *out = v;
+    return MPM_OK;
+}
+
+int mpm_get_state(const mpm_problem* prob, const mpm_particles* par, float* pos, float* vel, float* C, float* F,
+                  float* Jp, uint8_t* active, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    const int n = prob->n_particles;
+    if (n > 0) k_get_state<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*prob, *par, pos, vel, C, F, Jp, active);
+    return cuda_ok();
+}
+
+int mpm_set_state(const mpm_problem* prob, mpm_particles* par, const float* pos, const float* vel, const float* C,
+                  const float* F, const float* Jp, const uint8_t* active, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    const int n = prob->n_particles;
+    if (n > 0) k_set_state<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*prob, *par, pos, vel, C, F, Jp, active);
+    return cuda_ok();
+}
+
+int mpm_set_particles_pos(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, int32_t n,
+                          const int32_t* idx, const float* pos, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || n < 0 || (n > 0 && (!idx || !pos))) return MPM_E_INVALID;
+    if (n > 0)
+        k_set_pos<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*prob, tab->instances, tab->materials, *par, n,
+                                                                      idx, pos);
+    return cuda_ok();
+}
+
+int mpm_set_particles_vel(const mpm_problem* prob, mpm_particles* par, int32_t n, const int32_t* idx,
+                          const float* vel, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (n < 0 || (n > 0 && (!idx || !vel))) return MPM_E_INVALID;
+    if (n > 0) k_set_vel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*prob, *par, n, idx, vel);
+    return cuda_ok();
+}
+
+int mpm_set_particles_active(const mpm_problem* prob, mpm_particles* par, int32_t n, const int32_t* idx,
+                             const uint8_t* active, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (n < 0 || (n > 0 && (!idx || !active))) return MPM_E_INVALID;
+    if (n > 0)
+        k_set_flag<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*prob, *par, n, idx, active,
+                                                                       (uint8_t)MPM_PFLAG_ACTIVE);
+    return cuda_ok();
+}
+
+int mpm_set_particles_free(const mpm_problem* prob, mpm_particles* par, int32_t n, const int32_t* idx,
+                           const uint8_t* free_flag, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (n < 0 || (n > 0 && (!idx || !free_flag))) return MPM_E_INVALID;
+    if (n > 0)
+        k_set_flag<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*prob, *par, n, idx, free_flag,
+                                                                       (uint8_t)MPM_PFLAG_FREE);
+    return cuda_ok();
+}
+
+struct GraphHandle {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+int mpm_graph_create(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                     int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream,
+                     void** graph_out) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !workspace || !graph_out || n_substeps <= 0 || !stream)
+        return MPM_E_INVALID;
+    if (!dev_info()) return MPM_E_CUDA;  // occupancy queries must not run inside the capture
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return MPM_E_CUDA;
+    rc = substeps_impl(prob, tab, par, workspace, n_substeps, sort_interval, first_substep, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc ? rc : MPM_E_CUDA;
+    }
+    cudaGraphExec_t ex = nullptr;
+    if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return MPM_E_CUDA;
+    }
+    GraphHandle* h = new GraphHandle{g, ex};
+    *graph_out = h;
+    return MPM_OK;
+}
+
+int mpm_graph_launch(void* graph, void* stream) {
+    if (!graph) return MPM_E_INVALID;
+    GraphHandle* h = (GraphHandle*)graph;
+    if (cudaGraphLaunch(h->exec, (cudaStream_t)stream) != cudaSuccess) return MPM_E_CUDA;
+    return MPM_OK;
+}
+
+int mpm_graph_destroy(void* graph) {
+    if (!graph) return MPM_E_INVALID;
+    GraphHandle* h = (GraphHandle*)graph;
+    cudaGraphExecDestroy(h->exec);
+    cudaGraphDestroy(h->graph);
+    delete h;
+    return MPM_OK;
+}
+
+}  // extern "C"

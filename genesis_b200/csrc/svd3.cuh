@@ -1,0 +1,176 @@
+// Register-resident 3x3 singular value decomposition for the p2g kernel.
+//
+// Replaces ti.svd(F_tmp) at genesis/engine/solvers/mpm_solver.py:273.  gstaichi's
+// ti.svd follows McAdams et al. 2011 ("Computing the Singular Value Decomposition of
+// 3x3 matrices with minimal branching and elementary floating point operations"),
+// whose structure this implementation keeps:
+//   1. cyclic Jacobi eigen-analysis of the symmetric A^T A, accumulating V as a
+//      product of plane rotations (so det V = +1),
+//   2. sort the columns of B = A V by decreasing squared norm, negating one column on
+//      every swap so V stays a proper rotation,
+//   3. Givens QR of B with non-negative r00 and r11, giving a proper rotation U and
+//      the singular values on the diagonal of R; only the last one can be negative
+//      (det A < 0).
+// Unlike the paper's quaternion "approximate Givens" rotations, the Jacobi step uses
+// exact rotations (Golub & Van Loan, Alg. 8.4.2) with a fixed sweep count, which keeps
+// the kernel branch-light and converges to float32 round-off in 4-5 sweeps for the
+// deformation gradients MPM produces.
+#pragma once
+
+namespace gbm {
+
+// One Jacobi rotation in plane (P, Q) of the symmetric matrix a, accumulated into v.
+template <int P, int Q>
+__device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
+    constexpr int R = 3 - P - Q;
+    const float apq = a[P][Q];
+    const float app = a[P][P];
+    const float aqq = a[Q][Q];
+    float t = 0.f, c = 1.f, s = 0.f;
+    if (fabsf(apq) > 1e-30f) {
+        const float tau = (aqq - app) / (2.f * apq);
+        const float at = fabsf(tau);
+        t = (at > 1e15f) ? 0.5f / tau : copysignf(1.f, tau) / (at + sqrtf(1.f + tau * tau));
+        c = 1.f / sqrtf(1.f + t * t);
+        s = t * c;
+    }
+    a[P][P] = app - t * apq;
+    a[Q][Q] = aqq + t * apq;
+    a[P][Q] = 0.f;
+    a[Q][P] = 0.f;
+    const float arp = a[R][P];
+    const float arq = a[R][Q];
+    const float nrp = c * arp - s * arq;
+    const float nrq = s * arp + c * arq;
+    a[R][P] = nrp;
+    a[P][R] = nrp;
+    a[R][Q] = nrq;
+    a[Q][R] = nrq;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float vip = v[i][P];
+        const float viq = v[i][Q];
+        v[i][P] = c * vip - s * viq;
+        v[i][Q] = s * vip + c * viq;
+    }
+}
+
+__device__ __forceinline__ void givens(float a, float b, float& c, float& s) {
+    const float r = sqrtf(a * a + b * b);
+    if (r > 1e-30f) {
+        const float ir = 1.f / r;
+        c = a * ir;
+        s = b * ir;
+    } else {
+        c = 1.f;
+        s = 0.f;
+    }
+}
+
+template <int I, int J>
+__device__ __forceinline__ void swap_cols_neg(float (&b)[3][3], float (&v)[3][3], float& ni, float& nj) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        float tb = b[r][I];
+        b[r][I] = b[r][J];
+        b[r][J] = -tb;
+        float tv = v[r][I];
+        v[r][I] = v[r][J];
+        v[r][J] = -tv;
+    }
+    float tn = ni;
+    ni = nj;
+    nj = tn;
+}
+
+// A (row-major, 9 floats) = U diag(S) V^T with U, V proper rotations (row-major).
+template <int SWEEPS = 5>
+__device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* V) {
+    float a[3][3];
+    // A^T A
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = i; j < 3; ++j) {
+            float acc = A[0 * 3 + i] * A[0 * 3 + j] + A[1 * 3 + i] * A[1 * 3 + j] + A[2 * 3 + i] * A[2 * 3 + j];
+            a[i][j] = acc;
+            a[j][i] = acc;
+        }
+    float v[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
+#pragma unroll
+    for (int sw = 0; sw < SWEEPS; ++sw) {
+        jacobi_pq<0, 1>(a, v);
+        jacobi_pq<0, 2>(a, v);
+        jacobi_pq<1, 2>(a, v);
+    }
+    // B = A V
+    float b[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            b[i][j] = A[i * 3 + 0] * v[0][j] + A[i * 3 + 1] * v[1][j] + A[i * 3 + 2] * v[2][j];
+    float n0 = b[0][0] * b[0][0] + b[1][0] * b[1][0] + b[2][0] * b[2][0];
+    float n1 = b[0][1] * b[0][1] + b[1][1] * b[1][1] + b[2][1] * b[2][1];
+    float n2 = b[0][2] * b[0][2] + b[1][2] * b[1][2] + b[2][2] * b[2][2];
+    if (n0 < n1) swap_cols_neg<0, 1>(b, v, n0, n1);
+    if (n0 < n2) swap_cols_neg<0, 2>(b, v, n0, n2);
+    if (n1 < n2) swap_cols_neg<1, 2>(b, v, n1, n2);
+    // Givens QR: B = U R
+    float u[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
+    float c, s;
+    // rows (0,1), column 0
+    givens(b[0][0], b[1][0], c, s);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float t0 = b[0][j], t1 = b[1][j];
+        b[0][j] = c * t0 + s * t1;
+        b[1][j] = -s * t0 + c * t1;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float t0 = u[i][0], t1 = u[i][1];
+        u[i][0] = c * t0 + s * t1;
+        u[i][1] = -s * t0 + c * t1;
+    }
+    // rows (0,2), column 0
+    givens(b[0][0], b[2][0], c, s);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float t0 = b[0][j], t2 = b[2][j];
+        b[0][j] = c * t0 + s * t2;
+        b[2][j] = -s * t0 + c * t2;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float t0 = u[i][0], t2 = u[i][2];
+        u[i][0] = c * t0 + s * t2;
+        u[i][2] = -s * t0 + c * t2;
+    }
+    // rows (1,2), column 1
+    givens(b[1][1], b[2][1], c, s);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float t1 = b[1][j], t2 = b[2][j];
+        b[1][j] = c * t1 + s * t2;
+        b[2][j] = -s * t1 + c * t2;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float t1 = u[i][1], t2 = u[i][2];
+        u[i][1] = c * t1 + s * t2;
+        u[i][2] = -s * t1 + c * t2;
+    }
+    S[0] = b[0][0];
+    S[1] = b[1][1];
+    S[2] = b[2][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            U[i * 3 + j] = u[i][j];
+            V[i * 3 + j] = v[i][j];
+        }
+}
+
+}  // namespace gbm

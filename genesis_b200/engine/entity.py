@@ -1,0 +1,226 @@
+"""MPMEntity: particle sampling and per-entity state I/O
+(genesis/engine/entities/mpm_entity.py, particle_entity.py)."""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import morphs as _morphs
+from ..exceptions import GenesisException
+from .states import MPMEntityState
+
+
+def _as_tensor(x, dtype, device):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype)
+    return torch.as_tensor(np.asarray(x), dtype=dtype, device=device)
+
+
+class MPMEntity:
+    def __init__(self, scene, solver, material, morph, surface, particle_size, idx, particle_start, rng=None):
+        self._scene = scene
+        self._solver = solver
+        self._sim = solver.sim
+        self._material = material
+        self._morph = morph
+        self._surface = surface
+        self._particle_size = particle_size
+        self._idx = idx
+        self._particle_start = particle_start
+        sampler = material.sampler
+        self.sampler = sampler
+        self._particles = np.asarray(morph.sample(particle_size, sampler, rng), dtype=np.float64)
+        if self._particles.size == 0:
+            raise GenesisException("Entity has zero particles.")
+        self.active = not isinstance(morph, _morphs.Nowhere)
+        if self.active and not solver.boundary.is_inside(self._particles):
+            # particle_entity.py:330-336
+            raise GenesisException(
+                "Entity has particles outside solver boundary. Note that for MPMSolver, boundary is slightly "
+                "tighter than the specified domain due to safety padding.\n\n"
+                f"Current boundary:\n{solver.boundary}\n\nEntity to be added:\nmin: {self._particles.min(0)}\n"
+                f"max: {self._particles.max(0)}\n"
+            )
+        self._n_particles = len(self._particles)
+        origin = np.asarray(morph.pos, dtype=np.float64)
+        self._init_particles_offset = self._particles - origin
+        self._tgt = {"pos": None, "vel": None, "act": None}
+
+    # ------------------------------------------------------------ properties
+    @property
+    def scene(self):
+        return self._scene
+
+    @property
+    def sim(self):
+        return self._sim
+
+    @property
+    def solver(self):
+        return self._solver
+
+    @property
+    def material(self):
+        return self._material
+
+    @property
+    def morph(self):
+        return self._morph
+
+    @property
+    def surface(self):
+        return self._surface
+
+    @property
+    def idx(self):
+        return self._idx
+
+    @property
+    def n_particles(self):
+        return self._n_particles
+
+    @property
+    def particle_start(self):
+        return self._particle_start
+
+    @property
+    def particle_end(self):
+        return self._particle_start + self._n_particles
+
+    @property
+    def particle_size(self):
+        return self._particle_size
+
+    @property
+    def init_particles(self):
+        return self._particles
+
+    @property
+    def is_built(self):
+        return self._scene.is_built
+
+    # ---------------------------------------------------------------- helpers
+    def _envs(self, envs_idx):
+        return self._scene._sanitize_envs_idx(envs_idx)
+
+    def _flat_idx(self, particles_idx_local, envs_idx):
+        """Runtime (flattened over environments) indices, shape (M, K)."""
+        envs = self._envs(envs_idx)
+        N = self._solver.n_particles
+        dev = self._solver.device
+        if particles_idx_local is None:
+            local = torch.arange(self._n_particles, device=dev).expand(len(envs), -1)
+        else:
+            local = _as_tensor(particles_idx_local, torch.int64, dev)
+            if local.ndim == 1:
+                local = local.expand(len(envs), -1)
+            if (local < 0).any() or (local >= self._n_particles).any():
+                raise GenesisException("particle index out of range for this entity.")
+        return envs[:, None] * N + self._particle_start + local
+
+    def _values(self, vals, shape_tail, n_envs, n_p, dtype):
+        t = _as_tensor(vals, dtype, self._solver.device)
+        t = t.reshape((-1,) + tuple(shape_tail)) if t.ndim == len(shape_tail) else t
+        return t.expand((n_envs, n_p) + tuple(shape_tail)).reshape((-1,) + tuple(shape_tail)).contiguous()
+
+    def _check_built(self):
+        if not self._scene.is_built:
+            raise GenesisException("Scene is not built yet.")
+
+    # --------------------------------------------------------------- setters
+    def set_particles_pos(self, poss, particles_idx_local=None, envs_idx=None):
+        """Set positions; also resets v=0, F=I, C=0, Jp=default_Jp (mpm_solver.py:804-822)."""
+        self._check_built()
+        idx = self._flat_idx(particles_idx_local, envs_idx)
+        vals = self._values(poss, (3,), idx.shape[0], idx.shape[1], torch.float32)
+        self._solver.runtime.set_particles_pos(idx.reshape(-1), vals)
+
+    def set_particles_vel(self, vels, particles_idx_local=None, envs_idx=None):
+        self._check_built()
+        idx = self._flat_idx(particles_idx_local, envs_idx)
+        vals = self._values(vels, (3,), idx.shape[0], idx.shape[1], torch.float32)
+        self._solver.runtime.set_particles_vel(idx.reshape(-1), vals)
+
+    def set_particles_active(self, actives, particles_idx_local=None, envs_idx=None):
+        self._check_built()
+        idx = self._flat_idx(particles_idx_local, envs_idx)
+        vals = self._values(actives, (), idx.shape[0], idx.shape[1], torch.uint8)
+        self._solver.runtime.set_particles_active(idx.reshape(-1), vals)
+
+    def set_free(self, free, particles_idx_local=None):
+        """Non-free particles act as boundary conditions (mpm_solver.py:388-389)."""
+        self._check_built()
+        idx = self._flat_idx(particles_idx_local, None)
+        vals = self._values(free, (), idx.shape[0], idx.shape[1], torch.uint8)
+        self._solver.runtime.set_particles_free(idx.reshape(-1), vals)
+
+    # buffered targets applied at the next step (particle_entity.py:418-458, 503-578)
+    def set_position(self, value, envs_idx=None):
+        poss = _as_tensor(value, torch.float32, self._solver.device)
+        if poss.ndim == 1 or (poss.ndim == 2 and poss.shape[0] != self._n_particles):
+            off = torch.as_tensor(self._init_particles_offset, dtype=torch.float32, device=poss.device)
+            poss = off + poss[..., None, :]
+        self._tgt["pos"] = (poss, envs_idx)
+
+    def set_velocity(self, vels, envs_idx=None):
+        self._tgt["vel"] = (_as_tensor(vels, torch.float32, self._solver.device), envs_idx)
+
+    def set_active(self, active, envs_idx=None):
+        self._tgt["act"] = (_as_tensor(active, torch.uint8, self._solver.device), envs_idx)
+
+    def process_input(self, in_backward=False):
+        # positions first: setting positions resets velocities (particle_entity.py:439-440)
+        if self._tgt["pos"] is not None:
+            v, e = self._tgt["pos"]
+            if v.ndim == 1 or (v.ndim == 2 and v.shape[-1] == 3 and v.shape[0] != self._n_particles):
+                v = v.expand(self._n_particles, 3)
+            self.set_particles_pos(v, envs_idx=e)
+        if self._tgt["vel"] is not None:
+            v, e = self._tgt["vel"]
+            if v.ndim == 1:
+                v = v.expand(self._n_particles, 3)
+            self.set_particles_vel(v, envs_idx=e)
+        if self._tgt["act"] is not None:
+            v, e = self._tgt["act"]
+            if v.ndim == 0:
+                v = v.expand(self._n_particles)
+            self.set_particles_active(v, envs_idx=e)
+        for k in self._tgt:
+            self._tgt[k] = None
+
+    # --------------------------------------------------------------- getters
+    def _get(self, keys, envs_idx):
+        self._check_built()
+        envs = self._envs(envs_idx)
+        st = self._solver.runtime.get_state(keys)
+        B, N = self._solver.B, self._solver.n_particles
+        out = {}
+        for k, v in st.items():
+            v = v.reshape((B, N) + tuple(v.shape[1:]))[envs, self._particle_start : self.particle_end]
+            if k in ("C", "F"):
+                v = v.reshape(v.shape[:2] + (3, 3))
+            out[k] = v
+        return out
+
+    def _squeeze(self, t):
+        return t[0] if self._scene.n_envs == 0 else t
+
+    def get_particles_pos(self, envs_idx=None):
+        return self._squeeze(self._get(("pos",), envs_idx)["pos"])
+
+    def get_particles_vel(self, envs_idx=None):
+        return self._squeeze(self._get(("vel",), envs_idx)["vel"])
+
+    def get_particles_active(self, envs_idx=None):
+        return self._squeeze(self._get(("active",), envs_idx)["active"])
+
+    def get_state(self):
+        st = self._get(("pos", "vel", "C", "F", "Jp", "active"), None)
+        return MPMEntityState(self, self._sim.cur_step_global, st["pos"], st["vel"], st["C"], st["F"], st["Jp"],
+                              st["active"])
+
+    def get_mass(self):
+        """Total mass in kg, the 1e3 volume scale divided back out (mpm_solver.py:1000-1009)."""
+        return float(self._n_particles * self._solver.particle_volume * self._material.rho
+                     / self._solver.particle_volume_scale)

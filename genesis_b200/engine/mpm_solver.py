@@ -1,0 +1,315 @@
+"""MPMSolver facade: the reference's solver interface over the CUDA runtime.
+
+Method names and meanings follow genesis/engine/solvers/mpm_solver.py: the substep
+is split into ``substep_pre_coupling`` (p2g with F/SVD/material update, :471-483),
+``LegacyCoupler.couple`` (grid op, legacy_coupler.py:941-954) and
+``substep_post_coupling`` (g2p + NaN check, :498-509).  ``advance`` runs whole
+substeps back to back (one CUDA graph per sort interval) for ``Simulator.step``.
+"""
+
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from ..exceptions import GenesisException
+from .boundaries import CubeBoundary
+from .entity import MPMEntity
+from .runtime import InstanceSpec, MPMRuntime
+from .states import MPMSolverState
+
+log = logging.getLogger("genesis_b200")
+
+
+class MPMSolver:
+    def __init__(self, scene, sim, options, b200_options):
+        self._scene = scene
+        self._sim = sim
+        self._options = options
+        self._b200 = b200_options
+        self._dt = options.dt
+        self._substep_dt = options.dt / sim.substeps
+        self._init_gravity = options.gravity
+        self._grid_density = options.grid_density
+        self._particle_size = options.particle_size
+        self._upper_bound = np.array(options.upper_bound, dtype=np.float64)
+        self._lower_bound = np.array(options.lower_bound, dtype=np.float64)
+        self._enable_CPIC = options.enable_CPIC
+        # mpm_solver.py:43-61
+        self._particle_volume_real = float(self._particle_size**3)
+        self._particle_volume_scale = 1e3
+        self._particle_volume = self._particle_volume_real * self._particle_volume_scale
+        self._dx = float(1.0 / self._grid_density)
+        self._inv_dx = float(self._grid_density)
+        self._lower_bound_cell = np.round(self._grid_density * self._lower_bound).astype(np.int32)
+        self._upper_bound_cell = np.round(self._grid_density * self._upper_bound).astype(np.int32)
+        self._grid_res = self._upper_bound_cell - self._lower_bound_cell + 1
+        self._grid_offset = self._lower_bound_cell.copy()
+        if np.prod(self._grid_res.astype(np.float64)) > 1e9:
+            raise GenesisException(
+                "Grid size larger than 1e9 not supported by MPM solver. Please reduce 'grid_density', or set tighter "
+                "boundaries via 'lower_bound' / 'upper_bound'."
+            )
+        self._materials = []
+        self._materials_idx = []
+        self._entities: list[MPMEntity] = []
+        self.runtime: MPMRuntime | None = None
+        self._B = 1
+        self.setup_boundary()
+
+    def setup_boundary(self):
+        # mpm_solver.py:72-78
+        self.boundary_padding = 3 * self._dx
+        self.boundary = CubeBoundary(
+            lower=self._lower_bound + self.boundary_padding, upper=self._upper_bound - self.boundary_padding
+        )
+
+    # ----------------------------------------------------------------- build
+    def add_material(self, material):
+        # mpm_solver.py:240-251
+        for m in self._materials:
+            if material == m:
+                material._idx = m._idx
+                break
+        else:
+            material._idx = len(self._materials_idx)
+            self._materials_idx.append(material._idx)
+        self._materials.append(material)
+
+    def add_entity(self, idx, material, morph, surface, rng=None):
+        self.add_material(material)
+        ent = MPMEntity(self._scene, self, material, morph, surface, self._particle_size, idx, self.n_particles, rng)
+        self._entities.append(ent)
+        return ent
+
+    @property
+    def unique_materials(self):
+        seen = {}
+        for m in self._materials:
+            seen.setdefault(m._idx, m)
+        return [seen[i] for i in sorted(seen)]
+
+    def build(self):
+        self._B = self._sim._B
+        if not self.is_active:
+            return
+        suggested_dt = 2e-2 * self._dx
+        if self._substep_dt > suggested_dt:
+            log.warning(
+                f"Current `substep_dt` ({self._substep_dt:.6g}) is greater than suggested_dt ({suggested_dt:.6g}, "
+                "calculated based on `grid_density`). Simulation might be unstable."
+            )
+        gravity = self._init_gravity if self._init_gravity is not None else self._sim.gravity
+        N = self.n_particles
+        spec_kw = dict(
+            grid_density=self._grid_density,
+            lower_bound=tuple(self._lower_bound),
+            upper_bound=tuple(self._upper_bound),
+            particle_size=self._particle_size,
+            dt=self._substep_dt,
+            gravity=tuple(float(g) for g in gravity),
+            materials=self.unique_materials,
+            n_particles=N,
+        )
+        from .. import _globals
+
+        spec_kw["eps"] = _globals.EPS
+        specs = [InstanceSpec(**spec_kw) for _ in range(self._B)]
+        b = self._b200
+        self.runtime = MPMRuntime(
+            specs,
+            device=self._sim.device,
+            chunk_particles=b.chunk_particles,
+            sort_interval=b.sort_interval,
+            grid_ctas=b.grid_ctas,
+            use_graphs=b.use_cuda_graph,
+        )
+        pos = np.concatenate([e.init_particles for e in self._entities])
+        mat = np.concatenate([np.full(e.n_particles, e.material.idx, dtype=np.uint8) for e in self._entities])
+        act = np.concatenate([np.full(e.n_particles, e.active, dtype=bool) for e in self._entities])
+        self.runtime.init_particles(np.tile(pos, (self._B, 1)), np.tile(mat, self._B), active=np.tile(act, self._B))
+
+    # -------------------------------------------------------------- stepping
+    def process_input(self, in_backward=False):
+        for e in self._entities:
+            e.process_input(in_backward=in_backward)
+
+    def substep_pre_coupling(self, f):
+        """compute_F_tmp + svd + p2g (mpm_solver.py:471-483); reset_grid is folded into grid op."""
+        self.runtime.ensure_sorted()
+        self.runtime.p2g()
+
+    def substep_post_coupling(self, f):
+        """g2p (mpm_solver.py:498-509); the NaN check is a device status bit read at step end."""
+        self.runtime.g2p()
+        self.runtime._count += 1
+
+    def grid_op(self, f):
+        self.runtime.grid_op()
+
+    def advance(self, n_substeps: int):
+        self.runtime.substeps(n_substeps)
+
+    def check_state(self):
+        """Raise if any particle position became NaN (mpm_solver.py:505-509)."""
+        st = self.runtime.status(clear=False)
+        if st & nat.MPM_STATUS_NAN:
+            raise GenesisException(
+                "NaN detected in MPM states. Try reducing the time step size or adjusting simulation parameters."
+            )
+        return st
+
+    # ------------------------------------------------------------------- io
+    def get_state(self, f=None):
+        if not self.is_active:
+            return None
+        st = self.runtime.get_state()
+        B, N = self._B, self.n_particles
+        return MPMSolverState(
+            self._scene,
+            st["pos"].reshape(B, N, 3),
+            st["vel"].reshape(B, N, 3),
+            st["C"].reshape(B, N, 3, 3),
+            st["F"].reshape(B, N, 3, 3),
+            st["Jp"].reshape(B, N),
+            st["active"].reshape(B, N),
+        )
+
+    def set_state(self, f, state, envs_idx=None):
+        if not self.is_active:
+            return
+        B, N = self._B, self.n_particles
+        if envs_idx is not None:
+            cur = self.get_state()
+            envs = self._scene._sanitize_envs_idx(envs_idx)
+            fields = {}
+            for k in ("pos", "vel", "C", "F", "Jp", "active"):
+                t = getattr(cur, k).clone()
+                t[envs] = getattr(state, k).to(t.device, t.dtype)[: len(envs)] if getattr(state, k).shape[0] == len(envs) \
+                    else getattr(state, k).to(t.device, t.dtype)[envs]
+                fields[k] = t
+        else:
+            fields = {k: getattr(state, k) for k in ("pos", "vel", "C", "F", "Jp", "active")}
+        self.runtime.set_state(
+            pos=fields["pos"].reshape(B * N, 3), vel=fields["vel"].reshape(B * N, 3),
+            C_=fields["C"].reshape(B * N, 9), F=fields["F"].reshape(B * N, 9),
+            Jp=fields["Jp"].reshape(B * N), active=fields["active"].reshape(B * N).to(torch.uint8),
+        )
+
+    # ----------------------------------------------------------- properties
+    @property
+    def sim(self):
+        return self._sim
+
+    @property
+    def scene(self):
+        return self._scene
+
+    @property
+    def device(self):
+        return self._sim.device
+
+    @property
+    def B(self):
+        return self._B
+
+    @property
+    def entities(self):
+        return self._entities
+
+    @property
+    def is_active(self):
+        return self.n_particles > 0
+
+    @property
+    def n_particles(self):
+        return sum(e.n_particles for e in self._entities)
+
+    @property
+    def dt(self):
+        return self._dt
+
+    @property
+    def substep_dt(self):
+        return self._substep_dt
+
+    @property
+    def grid_density(self):
+        return self._grid_density
+
+    @property
+    def particle_size(self):
+        return self._particle_size
+
+    @property
+    def particle_radius(self):
+        return self._particle_size / 2.0
+
+    @property
+    def upper_bound(self):
+        return self._upper_bound
+
+    @property
+    def lower_bound(self):
+        return self._lower_bound
+
+    @property
+    def dx(self):
+        return self._dx
+
+    @property
+    def inv_dx(self):
+        return self._inv_dx
+
+    @property
+    def particle_volume_real(self):
+        return self._particle_volume_real
+
+    @property
+    def particle_volume(self):
+        return self._particle_volume
+
+    @property
+    def particle_volume_scale(self):
+        return self._particle_volume_scale
+
+    @property
+    def lower_bound_cell(self):
+        return self._lower_bound_cell
+
+    @property
+    def upper_bound_cell(self):
+        return self._upper_bound_cell
+
+    @property
+    def grid_res(self):
+        return self._grid_res
+
+    @property
+    def grid_offset(self):
+        return self._grid_offset
+
+    @property
+    def enable_CPIC(self):
+        return self._enable_CPIC
+
+    @property
+    def materials(self):
+        return self._materials
+
+
+class LegacyCoupler:
+    """Only the MPM grid update of LegacyCoupler is on this path (legacy_coupler.py:352-375, 495-496)."""
+
+    def __init__(self, sim):
+        self._sim = sim
+
+    def preprocess(self, f):
+        pass
+
+    def couple(self, f):
+        if self._sim.mpm_solver.is_active:
+            self._sim.mpm_solver.grid_op(f)

@@ -1,0 +1,457 @@
+"""Device-resident MPM problem: PyTorch owns every buffer, the C ABI does the work.
+
+One ``MPMRuntime`` advances one or more *instances* (independent scenes, or the
+``n_envs`` copies of one scene) together.  The layout is the one documented in
+include/genesis_b200_mpm.h: particles in planar SoA channels sorted by grid block,
+the grid block-major inside one workspace blob.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+
+F32_EPS = float(np.finfo(np.float32).eps)
+
+
+@dataclass
+class InstanceSpec:
+    """Constants of one scene (MPMSolver.__init__, mpm_solver.py:31-78)."""
+
+    grid_density: float
+    lower_bound: tuple
+    upper_bound: tuple
+    particle_size: float
+    dt: float  # substep dt
+    gravity: tuple
+    materials: list  # objects with ._native(p_vol) -> nat.Material
+    n_particles: int
+    eps: float = F32_EPS
+    # derived
+    dx: float = field(init=False)
+    inv_dx: float = field(init=False)
+    lower_cell: np.ndarray = field(init=False)
+    upper_cell: np.ndarray = field(init=False)
+    grid_res: np.ndarray = field(init=False)
+    p_vol: float = field(init=False)
+    bnd_lo: np.ndarray = field(init=False)
+    bnd_hi: np.ndarray = field(init=False)
+
+    def __post_init__(self):
+        self.dx = float(1.0 / self.grid_density)
+        self.inv_dx = float(self.grid_density)
+        lo = np.asarray(self.lower_bound, dtype=np.float64)
+        hi = np.asarray(self.upper_bound, dtype=np.float64)
+        self.lower_cell = np.round(self.grid_density * lo).astype(np.int64)
+        self.upper_cell = np.round(self.grid_density * hi).astype(np.int64)
+        self.grid_res = self.upper_cell - self.lower_cell + 1
+        self.p_vol = float(self.particle_size**3) * 1e3
+        pad = 3 * self.dx
+        self.bnd_lo = lo + pad
+        self.bnd_hi = hi - pad
+
+    @property
+    def nblk(self) -> np.ndarray:
+        return (self.grid_res + nat.MPM_BLOCK - 1) // nat.MPM_BLOCK
+
+    @property
+    def n_blocks(self) -> int:
+        return int(np.prod(self.nblk))
+
+
+def _cuda_stream_handle():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream or None)
+
+
+class MPMRuntime:
+    """Buffers + C-ABI calls for a set of instances.
+
+    Parameters
+    ----------
+    specs : list[InstanceSpec]
+    chunk_particles : particles per p2g/g2p work item (128, 256 or 512)
+    sort_interval : re-bin particles every this many substeps
+    per_particle_lame : allocate per-particle (mu, lam) overrides
+    """
+
+    def __init__(
+        self,
+        specs: list[InstanceSpec],
+        device=None,
+        chunk_particles: int = 256,
+        sort_interval: int = 16,
+        per_particle_lame: bool = False,
+        grid_ctas: int = 0,
+        use_graphs: bool = True,
+    ):
+        if not torch.cuda.is_available():
+            raise RuntimeError("genesis_b200 needs a CUDA device (sm_100a); there is no CPU path")
+        self.lib = nat.load()
+        self.device = torch.device(device or "cuda")
+        self.specs = list(specs)
+        self.sort_interval = int(sort_interval)
+        self.use_graphs = bool(use_graphs)
+        self._graphs: dict = {}
+        self._count = 0  # substeps executed
+        self._nonfree = False
+
+        insts, mats = [], []
+        p_begin = 0
+        blk_base = 0
+        for sp in self.specs:
+            I = nat.Instance()
+            I.p_begin = p_begin
+            I.p_count = int(sp.n_particles)
+            for d in range(3):
+                I.res[d] = int(sp.grid_res[d])
+                I.nblk[d] = int(sp.nblk[d])
+                I.lower_cell[d] = int(sp.lower_cell[d])
+                I.gravity[d] = float(sp.gravity[d])
+                I.bnd_lo[d] = float(sp.bnd_lo[d])
+                I.bnd_hi[d] = float(sp.bnd_hi[d])
+            I.mat_base = len(mats)
+            I.blk_base = blk_base
+            I.dx = sp.dx
+            I.inv_dx = sp.inv_dx
+            I.dt = float(sp.dt)
+            I.eps = float(sp.eps)
+            # (-dt * particle_volume * 4 * inv_dx * inv_dx) folded in float64 (mpm_solver.py:344)
+            I.stress_scale = -sp.dt * sp.p_vol * 4 * sp.inv_dx * sp.inv_dx
+            I.c_scale = 4 * sp.inv_dx
+            insts.append(I)
+            for m in sp.materials:
+                mats.append(m._native(sp.p_vol))
+            p_begin += int(sp.n_particles)
+            blk_base += sp.n_blocks
+        self.n = p_begin
+        self.n_blocks = blk_base
+        self.stride = max(64, (self.n + 63) // 64 * 64)
+        self._insts = insts
+        self._mats = mats
+
+        P = int(chunk_particles)
+        mc = C.c_int32()
+        nat.check("mpm_max_chunks", self.lib.mpm_max_chunks(self.n, self.n_blocks, P, C.byref(mc)))
+        self.prob = nat.Problem(
+            n_instances=len(insts),
+            n_particles=self.n,
+            n_blocks=self.n_blocks,
+            n_materials=len(mats),
+            chunk_particles=P,
+            max_chunks=mc.value,
+            grid_ctas=int(grid_ctas),
+            flags=0,
+        )
+        dev = self.device
+        self.inst_table = torch.from_numpy(nat.instances_to_bytes(insts)).to(dev)
+        self.mat_table = torch.from_numpy(nat.materials_to_bytes(mats)).to(dev)
+        self.tables = nat.Tables(self.inst_table.data_ptr(), self.mat_table.data_ptr())
+
+        self.state = torch.zeros((nat.MPM_STATE_CH, self.stride), dtype=torch.float32, device=dev)
+        self.mat = torch.zeros(max(self.n, 1), dtype=torch.uint8, device=dev)
+        self.pflags = torch.full((max(self.n, 1),), nat.PFLAG_ACTIVE | nat.PFLAG_FREE, dtype=torch.uint8, device=dev)
+        self.gid = torch.arange(max(self.n, 1), dtype=torch.int32, device=dev)
+        self.slot = torch.arange(max(self.n, 1), dtype=torch.int32, device=dev)
+        self.mu_p = self.lam_p = None
+        if per_particle_lame:
+            self.mu_p = torch.zeros(max(self.n, 1), dtype=torch.float32, device=dev)
+            self.lam_p = torch.zeros(max(self.n, 1), dtype=torch.float32, device=dev)
+        self.par = nat.Particles(
+            state=self.state.data_ptr(),
+            state_stride=self.stride,
+            mat=self.mat.data_ptr(),
+            pflags=self.pflags.data_ptr(),
+            gid=self.gid.data_ptr(),
+            slot=self.slot.data_ptr(),
+            mu_p=self.mu_p.data_ptr() if self.mu_p is not None else None,
+            lam_p=self.lam_p.data_ptr() if self.lam_p is not None else None,
+        )
+        nbytes = C.c_uint64()
+        nat.check("mpm_workspace_bytes", self.lib.mpm_workspace_bytes(C.byref(self.prob), C.byref(nbytes)))
+        self.workspace_bytes = int(nbytes.value)
+        self.workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=dev)
+        self._ws = C.c_void_p(self.workspace.data_ptr())
+        self._call("mpm_workspace_init", C.byref(self.prob), self._ws, _cuda_stream_handle())
+
+    # ------------------------------------------------------------------ utils
+    def _call(self, name, *args):
+        rc = getattr(self.lib, name)(*args)
+        nat.check(name, rc)
+
+    @property
+    def instance_offsets(self) -> list[int]:
+        return [int(I.p_begin) for I in self._insts]
+
+    def memory_bytes(self) -> int:
+        t = self.state.numel() * 4 + self.mat.numel() * 10 + self.workspace_bytes
+        if self.mu_p is not None:
+            t += self.mu_p.numel() * 8
+        return int(t)
+
+    # -------------------------------------------------------------- state I/O
+    def init_particles(self, pos, mat_idx, active=None, vel=None, default_jp=None):
+        """Initialise all particles in API order (the _kernel_add_particles semantics,
+        mpm_solver.py:768-801): v=0 (or vel), F=I, C=0, Jp=default_Jp, free=True."""
+        n = self.n
+        pos = np.asarray(pos, dtype=np.float32).reshape(n, 3)
+        host = np.zeros((nat.MPM_STATE_CH, n), dtype=np.float32)
+        host[nat.CH_X : nat.CH_X + 3] = pos.T
+        if vel is not None:
+            host[nat.CH_V : nat.CH_V + 3] = np.asarray(vel, dtype=np.float32).reshape(n, 3).T
+        for k in (0, 4, 8):
+            host[nat.CH_F + k] = 1.0
+        mat_idx = np.asarray(mat_idx, dtype=np.uint8).reshape(n)
+        if default_jp is None:
+            default_jp = np.zeros(n, dtype=np.float32)
+            for sp_i, I in enumerate(self._insts):
+                sl = slice(I.p_begin, I.p_begin + I.p_count)
+                djp = np.array([self._mats[I.mat_base + k].default_Jp for k in range(len(self.specs[sp_i].materials))],
+                               dtype=np.float32)
+                default_jp[sl] = djp[mat_idx[sl]]
+        host[nat.CH_JP] = np.asarray(default_jp, dtype=np.float32)
+        flags = np.full(n, nat.PFLAG_ACTIVE | nat.PFLAG_FREE, dtype=np.uint8)
+        if active is not None:
+            flags = np.where(np.asarray(active, dtype=bool).reshape(n), flags, nat.PFLAG_FREE).astype(np.uint8)
+        with torch.no_grad():
+            self.state[:, :n].copy_(torch.from_numpy(host))
+            self.mat[:n].copy_(torch.from_numpy(mat_idx))
+            self.pflags[:n].copy_(torch.from_numpy(flags))
+            self.gid[:n].copy_(torch.arange(n, dtype=torch.int32))
+            self.slot[:n].copy_(torch.arange(n, dtype=torch.int32))
+        self._count = 0
+
+    def set_lame(self, mu, lam):
+        """Per-particle Lame parameters in API order (requires per_particle_lame=True)."""
+        if self.mu_p is None:
+            raise RuntimeError("runtime was built without per-particle Lame parameters")
+        mu = torch.as_tensor(mu, dtype=torch.float32, device=self.device).reshape(self.n)
+        lam = torch.as_tensor(lam, dtype=torch.float32, device=self.device).reshape(self.n)
+        sl = self.slot[: self.n].long()
+        self.mu_p[sl] = mu
+        self.lam_p[sl] = lam
+
+    def get_state(self, which=("pos", "vel", "C", "F", "Jp", "active")):
+        """State in API order as device tensors: pos/vel [n,3], C/F [n,3,3], Jp [n], active [n] bool."""
+        n = self.n
+        dev = self.device
+        out = {}
+        shapes = {"pos": (n, 3), "vel": (n, 3), "C": (n, 3, 3), "F": (n, 3, 3), "Jp": (n,)}
+        ptr = {}
+        for k in ("pos", "vel", "C", "F", "Jp"):
+            if k in which:
+                out[k] = torch.empty(shapes[k], dtype=torch.float32, device=dev)
+                ptr[k] = out[k].data_ptr()
+            else:
+                ptr[k] = None
+        if "active" in which:
+            out["active"] = torch.empty(n, dtype=torch.uint8, device=dev)
+            ptr["active"] = out["active"].data_ptr()
+        else:
+            ptr["active"] = None
+        self._call(
+            "mpm_get_state", C.byref(self.prob), C.byref(self.par),
+            ptr["pos"], ptr["vel"], ptr["C"], ptr["F"], ptr["Jp"], ptr["active"], _cuda_stream_handle(),
+        )
+        if "active" in out:
+            out["active"] = out["active"].bool()
+        return out
+
+    def set_state(self, pos=None, vel=None, C_=None, F=None, Jp=None, active=None):
+        """Overwrite any subset of the state, arrays in API order (device or host)."""
+        dev = self.device
+        keep = []
+
+        def dptr(x, dtype, shape):
+            if x is None:
+                return None
+            t = torch.as_tensor(x).to(device=dev, dtype=dtype).reshape(shape).contiguous()
+            keep.append(t)
+            return t.data_ptr()
+
+        n = self.n
+        self._call(
+            "mpm_set_state", C.byref(self.prob), C.byref(self.par),
+            dptr(pos, torch.float32, (n, 3)), dptr(vel, torch.float32, (n, 3)),
+            dptr(C_, torch.float32, (n, 9)), dptr(F, torch.float32, (n, 9)),
+            dptr(Jp, torch.float32, (n,)), dptr(active, torch.uint8, (n,)), _cuda_stream_handle(),
+        )
+        return keep
+
+    def _idx_call(self, name, idx, values, vdtype, vshape, with_tables=False):
+        dev = self.device
+        idx = torch.as_tensor(idx).to(device=dev, dtype=torch.int32).reshape(-1).contiguous()
+        n = idx.numel()
+        vals = torch.as_tensor(values).to(device=dev, dtype=vdtype).reshape((n,) + vshape).contiguous()
+        args = [C.byref(self.prob)]
+        if with_tables:
+            args.append(C.byref(self.tables))
+        args += [C.byref(self.par), n, idx.data_ptr(), vals.data_ptr(), _cuda_stream_handle()]
+        self._call(name, *args)
+        return idx, vals
+
+    def set_particles_pos(self, idx, pos):
+        return self._idx_call("mpm_set_particles_pos", idx, pos, torch.float32, (3,), with_tables=True)
+
+    def set_particles_vel(self, idx, vel):
+        return self._idx_call("mpm_set_particles_vel", idx, vel, torch.float32, (3,))
+
+    def set_particles_active(self, idx, active):
+        return self._idx_call("mpm_set_particles_active", idx, active, torch.uint8, ())
+
+    def set_particles_free(self, idx, free):
+        keep = self._idx_call("mpm_set_particles_free", idx, free, torch.uint8, ())
+        if not bool(torch.as_tensor(free).bool().all()):
+            self._nonfree = True
+            self.prob.flags |= nat.PROBF_NONFREE
+            self._drop_graphs()
+        return keep
+
+    # ---------------------------------------------------------------- stepping
+    def sort(self):
+        self._call("mpm_sort_particles", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                   _cuda_stream_handle())
+
+    def p2g(self):
+        self._call("mpm_p2g", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                   _cuda_stream_handle())
+
+    def grid_op(self):
+        self._call("mpm_grid_op", C.byref(self.prob), C.byref(self.tables), self._ws, _cuda_stream_handle())
+
+    def g2p(self):
+        self._call("mpm_g2p", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                   _cuda_stream_handle())
+
+    def ensure_sorted(self):
+        if self._count % max(self.sort_interval, 1) == 0 or not getattr(self, "_sorted_once", False):
+            self.sort()
+            self._sorted_once = True
+
+    def substeps(self, n: int):
+        """Advance n substeps (p2g, grid op, g2p), re-sorting every sort_interval."""
+        K = max(self.sort_interval, 1)
+        n = int(n)
+        stream = _cuda_stream_handle()
+        while n > 0:
+            if not getattr(self, "_sorted_once", False):
+                self.sort()
+                self._sorted_once = True
+            phase = self._count % K
+            if self.use_graphs and phase == 0 and n >= K:
+                g = self._graph(K)
+                self._call("mpm_graph_launch", g, stream)
+                n -= K
+                self._count += K
+                continue
+            m = min(n, K - phase) if phase else min(n, K)
+            self._call("mpm_substeps", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                       m, K, self._count, stream)
+            n -= m
+            self._count += m
+
+    def _graph(self, K: int):
+        key = (K, self.prob.flags)
+        g = self._graphs.get(key)
+        if g is None:
+            side = torch.cuda.Stream(device=self.device)
+            side.wait_stream(torch.cuda.current_stream())
+            h = C.c_void_p()
+            with torch.cuda.stream(side):
+                self._call("mpm_graph_create", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                           K, K, 0, C.c_void_p(side.cuda_stream), C.byref(h))
+            torch.cuda.current_stream().wait_stream(side)
+            g = h
+            self._graphs[key] = g
+        return g
+
+    def _drop_graphs(self):
+        for g in self._graphs.values():
+            self.lib.mpm_graph_destroy(g)
+        self._graphs.clear()
+
+    def status(self, clear: bool = False) -> int:
+        v = C.c_uint32()
+        self._call("mpm_status", C.byref(self.prob), self._ws, int(clear), C.byref(v), _cuda_stream_handle())
+        return int(v.value)
+
+    def fallback_count(self, clear: bool = False) -> int:
+        v = C.c_uint64()
+        self._call("mpm_fallback_count", C.byref(self.prob), self._ws, int(clear), C.byref(v), _cuda_stream_handle())
+        return int(v.value)
+
+    @property
+    def substep_count(self) -> int:
+        return self._count
+
+    def __del__(self):
+        try:
+            self._drop_graphs()
+        except Exception:
+            pass
+
+
+def _grid_views(rt: MPMRuntime):
+    mm_off, gv_off = C.c_uint64(), C.c_uint64()
+    nat.check("mpm_grid_offsets", rt.lib.mpm_grid_offsets(C.byref(rt.prob), C.byref(mm_off), C.byref(gv_off)))
+    nodes = rt.n_blocks * nat.MPM_BLOCK**3
+    mm = rt.workspace[mm_off.value : mm_off.value + nodes * 16].view(torch.float32).view(nodes, 4)
+    gv = rt.workspace[gv_off.value : gv_off.value + nodes * 16].view(torch.float32).view(nodes, 4)
+    return mm, gv
+
+
+MPMRuntime.grid_views = _grid_views
+
+
+def block_major_to_dense(arr: np.ndarray, spec: InstanceSpec, blk_base: int) -> np.ndarray:
+    """[nodes, c] block-major grid slice of one instance -> dense [res_x, res_y, res_z, c]."""
+    B = nat.MPM_BLOCK
+    nb = spec.nblk
+    n_inst = int(np.prod(nb)) * B**3
+    a = arr[blk_base * B**3 : blk_base * B**3 + n_inst]
+    c = a.shape[-1]
+    a = a.reshape(nb[0], nb[1], nb[2], B, B, B, c).transpose(0, 3, 1, 4, 2, 5, 6)
+    a = a.reshape(nb[0] * B, nb[1] * B, nb[2] * B, c)
+    r = spec.grid_res
+    return a[: r[0], : r[1], : r[2]]
+
+
+def spec_from_desc(desc, materials) -> InstanceSpec:
+    return InstanceSpec(
+        grid_density=desc.grid_density,
+        lower_bound=tuple(desc.lower_bound),
+        upper_bound=tuple(desc.upper_bound),
+        particle_size=desc.particle_size,
+        dt=desc.dt,
+        gravity=tuple(desc.gravity),
+        materials=materials,
+        n_particles=desc.n_particles,
+    )
+
+
+def runtime_from_descs(descs, **kw) -> MPMRuntime:
+    """MPMRuntime advancing the given workloads.SceneDesc scenes together."""
+    from .. import workloads
+    from ..materials import MPM
+
+    specs = [spec_from_desc(d, workloads.make_materials(d, MPM)) for d in descs]
+    per_particle = any(d.E_particle is not None for d in descs)
+    rt = MPMRuntime(specs, per_particle_lame=per_particle, **kw)
+    pos = np.concatenate([d.pos for d in descs]) if descs else np.zeros((0, 3))
+    vel = np.concatenate([d.vel for d in descs]) if descs else np.zeros((0, 3))
+    mat = np.concatenate([d.mat_idx for d in descs]) if descs else np.zeros(0)
+    rt.init_particles(pos, mat, vel=vel)
+    if per_particle:
+        mus, lams = [], []
+        for d, sp in zip(descs, specs):
+            nu = sp.materials[0].nu
+            E = d.E_particle if d.E_particle is not None else np.full(d.n_particles, sp.materials[0].E)
+            mus.append(E / (2.0 * (1.0 + nu)))
+            lams.append(E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)))
+        rt.set_lame(np.concatenate(mus), np.concatenate(lams))
+    return rt

@@ -1,0 +1,141 @@
+"""gs.morphs used by MPM entities: Box, Sphere and Nowhere.
+
+Particle sampling follows the reference's simple samplers
+(genesis/utils/particle.py:174-202, ``_box_to_particles``): 'regular' places
+round(size / p_size) points per axis on [lower + p/2, upper - p/2]; 'random' draws
+n_particles_3D uniform points.  The reference's default 'pbs' sampler runs an external
+prebuilt executable that is not part of this build; 'pbs' requests are sampled as
+'regular'.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .exceptions import GenesisException
+
+
+def _quat_to_R(q):
+    w, x, y, z = q
+    return np.array(
+        [
+            [1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+            [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+            [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)],
+        ]
+    )
+
+
+def _euler_to_quat(euler_deg):
+    # scipy's extrinsic x-y-z convention (options/morphs.py docstring)
+    rx, ry, rz = np.deg2rad(np.asarray(euler_deg, dtype=np.float64)) / 2
+    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
+    return np.array(
+        [
+            cx * cy * cz + sx * sy * sz,
+            sx * cy * cz - cx * sy * sz,
+            cx * sy * cz + sx * cy * sz,
+            cx * cy * sz - sx * sy * cz,
+        ]
+    )
+
+
+def n_particles_1D(p_size=0.01, length=1.0):
+    return max(1, round(length / p_size))
+
+
+def n_particles_3D(p_size=0.01, size=(1.0, 1.0, 1.0)):
+    return n_particles_1D(p_size, size[0]) * n_particles_1D(p_size, size[1]) * n_particles_1D(p_size, size[2])
+
+
+class Morph:
+    def __init__(self, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, visualization=True, collision=True,
+                 **_ignored):
+        self.pos = tuple(float(v) for v in pos)
+        self.euler = tuple(euler)
+        self.quat = tuple(quat) if quat is not None else tuple(_euler_to_quat(euler))
+        self.visualization = visualization
+        self.collision = collision
+
+    def _local_particles(self, p_size, sampler, rng):
+        raise NotImplementedError
+
+    def sample(self, p_size, sampler, rng=None):
+        rng = rng or np.random.default_rng()
+        if sampler.startswith("pbs"):
+            sampler = "regular"
+        local = self._local_particles(p_size, sampler, rng)
+        R = _quat_to_R(self.quat)
+        return (local @ R.T + np.asarray(self.pos)).astype(np.float64)
+
+
+class Box(Morph):
+    """Axis-aligned box given by (pos, size) or (lower, upper); the latter wins."""
+
+    def __init__(self, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, lower=None, upper=None, size=None,
+                 **kw):
+        if lower is not None and upper is not None:
+            lower = np.asarray(lower, dtype=np.float64)
+            upper = np.asarray(upper, dtype=np.float64)
+            if not np.all(upper >= lower):
+                raise GenesisException("Invalid lower and upper corner.")
+            pos = tuple((lower + upper) / 2)
+            size = tuple(upper - lower)
+        elif size is None:
+            raise GenesisException("Either [`pos` and `size`] or [`lower` and `upper`] should be specified.")
+        super().__init__(pos=pos, euler=euler, quat=quat, **kw)
+        self.size = tuple(float(s) for s in size)
+        self.lower = tuple(np.asarray(self.pos) - np.asarray(self.size) / 2)
+        self.upper = tuple(np.asarray(self.pos) + np.asarray(self.size) / 2)
+
+    def _local_particles(self, p_size, sampler, rng):
+        size = np.asarray(self.size)
+        lower, upper = -size / 2, size / 2
+        if sampler == "random":
+            n = n_particles_3D(p_size, size)
+            return rng.uniform(low=lower, high=upper, size=(n, 3))
+        if sampler == "regular":
+            axes = []
+            for d in range(3):
+                n = n_particles_1D(p_size, size[d])
+                axes.append(np.linspace(lower[d] + 0.5 * p_size, upper[d] - 0.5 * p_size, n))
+            return np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+        raise GenesisException(f"Unsupported sampler method: {sampler}.")
+
+
+class Sphere(Morph):
+    def __init__(self, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, radius=0.5, **kw):
+        super().__init__(pos=pos, euler=euler, quat=quat, **kw)
+        self.radius = float(radius)
+
+    def _local_particles(self, p_size, sampler, rng):
+        r = self.radius
+        if sampler == "random":
+            n = max(1, round(4.0 / 3.0 * np.pi * r**3 / p_size**3))
+            d = rng.normal(size=(n, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            return d * (r * rng.uniform(size=(n, 1)) ** (1.0 / 3.0))
+        n = n_particles_1D(p_size, 2 * r)
+        ax = np.linspace(-r + 0.5 * p_size, r - 0.5 * p_size, n)
+        g = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), -1).reshape(-1, 3)
+        return g[np.linalg.norm(g, axis=1) <= r]
+
+
+class Nowhere(Morph):
+    """Inactive particles parked far away, activated later by an emitter (options/morphs.py: Nowhere)."""
+
+    def __init__(self, n_particles, **kw):
+        super().__init__(**kw)
+        if n_particles <= 0:
+            raise GenesisException("n_particles must be positive.")
+        self.n_particles = int(n_particles)
+
+    def _local_particles(self, p_size, sampler, rng):
+        return np.zeros((self.n_particles, 3))
+
+    def sample(self, p_size, sampler, rng=None):
+        # the reference parks them at gu.nowhere() (utils/geom.py:1703-1705)
+        return np.tile(np.array([2333333.0, 6666666.0, 5201314.0]), (self.n_particles, 1))
+
+
+__all__ = ["Morph", "Box", "Sphere", "Nowhere"]

@@ -1,0 +1,255 @@
+/*
+ * genesis_b200_mpm.h -- C ABI of the B200-native MLS-MPM substep.
+ *
+ * The library replaces the gstaichi kernels of Genesis's MPM hot path:
+ *   MPMSolver.substep_pre_coupling   genesis/engine/solvers/mpm_solver.py:471-483
+ *     (reset_grid_and_grad :540-550, compute_F_tmp :261-267, svd :269-275, p2g :290-389)
+ *   LegacyCoupler.couple -> mpm_grid_op   genesis/engine/couplers/legacy_coupler.py:941-954, 352-496
+ *   MPMSolver.substep_post_coupling  genesis/engine/solvers/mpm_solver.py:498-509
+ *     (g2p :391-449, _is_state_valid :451-457)
+ *   MPMSolver state I/O              genesis/engine/solvers/mpm_solver.py:686-741, 803-905
+ *
+ * Conventions
+ *   - Every entry point is extern "C", takes plain pointers and sizes, and returns an
+ *     int status: MPM_OK (0) or a negative MPM_E_* code.  Launch/config errors are
+ *     reported synchronously; numerical failures (NaN, stencil outside the grid) are
+ *     recorded in a device status word read with mpm_status().
+ *   - The caller (PyTorch on the Python side) owns all device memory.  The library
+ *     borrows pointers for the duration of a call, never allocates, never frees
+ *     (except mpm_graph_* which own a cudaGraphExec_t) and never synchronises except
+ *     in mpm_status().
+ *   - All work is enqueued on the stream passed in (a cudaStream_t as void*; NULL
+ *     means the legacy default stream).
+ *   - Arithmetic is float32 throughout, as with gs.init(precision="32").
+ *
+ * Data layout in device memory
+ *   particles (sorted by grid block; "slot" order):
+ *     state   float[MPM_STATE_CH][state_stride], planar: channel c of slot s is
+ *             state[c*state_stride + s].  Channels: x(0..2) v(3..5) C(6..14, row-major)
+ *             F(15..23, row-major) Jp(24).
+ *     mat     uint8[n]  material index local to the particle's instance
+ *     pflags  uint8[n]  bit0 active, bit1 free (non-free particles act as boundary)
+ *     gid     int32[n]  original (API-order) global index of the particle in slot s
+ *     slot    int32[n]  inverse of gid: slot of the particle with original index i
+ *     mu_p, lam_p  float[n] optional per-particle Lame parameters (NULL: use the table)
+ *   grid: block-major, MPM_BLOCK^3 nodes per block, blocks of instance k start at
+ *     instances[k].blk_base; workspace-resident (see mpm_workspace_bytes).
+ */
+#ifndef GENESIS_B200_MPM_H
+#define GENESIS_B200_MPM_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+#define MPM_OK 0
+#define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
+#define MPM_E_CUDA -2        /* a CUDA runtime call failed */
+#define MPM_E_CAPACITY -3    /* a size exceeds a compiled-in limit */
+#define MPM_E_NOT_SORTED -4  /* p2g/g2p called before the first mpm_sort_particles */
+
+/* device status word bits (mpm_status) */
+#define MPM_STATUS_NAN 1u          /* NaN/Inf in particle positions (mpm_solver.py:451-457) */
+#define MPM_STATUS_OUT_OF_GRID 2u  /* a stencil node fell outside the grid; contribution skipped */
+
+#define MPM_STATE_CH 25
+#define MPM_CH_X 0
+#define MPM_CH_V 3
+#define MPM_CH_C 6
+#define MPM_CH_F 15
+#define MPM_CH_JP 24
+
+#define MPM_BLOCK 4   /* grid block edge in nodes (sort bin and grid-op unit) */
+
+#define MPM_PFLAG_ACTIVE 1u
+#define MPM_PFLAG_FREE 2u
+
+/* material kinds (gs.materials.MPM.*) */
+#define MPM_MAT_ELASTIC 0        /* materials/MPM/elastic.py */
+#define MPM_MAT_ELASTOPLASTIC 1  /* materials/MPM/elasto_plastic.py */
+#define MPM_MAT_LIQUID 2         /* materials/MPM/liquid.py */
+#define MPM_MAT_SAND 3           /* materials/MPM/sand.py */
+#define MPM_MAT_SNOW 4           /* materials/MPM/snow.py */
+
+#define MPM_MATF_NEOHOOKEAN 1    /* Elastic(model="neohooken") */
+#define MPM_MATF_VON_MISES 2     /* ElastoPlastic(use_von_mises=True) */
+
+/* problem flags */
+#define MPM_PROBF_NONFREE 1      /* some particles are non-free: run the stencil-zeroing pass after p2g */
+
+/* One simulated scene (one environment).  Mirrors the derived constants of
+ * MPMSolver.__init__ (mpm_solver.py:31-78) and Simulator (simulator.py:110). */
+typedef struct mpm_instance {
+    int32_t p_begin;       /* first slot of this instance's particles */
+    int32_t p_count;       /* number of particles */
+    int32_t res[3];        /* grid_res = upper_cell - lower_cell + 1 */
+    int32_t nblk[3];       /* ceil(res / MPM_BLOCK) */
+    int32_t lower_cell[3]; /* grid_offset */
+    int32_t mat_base;      /* first entry of this instance in the material table */
+    int64_t blk_base;      /* first grid block of this instance */
+    float dx, inv_dx;
+    float dt;              /* substep dt */
+    float eps;             /* grid mass threshold gs.EPS (__init__.py:205-206) */
+    float gravity[3];
+    float bnd_lo[3], bnd_hi[3]; /* CubeBoundary with 3*dx padding (mpm_solver.py:72-78) */
+    float stress_scale;    /* -dt * particle_volume * 4 * inv_dx^2 (mpm_solver.py:344) */
+    float c_scale;         /* 4 * inv_dx (mpm_solver.py:430) */
+    float pad0;
+} mpm_instance;
+
+/* One material, resolved per instance. */
+typedef struct mpm_material {
+    int32_t kind;          /* MPM_MAT_* */
+    int32_t flags;         /* MPM_MATF_* */
+    float mu, lam;         /* Lame parameters (base.py:61-70; Liquid mu=0 unless viscous) */
+    float mass;            /* particle_volume * rho (mpm_solver.py:785) */
+    float default_Jp;      /* 1, or 0 for Sand (sand.py:45) */
+    float clamp_lo;        /* 1 - yield_lower  (elasto_plastic.py:89, snow.py:67) */
+    float clamp_hi;        /* 1 + yield_higher */
+    float vm_threshold;    /* von_mises_yield_stress / (2 mu) (elasto_plastic.py:75) */
+    float sand_c1;         /* (3 lam + 2 mu) / (2 mu)         (sand.py:67) */
+    float sand_alpha;      /* sqrt(2/3) * 2 sin(phi) / (3 - sin(phi)) (sand.py:47-49) */
+    float pad0;
+} mpm_material;
+
+/* Sizes of one problem (one or many instances advanced together). */
+typedef struct mpm_problem {
+    int32_t n_instances;
+    int32_t n_particles;      /* total over instances */
+    int64_t n_blocks;         /* total grid blocks over instances */
+    int32_t n_materials;      /* total material-table entries */
+    int32_t chunk_particles;  /* particles per p2g/g2p work item (64..1024, multiple of 32) */
+    int32_t max_chunks;       /* capacity of the chunk table (mpm_max_chunks) */
+    int32_t grid_ctas;        /* persistent CTAs for p2g/g2p/grid-op (0: library default) */
+    int32_t flags;            /* MPM_PROBF_* */
+} mpm_problem;
+
+typedef struct mpm_particles {
+    float* state;
+    int64_t state_stride;
+    uint8_t* mat;
+    uint8_t* pflags;
+    int32_t* gid;
+    int32_t* slot;
+    float* mu_p;   /* optional */
+    float* lam_p;  /* optional */
+} mpm_particles;
+
+typedef struct mpm_tables {
+    const mpm_instance* instances;  /* device, n_instances entries */
+    const mpm_material* materials;  /* device, n_materials entries */
+} mpm_tables;
+
+/* ---- sizing ------------------------------------------------------------ */
+
+/* ABI version of the loaded library (MPM_ABI_VERSION). */
+int mpm_abi_version(void);
+
+/* sizeof(mpm_instance), sizeof(mpm_material), sizeof(mpm_problem), sizeof(mpm_particles)
+ * as compiled into the library, so a binding can verify its mirror of these structs. */
+int mpm_struct_sizes(int32_t* out4);
+
+/* Upper bound on the number of p2g/g2p work items for a problem. */
+int mpm_max_chunks(int32_t n_particles, int64_t n_blocks, int32_t chunk_particles, int32_t* out);
+
+/* Bytes of device workspace a problem needs: grid momentum/mass and velocity,
+ * block flags, active-block list, sort bins, chunk table, permutation scratch and
+ * status counters.  The caller allocates it (256-byte aligned) and keeps it for the
+ * problem's lifetime. */
+int mpm_workspace_bytes(const mpm_problem* prob, uint64_t* out);
+
+/* Byte offsets, inside the workspace, of the grid arrays: momentum+mass as float4
+ * (x, y, z, mass) per node and velocity as float4 (x, y, z, 0), block-major: node
+ * (i, j, k) of instance k lives at ((blk_base + ((i/4)*nblk_y + j/4)*nblk_z + k/4) * 64
+ * + ((i%4)*4 + j%4)*4 + k%4).  The momentum/mass grid holds p2g's output between
+ * mpm_p2g and mpm_grid_op (grid op clears it); velocity holds grid op's output. */
+int mpm_grid_offsets(const mpm_problem* prob, uint64_t* mm_offset, uint64_t* vel_offset);
+
+/* Zero the workspace (grid, flags, counters).  Replaces the per-substep
+ * reset_grid_and_grad (mpm_solver.py:540-550), which the kernels fold into grid-op. */
+int mpm_workspace_init(const mpm_problem* prob, void* workspace, void* stream);
+
+/* ---- hot path ---------------------------------------------------------- */
+
+/* Counting-sort particles by grid block and rebuild the work-item table.  Required
+ * before the first p2g; afterwards optional at any interval (stale binning is still
+ * correct, only slower).  Permutes every particle array and updates gid/slot. */
+int mpm_sort_particles(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par,
+                       void* workspace, void* stream);
+
+/* compute_F_tmp + svd + material return mapping + stress + p2g scatter
+ * (mpm_solver.py:261-389).  Writes F and Jp of the next frame in place and leaves
+ * grid mass/momentum in the workspace. */
+int mpm_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+            void* stream);
+
+/* Grid update of LegacyCoupler.mpm_grid_op, MPM core (legacy_coupler.py:364-375, 495-496):
+ * momentum -> velocity, gravity, CubeBoundary.  Clears mass/momentum after reading. */
+int mpm_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* workspace, void* stream);
+
+/* g2p (mpm_solver.py:391-449) with the NaN check of _is_state_valid folded into a
+ * device status bit.  Updates x, v, C in place. */
+int mpm_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+            void* stream);
+
+/* n_substeps x (p2g, grid_op, g2p); re-sorts before substep i when
+ * sort_interval > 0 and (first_substep + i) % sort_interval == 0. */
+int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                 int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
+
+/* Read (and optionally clear) the device status word; synchronises the stream. */
+int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
+
+/* Number of particles handled by the out-of-tile path since the last clear (tuning aid). */
+int mpm_fallback_count(const mpm_problem* prob, void* workspace, int32_t clear, uint64_t* out,
+                       void* stream);
+
+/* ---- state I/O (API order) ----------------------------------------------
+ * Arrays are in original particle order, flattened over instances:
+ * pos/vel float[n][3], C/F float[n][9] (row-major), Jp float[n], active uint8[n].
+ * Any output pointer may be NULL to skip it. */
+
+/* _kernel_get_state (mpm_solver.py:723-741) */
+int mpm_get_state(const mpm_problem* prob, const mpm_particles* par, float* pos, float* vel, float* C,
+                  float* F, float* Jp, uint8_t* active, void* stream);
+
+/* _kernel_set_state (mpm_solver.py:691-712) */
+int mpm_set_state(const mpm_problem* prob, mpm_particles* par, const float* pos, const float* vel,
+                  const float* C, const float* F, const float* Jp, const uint8_t* active, void* stream);
+
+/* _kernel_set_particles_pos (mpm_solver.py:804-822): sets x of the listed particles
+ * (original indices) and resets v=0, F=I, C=0, Jp=default_Jp. */
+int mpm_set_particles_pos(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par,
+                          int32_t n, const int32_t* idx, const float* pos, void* stream);
+
+/* _kernel_set_particles_vel (mpm_solver.py:853-864) */
+int mpm_set_particles_vel(const mpm_problem* prob, mpm_particles* par, int32_t n, const int32_t* idx,
+                          const float* vel, void* stream);
+
+/* _kernel_set_particles_active (mpm_solver.py:895-905); active uint8 0/1 */
+int mpm_set_particles_active(const mpm_problem* prob, mpm_particles* par, int32_t n,
+                             const int32_t* idx, const uint8_t* active, void* stream);
+
+/* _kernel_set_particles_free (mpm_solver.py:988-992); free uint8 0/1 */
+int mpm_set_particles_free(const mpm_problem* prob, mpm_particles* par, int32_t n, const int32_t* idx,
+                           const uint8_t* free_flag, void* stream);
+
+/* ---- CUDA graphs --------------------------------------------------------
+ * Capture n_substeps of mpm_substeps into an executable graph (the pointers in
+ * prob/tab/par/workspace are baked in and must stay valid). */
+int mpm_graph_create(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par,
+                     void* workspace, int32_t n_substeps, int32_t sort_interval,
+                     int64_t first_substep, void* stream, void** graph_out);
+int mpm_graph_launch(void* graph, void* stream);
+int mpm_graph_destroy(void* graph);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GENESIS_B200_MPM_H */

@@ -1,0 +1,116 @@
+"""ctypes driver of the C/OpenMP restatement (oracle/mpm_ref.c) -- TEST INFRASTRUCTURE ONLY.
+
+Builds oracle/_build/libmpm_ref_{f32,f64}.so with gcc on first use (no CUDA needed).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from . import mpm_ref as R
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+
+
+def build(force: bool = False):
+    outs = [os.path.join(BUILD, f"libmpm_ref_{t}.so") for t in ("f32", "f64")]
+    src = os.path.join(HERE, "mpm_ref.c")
+    if force or not all(os.path.exists(o) and os.path.getmtime(o) >= os.path.getmtime(src) for o in outs):
+        subprocess.run(["make", "-C", HERE, "-B" if force else "all"], check=True, capture_output=True)
+    return outs
+
+
+def _real(dtype):
+    return C.c_float if np.dtype(dtype) == np.float32 else C.c_double
+
+
+def _structs(dtype):
+    Rt = _real(dtype)
+
+    class Params(C.Structure):
+        _fields_ = [
+            ("res", C.c_int32 * 3),
+            ("lower_cell", C.c_int32 * 3),
+            ("dx", Rt), ("inv_dx", Rt), ("dt", Rt), ("eps", Rt),
+            ("gravity", Rt * 3), ("bnd_lo", Rt * 3), ("bnd_hi", Rt * 3),
+            ("stress_scale", Rt), ("c_scale", Rt),
+        ]
+
+    class Mat(C.Structure):
+        _fields_ = [
+            ("kind", C.c_int32), ("flags", C.c_int32),
+            ("mu", Rt), ("lam", Rt), ("mass", Rt),
+            ("clamp_lo", Rt), ("clamp_hi", Rt), ("vm_threshold", Rt), ("sand_c1", Rt), ("sand_alpha", Rt),
+        ]
+
+    return Params, Mat
+
+
+_libs = {}
+
+
+def lib(dtype):
+    key = np.dtype(dtype).name
+    if key not in _libs:
+        build()
+        path = os.path.join(BUILD, "libmpm_ref_f32.so" if key == "float32" else "libmpm_ref_f64.so")
+        L = C.CDLL(path)
+        L.ref_substeps.restype = C.c_int
+        L.ref_max_threads.restype = C.c_int
+        _libs[key] = L
+    return _libs[key]
+
+
+def max_threads() -> int:
+    return int(lib(np.float64).ref_max_threads())
+
+
+def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_threads: int = 0) -> tuple[dict, int]:
+    """Run n_substeps in C on a copy of the state; returns (new_state, status)."""
+    dt = np.dtype(p.dtype)
+    L = lib(dt)
+    Params, Mat = _structs(dt)
+    P = Params()
+    for d in range(3):
+        P.res[d] = int(p.grid_res[d])
+        P.lower_cell[d] = int(p.lower_cell[d])
+        P.gravity[d] = float(p.gravity[d])
+        P.bnd_lo[d] = float(p.bnd_lo[d])
+        P.bnd_hi[d] = float(p.bnd_hi[d])
+    P.dx, P.inv_dx, P.dt, P.eps = p.dx, p.inv_dx, p.dt, p.eps
+    P.stress_scale = -p.dt * p.p_vol * 4 * p.inv_dx * p.inv_dx
+    P.c_scale = 4 * p.inv_dx
+    marr = (Mat * len(mats))()
+    for i, m in enumerate(mats):
+        flags = (1 if (m.kind == R.KIND_ELASTIC and m.neohookean) else 0) | (
+            2 if (m.kind == R.KIND_ELASTOPLASTIC and m.use_von_mises) else 0)
+        marr[i].kind = m.kind
+        marr[i].flags = flags
+        marr[i].mu, marr[i].lam = m.mu, m.lam
+        marr[i].mass = R.particle_mass(p, m)
+        marr[i].clamp_lo, marr[i].clamp_hi = 1 - m.yield_lower, 1 + m.yield_higher
+        marr[i].vm_threshold = m.von_mises_yield_stress / (2 * m.mu) if m.mu else 0.0
+        marr[i].sand_c1 = (3 * m.lam + 2 * m.mu) / (2 * m.mu) if m.mu else 0.0
+        marr[i].sand_alpha = m.alpha
+    n = st["x"].shape[0]
+    x = np.ascontiguousarray(st["x"], dtype=dt).copy()
+    v = np.ascontiguousarray(st["v"], dtype=dt).copy()
+    Cm = np.ascontiguousarray(st["C"], dtype=dt).reshape(n, 9).copy()
+    F = np.ascontiguousarray(st["F"], dtype=dt).reshape(n, 9).copy()
+    Jp = np.ascontiguousarray(st["Jp"], dtype=dt).copy()
+    mat = np.ascontiguousarray(st["mat"], dtype=np.int32)
+    act = np.ascontiguousarray(st["active"], dtype=np.uint8)
+    G = int(np.prod(p.grid_res))
+    grid = np.zeros(4 * G, dtype=dt)
+    gvel = np.zeros(3 * G, dtype=dt)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = L.ref_substeps(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
+                        int(n_substeps), ptr(grid), ptr(gvel), int(n_threads))
+    out = dict(st)
+    out.update(x=x, v=v, C=Cm.reshape(n, 3, 3), F=F.reshape(n, 3, 3), Jp=Jp)
+    return out, int(rc)

@@ -1,0 +1,426 @@
+/*
+ * C/OpenMP restatement of Genesis's MLS-MPM substep -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Used as (a) the timed CPU baseline of bench.py (the reference itself runs on
+ * gstaichi, which is not installed, so this port stands in for the reference's CPU
+ * backend; "kind": "port") and (b) a second checker beside the numpy oracle
+ * (oracle/mpm_ref.py).  Never linked into the product.
+ *
+ * Follows, in the reference:
+ *   compute_F_tmp  genesis/engine/solvers/mpm_solver.py:261-267
+ *   svd            mpm_solver.py:269-275 (ti.svd; restated as Jacobi eigen-analysis of
+ *                  A^T A + Givens QR, the McAdams et al. 2011 structure)
+ *   p2g            mpm_solver.py:290-389 (return mappings and stress of materials/MPM/)
+ *   grid op        genesis/engine/couplers/legacy_coupler.py:364-375, 495-496
+ *   g2p            mpm_solver.py:391-449
+ *   boundary       genesis/engine/boundaries/boundaries.py:23-33
+ *
+ * Parity is unpinned (no reference outputs exist for this path); see mpm_ref.py.
+ * Compiled twice: REAL=float (f32) and REAL=double (f64).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef REAL
+#define REAL double
+#endif
+
+#if defined(REAL_IS_FLOAT)
+#define R_SQRT(x) sqrtf(x)
+#define RLOG(x) logf(x)
+#define REXP(x) expf(x)
+#define RPOW(x, y) powf(x, y)
+#define RFLOOR(x) floorf(x)
+#define RABS(x) fabsf(x)
+#define RMAX(a, b) fmaxf(a, b)
+#define RMIN(a, b) fminf(a, b)
+#else
+#define R_SQRT(x) sqrt(x)
+#define RLOG(x) log(x)
+#define REXP(x) exp(x)
+#define RPOW(x, y) pow(x, y)
+#define RFLOOR(x) floor(x)
+#define RABS(x) fabs(x)
+#define RMAX(a, b) fmax(a, b)
+#define RMIN(a, b) fmin(a, b)
+#endif
+
+typedef struct {
+    int32_t res[3];
+    int32_t lower_cell[3];
+    REAL dx, inv_dx, dt, eps;
+    REAL gravity[3];
+    REAL bnd_lo[3], bnd_hi[3];
+    REAL stress_scale; /* -dt * p_vol * 4 * inv_dx^2 */
+    REAL c_scale;      /* 4 * inv_dx */
+} ref_params;
+
+typedef struct {
+    int32_t kind; /* 0 elastic 1 elastoplastic 2 liquid 3 sand 4 snow */
+    int32_t flags; /* 1 neohookean, 2 von mises */
+    REAL mu, lam, mass;
+    REAL clamp_lo, clamp_hi, vm_threshold, sand_c1, sand_alpha;
+} ref_material;
+
+/* ---------------------------------------------------------------- SVD */
+
+static void jacobi(REAL a[3][3], REAL v[3][3], int P, int Q) {
+    int R = 3 - P - Q;
+    REAL apq = a[P][Q], app = a[P][P], aqq = a[Q][Q];
+    REAL t = 0, c = 1, s = 0;
+    if (RABS(apq) > (REAL)1e-30) {
+        REAL tau = (aqq - app) / (2 * apq);
+        REAL at = RABS(tau);
+        t = at > (REAL)1e15 ? (REAL)0.5 / tau : (tau >= 0 ? 1 : -1) / (at + R_SQRT(1 + tau * tau));
+        c = 1 / R_SQRT(1 + t * t);
+        s = t * c;
+    }
+    a[P][P] = app - t * apq;
+    a[Q][Q] = aqq + t * apq;
+    a[P][Q] = a[Q][P] = 0;
+    REAL arp = a[R][P], arq = a[R][Q];
+    a[R][P] = a[P][R] = c * arp - s * arq;
+    a[R][Q] = a[Q][R] = s * arp + c * arq;
+    for (int i = 0; i < 3; ++i) {
+        REAL vip = v[i][P], viq = v[i][Q];
+        v[i][P] = c * vip - s * viq;
+        v[i][Q] = s * vip + c * viq;
+    }
+}
+
+static void givens(REAL a, REAL b, REAL* c, REAL* s) {
+    REAL r = R_SQRT(a * a + b * b);
+    if (r > (REAL)1e-30) {
+        *c = a / r;
+        *s = b / r;
+    } else {
+        *c = 1;
+        *s = 0;
+    }
+}
+
+static void swap_neg(REAL b[3][3], REAL v[3][3], REAL* n, int I, int J) {
+    for (int r = 0; r < 3; ++r) {
+        REAL tb = b[r][I];
+        b[r][I] = b[r][J];
+        b[r][J] = -tb;
+        REAL tv = v[r][I];
+        v[r][I] = v[r][J];
+        v[r][J] = -tv;
+    }
+    REAL t = n[I];
+    n[I] = n[J];
+    n[J] = t;
+}
+
+static void rot_rows(REAL b[3][3], REAL u[3][3], int I, int J, REAL c, REAL s) {
+    for (int j = 0; j < 3; ++j) {
+        REAL t0 = b[I][j], t1 = b[J][j];
+        b[I][j] = c * t0 + s * t1;
+        b[J][j] = -s * t0 + c * t1;
+    }
+    for (int i = 0; i < 3; ++i) {
+        REAL t0 = u[i][I], t1 = u[i][J];
+        u[i][I] = c * t0 + s * t1;
+        u[i][J] = -s * t0 + c * t1;
+    }
+}
+
+void ref_svd3(const REAL* A, REAL* U, REAL* S, REAL* V) {
+    REAL a[3][3], v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, b[3][3], u[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) a[i][j] = A[0 * 3 + i] * A[0 * 3 + j] + A[1 * 3 + i] * A[1 * 3 + j] + A[2 * 3 + i] * A[2 * 3 + j];
+    int sweeps = sizeof(REAL) == 4 ? 5 : 8;
+    for (int sw = 0; sw < sweeps; ++sw) {
+        jacobi(a, v, 0, 1);
+        jacobi(a, v, 0, 2);
+        jacobi(a, v, 1, 2);
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) b[i][j] = A[i * 3 + 0] * v[0][j] + A[i * 3 + 1] * v[1][j] + A[i * 3 + 2] * v[2][j];
+    REAL n[3];
+    for (int j = 0; j < 3; ++j) n[j] = b[0][j] * b[0][j] + b[1][j] * b[1][j] + b[2][j] * b[2][j];
+    if (n[0] < n[1]) swap_neg(b, v, n, 0, 1);
+    if (n[0] < n[2]) swap_neg(b, v, n, 0, 2);
+    if (n[1] < n[2]) swap_neg(b, v, n, 1, 2);
+    REAL c, s;
+    givens(b[0][0], b[1][0], &c, &s);
+    rot_rows(b, u, 0, 1, c, s);
+    givens(b[0][0], b[2][0], &c, &s);
+    rot_rows(b, u, 0, 2, c, s);
+    givens(b[1][1], b[2][1], &c, &s);
+    rot_rows(b, u, 1, 2, c, s);
+    S[0] = b[0][0];
+    S[1] = b[1][1];
+    S[2] = b[2][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            U[i * 3 + j] = u[i][j];
+            V[i * 3 + j] = v[i][j];
+        }
+}
+
+/* ---------------------------------------------------------------- materials */
+
+static void usvt(const REAL* U, const REAL* s, const REAL* V, REAL* M) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            M[i * 3 + j] = U[i * 3 + 0] * s[0] * V[j * 3 + 0] + U[i * 3 + 1] * s[1] * V[j * 3 + 1] + U[i * 3 + 2] * s[2] * V[j * 3 + 2];
+}
+
+static void corot(REAL mu, REAL lam, REAL J, const REAL* F, const REAL* U, const REAL* V, REAL* out) {
+    REAL R[9];
+    REAL one[3] = {1, 1, 1};
+    usvt(U, one, V, R);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            REAL acc = 0;
+            for (int k = 0; k < 3; ++k) acc += (F[i * 3 + k] - R[i * 3 + k]) * F[j * 3 + k];
+            out[i * 3 + j] = 2 * mu * acc + (i == j ? lam * J * (J - 1) : 0);
+        }
+}
+
+static void constitutive(const ref_material* m, REAL eps, REAL J, const REAL* Ft, const REAL* U, const REAL* S,
+                         const REAL* V, REAL Jp, REAL* Fn, REAL* Jpn, REAL* st) {
+    REAL mu = m->mu, lam = m->lam, Sn[3];
+    switch (m->kind) {
+        case 0: /* elastic.py:62-83 */
+            memcpy(Fn, Ft, 9 * sizeof(REAL));
+            *Jpn = Jp;
+            if (m->flags & 1) {
+                REAL d = lam * RLOG(J) - mu;
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        REAL acc = Ft[i * 3 + 0] * Ft[j * 3 + 0] + Ft[i * 3 + 1] * Ft[j * 3 + 1] + Ft[i * 3 + 2] * Ft[j * 3 + 2];
+                        st[i * 3 + j] = mu * acc + (i == j ? d : 0);
+                    }
+            } else {
+                corot(mu, lam, J, Fn, U, V, st);
+            }
+            break;
+        case 2: { /* liquid.py:50-64 */
+            REAL c = RPOW(J, (REAL)(1.0 / 3.0));
+            for (int k = 0; k < 9; ++k) Fn[k] = (k % 4 == 0) ? c : 0;
+            *Jpn = Jp;
+            corot(mu, lam, J, Ft, U, V, st);
+            break;
+        }
+        case 1: /* elasto_plastic.py:66-93 */
+            if (m->flags & 2) {
+                REAL e[3], eh[3];
+                for (int d = 0; d < 3; ++d) e[d] = RLOG(RMAX(S[d], (REAL)0.05));
+                REAL mean = (e[0] + e[1] + e[2]) / 3;
+                for (int d = 0; d < 3; ++d) eh[d] = e[d] - mean;
+                REAL ehn = R_SQRT(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
+                REAL dg = ehn - m->vm_threshold;
+                if (dg > 0) {
+                    for (int d = 0; d < 3; ++d) Sn[d] = REXP(e[d] - (dg / ehn) * eh[d]);
+                    usvt(U, Sn, V, Fn);
+                } else {
+                    memcpy(Fn, Ft, 9 * sizeof(REAL));
+                }
+            } else {
+                for (int d = 0; d < 3; ++d) Sn[d] = RMIN(RMAX(S[d], m->clamp_lo), m->clamp_hi);
+                usvt(U, Sn, V, Fn);
+            }
+            *Jpn = Jp;
+            corot(mu, lam, J, Fn, U, V, st);
+            break;
+        case 4: { /* snow.py:62-81 */
+            REAL jp = Jp;
+            for (int d = 0; d < 3; ++d) {
+                Sn[d] = RMIN(RMAX(S[d], m->clamp_lo), m->clamp_hi);
+                jp = jp * (S[d] / Sn[d]);
+            }
+            *Jpn = jp;
+            usvt(U, Sn, V, Fn);
+            REAL h = REXP(10 * (1 - Jp));
+            corot(mu * h, lam * h, J, Fn, U, V, st);
+            break;
+        }
+        default: { /* sand.py:51-89 */
+            REAL e[3], eh[3];
+            for (int d = 0; d < 3; ++d) e[d] = RLOG(RMAX(RABS(S[d]), (REAL)1e-4));
+            REAL tr = e[0] + e[1] + e[2] + Jp;
+            for (int d = 0; d < 3; ++d) eh[d] = e[d] - tr / 3;
+            REAL ehn = R_SQRT(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
+            if (tr >= 0) {
+                *Jpn = tr;
+                Sn[0] = Sn[1] = Sn[2] = 1;
+            } else {
+                *Jpn = 0;
+                REAL dg = ehn + m->sand_c1 * tr * m->sand_alpha;
+                for (int d = 0; d < 3; ++d) Sn[d] = REXP(e[d] - RMAX(0, dg) / ehn * eh[d]);
+            }
+            usvt(U, Sn, V, Fn);
+            REAL l[3], center[3], M[9];
+            for (int d = 0; d < 3; ++d) l[d] = RLOG(Sn[d]);
+            REAL ls = l[0] + l[1] + l[2];
+            for (int d = 0; d < 3; ++d) center[d] = 2 * mu * l[d] * (1 / Sn[d]) + lam * ls * (1 / Sn[d]);
+            usvt(U, center, V, M);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    st[i * 3 + j] = M[i * 3 + 0] * Fn[j * 3 + 0] + M[i * 3 + 1] * Fn[j * 3 + 1] + M[i * 3 + 2] * Fn[j * 3 + 2];
+            break;
+        }
+    }
+}
+
+static REAL bc_vel(REAL pos, REAL vel, REAL lo, REAL hi) {
+    if (pos >= hi && vel >= 0) return vel * (REAL)-0.0;
+    if (pos <= lo && vel <= 0) return vel * (REAL)-0.0;
+    return vel;
+}
+
+static inline int64_t gidx(const ref_params* p, int i, int j, int k) {
+    return ((int64_t)i * p->res[1] + j) * p->res[2] + k;
+}
+
+/*
+ * n_substeps full substeps in place.  State arrays (API order): x,v [n*3], C,F [n*9], Jp [n];
+ * mat [n] material index, active [n] (0/1).  grid: caller scratch of 4*res^3 (momentum.xyz, mass)
+ * and vel 3*res^3.  Returns 0, or 1 if a stencil left the grid, 2 if a position became NaN.
+ */
+int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F, REAL* Jp,
+                 const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel, int n_threads) {
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+    const int64_t G = (int64_t)p->res[0] * p->res[1] * p->res[2];
+    int status = 0;
+    for (int step = 0; step < n_substeps; ++step) {
+#pragma omp parallel for schedule(static)
+        for (int64_t g = 0; g < G; ++g) {
+            grid[4 * g + 0] = grid[4 * g + 1] = grid[4 * g + 2] = grid[4 * g + 3] = 0;
+        }
+        /* p2g (mpm_solver.py:290-389) */
+#pragma omp parallel for schedule(static) reduction(| : status)
+        for (int i = 0; i < n; ++i) {
+            if (!active[i]) continue;
+            const REAL* Ci = C + 9 * i;
+            REAL* Fi = F + 9 * i;
+            REAL Ft[9], U[9], S[3], V[9], Fn[9], st[9], Jpn;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    REAL acc = Fi[a * 3 + b];
+                    for (int k = 0; k < 3; ++k) acc += p->dt * Ci[a * 3 + k] * Fi[k * 3 + b];
+                    Ft[a * 3 + b] = acc;
+                }
+            ref_svd3(Ft, U, S, V);
+            REAL J = S[0] * (S[1] * S[2]);
+            const ref_material* m = &mats[mat[i]];
+            constitutive(m, p->eps, J, Ft, U, S, V, Jp[i], Fn, &Jpn, st);
+            memcpy(Fi, Fn, 9 * sizeof(REAL));
+            Jp[i] = Jpn;
+            REAL A[9];
+            for (int k = 0; k < 9; ++k) A[k] = p->stress_scale * st[k] + m->mass * Ci[k];
+            int base[3];
+            REAL fx[3], w[3][3];
+            for (int d = 0; d < 3; ++d) {
+                REAL xi = x[3 * i + d] * p->inv_dx;
+                REAL bf = RFLOOR(xi - (REAL)0.5);
+                base[d] = (int)bf - p->lower_cell[d];
+                fx[d] = xi - bf;
+                w[0][d] = (REAL)0.5 * ((REAL)1.5 - fx[d]) * ((REAL)1.5 - fx[d]);
+                w[1][d] = (REAL)0.75 - (fx[d] - 1) * (fx[d] - 1);
+                w[2][d] = (REAL)0.5 * (fx[d] - (REAL)0.5) * (fx[d] - (REAL)0.5);
+            }
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c) {
+                        int gi = base[0] + a, gj = base[1] + b, gk = base[2] + c;
+                        if (gi < 0 || gj < 0 || gk < 0 || gi >= p->res[0] || gj >= p->res[1] || gk >= p->res[2]) {
+                            status |= 1;
+                            continue;
+                        }
+                        REAL wt = w[a][0] * w[b][1] * w[c][2];
+                        REAL dp[3] = {(a - fx[0]) * p->dx, (b - fx[1]) * p->dx, (c - fx[2]) * p->dx};
+                        REAL* cell = grid + 4 * gidx(p, gi, gj, gk);
+                        for (int d = 0; d < 3; ++d) {
+                            REAL q = wt * (m->mass * v[3 * i + d] + A[d * 3 + 0] * dp[0] + A[d * 3 + 1] * dp[1] + A[d * 3 + 2] * dp[2]);
+#pragma omp atomic
+                            cell[d] += q;
+                        }
+#pragma omp atomic
+                        cell[3] += wt * m->mass;
+                    }
+        }
+        /* grid op (legacy_coupler.py:364-375, 495-496) */
+#pragma omp parallel for schedule(static)
+        for (int64_t g = 0; g < G; ++g) {
+            REAL* cell = grid + 4 * g;
+            REAL* out = gvel + 3 * g;
+            out[0] = out[1] = out[2] = 0;
+            if (cell[3] > p->eps) {
+                int k = (int)(g % p->res[2]);
+                int j = (int)((g / p->res[2]) % p->res[1]);
+                int ii = (int)(g / ((int64_t)p->res[1] * p->res[2]));
+                int I[3] = {ii, j, k};
+                REAL inv = 1 / cell[3];
+                for (int d = 0; d < 3; ++d) {
+                    REAL vel = inv * cell[d] + p->dt * p->gravity[d];
+                    REAL pos = (REAL)(I[d] + p->lower_cell[d]) * p->dx;
+                    out[d] = bc_vel(pos, vel, p->bnd_lo[d], p->bnd_hi[d]);
+                }
+            }
+        }
+        /* g2p (mpm_solver.py:391-449) */
+#pragma omp parallel for schedule(static) reduction(| : status)
+        for (int i = 0; i < n; ++i) {
+            if (!active[i]) continue;
+            int base[3];
+            REAL fx[3], w[3][3];
+            for (int d = 0; d < 3; ++d) {
+                REAL xi = x[3 * i + d] * p->inv_dx;
+                REAL bf = RFLOOR(xi - (REAL)0.5);
+                base[d] = (int)bf - p->lower_cell[d];
+                fx[d] = xi - bf;
+                w[0][d] = (REAL)0.5 * ((REAL)1.5 - fx[d]) * ((REAL)1.5 - fx[d]);
+                w[1][d] = (REAL)0.75 - (fx[d] - 1) * (fx[d] - 1);
+                w[2][d] = (REAL)0.5 * (fx[d] - (REAL)0.5) * (fx[d] - (REAL)0.5);
+            }
+            REAL nv[3] = {0, 0, 0}, nC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c) {
+                        int gi = base[0] + a, gj = base[1] + b, gk = base[2] + c;
+                        if (gi < 0 || gj < 0 || gk < 0 || gi >= p->res[0] || gj >= p->res[1] || gk >= p->res[2]) {
+                            status |= 1;
+                            continue;
+                        }
+                        REAL wt = w[a][0] * w[b][1] * w[c][2];
+                        const REAL* gv = gvel + 3 * gidx(p, gi, gj, gk);
+                        REAL dp[3] = {a - fx[0], b - fx[1], c - fx[2]};
+                        for (int d = 0; d < 3; ++d) {
+                            nv[d] += wt * gv[d];
+                            for (int e = 0; e < 3; ++e) nC[d * 3 + e] += p->c_scale * wt * gv[d] * dp[e];
+                        }
+                    }
+            for (int d = 0; d < 3; ++d) {
+                REAL nx = x[3 * i + d] + p->dt * nv[d];
+                REAL vv = bc_vel(nx, nv[d], p->bnd_lo[d], p->bnd_hi[d]);
+                nx = RMAX(RMIN(nx, p->bnd_hi[d]), p->bnd_lo[d]);
+                if (nx != nx) status |= 2;
+                x[3 * i + d] = nx;
+                v[3 * i + d] = vv;
+            }
+            memcpy(C + 9 * i, nC, 9 * sizeof(REAL));
+        }
+    }
+    return status;
+}
+
+int ref_sizeof_params(void) { return (int)sizeof(ref_params); }
+int ref_sizeof_material(void) { return (int)sizeof(ref_material); }
+int ref_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

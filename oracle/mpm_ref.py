@@ -1,0 +1,472 @@
+"""CPU oracle for the MLS-MPM substep.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import this module,
+and only as the checker.  The product path (``genesis_b200``) never calls it.
+
+This is a numpy restatement of Genesis's MPM substep, parameterised by dtype
+(float32 or float64), following the reference line by line:
+
+* solver constants          genesis/engine/solvers/mpm_solver.py:31-78
+* compute_F_tmp / svd       genesis/engine/solvers/mpm_solver.py:261-275
+* p2g                       genesis/engine/solvers/mpm_solver.py:290-389
+* grid op (MPM core only)   genesis/engine/couplers/legacy_coupler.py:352-375, 495-496
+* g2p                       genesis/engine/solvers/mpm_solver.py:391-449
+* NaN check                 genesis/engine/solvers/mpm_solver.py:451-457, 505-509
+* CubeBoundary              genesis/engine/boundaries/boundaries.py:12-33
+* materials                 genesis/engine/materials/MPM/{base,elastic,elasto_plastic,liquid,sand,snow}.py
+* EPS                       genesis/__init__.py:205-206
+
+Parity status: UNPINNED.  The reference runs on gstaichi (pyproject.toml:13,
+gstaichi==4.5.0), which is not installed here, and the reference test-suite holds no
+golden vectors for MPM (its MPM tests only check qualitative invariants).  The
+oracle is therefore checked against (a) those qualitative invariants, (b) an
+independent C restatement (``oracle/mpm_ref.c``), and (c) exact algebraic
+identities (SVD reconstruction, partition of unity, mass/momentum conservation).
+
+SVD convention.  ``ti.svd`` (gstaichi) follows McAdams et al. 2011, "Computing the
+Singular Value Decomposition of 3x3 matrices with minimal branching and elementary
+floating point operations": U and V are proper rotations, singular values are
+ordered by decreasing magnitude and only the last one may be negative.  The oracle
+obtains the same factorisation from LAPACK's SVD by moving any reflection into the
+sign of the last singular value.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+KIND_ELASTIC = 0
+KIND_ELASTOPLASTIC = 1
+KIND_LIQUID = 2
+KIND_SAND = 3
+KIND_SNOW = 4
+KIND_NAMES = ("elastic", "elastoplastic", "liquid", "sand", "snow")
+
+
+def lame(E: float, nu: float) -> tuple[float, float]:
+    """Lame parameters (mu, lam) from E and nu (materials/MPM/base.py:61-70)."""
+    mu = E / (2.0 * (1.0 + nu))
+    lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    return mu, lam
+
+
+@dataclass
+class Material:
+    """Plain-data restatement of one gs.materials.MPM.* object."""
+
+    kind: int
+    E: float = 1e6
+    nu: float = 0.2
+    rho: float = 1000.0
+    mu: float = 0.0
+    lam: float = 0.0
+    default_Jp: float = 1.0
+    neohookean: bool = False  # Elastic(model="neohooken") (elastic.py:53-58)
+    use_von_mises: bool = True  # ElastoPlastic (elasto_plastic.py:53)
+    von_mises_yield_stress: float = 1e4
+    yield_lower: float = 2.5e-2
+    yield_higher: float = 4.5e-3
+    friction_angle: float = 45.0  # Sand, degrees (sand.py:41-49)
+
+    @property
+    def alpha(self) -> float:
+        # sand.py:47-49
+        sin_phi = math.sin(math.radians(self.friction_angle))
+        return math.sqrt(2.0 / 3.0) * 2.0 * sin_phi / (3.0 - sin_phi)
+
+
+def make_material(kind: str, **kw) -> Material:
+    """Construct a Material with the reference class defaults for ``kind``.
+
+    Defaults: Elastic E=3e5 (elastic.py:40), others E=1e6; nu=0.2 and rho=1000 for all
+    (base.py:36-38).  Liquid sets mu=0 unless viscous (liquid.py:47-48).  Sand uses
+    default_Jp=0 (sand.py:45).  Snow is the non-von-Mises ElastoPlastic (snow.py:50-60).
+    """
+    kind = kind.lower()
+    viscous = kw.pop("viscous", False)
+    model = kw.pop("model", "corotation")
+    E = kw.pop("E", 3e5 if kind == "elastic" else 1e6)
+    nu = kw.pop("nu", 0.2)
+    mu_kw = kw.pop("mu", None)
+    lam_kw = kw.pop("lam", None)
+    mu, lam = lame(E, nu)
+    if mu_kw is not None:
+        mu = mu_kw
+    if lam_kw is not None:
+        lam = lam_kw
+    m = Material(kind=KIND_NAMES.index(kind), E=E, nu=nu, mu=mu, lam=lam, **kw)
+    if kind == "elastic":
+        m.neohookean = model == "neohooken"
+    elif kind == "liquid":
+        if not viscous:
+            m.mu = 0.0
+    elif kind == "sand":
+        m.default_Jp = 0.0
+    elif kind == "snow":
+        m.use_von_mises = False
+    return m
+
+
+@dataclass
+class Params:
+    """Solver constants (mpm_solver.py:31-78, simulator.py:110)."""
+
+    grid_density: float = 64.0
+    lower_bound: tuple = (0.0, 0.0, 0.0)
+    upper_bound: tuple = (1.0, 1.0, 1.0)
+    particle_size: float | None = None
+    dt: float = 1e-4  # substep dt
+    gravity: tuple = (0.0, 0.0, -9.8)
+    dtype: type = np.float64
+    # derived
+    dx: float = field(init=False)
+    inv_dx: float = field(init=False)
+    lower_cell: np.ndarray = field(init=False)
+    upper_cell: np.ndarray = field(init=False)
+    grid_res: np.ndarray = field(init=False)
+    p_vol: float = field(init=False)
+    bnd_lo: np.ndarray = field(init=False)
+    bnd_hi: np.ndarray = field(init=False)
+    eps: float = field(init=False)
+
+    def __post_init__(self):
+        if self.particle_size is None:
+            # options/solvers.py:490-491
+            self.particle_size = 0.01 * 64.0 / self.grid_density
+        self.dx = float(1.0 / self.grid_density)
+        self.inv_dx = float(self.grid_density)
+        lo = np.asarray(self.lower_bound, dtype=np.float64)
+        hi = np.asarray(self.upper_bound, dtype=np.float64)
+        self.lower_cell = np.round(self.grid_density * lo).astype(np.int64)
+        self.upper_cell = np.round(self.grid_density * hi).astype(np.int64)
+        self.grid_res = self.upper_cell - self.lower_cell + 1
+        # particle volume with the 1e3 scale (mpm_solver.py:43-48)
+        self.p_vol = float(self.particle_size**3) * 1e3
+        pad = 3 * self.dx
+        self.bnd_lo = lo + pad
+        self.bnd_hi = hi - pad
+        # EPS = max(1e-15, finfo.eps) (__init__.py:205-206)
+        self.eps = max(1e-15, float(np.finfo(self.dtype).eps))
+
+
+def particle_mass(p: Params, mat: Material) -> float:
+    # _kernel_add_particles: mass = particle_volume * rho (mpm_solver.py:785), in the solver dtype
+    dt = p.dtype
+    return float(dt(dt(p.p_vol) * dt(mat.rho)))
+
+
+def svd3(F: np.ndarray):
+    """Batched SVD with the rotation convention of ti.svd (see module docstring)."""
+    U, s, Vh = np.linalg.svd(F)
+    V = np.swapaxes(Vh, -1, -2).copy()
+    U = U.copy()
+    s = s.copy()
+    fu = np.linalg.det(U) < 0
+    U[fu, :, 2] *= -1
+    s[fu, 2] *= -1
+    fv = np.linalg.det(V) < 0
+    V[fv, :, 2] *= -1
+    s[fv, 2] *= -1
+    return U, s, V
+
+
+def _diag(s):
+    n = s.shape[0]
+    D = np.zeros((n, 3, 3), dtype=s.dtype)
+    D[:, 0, 0] = s[:, 0]
+    D[:, 1, 1] = s[:, 1]
+    D[:, 2, 2] = s[:, 2]
+    return D
+
+
+def _mT(A):
+    return np.swapaxes(A, -1, -2)
+
+
+def update_F_S_Jp(mat: Material, eps: float, J, F_tmp, U, S, V, Jp):
+    """Return mapping per material; S is the vector of singular values."""
+    dt = F_tmp.dtype.type
+    k = mat.kind
+    if k == KIND_ELASTIC:
+        # elastic.py:62-67
+        return F_tmp.copy(), S.copy(), Jp.copy()
+    if k == KIND_LIQUID:
+        # liquid.py:50-55
+        with np.errstate(invalid="ignore"):
+            c = np.power(J, dt(1.0 / 3.0))
+        F_new = np.zeros_like(F_tmp)
+        for d in range(3):
+            F_new[:, d, d] = c
+        return F_new, S.copy(), Jp.copy()
+    if k == KIND_ELASTOPLASTIC and mat.use_von_mises:
+        # elasto_plastic.py:70-84
+        Sc = np.maximum(S, dt(0.05))
+        e = np.log(Sc)
+        eh = e - (e.sum(axis=1, keepdims=True) / dt(3))
+        ehn = np.sqrt((eh * eh).sum(axis=1) + dt(eps))
+        dg = ehn - dt(mat.von_mises_yield_stress / (2 * mat.mu))
+        yields = dg > 0
+        e2 = e - (dg / ehn)[:, None] * eh
+        S_y = np.exp(e2)
+        S_new = np.where(yields[:, None], S_y, Sc)
+        F_y = U @ _diag(S_y) @ _mT(V)
+        F_new = np.where(yields[:, None, None], F_y, F_tmp)
+        return F_new, S_new, Jp.copy()
+    if k in (KIND_ELASTOPLASTIC, KIND_SNOW):
+        # elasto_plastic.py:86-90 / snow.py:62-70
+        S_new = np.minimum(np.maximum(S, dt(1 - mat.yield_lower)), dt(1 + mat.yield_higher))
+        F_new = U @ _diag(S_new) @ _mT(V)
+        Jp_new = Jp.copy()
+        if k == KIND_SNOW:
+            for d in range(3):
+                Jp_new = Jp_new * (S[:, d] / S_new[:, d])
+        return F_new, S_new, Jp_new
+    if k == KIND_SAND:
+        # sand.py:51-77
+        e = np.log(np.maximum(np.abs(S), dt(1e-4)))
+        tr = e.sum(axis=1) + Jp
+        eh = e - (tr / dt(3))[:, None]
+        ehn = np.sqrt((eh * eh).sum(axis=1) + dt(eps))
+        expand = tr >= 0
+        c1 = dt((3 * mat.lam + 2 * mat.mu) / (2 * mat.mu))
+        dg = ehn + c1 * tr * dt(mat.alpha)
+        S_c = np.exp(e - (np.maximum(dt(0), dg) / ehn)[:, None] * eh)
+        S_new = np.where(expand[:, None], dt(1), S_c)
+        Jp_new = np.where(expand, tr, dt(0))
+        F_new = U @ _diag(S_new) @ _mT(V)
+        return F_new, S_new, Jp_new
+    raise ValueError(f"unknown material kind {k}")
+
+
+def update_stress(mat: Material, U, S_new, V, F_tmp, F_new, J, Jp_old):
+    dt = F_tmp.dtype.type
+    n = F_tmp.shape[0]
+    eye = np.broadcast_to(np.eye(3, dtype=F_tmp.dtype), (n, 3, 3))
+    k = mat.kind
+    mu, lam = dt(mat.mu), dt(mat.lam)
+    if k == KIND_ELASTIC and mat.neohookean:
+        # elastic.py:77-83
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lj = np.log(J)
+        return mu * (F_tmp @ _mT(F_tmp)) + eye * (lam * lj - mu)[:, None, None]
+    if k == KIND_LIQUID:
+        # liquid.py:57-64 (uses F_tmp)
+        R = U @ _mT(V)
+        return dt(2) * mu * (F_tmp - R) @ _mT(F_tmp) + eye * (lam * J * (J - dt(1)))[:, None, None]
+    if k == KIND_SAND:
+        # sand.py:79-89 (S is S_new, mpm_solver.py:335)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lS = np.log(S_new)
+        lsum = lS.sum(axis=1)
+        center = dt(2.0) * mu * lS * (dt(1) / S_new) + lam * lsum[:, None] * (dt(1) / S_new)
+        return U @ _diag(center) @ _mT(V) @ _mT(F_new)
+    if k == KIND_SNOW:
+        # snow.py:72-81 (hardening uses the previous Jp, mpm_solver.py:329,340)
+        h = np.exp(dt(10) * (dt(1.0) - Jp_old))
+        muh, lamh = mu * h, lam * h
+        R = U @ _mT(V)
+        return (dt(2) * muh)[:, None, None] * (F_new - R) @ _mT(F_new) + eye * (lamh * J * (J - dt(1)))[:, None, None]
+    # Elastic corotated (elastic.py:69-75) and ElastoPlastic (base.py:83-90)
+    R = U @ _mT(V)
+    return dt(2) * mu * (F_new - R) @ _mT(F_new) + eye * (lam * J * (J - dt(1)))[:, None, None]
+
+
+def _weights(fx):
+    dt = fx.dtype.type
+    return (
+        dt(0.5) * (dt(1.5) - fx) ** 2,
+        dt(0.75) - (fx - dt(1)) ** 2,
+        dt(0.5) * (fx - dt(0.5)) ** 2,
+    )
+
+
+def boundary(p: Params, pos, vel):
+    """CubeBoundary.impose_pos_vel with restitution 0 (boundaries.py:23-33)."""
+    dt = pos.dtype.type
+    lo = p.bnd_lo.astype(pos.dtype)
+    hi = p.bnd_hi.astype(pos.dtype)
+    vel = vel.copy()
+    for i in range(3):
+        up = (pos[:, i] >= hi[i]) & (vel[:, i] >= 0)
+        dn = (~up) & (pos[:, i] <= lo[i]) & (vel[:, i] <= 0)
+        vel[:, i] = np.where(up | dn, vel[:, i] * dt(-0.0), vel[:, i])
+    pos = np.maximum(np.minimum(pos, hi), lo)
+    return pos, vel
+
+
+def p2g(p: Params, mats: list[Material], st: dict):
+    """compute_F_tmp + svd + p2g (mpm_solver.py:261-389).
+
+    Returns (grid_mass[res], grid_mom[res,3], F_new, Jp_new).
+    """
+    dt = p.dtype
+    x, v, C, F, Jp = st["x"], st["v"], st["C"], st["F"], st["Jp"]
+    mat_idx, active = st["mat"], st["active"]
+    free = st.get("free")
+    N = x.shape[0]
+    res = tuple(int(r) for r in p.grid_res)
+    F_new = F.copy()
+    Jp_new = Jp.copy()
+    gm = np.zeros(res, dtype=np.float64)
+    gp = np.zeros(res + (3,), dtype=np.float64)
+    act = np.nonzero(active)[0]
+    if act.size == 0:
+        return gm.astype(dt), gp.astype(dt), F_new, Jp_new
+    eye = np.eye(3, dtype=dt)
+    sdt = dt(p.dt)
+    # compute_F_tmp (mpm_solver.py:261-267)
+    F_tmp = (eye + sdt * C[act]) @ F[act]
+    # svd (mpm_solver.py:269-275)
+    U, S, V = svd3(F_tmp)
+    U, S, V = U.astype(dt), S.astype(dt), V.astype(dt)
+    # J = S.determinant() with S diagonal (mpm_solver.py:305)
+    J = S[:, 0] * (S[:, 1] * S[:, 2])
+    stress = np.zeros((act.size, 3, 3), dtype=dt)
+    Fn = np.empty_like(F_tmp)
+    Jn = np.empty(act.size, dtype=dt)
+    mass = np.empty(act.size, dtype=dt)
+    ma = mat_idx[act]
+    for mi, mat in enumerate(mats):
+        sel = np.nonzero(ma == mi)[0]
+        if sel.size == 0:
+            continue
+        f_n, s_n, j_n = update_F_S_Jp(mat, p.eps, J[sel], F_tmp[sel], U[sel], S[sel], V[sel], Jp[act][sel])
+        Fn[sel] = f_n
+        Jn[sel] = j_n
+        stress[sel] = update_stress(mat, U[sel], s_n, V[sel], F_tmp[sel], f_n, J[sel], Jp[act][sel])
+        mass[sel] = particle_mass(p, mat)
+    F_new[act] = Fn
+    Jp_new[act] = Jn
+    # mpm_solver.py:344-345
+    scale = dt(-p.dt * p.p_vol * 4 * p.inv_dx * p.inv_dx)
+    affine = scale * stress + mass[:, None, None] * C[act]
+    xa = x[act]
+    xi = xa * dt(p.inv_dx)
+    base = np.floor(xi - dt(0.5)).astype(np.int64)
+    fx = xi - base.astype(dt)
+    w = _weights(fx)
+    mv = mass[:, None] * v[act]
+    node0 = base - p.lower_cell[None, :]
+    flat_size = int(np.prod(res))
+    gm_f = gm.reshape(-1)
+    gp_f = gp.reshape(-1, 3)
+    zero_nodes = []
+    nonfree = None
+    if free is not None:
+        nonfree = ~free[act]
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                off = np.array([i, j, k], dtype=dt)
+                dpos = (off[None, :] - fx) * dt(p.dx)
+                weight = w[i][:, 0] * w[j][:, 1] * w[k][:, 2]
+                contrib = weight[:, None] * (mv + np.einsum("nij,nj->ni", affine, dpos))
+                node = node0 + np.array([i, j, k])
+                if np.any(node < 0) or np.any(node >= np.asarray(res)):
+                    raise IndexError("particle stencil outside the grid")
+                lin = np.ravel_multi_index(node.T, res)
+                gm_f += np.bincount(lin, weights=(weight * mass).astype(np.float64), minlength=flat_size)
+                for d in range(3):
+                    gp_f[:, d] += np.bincount(lin, weights=contrib[:, d].astype(np.float64), minlength=flat_size)
+                if nonfree is not None and nonfree.any():
+                    zero_nodes.append(lin[nonfree])
+    for zn in zero_nodes:
+        gp_f[zn] = 0.0  # non-free particles zero vel_in (mpm_solver.py:388-389)
+    return gm.astype(dt), gp.astype(dt), F_new, Jp_new
+
+
+def grid_op(p: Params, gm, gp):
+    """MPM core of LegacyCoupler.mpm_grid_op (legacy_coupler.py:364-375, 495-496)."""
+    dt = p.dtype
+    res = gm.shape
+    vel = np.zeros(res + (3,), dtype=dt)
+    act = gm > dt(p.eps)
+    m = gm[act]
+    v = (dt(1) / m)[:, None] * gp[act]
+    v = v + dt(p.dt) * np.asarray(p.gravity, dtype=dt)[None, :]
+    idx = np.argwhere(act)
+    pos = (idx + p.lower_cell[None, :]).astype(dt) * dt(p.dx)
+    _, v = boundary(p, pos, v)
+    vel[act] = v
+    return vel
+
+
+def g2p(p: Params, st: dict, vel):
+    """g2p (mpm_solver.py:391-449); returns new x, v, C for active particles."""
+    dt = p.dtype
+    x, v, C = st["x"], st["v"], st["C"]
+    active = st["active"]
+    res = vel.shape[:3]
+    xn, vn, Cn = x.copy(), v.copy(), C.copy()
+    act = np.nonzero(active)[0]
+    if act.size == 0:
+        return xn, vn, Cn
+    xa = x[act]
+    xi = xa * dt(p.inv_dx)
+    base = np.floor(xi - dt(0.5)).astype(np.int64)
+    fx = xi - base.astype(dt)
+    w = _weights(fx)
+    node0 = base - p.lower_cell[None, :]
+    new_v = np.zeros((act.size, 3), dtype=dt)
+    new_C = np.zeros((act.size, 3, 3), dtype=dt)
+    vflat = vel.reshape(-1, 3)
+    c4 = dt(4 * p.inv_dx)
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                off = np.array([i, j, k], dtype=dt)
+                dpos = off[None, :] - fx
+                weight = w[i][:, 0] * w[j][:, 1] * w[k][:, 2]
+                node = node0 + np.array([i, j, k])
+                lin = np.ravel_multi_index(node.T, res)
+                gv = vflat[lin]
+                new_v += weight[:, None] * gv
+                new_C += (c4 * weight)[:, None, None] * (gv[:, :, None] * dpos[:, None, :])
+    new_x = xa + dt(p.dt) * new_v
+    new_x, new_v = boundary(p, new_x, new_v)
+    xn[act] = new_x
+    vn[act] = new_v
+    Cn[act] = new_C
+    return xn, vn, Cn
+
+
+def substep(p: Params, mats: list[Material], st: dict, return_grid: bool = False):
+    """One full substep: p2g, grid op, g2p.  ``st`` is not modified."""
+    gm, gp, F_new, Jp_new = p2g(p, mats, st)
+    vel = grid_op(p, gm, gp)
+    xn, vn, Cn = g2p(p, st, vel)
+    out = dict(st)
+    out.update(x=xn, v=vn, C=Cn, F=F_new, Jp=Jp_new)
+    if np.isnan(xn).any():
+        raise FloatingPointError("NaN detected in MPM states (mpm_solver.py:505-509)")
+    if return_grid:
+        return out, (gm, gp, vel)
+    return out
+
+
+def make_state(x, mats: list[Material], mat_idx, dtype, v=None, active=None):
+    """Fresh particle state as _kernel_add_particles / set_particles_pos leave it
+    (mpm_solver.py:768-801, 803-822): v=0 unless given, F=I, C=0, Jp=default_Jp."""
+    x = np.asarray(x, dtype=dtype)
+    N = x.shape[0]
+    mat_idx = np.asarray(mat_idx, dtype=np.int64)
+    st = dict(
+        x=x.copy(),
+        v=np.zeros((N, 3), dtype=dtype) if v is None else np.asarray(v, dtype=dtype).copy(),
+        C=np.zeros((N, 3, 3), dtype=dtype),
+        F=np.broadcast_to(np.eye(3, dtype=dtype), (N, 3, 3)).copy(),
+        Jp=np.array([mats[m].default_Jp for m in mat_idx], dtype=dtype) if N else np.zeros(0, dtype),
+        mat=mat_idx,
+        active=np.ones(N, dtype=bool) if active is None else np.asarray(active, dtype=bool).copy(),
+    )
+    return st
+
+
+def run(p: Params, mats, st, n_substeps: int):
+    for _ in range(n_substeps):
+        st = substep(p, mats, st)
+    return st

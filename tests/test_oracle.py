@@ -1,0 +1,170 @@
+"""CPU checks of the oracle itself (no GPU): algebraic identities, the reference's
+qualitative MPM invariants, and agreement of the numpy and C restatements."""
+
+import numpy as np
+import pytest
+
+from genesis_b200 import workloads as W
+from oracle import bridge, cref
+from oracle import mpm_ref as R
+
+
+def _rand_F(rng, n, scale=0.2):
+    return np.eye(3)[None] + scale * rng.normal(size=(n, 3, 3))
+
+
+def test_svd_convention_and_reconstruction():
+    rng = np.random.default_rng(0)
+    F = _rand_F(rng, 2000, 0.6)
+    F[:10] = -F[:10]  # det < 0 cases
+    U, S, V = R.svd3(F)
+    assert np.allclose(np.linalg.det(U), 1.0)
+    assert np.allclose(np.linalg.det(V), 1.0)
+    assert np.allclose(U @ (S[:, :, None] * np.swapaxes(V, 1, 2)), F, atol=1e-12)
+    assert np.all(S[:, 0] >= np.abs(S[:, 1]) - 1e-12) and np.all(S[:, 1] >= np.abs(S[:, 2]) - 1e-12)
+    assert np.all(S[:, :2] >= 0)
+    neg = np.linalg.det(F) < 0
+    assert np.all(S[neg, 2] < 0) and np.all(S[~neg, 2] >= 0)
+
+
+def test_c_svd_matches_lapack_convention():
+    """The C port's Jacobi+QR SVD and LAPACK agree on rotation-invariant outputs."""
+    rng = np.random.default_rng(1)
+    d = W.elastic_cube(n_side=4)
+    p, mats, st = bridge.from_desc(d, np.float64)
+    st["F"] = _rand_F(rng, st["x"].shape[0], 0.3)
+    st["C"] = 50 * rng.normal(size=st["C"].shape)
+    a = R.substep(p, mats, st)
+    b, rc = cref.substeps(p, mats, st, 1)
+    assert rc == 0
+    for k in ("x", "v", "C", "F", "Jp"):
+        assert np.allclose(a[k], b[k], rtol=1e-9, atol=1e-12), k
+
+
+def test_bspline_partition_of_unity_and_first_moment():
+    fx = np.random.default_rng(2).uniform(0.5, 1.5, size=(1000, 3))
+    w = R._weights(fx)
+    s = sum(w)
+    assert np.allclose(s, 1.0)
+    # sum_i w_i (i - fx) = 0 : APIC affine term carries no net momentum
+    m1 = sum(w[i] * (i - fx) for i in range(3))
+    assert np.allclose(m1, 0.0, atol=1e-14)
+
+
+@pytest.mark.parametrize("kind", ["elastic", "elastoplastic", "liquid", "sand", "snow"])
+def test_p2g_conserves_mass_and_momentum(kind):
+    rng = np.random.default_rng(3)
+    d = W.elastic_cube(n_side=8)
+    d.materials = [(kind, {})]
+    d.vel = rng.normal(0, 0.5, size=d.vel.shape)
+    p, mats, st = bridge.from_desc(d, np.float64)
+    st["F"] = _rand_F(rng, st["x"].shape[0], 0.05)
+    st["C"] = rng.normal(size=st["C"].shape)
+    gm, gp, _, _ = R.p2g(p, mats, st)
+    m = R.particle_mass(p, mats[0])
+    n = st["x"].shape[0]
+    assert np.isclose(gm.sum(), n * m, rtol=1e-12)
+    # stress contributions sum to zero (sum_i w_i dpos_i = 0); momentum = sum m v + sum m C @ 0
+    assert np.allclose(gp.reshape(-1, 3).sum(0), m * st["v"].sum(0), rtol=1e-9, atol=1e-9)
+
+
+def test_grid_op_gravity_and_boundary():
+    d = W.elastic_cube(n_side=4)
+    p, mats, st = bridge.from_desc(d, np.float64)
+    res = tuple(p.grid_res)
+    gm = np.zeros(res)
+    gp = np.zeros(res + (3,))
+    gm[10, 10, 10] = 2.0
+    gp[10, 10, 10] = [2.0, 0.0, 0.0]
+    gm[1, 10, 10] = 1.0
+    gp[1, 10, 10] = [-1.0, 0.5, 0.0]  # outside the padded lower x wall, moving out
+    gm[20, 20, 20] = 1e-9  # below EPS? (f64 EPS = 2.2e-16: still active)
+    vel = R.grid_op(p, gm, gp)
+    assert np.allclose(vel[10, 10, 10], [1.0, 0.0, -9.8 * p.dt])
+    assert vel[1, 10, 10, 0] == 0.0 and np.isclose(vel[1, 10, 10, 1], 0.5)
+    assert np.all(vel[0, 0, 0] == 0)
+
+
+def test_g2p_uniform_field_is_exact():
+    d = W.elastic_cube(n_side=6)
+    p, mats, st = bridge.from_desc(d, np.float64)
+    res = tuple(p.grid_res)
+    vel = np.zeros(res + (3,))
+    vel[...] = [0.1, -0.2, 0.3]
+    xn, vn, Cn = R.g2p(p, st, vel)
+    assert np.allclose(vn, [0.1, -0.2, 0.3])
+    assert np.allclose(Cn, 0.0, atol=1e-10)
+    assert np.allclose(xn, st["x"] + p.dt * vn)
+
+
+def test_material_return_mappings():
+    rng = np.random.default_rng(4)
+    n = 500
+    F = _rand_F(rng, n, 0.15)
+    U, S, V = R.svd3(F)
+    J = S[:, 0] * S[:, 1] * S[:, 2]
+    Jp = np.ones(n)
+    # von Mises: after projection the deviatoric log-strain norm is at most the yield radius
+    ep = R.make_material("elastoplastic", von_mises_yield_stress=1e4)
+    Fn, Sn, _ = R.update_F_S_Jp(ep, 2.2e-16, J, F, U, S, V, Jp)
+    e = np.log(np.maximum(Sn, 0.05))
+    eh = e - e.mean(1, keepdims=True)
+    assert np.all(np.linalg.norm(eh, axis=1) <= ep.von_mises_yield_stress / (2 * ep.mu) + 1e-6)
+    # snow: clamp and Jp bookkeeping keeps Jp * det(F_new) = det(F_tmp)
+    sn = R.make_material("snow", yield_lower=2.5e-2, yield_higher=7.5e-3)
+    Fn, Sn, Jpn = R.update_F_S_Jp(sn, 2.2e-16, J, F, U, S, V, Jp)
+    assert np.all(Sn >= 1 - 2.5e-2 - 1e-12) and np.all(Sn <= 1 + 7.5e-3 + 1e-12)
+    assert np.allclose(Jpn * np.linalg.det(Fn), np.linalg.det(F))
+    # sand: expansion (tr >= 0) resets to identity singular values
+    sd = R.make_material("sand")
+    Fn, Sn, Jpn = R.update_F_S_Jp(sd, 2.2e-16, J, F, U, S, V, np.zeros(n))
+    tr = np.log(np.maximum(np.abs(S), 1e-4)).sum(1)
+    assert np.allclose(Sn[tr >= 0], 1.0) and np.allclose(Jpn[tr >= 0], tr[tr >= 0])
+    # liquid: F_new = J^(1/3) I
+    lq = R.make_material("liquid")
+    Fn, _, _ = R.update_F_S_Jp(lq, 2.2e-16, J, F, U, S, V, Jp)
+    assert np.allclose(Fn, np.cbrt(J)[:, None, None] * np.eye(3))
+
+
+def test_material_defaults_follow_reference():
+    assert R.make_material("elastic").E == 3e5  # elastic.py:40
+    assert R.make_material("elastoplastic").yield_higher == 4.5e-3  # elasto_plastic.py:52
+    assert R.make_material("sand").default_Jp == 0.0  # sand.py:45
+    assert R.make_material("liquid").mu == 0.0  # liquid.py:47-48
+    assert not R.make_material("snow").use_von_mises  # snow.py:59
+    p = R.Params(grid_density=64, lower_bound=(0, 0, 0), upper_bound=(1, 1, 1))
+    assert tuple(p.grid_res) == (65, 65, 65)  # mpm_solver.py:53-55
+    assert np.isclose(p.particle_size, 0.01)  # options/solvers.py:490-491
+    assert np.isclose(p.p_vol, 1e-6 * 1e3)
+    assert R.Params(dtype=np.float32).eps == np.finfo(np.float32).eps
+
+
+def test_numpy_and_c_oracles_agree_f32_and_f64():
+    d = W.mixed_500k(n_side=6, grid_density=64)
+    for dtype, tol in ((np.float64, 1e-12), (np.float32, 2e-5)):
+        p, mats, st = bridge.from_desc(d, dtype)
+        a = R.run(p, mats, st, 5)
+        b, rc = cref.substeps(p, mats, st, 5, n_threads=2)
+        assert rc == 0
+        assert np.abs(a["x"] - b["x"]).max() < tol
+        assert np.abs(a["v"] - b["v"]).max() < 100 * tol
+
+
+def test_reference_invariants_cube_falls_and_stays_in_domain():
+    """tests/test_deformable_physics.py:209-219 asserts the MPM cube moved and stays above
+    the floor; here: it falls under gravity and never leaves the padded boundary."""
+    d = W.elastic_cube(n_side=8)
+    p, mats, st = bridge.from_desc(d, np.float64)
+    out, rc = cref.substeps(p, mats, st, 300, n_threads=2)
+    assert rc == 0
+    assert out["x"][:, 2].mean() < st["x"][:, 2].mean() - 1e-4
+    assert np.all(out["x"] >= p.bnd_lo - 1e-12) and np.all(out["x"] <= p.bnd_hi + 1e-12)
+    assert np.all(np.isfinite(out["x"]))
+
+
+def test_f32_oracle_error_is_small_over_100_substeps():
+    """Inherent float32 drift of the restatement (the CUDA tolerance is set against it)."""
+    d = W.elastic_cube(n_side=10)
+    a, _ = cref.substeps(*bridge.from_desc(d, np.float64), 100)
+    b, _ = cref.substeps(*bridge.from_desc(d, np.float32), 100)
+    assert np.abs(a["x"] - b["x"]).max() < 1e-5
