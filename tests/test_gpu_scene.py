@@ -15,6 +15,7 @@ def _init():
 
 
 def _scene(n_envs=0, substeps=10, **b200):
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")  # same particle samples per scene
     scene = gs.Scene(
         sim_options=gs.options.SimOptions(dt=1e-4 * substeps, substeps=substeps, gravity=(0, 0, -9.8)),
         mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
