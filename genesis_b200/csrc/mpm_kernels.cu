@@ -425,29 +425,59 @@ struct P2GArgs {
     Ws w;
 };
 
+// Shared tile in int32 fixed point.  On sm_100 shared-memory float atomicAdd is not a
+// native operation (it measures 3.3x slower than int32 even without conflicts, 4x with
+// the random conflicts of a stencil scatter) while int32 shared atomics are; the tile is
+// therefore accumulated as integers.  Each chunk picks, per channel, a power-of-two scale
+// s with n * b * s < 2^30, where n is the number of particles in the chunk and b bounds
+// |contribution| of any of them to any node (w <= 1, |off - fx| <= 1.5), so no node sum
+// can overflow; the quantisation step is ~1e-7 of the chunk's largest contribution, on a
+// par with float32 accumulation.  The tile uses an x-stride of 68 words so the banks of a
+// 4x4x4 block's nodes spread over all 32 banks.
+constexpr int TXS = TILE * TILE + 4;       // skewed x-stride of the shared tile (words)
+constexpr int TWORDS = TILE * TXS;         // words per channel (544)
+
+__device__ __forceinline__ int tidx(int x, int y, int z) { return x * TXS + y * TILE + z; }
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 template <int P>
-__global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
-    __shared__ float s_m[TN], s_px[TN], s_py[TN], s_pz[TN];
+__global__ void __launch_bounds__(P, 1024 / P) k_p2g(P2GArgs a) {
+    __shared__ int s_t[4][TWORDS];  // momentum x, y, z, mass
+    __shared__ float s_red[2][P / 32];
     __shared__ uint32_t s_mask;
+    __shared__ int s_cnt;
     Ws& w = a.w;
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     float* __restrict__ S = a.par.state;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
         const BlockCoord bc = block_coord(ch.y, I);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        for (int n = threadIdx.x; n < TN; n += P) {
-            s_m[n] = 0.f;
-            s_px[n] = 0.f;
-            s_py[n] = 0.f;
-            s_pz[n] = 0.f;
+        for (int n = threadIdx.x; n < TWORDS; n += P) {
+            s_t[0][n] = 0;
+            s_t[1][n] = 0;
+            s_t[2][n] = 0;
+            s_t[3][n] = 0;
         }
-        if (threadIdx.x == 0) s_mask = 0u;
-        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_mask = 0u;
+            s_cnt = 0;
+        }
 
+        // ---- phase 1: per-particle deformation update, stress, affine momentum
         const int p = ch.z + threadIdx.x;
+        bool live = false, in_tile = false;
+        float mass = 0.f, A[9], q[3], fx[3];
+        int base[3] = {0, 0, 0};
+        float bq = 0.f;
         if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
             float C[9], F[9];
 #pragma unroll
@@ -481,10 +511,8 @@ __global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
 #pragma unroll
             for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
             S[MPM_CH_JP * st + p] = Jpn;
-            // affine = stress*scale + mass*C (mpm_solver.py:344-345); C re-read (L1) to keep
-            // it out of registers across the SVD
-            const float mass = m.mass;
-            float A[9];
+            // affine = stress*scale + mass*C (mpm_solver.py:344-345); C re-read (L1)
+            mass = m.mass;
 #pragma unroll
             for (int k = 0; k < 9; ++k) A[k] = I.stress_scale * stress[k] + mass * __ldg(&S[(MPM_CH_C + k) * st + p]);
             float x[3], v[3];
@@ -494,8 +522,7 @@ __global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
                 v[d] = __ldg(&S[(MPM_CH_V + d) * st + p]);
             }
             if (finite3(x[0], x[1], x[2])) {
-                float fx[3], wx[3], wy[3], wz[3];
-                int base[3];
+                live = true;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const float xi = x[d] * I.inv_dx;
@@ -503,72 +530,108 @@ __global__ void __launch_bounds__(P) k_p2g(P2GArgs a) {
                     base[d] = (int)fminf(fmaxf(bf, -1e8f), 1e8f) - I.lower_cell[d];
                     fx[d] = xi - bf;
                 }
-                bspline(fx[0], wx);
-                bspline(fx[1], wy);
-                bspline(fx[2], wz);
-                // mass*v + affine @ dpos with dpos = (off - fx) * dx
+                // m v + A (off - fx) dx  =  q + dx * A off
                 const float dx = I.dx;
-                float q[3];
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+                for (int i = 0; i < 3; ++i) {
                     q[i] = mass * v[i] - (A[i * 3 + 0] * fx[0] + A[i * 3 + 1] * fx[1] + A[i * 3 + 2] * fx[2]) * dx;
-                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
-                const bool in_tile = lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3;
-                if (in_tile) {
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j)
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) {
-                                const float wt = wx[i] * wy[j] * wz[k];
-                                const float ax = q[0] + dx * (A[0] * i + A[1] * j + A[2] * k);
-                                const float ay = q[1] + dx * (A[3] * i + A[4] * j + A[5] * k);
-                                const float az = q[2] + dx * (A[6] * i + A[7] * j + A[8] * k);
-                                const int n = ((lx + i) * TILE + (ly + j)) * TILE + (lz + k);
-                                atomicAdd(&s_m[n], wt * mass);
-                                atomicAdd(&s_px[n], wt * ax);
-                                atomicAdd(&s_py[n], wt * ay);
-                                atomicAdd(&s_pz[n], wt * az);
-                            }
-                } else {
-                    // drifted since the last sort: bounds-checked global path
-                    atomicAdd((unsigned long long*)&w.counters[CNT_FALLBACK], 1ull);
-#pragma unroll 1
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll 1
-                        for (int j = 0; j < 3; ++j)
-#pragma unroll 1
-                            for (int k = 0; k < 3; ++k) {
-                                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
-                                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                                    set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
-                                    continue;
-                                }
-                                const float wt = wx[i] * wy[j] * wz[k];
-                                const float ax = q[0] + dx * (A[0] * i + A[1] * j + A[2] * k);
-                                const float ay = q[1] + dx * (A[3] * i + A[4] * j + A[5] * k);
-                                const float az = q[2] + dx * (A[6] * i + A[7] * j + A[8] * k);
-                                atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(wt * ax, wt * ay, wt * az, wt * mass));
-                                mark_block(w, ch.x, I, gx >> 2, gy >> 2, gz >> 2);
-                            }
+                    const float b = fabsf(mass * v[i]) +
+                                    1.5f * dx * (fabsf(A[i * 3 + 0]) + fabsf(A[i * 3 + 1]) + fabsf(A[i * 3 + 2]));
+                    bq = fmaxf(bq, b);
                 }
+#pragma unroll
+                for (int k = 0; k < 9; ++k) A[k] *= dx;
+                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+                in_tile = lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3 &&
+                          isfinite(bq);
             } else {
                 set_status(w.counters, MPM_STATUS_NAN);
             }
         }
+        // chunk-wide bounds for the fixed-point scales
+        const float wbq = warp_max(in_tile ? bq : 0.f);
+        const float wbm = warp_max(in_tile ? mass : 0.f);
+        const unsigned nb = __ballot_sync(0xffffffffu, in_tile);
+        if (lane == 0) {
+            s_red[0][wid] = wbq;
+            s_red[1][wid] = wbm;
+            if (nb) atomicAdd(&s_cnt, __popc(nb));
+        }
         __syncthreads();
-        // flush non-empty tile nodes: one 16-byte reduction per node
+        float Bq = 0.f, Bm = 0.f;
+#pragma unroll
+        for (int i = 0; i < P / 32; ++i) {
+            Bq = fmaxf(Bq, s_red[0][i]);
+            Bm = fmaxf(Bm, s_red[1][i]);
+        }
+        const float nin = (float)max(s_cnt, 1);
+        // scale = 2^(29 - floor(log2(n * B))): n * B * scale < 2^30
+        const float sq = Bq > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bq)))) : 1.f;
+        const float sm = Bm > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bm)))) : 1.f;
+
+        // ---- phase 2: scatter (27-node quadratic B-spline stencil, mpm_solver.py:347-386)
+        if (live) {
+            float wx[3], wy[3], wz[3];
+            bspline(fx[0], wx);
+            bspline(fx[1], wy);
+            bspline(fx[2], wz);
+            if (in_tile) {
+                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+                const float mq0 = q[0] * sq, mq1 = q[1] * sq, mq2 = q[2] * sq, ms = mass * sm;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const float wt = wx[i] * wy[j] * wz[k];
+                            const float ax = mq0 + sq * (A[0] * i + A[1] * j + A[2] * k);
+                            const float ay = mq1 + sq * (A[3] * i + A[4] * j + A[5] * k);
+                            const float az = mq2 + sq * (A[6] * i + A[7] * j + A[8] * k);
+                            const int n = tidx(lx + i, ly + j, lz + k);
+                            atomicAdd(&s_t[0][n], __float2int_rn(wt * ax));
+                            atomicAdd(&s_t[1][n], __float2int_rn(wt * ay));
+                            atomicAdd(&s_t[2][n], __float2int_rn(wt * az));
+                            atomicAdd(&s_t[3][n], __float2int_rn(wt * ms));
+                        }
+            } else {
+                // drifted since the last sort (or a non-finite stress): bounds-checked global path
+                atomicAdd((unsigned long long*)&w.counters[CNT_FALLBACK], 1ull);
+#pragma unroll 1
+                for (int i = 0; i < 3; ++i)
+#pragma unroll 1
+                    for (int j = 0; j < 3; ++j)
+#pragma unroll 1
+                        for (int k = 0; k < 3; ++k) {
+                            const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
+                            if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                                set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                                continue;
+                            }
+                            const float wt = wx[i] * wy[j] * wz[k];
+                            const float ax = q[0] + (A[0] * i + A[1] * j + A[2] * k);
+                            const float ay = q[1] + (A[3] * i + A[4] * j + A[5] * k);
+                            const float az = q[2] + (A[6] * i + A[7] * j + A[8] * k);
+                            atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(wt * ax, wt * ay, wt * az, wt * mass));
+                            mark_block(w, ch.x, I, gx >> 2, gy >> 2, gz >> 2);
+                        }
+            }
+        }
+        __syncthreads();
+        // ---- phase 3: flush non-empty tile nodes, one 16-byte reduction each
+        const float iq = 1.f / sq, im = 1.f / sm;
         for (int n = threadIdx.x; n < TN; n += P) {
-            const float mval = s_m[n];
-            if (mval != 0.f) {
-                const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
+            const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
+            const int t = tidx(tx, ty, tz);
+            const int mi = s_t[3][t];
+            if (mi != 0) {
                 const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
                 if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
                     set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
                     continue;
                 }
-                atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(s_px[n], s_py[n], s_pz[n], mval));
+                atomicAdd(&w.mm[node_addr(I, gx, gy, gz)],
+                          make_float4((float)s_t[0][t] * iq, (float)s_t[1][t] * iq, (float)s_t[2][t] * iq, (float)mi * im));
                 const int bit = ((gx >> 2) - bc.bx + 1) * 9 + ((gy >> 2) - bc.by + 1) * 3 + ((gz >> 2) - bc.bz + 1);
                 atomicOr(&s_mask, 1u << bit);
             }
@@ -646,7 +709,7 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
 // ---------------------------------------------------------------- g2p
 
 template <int P>
-__global__ void __launch_bounds__(P) k_g2p(P2GArgs a) {
+__global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
     __shared__ float4 s_v[TN];
     Ws& w = a.w;
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
