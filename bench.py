@@ -47,6 +47,10 @@ BYTES = {
     "p2g": (148, 16),  # read x,v,C,F,Jp (100) + material idx & mass (8); write F,Jp (40); grid m+mom (16)
     "grid_op": (0, 28),  # read m+mom (16), write v (12)
     "g2p": (60, 12),  # write x,v,C (60); read grid v (12)  (x read counted in p2g)
+    # fused g2p of substep n + p2g of n+1: one substep's particle bytes (208) + grid v read
+    # (12) and m+mom write (16).  v and C never leave registers, so the DRAM bytes it must
+    # move are lower (x, F, Jp read + written: ~106 B/particle); 'traffic' reports ncu's count.
+    "g2p2g": (208, 28),
 }
 SUBSTEP_BYTES = (208, 56)
 
@@ -58,7 +62,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--substeps-per-step", type=int, default=100)
-    ap.add_argument("--sort-interval", type=int, default=16)
+    ap.add_argument("--sort-interval", type=int, default=50)
     ap.add_argument("--chunk", type=int, default=256)
     ap.add_argument("--n-side", type=int, default=50, help="particles per box edge (50 -> 500k)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -242,34 +246,39 @@ def run_reference(args, world, rank):
 
 # ------------------------------------------------------------------ GPU (our arm)
 def kernel_breakdown(rt, n_substeps=20):
-    """Per-kernel CUDA-event durations (ms) over eager substeps on the launch stream."""
+    """Per-kernel CUDA-event durations (ms) over the same launch sequence mpm_substeps uses:
+    p2g + grid_op for the first substep, then fused g2p2g + grid_op, with g2p / sort / p2g
+    where a re-sort falls; the GPU is kept busy so events bracket kernels back to back."""
     import torch
 
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    acc = {"sort": [], "p2g": [], "grid_op": [], "g2p": []}
+    acc = {"sort": [], "p2g": [], "grid_op": [], "g2p": [], "g2p2g": []}
     K = max(rt.sort_interval, 1)
     torch.cuda.synchronize()
-    # keep the GPU busy while the host enqueues, so events bracket kernels back to back
     torch.cuda._sleep(int(2e8))
-    for _ in range(n_substeps):
-        if rt._count % K == 0:
-            a, b = ev(), ev()
-            a.record()
-            rt.sort()
-            b.record()
-            acc["sort"].append((a, b))
-        e = [ev() for _ in range(4)]
-        e[0].record()
-        rt.p2g()
-        e[1].record()
-        rt.grid_op()
-        e[2].record()
-        rt.g2p()
-        e[3].record()
+
+    def timed(name, fn):
+        a, b = ev(), ev()
+        a.record()
+        fn()
+        b.record()
+        acc[name].append((a, b))
+
+    for i in range(n_substeps):
+        due = rt._count % K == 0
+        if i == 0:
+            if due:
+                timed("sort", rt.sort)
+            timed("p2g", rt.p2g)
+        elif due:
+            timed("g2p", rt.g2p)
+            timed("sort", rt.sort)
+            timed("p2g", rt.p2g)
+        else:
+            timed("g2p2g", rt.g2p2g)
+        timed("grid_op", rt.grid_op)
         rt._count += 1
-        acc["p2g"].append((e[0], e[1]))
-        acc["grid_op"].append((e[1], e[2]))
-        acc["g2p"].append((e[2], e[3]))
+    timed("g2p", rt.g2p)
     torch.cuda.synchronize()
     return {k: (statistics.mean(a.elapsed_time(b) for a, b in v) if v else 0.0, len(v)) for k, v in acc.items()}
 
@@ -298,7 +307,7 @@ def build_scene(d, S):
         sim_options=gs.options.SimOptions(dt=d.dt * S, substeps=S, gravity=d.gravity),
         mpm_options=gs.options.MPMOptions(lower_bound=d.lower_bound, upper_bound=d.upper_bound,
                                           grid_density=d.grid_density, particle_size=d.particle_size),
-        b200_options=gs.options.B200Options(sort_interval=16, check_nan="step"),
+        b200_options=gs.options.B200Options(sort_interval=50, check_nan="step"),
     )
     from genesis_b200 import workloads as W
 
@@ -395,18 +404,20 @@ def run_ours(args, world, rank, local):
     n_act = active_nodes(rt)
     kb = kernel_breakdown(rt, 3 * args.sort_interval)
     hbm, src = peaks()
-    dom = max(("p2g", "grid_op", "g2p"), key=lambda k: kb[k][0])
+    dom = max(("p2g", "grid_op", "g2p", "g2p2g"), key=lambda k: kb[k][0] * kb[k][1])
     bp, bc = BYTES[dom]
     alg = bp * d.n_particles + bc * n_act
     t_dom = kb[dom][0] * 1e-3
     achieved = alg / t_dom / 1e9
     tr = ncu_traffic()
     traffic = tr.get(f"{dom}_dram_bytes_per_launch")
-    sub_ms = sum(kb[k][0] for k in ("p2g", "grid_op", "g2p")) + kb["sort"][0] / max(args.sort_interval, 1)
+    nsub = 3 * args.sort_interval
+    sub_ms = sum(kb[k][0] * kb[k][1] for k in kb) / nsub
     sub_alg = SUBSTEP_BYTES[0] * d.n_particles + SUBSTEP_BYTES[1] * n_act
-    launches_per_substep = 3
-    sorts = sum(1 for i in range(S * args.steps) if (rt._count + i) % args.sort_interval == 0)
-    gpu_launches = launches_per_substep * S * args.steps + 7 * sorts
+    # launches per timed step: 2 per substep (g2p2g + grid_op), +1 (g2p) at the end and
+    # +8 (g2p, 7 sort kernels, p2g replacing g2p2g) at each re-sort
+    sorts = sum(1 for i in range(S) if i % args.sort_interval == 0)
+    gpu_launches = args.steps * (2 * S + 1 + 8 * sorts)
 
     res = {
         "metric": METRIC,

@@ -141,6 +141,7 @@ SIGNATURES = {
     "mpm_p2g": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
     "mpm_grid_op": (C.c_int, [_P(Problem), _P(Tables), vp, vp]),
     "mpm_g2p": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
+    "mpm_g2p2g": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
     "mpm_substeps": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),
@@ -165,7 +166,7 @@ def load(path: str | None = None):
     with _lock:
         if _lib is not None:
             return _lib
-        p = path or LIB_PATH
+        p = path or os.environ.get("GENESIS_B200_LIB") or LIB_PATH
         if not os.path.exists(p):
             raise NativeLibraryError(
                 f"{LIB_NAME} not found at {p}; build it with `python -c 'import genesis_b200.build as b; b.build()'`"

@@ -36,6 +36,11 @@
 
 namespace gbm {
 
+// resident threads per SM the register allocation of p2g / g2p2g is sized for
+#ifndef GBM_P2G_THREADS_PER_SM
+#define GBM_P2G_THREADS_PER_SM 768
+#endif
+
 constexpr int BLK = MPM_BLOCK;         // grid block edge
 constexpr int BLK3 = BLK * BLK * BLK;  // nodes per block
 constexpr int MARGIN = 1;              // drift margin of the shared tile (nodes)
@@ -47,7 +52,7 @@ constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
 constexpr int MAX_SCAN_TILES = SCAN_T * SCAN_ITEMS;  // single-CTA scan of tile sums
 constexpr int64_t MAX_BLOCKS = (int64_t)SCAN_TILE * MAX_SCAN_TILES;
 
-enum Counter { CNT_ACTIVE = 0, CNT_CHUNKS = 1, CNT_STATUS = 2, CNT_SORTED = 3, CNT_FALLBACK = 4 /* u64 at 4,5 */ };
+enum Counter { CNT_ACTIVE = 0, CNT_CHUNKS = 1, CNT_STATUS = 2, CNT_SORTED = 3, CNT_FALLBACK = 4 /* u64 at 4,5 */, CNT_DONE = 6 };
 constexpr int N_COUNTERS = 16;
 
 struct Ws {
@@ -429,11 +434,12 @@ struct P2GArgs {
 // native operation (it measures 3.3x slower than int32 even without conflicts, 4x with
 // the random conflicts of a stencil scatter) while int32 shared atomics are; the tile is
 // therefore accumulated as integers.  Each chunk picks, per channel, a power-of-two scale
-// s with n * b * s < 2^30, where n is the number of particles in the chunk and b bounds
-// |contribution| of any of them to any node (w <= 1, |off - fx| <= 1.5), so no node sum
-// can overflow; the quantisation step is ~1e-7 of the chunk's largest contribution, on a
-// par with float32 accumulation.  The tile uses an x-stride of 68 words so the banks of a
-// 4x4x4 block's nodes spread over all 32 banks.
+// s with max(n, 256) * b * s < 2^30, where n is the number of particles in the chunk and b
+// bounds |contribution| of any of them to any node (w <= 1, |off - fx| <= 1.5): no node
+// sum can overflow, every contribution is below 2^22 (so round-to-nearest is one float add
+// of 1.5 * 2^23, exact), and the quantisation step is 2^-22 of the chunk's largest
+// contribution, on a par with float32 accumulation.  The tile uses an x-stride of 68
+// words so the banks of a 4x4x4 block's nodes spread over all 32 banks.
 constexpr int TXS = TILE * TILE + 4;       // skewed x-stride of the shared tile (words)
 constexpr int TWORDS = TILE * TXS;         // words per channel (544)
 
@@ -445,203 +451,425 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
+// round-to-nearest float -> int for |f| < 2^22: the add leaves round(f) in the low mantissa bits
+__device__ __forceinline__ int fix(float f) { return __float_as_int(f + 12582912.0f) - 0x4B400000; }
+
+struct Tile {
+    int t[4][TWORDS];  // momentum x, y, z, mass
+    float red[2][32];
+    uint32_t mask;
+    int cnt;
+};
+
+struct VelTile {
+    float4 v[TN];
+};
+
+// Per-thread scatter payload of one particle: mass * v + affine (off - fx) dx = q + A off.
+struct Payload {
+    float q[3], A[9], fx[3];
+    float mass, bq;
+    int base[3];
+    bool live, in_tile;
+};
+
+// element i of a 3-array without dynamic indexing (keeps it in registers in rolled loops)
+__device__ __forceinline__ float sel3(const float* w, int i) { return i == 0 ? w[0] : (i == 1 ? w[1] : w[2]); }
+
+__device__ __forceinline__ void locate(const mpm_instance& I, const float* x, int* base, float* fx) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float xi = x[d] * I.inv_dx;
+        const float bf = floorf(xi - 0.5f);
+        base[d] = (int)fminf(fmaxf(bf, -1e8f), 1e8f) - I.lower_cell[d];
+        fx[d] = xi - bf;
+    }
+}
+
+__device__ __forceinline__ bool tile_contains(const int* base, int ox, int oy, int oz) {
+    const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+    return lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3;
+}
+
+// compute_F_tmp + svd + return mapping + stress (mpm_solver.py:261-345) for slot p with
+// velocity v and affine C; writes F and Jp of the next frame and fills the scatter payload
+// for position x.
+__device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm_material* __restrict__ mats,
+                                                const mpm_particles& par, int p, const float* x, const float* v,
+                                                const float* C, int ox, int oy, int oz, Payload& o, uint32_t* counters) {
+    const int64_t st = par.state_stride;
+    float* __restrict__ S = par.state;
+    float F[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = S[(MPM_CH_F + k) * st + p];
+    const float Jp = S[MPM_CH_JP * st + p];
+    const mpm_material m = mats[I.mat_base + par.mat[p]];
+    float mu = m.mu, lam = m.lam;
+    if (par.mu_p) {
+        mu = par.mu_p[p];
+        lam = par.lam_p[p];
+    }
+    // compute_F_tmp: (I + dt C) F   (mpm_solver.py:264-266)
+    float Ft[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float acc = F[i * 3 + j];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc += I.dt * C[i * 3 + k] * F[k * 3 + j];
+            Ft[i * 3 + j] = acc;
+        }
+    float U[9], Sg[3], V[9];
+    svd3(Ft, U, Sg, V);
+    const float J = Sg[0] * (Sg[1] * Sg[2]);
+    float Fn[9], stress[9], Jpn;
+    constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, stress);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
+    S[MPM_CH_JP * st + p] = Jpn;
+    // affine = stress * (-dt vol 4 inv_dx^2) + mass C (mpm_solver.py:344-345)
+    o.mass = m.mass;
+    float A[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) A[k] = I.stress_scale * stress[k] + o.mass * C[k];
+    o.live = false;
+    o.in_tile = false;
+    o.bq = 0.f;
+    if (finite3(x[0], x[1], x[2])) {
+        o.live = true;
+        locate(I, x, o.base, o.fx);
+        const float dx = I.dx;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            o.q[i] = o.mass * v[i] - (A[i * 3 + 0] * o.fx[0] + A[i * 3 + 1] * o.fx[1] + A[i * 3 + 2] * o.fx[2]) * dx;
+            const float b =
+                fabsf(o.mass * v[i]) + 1.5f * dx * (fabsf(A[i * 3 + 0]) + fabsf(A[i * 3 + 1]) + fabsf(A[i * 3 + 2]));
+            o.bq = fmaxf(o.bq, b);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o.A[k] = A[k] * dx;
+        o.in_tile = tile_contains(o.base, ox, oy, oz) && isfinite(o.bq);
+    } else {
+        set_status(counters, MPM_STATUS_NAN);
+    }
+}
+
+__device__ __forceinline__ void tile_zero(Tile& T, int P) {
+    for (int n = threadIdx.x; n < TWORDS; n += P) {
+        T.t[0][n] = 0;
+        T.t[1][n] = 0;
+        T.t[2][n] = 0;
+        T.t[3][n] = 0;
+    }
+    if (threadIdx.x == 0) {
+        T.mask = 0u;
+        T.cnt = 0;
+    }
+}
+
+// Chunk-wide fixed-point scales, the 27-node scatter, the flush of non-empty nodes to the
+// block-major grid and the marking of touched grid blocks.  Must be called by every
+// thread of the CTA (contains barriers); T must be zeroed and a barrier passed before.
 template <int P>
-__global__ void __launch_bounds__(P, 1024 / P) k_p2g(P2GArgs a) {
-    __shared__ int s_t[4][TWORDS];  // momentum x, y, z, mass
-    __shared__ float s_red[2][P / 32];
-    __shared__ uint32_t s_mask;
-    __shared__ int s_cnt;
+__device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const mpm_instance& I, int inst,
+                                              const BlockCoord& bc, int ox, int oy, int oz, Ws& w) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const float wbq = warp_max(o.in_tile ? o.bq : 0.f);
+    const float wbm = warp_max(o.in_tile ? o.mass : 0.f);
+    const unsigned nb = __ballot_sync(0xffffffffu, o.in_tile);
+    if (lane == 0) {
+        T.red[0][wid] = wbq;
+        T.red[1][wid] = wbm;
+        if (nb) atomicAdd(&T.cnt, __popc(nb));
+    }
+    __syncthreads();
+    float Bq = 0.f, Bm = 0.f;
+#pragma unroll
+    for (int i = 0; i < P / 32; ++i) {
+        Bq = fmaxf(Bq, T.red[0][i]);
+        Bm = fmaxf(Bm, T.red[1][i]);
+    }
+    const float nin = (float)max(T.cnt, 256);
+    // scale = 2^(29 - floor(log2(n * B))): n * B * scale < 2^30
+    const float sq = Bq > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bq)))) : 1.f;
+    const float sm = Bm > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bm)))) : 1.f;
+    if (o.live) {
+        float wx[3], wy[3], wz[3];
+        bspline(o.fx[0], wx);
+        bspline(o.fx[1], wy);
+        bspline(o.fx[2], wz);
+        if (o.in_tile) {
+            const int lx = o.base[0] - ox, ly = o.base[1] - oy, lz = o.base[2] - oz;
+            const float mq0 = o.q[0] * sq, mq1 = o.q[1] * sq, mq2 = o.q[2] * sq, ms = o.mass * sm;
+            float As[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) As[k] = o.A[k] * sq;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float wt = wx[i] * wy[j] * wz[k];
+                        const float ax = mq0 + (As[0] * i + As[1] * j + As[2] * k);
+                        const float ay = mq1 + (As[3] * i + As[4] * j + As[5] * k);
+                        const float az = mq2 + (As[6] * i + As[7] * j + As[8] * k);
+                        const int n = tidx(lx + i, ly + j, lz + k);
+                        atomicAdd(&T.t[0][n], fix(wt * ax));
+                        atomicAdd(&T.t[1][n], fix(wt * ay));
+                        atomicAdd(&T.t[2][n], fix(wt * az));
+                        atomicAdd(&T.t[3][n], fix(wt * ms));
+                    }
+        } else {
+            // drifted since the last sort (or a non-finite stress): bounds-checked global path
+            atomicAdd((unsigned long long*)&w.counters[CNT_FALLBACK], 1ull);
+#pragma unroll 1
+            for (int i = 0; i < 3; ++i)
+#pragma unroll 1
+                for (int j = 0; j < 3; ++j)
+#pragma unroll 1
+                    for (int k = 0; k < 3; ++k) {
+                        const int gx = o.base[0] + i, gy = o.base[1] + j, gz = o.base[2] + k;
+                        if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                            set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                            continue;
+                        }
+                        const float wt = sel3(wx, i) * sel3(wy, j) * sel3(wz, k);
+                        const float ax = o.q[0] + (o.A[0] * i + o.A[1] * j + o.A[2] * k);
+                        const float ay = o.q[1] + (o.A[3] * i + o.A[4] * j + o.A[5] * k);
+                        const float az = o.q[2] + (o.A[6] * i + o.A[7] * j + o.A[8] * k);
+                        atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(wt * ax, wt * ay, wt * az, wt * o.mass));
+                        mark_block(w, inst, I, gx >> 2, gy >> 2, gz >> 2);
+                    }
+        }
+    }
+    __syncthreads();
+    // flush non-empty tile nodes, one 16-byte reduction each
+    const float iq = 1.f / sq, im = 1.f / sm;
+    for (int n = threadIdx.x; n < TN; n += P) {
+        const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
+        const int t = tidx(tx, ty, tz);
+        const int mi = T.t[3][t];
+        if (mi != 0) {
+            const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
+            if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                continue;
+            }
+            atomicAdd(&w.mm[node_addr(I, gx, gy, gz)],
+                      make_float4((float)T.t[0][t] * iq, (float)T.t[1][t] * iq, (float)T.t[2][t] * iq, (float)mi * im));
+            const int bit = ((gx >> 2) - bc.bx + 1) * 9 + ((gy >> 2) - bc.by + 1) * 3 + ((gz >> 2) - bc.bz + 1);
+            atomicOr(&T.mask, 1u << bit);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 27 && ((T.mask >> threadIdx.x) & 1u)) {
+        const int t = threadIdx.x;
+        mark_block(w, inst, I, bc.bx + t / 9 - 1, bc.by + (t / 3) % 3 - 1, bc.bz + t % 3 - 1);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const mpm_instance& I, int ox, int oy, int oz,
+                                              int P) {
+    for (int n = threadIdx.x; n < TN; n += P) {
+        const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
+        const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
+        float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < I.res[0] && gy < I.res[1] && gz < I.res[2])
+            val = w.gv[node_addr(I, gx, gy, gz)];
+        VT.v[n] = val;
+    }
+}
+
+// g2p gather (mpm_solver.py:396-431): v = sum w v_i, C = 4 inv_dx sum w v_i (off - fx)^T;
+// then x += dt v and the boundary (mpm_solver.py:434-437).  Returns false if nothing
+// could be gathered (non-finite x).
+__device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm_instance& I, float* x, float* nv,
+                                       float* nC, int ox, int oy, int oz) {
+    if (!finite3(x[0], x[1], x[2])) {
+        set_status(w.counters, MPM_STATUS_NAN);
+        return false;
+    }
+    float fx[3], wx[3], wy[3], wz[3];
+    int base[3];
+    locate(I, x, base, fx);
+    bspline(fx[0], wx);
+    bspline(fx[1], wy);
+    bspline(fx[2], wz);
+    nv[0] = nv[1] = nv[2] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nC[k] = 0.f;
+    if (tile_contains(base, ox, oy, oz)) {
+        const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float4 g = VT.v[((lx + i) * TILE + (ly + j)) * TILE + (lz + k)];
+                    const float wt = wx[i] * wy[j] * wz[k];
+                    const float d0 = (float)i - fx[0], d1 = (float)j - fx[1], d2 = (float)k - fx[2];
+                    nv[0] += wt * g.x;
+                    nv[1] += wt * g.y;
+                    nv[2] += wt * g.z;
+                    const float cw = I.c_scale * wt;
+                    nC[0] += cw * g.x * d0;
+                    nC[1] += cw * g.x * d1;
+                    nC[2] += cw * g.x * d2;
+                    nC[3] += cw * g.y * d0;
+                    nC[4] += cw * g.y * d1;
+                    nC[5] += cw * g.y * d2;
+                    nC[6] += cw * g.z * d0;
+                    nC[7] += cw * g.z * d1;
+                    nC[8] += cw * g.z * d2;
+                }
+    } else {
+#pragma unroll 1
+        for (int i = 0; i < 3; ++i)
+#pragma unroll 1
+            for (int j = 0; j < 3; ++j)
+#pragma unroll 1
+                for (int k = 0; k < 3; ++k) {
+                    const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
+                    if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+                        set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                        continue;
+                    }
+                    const float4 g = w.gv[node_addr(I, gx, gy, gz)];
+                    const float wt = sel3(wx, i) * sel3(wy, j) * sel3(wz, k);
+                    const float d0 = (float)i - fx[0], d1 = (float)j - fx[1], d2 = (float)k - fx[2];
+                    nv[0] += wt * g.x;
+                    nv[1] += wt * g.y;
+                    nv[2] += wt * g.z;
+                    const float cw = I.c_scale * wt;
+                    nC[0] += cw * g.x * d0;
+                    nC[1] += cw * g.x * d1;
+                    nC[2] += cw * g.x * d2;
+                    nC[3] += cw * g.y * d0;
+                    nC[4] += cw * g.y * d1;
+                    nC[5] += cw * g.y * d2;
+                    nC[6] += cw * g.z * d0;
+                    nC[7] += cw * g.z * d1;
+                    nC[8] += cw * g.z * d2;
+                }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float nx = x[d] + I.dt * nv[d];
+        nv[d] = bc_vel(nx, nv[d], I.bnd_lo[d], I.bnd_hi[d]);
+        x[d] = fmaxf(fminf(nx, I.bnd_hi[d]), I.bnd_lo[d]);
+    }
+    if (!finite3(x[0], x[1], x[2])) set_status(w.counters, MPM_STATUS_NAN);
+    return true;
+}
+
+// ---------------------------------------------------------------- p2g
+
+template <int P>
+__global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a) {
+    __shared__ Tile T;
     Ws& w = a.w;
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
-    float* __restrict__ S = a.par.state;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const float* __restrict__ S = a.par.state;
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
         const BlockCoord bc = block_coord(ch.y, I);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        for (int n = threadIdx.x; n < TWORDS; n += P) {
-            s_t[0][n] = 0;
-            s_t[1][n] = 0;
-            s_t[2][n] = 0;
-            s_t[3][n] = 0;
-        }
-        if (threadIdx.x == 0) {
-            s_mask = 0u;
-            s_cnt = 0;
-        }
-
-        // ---- phase 1: per-particle deformation update, stress, affine momentum
+        tile_zero(T, P);
+        Payload o;
+        o.live = o.in_tile = false;
+        o.mass = o.bq = 0.f;
         const int p = ch.z + threadIdx.x;
-        bool live = false, in_tile = false;
-        float mass = 0.f, A[9], q[3], fx[3];
-        int base[3] = {0, 0, 0};
-        float bq = 0.f;
         if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
-            float C[9], F[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
-                F[k] = S[(MPM_CH_F + k) * st + p];
-            }
-            const float Jp = S[MPM_CH_JP * st + p];
-            const mpm_material m = a.mats[I.mat_base + a.par.mat[p]];
-            float mu = m.mu, lam = m.lam;
-            if (a.par.mu_p) {
-                mu = a.par.mu_p[p];
-                lam = a.par.lam_p[p];
-            }
-            // compute_F_tmp: (I + dt C) F   (mpm_solver.py:264-266)
-            float Ft[9];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    float acc = F[i * 3 + j];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) acc += I.dt * C[i * 3 + k] * F[k * 3 + j];
-                    Ft[i * 3 + j] = acc;
-                }
-            float U[9], Sg[3], V[9];
-            svd3(Ft, U, Sg, V);
-            const float J = Sg[0] * (Sg[1] * Sg[2]);
-            float Fn[9], stress[9], Jpn;
-            constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, stress);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
-            S[MPM_CH_JP * st + p] = Jpn;
-            // affine = stress*scale + mass*C (mpm_solver.py:344-345); C re-read (L1)
-            mass = m.mass;
-#pragma unroll
-            for (int k = 0; k < 9; ++k) A[k] = I.stress_scale * stress[k] + mass * __ldg(&S[(MPM_CH_C + k) * st + p]);
-            float x[3], v[3];
+            float x[3], v[3], C[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 x[d] = __ldg(&S[(MPM_CH_X + d) * st + p]);
                 v[d] = __ldg(&S[(MPM_CH_V + d) * st + p]);
             }
-            if (finite3(x[0], x[1], x[2])) {
-                live = true;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
+            particle_update(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w.counters);
+        }
+        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w);
+    }
+}
+
+// ---------------------------------------------------------------- g2p
+
+template <int P>
+__global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
+    __shared__ VelTile VT;
+    Ws& w = a.w;
+    const int n_chunks = (int)w.counters[CNT_CHUNKS];
+    const int64_t st = a.par.state_stride;
+    float* __restrict__ S = a.par.state;
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        const int4 ch = w.chunks[ci];
+        const mpm_instance& I = a.inst[ch.x];
+        const BlockCoord bc = block_coord(ch.y, I);
+        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
+        vel_tile_load(VT, w, I, ox, oy, oz, P);
+        __syncthreads();
+        const int p = ch.z + threadIdx.x;
+        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
+            float x[3], nv[3], nC[9];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
+            if (gather(VT, w, I, x, nv, nC, ox, oy, oz)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    const float xi = x[d] * I.inv_dx;
-                    const float bf = floorf(xi - 0.5f);
-                    base[d] = (int)fminf(fmaxf(bf, -1e8f), 1e8f) - I.lower_cell[d];
-                    fx[d] = xi - bf;
-                }
-                // m v + A (off - fx) dx  =  q + dx * A off
-                const float dx = I.dx;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    q[i] = mass * v[i] - (A[i * 3 + 0] * fx[0] + A[i * 3 + 1] * fx[1] + A[i * 3 + 2] * fx[2]) * dx;
-                    const float b = fabsf(mass * v[i]) +
-                                    1.5f * dx * (fabsf(A[i * 3 + 0]) + fabsf(A[i * 3 + 1]) + fabsf(A[i * 3 + 2]));
-                    bq = fmaxf(bq, b);
+                    S[(MPM_CH_X + d) * st + p] = x[d];
+                    S[(MPM_CH_V + d) * st + p] = nv[d];
                 }
 #pragma unroll
-                for (int k = 0; k < 9; ++k) A[k] *= dx;
-                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
-                in_tile = lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3 &&
-                          isfinite(bq);
-            } else {
-                set_status(w.counters, MPM_STATUS_NAN);
+                for (int k = 0; k < 9; ++k) S[(MPM_CH_C + k) * st + p] = nC[k];
             }
         }
-        // chunk-wide bounds for the fixed-point scales
-        const float wbq = warp_max(in_tile ? bq : 0.f);
-        const float wbm = warp_max(in_tile ? mass : 0.f);
-        const unsigned nb = __ballot_sync(0xffffffffu, in_tile);
-        if (lane == 0) {
-            s_red[0][wid] = wbq;
-            s_red[1][wid] = wbm;
-            if (nb) atomicAdd(&s_cnt, __popc(nb));
-        }
         __syncthreads();
-        float Bq = 0.f, Bm = 0.f;
-#pragma unroll
-        for (int i = 0; i < P / 32; ++i) {
-            Bq = fmaxf(Bq, s_red[0][i]);
-            Bm = fmaxf(Bm, s_red[1][i]);
-        }
-        const float nin = (float)max(s_cnt, 1);
-        // scale = 2^(29 - floor(log2(n * B))): n * B * scale < 2^30
-        const float sq = Bq > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bq)))) : 1.f;
-        const float sm = Bm > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bm)))) : 1.f;
+    }
+}
 
-        // ---- phase 2: scatter (27-node quadratic B-spline stencil, mpm_solver.py:347-386)
-        if (live) {
-            float wx[3], wy[3], wz[3];
-            bspline(fx[0], wx);
-            bspline(fx[1], wy);
-            bspline(fx[2], wz);
-            if (in_tile) {
-                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
-                const float mq0 = q[0] * sq, mq1 = q[1] * sq, mq2 = q[2] * sq, ms = mass * sm;
+// ---------------------------------------------------------------- fused g2p + p2g
+
+// g2p of substep n fused with p2g of substep n+1: the new v and C never leave registers
+// (they are recomputed from the grid by the next gather), only x, F and Jp are stored.
+template <int P>
+__global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs a) {
+    __shared__ VelTile VT;
+    __shared__ Tile T;
+    Ws& w = a.w;
+    const int n_chunks = (int)w.counters[CNT_CHUNKS];
+    const int64_t st = a.par.state_stride;
+    float* __restrict__ S = a.par.state;
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        const int4 ch = w.chunks[ci];
+        const mpm_instance& I = a.inst[ch.x];
+        const BlockCoord bc = block_coord(ch.y, I);
+        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
+        vel_tile_load(VT, w, I, ox, oy, oz, P);
+        tile_zero(T, P);
+        __syncthreads();
+        Payload o;
+        o.live = o.in_tile = false;
+        o.mass = o.bq = 0.f;
+        const int p = ch.z + threadIdx.x;
+        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
+            float x[3], nv[3], nC[9];
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
+            if (gather(VT, w, I, x, nv, nC, ox, oy, oz)) {
 #pragma unroll
-                    for (int j = 0; j < 3; ++j)
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            const float wt = wx[i] * wy[j] * wz[k];
-                            const float ax = mq0 + sq * (A[0] * i + A[1] * j + A[2] * k);
-                            const float ay = mq1 + sq * (A[3] * i + A[4] * j + A[5] * k);
-                            const float az = mq2 + sq * (A[6] * i + A[7] * j + A[8] * k);
-                            const int n = tidx(lx + i, ly + j, lz + k);
-                            atomicAdd(&s_t[0][n], __float2int_rn(wt * ax));
-                            atomicAdd(&s_t[1][n], __float2int_rn(wt * ay));
-                            atomicAdd(&s_t[2][n], __float2int_rn(wt * az));
-                            atomicAdd(&s_t[3][n], __float2int_rn(wt * ms));
-                        }
-            } else {
-                // drifted since the last sort (or a non-finite stress): bounds-checked global path
-                atomicAdd((unsigned long long*)&w.counters[CNT_FALLBACK], 1ull);
-#pragma unroll 1
-                for (int i = 0; i < 3; ++i)
-#pragma unroll 1
-                    for (int j = 0; j < 3; ++j)
-#pragma unroll 1
-                        for (int k = 0; k < 3; ++k) {
-                            const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
-                            if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                                set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
-                                continue;
-                            }
-                            const float wt = wx[i] * wy[j] * wz[k];
-                            const float ax = q[0] + (A[0] * i + A[1] * j + A[2] * k);
-                            const float ay = q[1] + (A[3] * i + A[4] * j + A[5] * k);
-                            const float az = q[2] + (A[6] * i + A[7] * j + A[8] * k);
-                            atomicAdd(&w.mm[node_addr(I, gx, gy, gz)], make_float4(wt * ax, wt * ay, wt * az, wt * mass));
-                            mark_block(w, ch.x, I, gx >> 2, gy >> 2, gz >> 2);
-                        }
+                for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
+                particle_update(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w.counters);
             }
         }
-        __syncthreads();
-        // ---- phase 3: flush non-empty tile nodes, one 16-byte reduction each
-        const float iq = 1.f / sq, im = 1.f / sm;
-        for (int n = threadIdx.x; n < TN; n += P) {
-            const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
-            const int t = tidx(tx, ty, tz);
-            const int mi = s_t[3][t];
-            if (mi != 0) {
-                const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
-                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                    set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
-                    continue;
-                }
-                atomicAdd(&w.mm[node_addr(I, gx, gy, gz)],
-                          make_float4((float)s_t[0][t] * iq, (float)s_t[1][t] * iq, (float)s_t[2][t] * iq, (float)mi * im));
-                const int bit = ((gx >> 2) - bc.bx + 1) * 9 + ((gy >> 2) - bc.by + 1) * 3 + ((gz >> 2) - bc.bz + 1);
-                atomicOr(&s_mask, 1u << bit);
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x < 27 && ((s_mask >> threadIdx.x) & 1u)) {
-            const int t = threadIdx.x;
-            mark_block(w, ch.x, I, bc.bx + t / 9 - 1, bc.by + (t / 3) % 3 - 1, bc.bz + t % 3 - 1);
-        }
-        __syncthreads();
+        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w);
     }
 }
 
@@ -704,107 +932,16 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
         w.mm[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ln == 0) w.flag[I.blk_base + e.y] = 0u;
     }
-}
-
-// ---------------------------------------------------------------- g2p
-
-template <int P>
-__global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
-    __shared__ float4 s_v[TN];
-    Ws& w = a.w;
-    const int n_chunks = (int)w.counters[CNT_CHUNKS];
-    const int64_t st = a.par.state_stride;
-    float* __restrict__ S = a.par.state;
-    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[CNT_ACTIVE] = 0u;  // grid op is done with it
-    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
-        const int4 ch = w.chunks[ci];
-        const mpm_instance& I = a.inst[ch.x];
-        const BlockCoord bc = block_coord(ch.y, I);
-        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        for (int n = threadIdx.x; n < TN; n += P) {
-            const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
-            const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
-            float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (gx >= 0 && gy >= 0 && gz >= 0 && gx < I.res[0] && gy < I.res[1] && gz < I.res[2])
-                val = w.gv[node_addr(I, gx, gy, gz)];
-            s_v[n] = val;
+    // the last CTA to finish resets the active-block count for the next p2g (every CTA has
+    // read it by then); no CTA waits on another
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&w.counters[CNT_DONE], 1u) == gridDim.x - 1) {
+            w.counters[CNT_ACTIVE] = 0u;
+            w.counters[CNT_DONE] = 0u;
+            __threadfence();
         }
-        __syncthreads();
-        const int p = ch.z + threadIdx.x;
-        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
-            float x[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (finite3(x[0], x[1], x[2])) {
-                float fx[3], wx[3], wy[3], wz[3];
-                int base[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const float xi = x[d] * I.inv_dx;
-                    const float bf = floorf(xi - 0.5f);
-                    base[d] = (int)fminf(fmaxf(bf, -1e8f), 1e8f) - I.lower_cell[d];
-                    fx[d] = xi - bf;
-                }
-                bspline(fx[0], wx);
-                bspline(fx[1], wy);
-                bspline(fx[2], wz);
-                float nv[3] = {0.f, 0.f, 0.f};
-                float nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
-                const bool in_tile = lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3;
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            float4 gvv;
-                            if (in_tile) {
-                                gvv = s_v[((lx + i) * TILE + (ly + j)) * TILE + (lz + k)];
-                            } else {
-                                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
-                                if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                                    set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
-                                    continue;
-                                }
-                                gvv = w.gv[node_addr(I, gx, gy, gz)];
-                            }
-                            const float wt = wx[i] * wy[j] * wz[k];
-                            const float d0 = (float)i - fx[0], d1 = (float)j - fx[1], d2 = (float)k - fx[2];
-                            nv[0] += wt * gvv.x;
-                            nv[1] += wt * gvv.y;
-                            nv[2] += wt * gvv.z;
-                            const float cw = I.c_scale * wt;
-                            nC[0] += cw * gvv.x * d0;
-                            nC[1] += cw * gvv.x * d1;
-                            nC[2] += cw * gvv.x * d2;
-                            nC[3] += cw * gvv.y * d0;
-                            nC[4] += cw * gvv.y * d1;
-                            nC[5] += cw * gvv.y * d2;
-                            nC[6] += cw * gvv.z * d0;
-                            nC[7] += cw * gvv.z * d1;
-                            nC[8] += cw * gvv.z * d2;
-                        }
-                float nx[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    nx[d] = x[d] + I.dt * nv[d];
-                    nv[d] = bc_vel(nx[d], nv[d], I.bnd_lo[d], I.bnd_hi[d]);
-                    nx[d] = fmaxf(fminf(nx[d], I.bnd_hi[d]), I.bnd_lo[d]);
-                }
-                if (!finite3(nx[0], nx[1], nx[2])) set_status(w.counters, MPM_STATUS_NAN);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    S[(MPM_CH_X + d) * st + p] = nx[d];
-                    S[(MPM_CH_V + d) * st + p] = nv[d];
-                }
-#pragma unroll
-                for (int k = 0; k < 9; ++k) S[(MPM_CH_C + k) * st + p] = nC[k];
-            } else {
-                set_status(w.counters, MPM_STATUS_NAN);
-            }
-        }
-        __syncthreads();
     }
 }
 
@@ -891,6 +1028,7 @@ struct DevInfo {
     int sms = 0;
     int occ_p2g[3] = {0, 0, 0};
     int occ_g2p[3] = {0, 0, 0};
+    int occ_g2p2g[3] = {0, 0, 0};
     int occ_grid = 0;
 };
 
@@ -918,6 +1056,9 @@ static const DevInfo* dev_info() {
         d.occ_g2p[0] = occ_of<128>(k_g2p<128>);
         d.occ_g2p[1] = occ_of<256>(k_g2p<256>);
         d.occ_g2p[2] = occ_of<512>(k_g2p<512>);
+        d.occ_g2p2g[0] = occ_of<128>(k_g2p2g<128>);
+        d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256>);
+        d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512>);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op, 256, 0);
         d.occ_grid = n > 0 ? n : 1;
@@ -1022,6 +1163,23 @@ static int launch_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_partic
     return cuda_ok();
 }
 
+static int launch_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws,
+                        cudaStream_t s) {
+    const DevInfo* d = dev_info();
+    if (!d) return MPM_E_CUDA;
+    P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
+    const int pi = p_index(prob->chunk_particles);
+    const int ctas = persistent_ctas(prob, d->occ_g2p2g[pi]);
+    switch (prob->chunk_particles) {
+        case 128: k_g2p2g<128><<<ctas, 128, 0, s>>>(a); break;
+        case 256: k_g2p2g<256><<<ctas, 256, 0, s>>>(a); break;
+        case 512: k_g2p2g<512><<<ctas, 512, 0, s>>>(a); break;
+    }
+    if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
+        k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);
+    return cuda_ok();
+}
+
 }  // namespace gbm
 
 using namespace gbm;
@@ -1105,18 +1263,37 @@ int mpm_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, 
     return launch_g2p(prob, tab, par, workspace, (cudaStream_t)stream);
 }
 
+// n substeps.  The first substep starts with p2g; between substeps the g2p of substep i
+// and the p2g of substep i+1 run fused (k_g2p2g) unless a re-sort falls between them, in
+// which case g2p, sort and p2g run separately; the last substep ends with g2p, so x, v, C,
+// F, Jp are all materialised when the call returns.
 static int substeps_impl(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, int32_t n,
                          int32_t sort_interval, int64_t first, cudaStream_t s) {
-    for (int32_t i = 0; i < n; ++i) {
-        int rc;
-        if (sort_interval > 0 && ((first + i) % sort_interval) == 0) {
+    if (n <= 0) return MPM_OK;
+    int rc;
+    auto sort_due = [&](int32_t i) { return sort_interval > 0 && ((first + i) % sort_interval) == 0; };
+    if (sort_due(0) && (rc = launch_sort(prob, tab, par, ws, s))) return rc;
+    if ((rc = launch_p2g(prob, tab, par, ws, s))) return rc;
+    if ((rc = launch_grid_op(prob, tab, ws, s))) return rc;
+    for (int32_t i = 1; i < n; ++i) {
+        if (sort_due(i)) {
+            if ((rc = launch_g2p(prob, tab, par, ws, s))) return rc;
             if ((rc = launch_sort(prob, tab, par, ws, s))) return rc;
+            if ((rc = launch_p2g(prob, tab, par, ws, s))) return rc;
+        } else {
+            if ((rc = launch_g2p2g(prob, tab, par, ws, s))) return rc;
         }
-        if ((rc = launch_p2g(prob, tab, par, ws, s))) return rc;
         if ((rc = launch_grid_op(prob, tab, ws, s))) return rc;
-        if ((rc = launch_g2p(prob, tab, par, ws, s))) return rc;
     }
-    return MPM_OK;
+    return launch_g2p(prob, tab, par, ws, s);
+}
+
+int mpm_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !workspace) return MPM_E_INVALID;
+    return launch_g2p2g(prob, tab, par, workspace, (cudaStream_t)stream);
 }
 
 int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,

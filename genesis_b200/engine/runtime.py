@@ -85,7 +85,7 @@ class MPMRuntime:
         specs: list[InstanceSpec],
         device=None,
         chunk_particles: int = 256,
-        sort_interval: int = 16,
+        sort_interval: int = 50,
         per_particle_lame: bool = False,
         grid_ctas: int = 0,
         use_graphs: bool = True,
@@ -326,6 +326,10 @@ class MPMRuntime:
 
     def g2p(self):
         self._call("mpm_g2p", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                   _cuda_stream_handle())
+
+    def g2p2g(self):
+        self._call("mpm_g2p2g", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
                    _cuda_stream_handle())
 
     def ensure_sorted(self):

@@ -103,7 +103,7 @@ class B200Options(Options):
                      'never' (call scene.check_state() yourself)
     """
 
-    sort_interval: int = 16
+    sort_interval: int = 50
     chunk_particles: int = 256
     use_cuda_graph: bool = True
     check_nan: str = "step"

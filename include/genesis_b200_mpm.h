@@ -197,6 +197,13 @@ int mpm_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* workspace,
 int mpm_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
             void* stream);
 
+/* g2p of one substep fused with p2g of the next: gathers v, C from the grid velocity of
+ * the last grid op, moves x, then updates F/Jp and scatters mass and momentum for the
+ * next grid op.  v and C stay in registers (not stored); a later mpm_g2p stores them.
+ * Equivalent to mpm_g2p followed by mpm_p2g. */
+int mpm_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+              void* stream);
+
 /* n_substeps x (p2g, grid_op, g2p); re-sorts before substep i when
  * sort_interval > 0 and (first_substep + i) % sort_interval == 0. */
 int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
