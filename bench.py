@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--substeps-per-step", type=int, default=100)
     ap.add_argument("--sort-interval", type=int, default=50)
-    ap.add_argument("--chunk", type=int, default=256)
+    ap.add_argument("--chunk", type=int, default=128)
     ap.add_argument("--n-side", type=int, default=50, help="particles per box edge (50 -> 500k)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -84,7 +84,7 @@ class MPMRuntime:
         self,
         specs: list[InstanceSpec],
         device=None,
-        chunk_particles: int = 256,
+        chunk_particles: int = 128,
         sort_interval: int = 50,
         per_particle_lame: bool = False,
         grid_ctas: int = 0,
@@ -100,6 +100,7 @@ class MPMRuntime:
         self._graphs: dict = {}
         self._count = 0  # substeps executed
         self._nonfree = False
+        self._dirty = False  # positions written since the last sort
 
         insts, mats = [], []
         p_begin = 0
@@ -225,6 +226,7 @@ class MPMRuntime:
             self.gid[:n].copy_(torch.arange(n, dtype=torch.int32))
             self.slot[:n].copy_(torch.arange(n, dtype=torch.int32))
         self._count = 0
+        self._dirty = True
 
     def set_lame(self, mu, lam):
         """Per-particle Lame parameters in API order (requires per_particle_lame=True)."""
@@ -275,6 +277,8 @@ class MPMRuntime:
             return t.data_ptr()
 
         n = self.n
+        if pos is not None:
+            self._dirty = True
         self._call(
             "mpm_set_state", C.byref(self.prob), C.byref(self.par),
             dptr(pos, torch.float32, (n, 3)), dptr(vel, torch.float32, (n, 3)),
@@ -296,6 +300,7 @@ class MPMRuntime:
         return idx, vals
 
     def set_particles_pos(self, idx, pos):
+        self._dirty = True
         return self._idx_call("mpm_set_particles_pos", idx, pos, torch.float32, (3,), with_tables=True)
 
     def set_particles_vel(self, idx, vel):
@@ -333,9 +338,13 @@ class MPMRuntime:
                    _cuda_stream_handle())
 
     def ensure_sorted(self):
-        if self._count % max(self.sort_interval, 1) == 0 or not getattr(self, "_sorted_once", False):
+        """Re-bin before a p2g that starts a sort interval, the first one, or one after
+        positions were overwritten (particles far from their bins would all take the
+        slow out-of-tile path)."""
+        if self._count % max(self.sort_interval, 1) == 0 or not getattr(self, "_sorted_once", False) or self._dirty:
             self.sort()
             self._sorted_once = True
+            self._dirty = False
 
     def substeps(self, n: int):
         """Advance n substeps (p2g, grid op, g2p), re-sorting every sort_interval."""
@@ -343,10 +352,11 @@ class MPMRuntime:
         n = int(n)
         stream = _cuda_stream_handle()
         while n > 0:
-            if not getattr(self, "_sorted_once", False):
+            phase = self._count % K
+            if not getattr(self, "_sorted_once", False) or (self._dirty and phase != 0):
                 self.sort()
                 self._sorted_once = True
-            phase = self._count % K
+            self._dirty = False
             if self.use_graphs and phase == 0 and n >= K:
                 g = self._graph(K)
                 self._call("mpm_graph_launch", g, stream)

@@ -104,7 +104,7 @@ class B200Options(Options):
     """
 
     sort_interval: int = 50
-    chunk_particles: int = 256
+    chunk_particles: int = 128
     use_cuda_graph: bool = True
     check_nan: str = "step"
     grid_ctas: int = 0
