@@ -33,6 +33,8 @@ ERROR_NAMES = {
 MPM_STATUS_NAN = 1
 MPM_STATUS_OUT_OF_GRID = 2
 
+NOALLOC_SCRATCH_BYTES = 32 << 20
+
 MPM_STATE_CH = 25
 CH_X, CH_V, CH_C, CH_F, CH_JP = 0, 3, 6, 15, 24
 MPM_BLOCK = 4
@@ -143,6 +145,7 @@ SIGNATURES = {
     "mpm_g2p": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
     "mpm_g2p2g": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
     "mpm_substeps": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp]),
+    "mpm_substeps_noalloc": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, i64, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),
     "mpm_get_state": (C.c_int, [_P(Problem), _P(Particles), vp, vp, vp, vp, vp, vp, vp]),

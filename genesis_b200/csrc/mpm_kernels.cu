@@ -1305,6 +1305,55 @@ int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* 
     return substeps_impl(prob, tab, par, workspace, n_substeps, sort_interval, first_substep, (cudaStream_t)stream);
 }
 
+// ---------------------------------------------------------------- allocation-free variant
+// Scratch for mpm_substeps_noalloc.  It lives in the module's static device memory, so a
+// caller that may not allocate (a plugin host that forbids cudaMalloc, a pre-reserved
+// memory pool, code running inside another runtime's allocator) still gets the full
+// substep.  Every GPU that loads this library holds these bytes until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MPM_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[64];
+
+// Device address of the scratch array on the current device.  In host code the array's
+// name is only a host-side stand-in, so the address must come from cudaGetSymbolAddress,
+// asked once per device with that device current.
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MPM_E_CUDA;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return MPM_E_CUDA;
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return MPM_OK;
+}
+
+int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, int32_t n_substeps,
+                         int32_t sort_interval, int64_t first_substep, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || n_substeps < 0) return MPM_E_INVALID;
+    const uint64_t need = layout_of(*prob).total;
+    if (need > (uint64_t)MPM_NOALLOC_SCRATCH_BYTES) return MPM_E_CAPACITY;
+    void* ws = nullptr;
+    if ((rc = noalloc_scratch(&ws))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    // the array keeps the previous call's contents (possibly another problem's layout):
+    // start from the zeroed state mpm_workspace_init gives, then bin the particles
+    if (cudaMemsetAsync(ws, 0, need, s) != cudaSuccess) return MPM_E_CUDA;
+    if (n_substeps == 0) return MPM_OK;
+    const bool sorts_first = sort_interval > 0 && (first_substep % sort_interval) == 0;
+    if (!sorts_first && (rc = launch_sort(prob, tab, par, ws, s))) return rc;
+    return substeps_impl(prob, tab, par, ws, n_substeps, sort_interval, first_substep, s);
+}
+
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream) {
     int rc = check_problem(prob);
     if (rc) return rc;

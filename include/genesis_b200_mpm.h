@@ -209,6 +209,24 @@ int mpm_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par
 int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
                  int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
 
+/* Allocation-free mpm_substeps, for callers that cannot allocate device memory: host
+ * applications whose own allocator reserves the GPU's memory up front (game engines and
+ * simulators that run from a fixed pool), and plugin hosts that forbid their plugins to
+ * call cudaMalloc.  The caller still passes the particle buffers and tables; the
+ * workspace of mpm_workspace_bytes() is instead a static device array of
+ * MPM_NOALLOC_SCRATCH_BYTES (32 MiB) compiled into this library, which every GPU that
+ * loads the library holds until the process exits.  Problems whose workspace exceeds it
+ * return MPM_E_CAPACITY (a 65^3 grid with 100k particles needs ~22 MiB).  The first call
+ * on a device does a one-time set-up: it looks the array's device address up
+ * (cudaGetSymbolAddress) with that device current; that first call should come before
+ * any stream capture.  Each call clears the bytes it uses and re-bins the particles, so
+ * its results match mpm_substeps; all calls share the one array, so calls that overlap
+ * on the GPU (other streams, other threads) race and must be serialised by the caller.
+ * No counterpart in the reference. */
+#define MPM_NOALLOC_SCRATCH_BYTES (32u << 20)
+int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par,
+                         int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
+
 /* Read (and optionally clear) the device status word; synchronises the stream. */
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
 
