@@ -317,6 +317,34 @@ class MPMRuntime:
             self._drop_graphs()
         return keep
 
+    def retune(self, chunk_particles=None, sort_interval=None, grid_ctas=None):
+        """Change the launch configuration between substeps (the particle state is kept;
+        the workspace is re-laid-out and the particles re-binned)."""
+        if chunk_particles is not None and int(chunk_particles) != self.prob.chunk_particles:
+            P = int(chunk_particles)
+            mc = C.c_int32()
+            nat.check("mpm_max_chunks", self.lib.mpm_max_chunks(self.n, self.n_blocks, P, C.byref(mc)))
+            self.prob.chunk_particles = P
+            self.prob.max_chunks = mc.value
+            nbytes = C.c_uint64()
+            nat.check("mpm_workspace_bytes", self.lib.mpm_workspace_bytes(C.byref(self.prob), C.byref(nbytes)))
+            if int(nbytes.value) > self.workspace.numel():
+                self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+                self._ws = C.c_void_p(self.workspace.data_ptr())
+            self.workspace_bytes = int(nbytes.value)
+            self._call("mpm_workspace_init", C.byref(self.prob), self._ws, _cuda_stream_handle())
+            self._sorted_once = False
+        if sort_interval is not None:
+            self.sort_interval = int(sort_interval)
+        if grid_ctas is not None:
+            self.prob.grid_ctas = int(grid_ctas)
+        self._drop_graphs()
+
+    @property
+    def config(self) -> dict:
+        return {"chunk_particles": int(self.prob.chunk_particles), "sort_interval": int(self.sort_interval),
+                "grid_ctas": int(self.prob.grid_ctas)}
+
     # ---------------------------------------------------------------- stepping
     def sort(self):
         self._call("mpm_sort_particles", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,

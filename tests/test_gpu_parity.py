@@ -269,3 +269,34 @@ def test_full_size_mixed_500k_conservation():
     assert np.all(np.isfinite(s["pos"]))
     assert np.all(s["pos"] >= sp.bnd_lo.astype(np.float32)) and np.all(s["pos"] <= sp.bnd_hi.astype(np.float32))
     assert rt.status() == 0
+
+
+def test_retune_and_autotune_preserve_the_simulation():
+    from genesis_b200 import autotune
+
+    d = W.mixed_500k(n_side=10)
+    a = _rt([d], use_graphs=False)
+    b = _rt([d], use_graphs=False)
+    best, times = autotune.tune(b, candidates={"chunk_particles": (128, 256), "sort_interval": (10, 20)},
+                                trial_substeps=20, use_cache=False)
+    assert set(best) == {"chunk_particles", "sort_interval", "grid_ctas"} and len(times) == 4
+    assert np.array_equal(_state_np(a)["pos"], _state_np(b)["pos"])  # trials were rolled back
+    a.substeps(30)
+    b.substeps(30)
+    assert np.abs(_state_np(a)["pos"] - _state_np(b)["pos"]).max() < 1e-6
+
+
+def test_batched_many_small_scenes_faster_than_sequential():
+    from genesis_b200.batch import BatchedScenes, run_sequential
+
+    descs = W.batch_scenes(n_scenes=24, n_range=(2e3, 5e3), densities=(32,))
+    bs = BatchedScenes(descs, tune=False)
+    bs.substeps(bs.rt.sort_interval)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    bs.substeps(100)
+    b.record()
+    torch.cuda.synchronize()
+    t_batched = a.elapsed_time(b) * 1e-3
+    t_seq = run_sequential(descs, 100)
+    assert t_seq > 2.0 * t_batched, (t_seq, t_batched)
