@@ -932,15 +932,14 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
         w.mm[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ln == 0) w.flag[I.blk_base + e.y] = 0u;
     }
-    // the last CTA to finish resets the active-block count for the next p2g (every CTA has
-    // read it by then); no CTA waits on another
+    // the last CTA to finish resets the active-block count for the next p2g: every CTA read
+    // the count into registers before this barrier, so no fence is needed; no CTA waits on
+    // another
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
         if (atomicAdd(&w.counters[CNT_DONE], 1u) == gridDim.x - 1) {
             w.counters[CNT_ACTIVE] = 0u;
             w.counters[CNT_DONE] = 0u;
-            __threadfence();
         }
     }
 }
