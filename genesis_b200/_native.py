@@ -32,6 +32,7 @@ ERROR_NAMES = {
 
 MPM_STATUS_NAN = 1
 MPM_STATUS_OUT_OF_GRID = 2
+MPM_STATUS_NONFINITE_VEL = 4
 
 NOALLOC_SCRATCH_BYTES = 32 << 20
 
@@ -148,6 +149,7 @@ SIGNATURES = {
     "mpm_substeps_noalloc": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, i64, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),
+    "mpm_instance_status": (C.c_int, [_P(Problem), vp, i32, vp, vp]),
     "mpm_get_state": (C.c_int, [_P(Problem), _P(Particles), vp, vp, vp, vp, vp, vp, vp]),
     "mpm_set_state": (C.c_int, [_P(Problem), _P(Particles), vp, vp, vp, vp, vp, vp, vp]),
     "mpm_set_particles_pos": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, vp, vp, vp]),

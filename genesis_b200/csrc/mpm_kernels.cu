@@ -74,13 +74,14 @@ struct Ws {
     float* mu_tmp;
     float* lam_tmp;
     uint32_t* counters;
+    uint32_t* inst_status;  // per instance status bits
     int64_t tmp_stride;
 };
 
 static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
-    uint64_t off[18];
+    uint64_t off[19];
     uint64_t total;
 };
 
@@ -90,7 +91,7 @@ static Layout layout_of(const mpm_problem& p) {
     const uint64_t n = (uint64_t)p.n_particles;
     const uint64_t ntiles = (nb + SCAN_TILE - 1) / SCAN_TILE;
     const uint64_t stride = align_up(n > 0 ? n : 1, 64);
-    uint64_t sizes[18] = {
+    uint64_t sizes[19] = {
         nb * BLK3 * 16,            // mm
         nb * BLK3 * 16,            // gv
         nb * 4,                    // flag
@@ -109,9 +110,10 @@ static Layout layout_of(const mpm_problem& p) {
         n * 4,                     // mu_tmp
         n * 4,                     // lam_tmp
         N_COUNTERS * 4,            // counters
+        (uint64_t)p.n_instances * 4,  // per-instance status
     };
     uint64_t o = 0;
-    for (int i = 0; i < 18; ++i) {
+    for (int i = 0; i < 19; ++i) {
         L.off[i] = o;
         o = align_up(o + (sizes[i] ? sizes[i] : 1), 256);
     }
@@ -141,6 +143,7 @@ static Ws ws_of(const mpm_problem& p, void* base) {
     w.mu_tmp = (float*)(b + L.off[15]);
     w.lam_tmp = (float*)(b + L.off[16]);
     w.counters = (uint32_t*)(b + L.off[17]);
+    w.inst_status = (uint32_t*)(b + L.off[18]);
     w.tmp_stride = (int64_t)align_up(p.n_particles > 0 ? p.n_particles : 1, 64);
     return w;
 }
@@ -165,8 +168,11 @@ __device__ __forceinline__ int find_instance_by_block(const mpm_instance* inst, 
     return lo;
 }
 
-__device__ __forceinline__ void set_status(uint32_t* counters, uint32_t bit) {
-    atomicOr(&counters[CNT_STATUS], bit);
+// status bits: one word for the whole problem and one per instance (so a served request
+// that went NaN can be evicted without touching the others)
+__device__ __forceinline__ void set_status(const Ws& w, int inst, uint32_t bit) {
+    atomicOr(&w.counters[CNT_STATUS], bit);
+    atomicOr(&w.inst_status[inst], bit);
 }
 
 // quadratic B-spline weights (mpm_solver.py:350, 397)
@@ -496,7 +502,8 @@ __device__ __forceinline__ bool tile_contains(const int* base, int ox, int oy, i
 // for position x.
 __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm_material* __restrict__ mats,
                                                 const mpm_particles& par, int p, const float* x, const float* v,
-                                                const float* C, int ox, int oy, int oz, Payload& o, uint32_t* counters) {
+                                                const float* C, int ox, int oy, int oz, Payload& o, const Ws& w,
+                                                int inst) {
     const int64_t st = par.state_stride;
     float* __restrict__ S = par.state;
     float F[9];
@@ -551,7 +558,7 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
         for (int k = 0; k < 9; ++k) o.A[k] = A[k] * dx;
         o.in_tile = tile_contains(o.base, ox, oy, oz) && isfinite(o.bq);
     } else {
-        set_status(counters, MPM_STATUS_NAN);
+        set_status(w, inst, MPM_STATUS_NAN);
     }
 }
 
@@ -632,7 +639,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
                     for (int k = 0; k < 3; ++k) {
                         const int gx = o.base[0] + i, gy = o.base[1] + j, gz = o.base[2] + k;
                         if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                            set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                            set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
                             continue;
                         }
                         const float wt = sel3(wx, i) * sel3(wy, j) * sel3(wz, k);
@@ -654,7 +661,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
         if (mi != 0) {
             const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
             if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
                 continue;
             }
             atomicAdd(&w.mm[node_addr(I, gx, gy, gz)],
@@ -686,10 +693,10 @@ __device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const mp
 // g2p gather (mpm_solver.py:396-431): v = sum w v_i, C = 4 inv_dx sum w v_i (off - fx)^T;
 // then x += dt v and the boundary (mpm_solver.py:434-437).  Returns false if nothing
 // could be gathered (non-finite x).
-__device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm_instance& I, float* x, float* nv,
-                                       float* nC, int ox, int oy, int oz) {
+__device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm_instance& I, int inst, float* x,
+                                       float* nv, float* nC, int ox, int oy, int oz) {
     if (!finite3(x[0], x[1], x[2])) {
-        set_status(w.counters, MPM_STATUS_NAN);
+        set_status(w, inst, MPM_STATUS_NAN);
         return false;
     }
     float fx[3], wx[3], wy[3], wz[3];
@@ -735,7 +742,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
                 for (int k = 0; k < 3; ++k) {
                     const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
                     if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
-                        set_status(w.counters, MPM_STATUS_OUT_OF_GRID);
+                        set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
                         continue;
                     }
                     const float4 g = w.gv[node_addr(I, gx, gy, gz)];
@@ -756,13 +763,17 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
                     nC[8] += cw * g.z * d2;
                 }
     }
+    // a non-finite velocity is flagged separately: the boundary clamp (fminf/fmaxf, like
+    // ti.min/ti.max) maps a NaN position back onto the wall, so the reference's
+    // position-only check would not see it
+    if (!finite3(nv[0], nv[1], nv[2])) set_status(w, inst, MPM_STATUS_NONFINITE_VEL);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const float nx = x[d] + I.dt * nv[d];
         nv[d] = bc_vel(nx, nv[d], I.bnd_lo[d], I.bnd_hi[d]);
         x[d] = fmaxf(fminf(nx, I.bnd_hi[d]), I.bnd_lo[d]);
     }
-    if (!finite3(x[0], x[1], x[2])) set_status(w.counters, MPM_STATUS_NAN);
+    if (!finite3(x[0], x[1], x[2])) set_status(w, inst, MPM_STATUS_NAN);
     return true;
 }
 
@@ -794,7 +805,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
             }
 #pragma unroll
             for (int k = 0; k < 9; ++k) C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
-            particle_update(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w.counters);
+            particle_update(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x);
         }
         scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w);
     }
@@ -821,7 +832,7 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
             float x[3], nv[3], nC[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather(VT, w, I, x, nv, nC, ox, oy, oz)) {
+            if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     S[(MPM_CH_X + d) * st + p] = x[d];
@@ -863,10 +874,10 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
             float x[3], nv[3], nC[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather(VT, w, I, x, nv, nC, ox, oy, oz)) {
+            if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
-                particle_update(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w.counters);
+                particle_update(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x);
             }
         }
         scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w);
@@ -1364,6 +1375,19 @@ int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t
     if (cudaStreamSynchronize(s) != cudaSuccess) return MPM_E_CUDA;
     if (clear && cudaMemsetAsync(&w.counters[CNT_STATUS], 0, 4, s) != cudaSuccess) return MPM_E_CUDA;
     *out = v;
+    return MPM_OK;
+}
+
+int mpm_instance_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!workspace || !out) return MPM_E_INVALID;
+    Ws w = ws_of(*prob, workspace);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = (size_t)prob->n_instances * 4;
+    if (cudaMemcpyAsync(out, w.inst_status, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPM_E_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPM_E_CUDA;
+    if (clear && cudaMemsetAsync(w.inst_status, 0, bytes, s) != cudaSuccess) return MPM_E_CUDA;
     return MPM_OK;
 }
 

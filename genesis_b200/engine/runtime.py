@@ -422,6 +422,46 @@ class MPMRuntime:
         self._call("mpm_status", C.byref(self.prob), self._ws, int(clear), C.byref(v), _cuda_stream_handle())
         return int(v.value)
 
+    def instance_status(self, clear: bool = False) -> np.ndarray:
+        out = np.zeros(len(self._insts), dtype=np.uint32)
+        self._call("mpm_instance_status", C.byref(self.prob), self._ws, int(clear),
+                   out.ctypes.data_as(C.c_void_p), _cuda_stream_handle())
+        return out
+
+    def load_state(self, pos, vel, C_, F, Jp, active, mat):
+        """Overwrite the whole particle state from device tensors in API order
+        (pos/vel [n,3], C/F [n,9] or [n,3,3], Jp [n], active [n] bool, mat [n] uint8) and
+        reset the slot permutation to the identity; the next substep re-bins."""
+        n = self.n
+        with torch.no_grad():
+            self.gid[:n].copy_(torch.arange(n, dtype=torch.int32, device=self.device))
+            self.slot[:n].copy_(self.gid[:n])
+            self.state[0:3, :n].copy_(pos.reshape(n, 3).t())
+            self.state[3:6, :n].copy_(vel.reshape(n, 3).t())
+            self.state[6:15, :n].copy_(C_.reshape(n, 9).t())
+            self.state[15:24, :n].copy_(F.reshape(n, 9).t())
+            self.state[24, :n].copy_(Jp.reshape(n))
+            self.mat[:n].copy_(mat.reshape(n).to(torch.uint8))
+            act = active.reshape(n).to(torch.bool)
+            self.pflags[:n].copy_(torch.where(act, nat.PFLAG_ACTIVE | nat.PFLAG_FREE, nat.PFLAG_FREE).to(torch.uint8))
+        self._dirty = True
+        self._sorted_once = False
+
+    def export_instances(self):
+        """Per-instance state in API order as device tensors (for repacking): a list of dicts
+        with pos, vel, C, F, Jp, active, mat."""
+        st = self.get_state()
+        n = self.n
+        mat = torch.empty(n, dtype=torch.uint8, device=self.device)
+        mat[self.gid[:n].long()] = self.mat[:n]
+        out = []
+        for I in self._insts:
+            sl = slice(int(I.p_begin), int(I.p_begin) + int(I.p_count))
+            d = {k: v[sl] for k, v in st.items()}
+            d["mat"] = mat[sl]
+            out.append(d)
+        return out
+
     def fallback_count(self, clear: bool = False) -> int:
         v = C.c_uint64()
         self._call("mpm_fallback_count", C.byref(self.prob), self._ws, int(clear), C.byref(v), _cuda_stream_handle())

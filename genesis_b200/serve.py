@@ -1,0 +1,253 @@
+"""Serving: continuous batching of MPM rollout requests on one GPU.
+
+Requests (a scene plus a number of substeps) arrive over time.  The server keeps every
+admitted rollout's particle state resident in HBM, admits queued requests as soon as
+slots and the memory budget allow, and advances all admitted rollouts together in the
+batched kernels (one instance per rollout), a tick of at most ``tick_substeps`` substeps
+at a time.  Between ticks finished rollouts are read back and retired, rollouts whose
+instance status shows NaN are evicted with an error, newly admitted ones are packed in,
+and the particle state of the continuing ones is carried over device to device.
+A request's result does not depend on what it shares the GPU with: instances never
+share grid memory or work items.  There is no counterpart in the reference.
+"""
+
+from __future__ import annotations
+
+import collections
+import dataclasses
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from . import workloads as W
+from .engine.runtime import MPMRuntime, spec_from_desc
+from .materials import MPM
+
+
+def estimate_bytes(desc, chunk_particles: int = 128) -> int:
+    """HBM a request holds while admitted: particle state and ids, plus its share of the
+    workspace (grids, bins, chunk table, permutation scratch)."""
+    n = desc.n_particles
+    res = desc.grid_res
+    nblk = (res + nat.MPM_BLOCK - 1) // nat.MPM_BLOCK
+    blocks = nblk**3
+    per_particle = 25 * 4 + 10 + (8 + 25 * 4 + 14)  # state+ids, sort keys/ranks + permutation scratch
+    per_block = nat.MPM_BLOCK**3 * 32 + 24  # two float4 grids + flags/active/bins
+    chunks = (n // chunk_particles + min(n, blocks) + 1) * 16
+    return int(n * per_particle + blocks * per_block + chunks)
+
+
+@dataclasses.dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float | None = None
+    finished: float | None = None
+    pos: np.ndarray | None = None
+    vel: np.ndarray | None = None
+    error: str | None = None
+
+    @property
+    def latency(self) -> float | None:
+        return None if self.finished is None else self.finished - self.arrival
+
+
+@dataclasses.dataclass
+class _Slot:
+    req: W.Request
+    remaining: int
+    bytes: int
+    state: dict | None = None  # device tensors in API order while being repacked
+    retired: bool = False  # finished or evicted; a hole until the next repack
+
+
+class AdmissionQueue:
+    """FIFO admission against a byte budget and a slot cap (head-of-line order kept)."""
+
+    def __init__(self, budget_bytes: float, max_active: int, chunk_particles: int = 128):
+        self.budget = float(budget_bytes)
+        self.max_active = int(max_active)
+        self.chunk = chunk_particles
+        self.pending: collections.deque = collections.deque()
+        self.in_use = 0
+
+    def push(self, req) -> str | None:
+        need = estimate_bytes(req.scene, self.chunk)
+        if need > self.budget:
+            return f"request needs {need} bytes, more than the whole budget ({int(self.budget)})"
+        self.pending.append((req, need))
+        return None
+
+    def pop_admissible(self, n_active: int) -> list:
+        out = []
+        while self.pending and n_active + len(out) < self.max_active and self.in_use + self.pending[0][1] <= self.budget:
+            req, need = self.pending.popleft()
+            self.in_use += need
+            out.append((req, need))
+        return out
+
+    def release(self, need: int):
+        self.in_use -= need
+
+
+class MPMServer:
+    def __init__(self, budget_bytes: float = 150e9, tick_substeps: int = 50, max_active: int = 512,
+                 chunk_particles: int = 128, sort_interval: int = 50, keep_results: bool = True,
+                 use_graphs: bool = False):
+        self.tick = int(tick_substeps)
+        self.queue = AdmissionQueue(budget_bytes, max_active, chunk_particles)
+        self.chunk = chunk_particles
+        self.sort_interval = sort_interval
+        self.keep_results = keep_results
+        self.use_graphs = use_graphs  # runtimes are short-lived; capture would not amortise
+        self.rt: MPMRuntime | None = None
+        self.active: list[_Slot] = []
+        self.ticks = 0
+        self.repacks = 0
+        self.particle_substeps = 0
+
+    # ------------------------------------------------------------------ packing
+    def _repack(self, new_slots):
+        """Build a runtime for the live rollouts plus new_slots: continuing rollouts keep
+        their device state; retired ones (holes) are dropped."""
+        live = [s for s in self.active if not s.retired]
+        if self.rt is not None and live:
+            exported = self.rt.export_instances()
+            for slot, st in zip(self.active, exported):
+                if not slot.retired:
+                    slot.state = st
+        self.rt = None
+        self.active = live + list(new_slots)
+        if not self.active:
+            return
+        dev = torch.device("cuda")
+        specs = []
+        parts = {k: [] for k in ("pos", "vel", "C", "F", "Jp", "active", "mat")}
+        for slot in self.active:
+            d = slot.req.scene
+            mats = W.make_materials(d, MPM)
+            specs.append(spec_from_desc(d, mats))
+            if slot.state is None:  # newly admitted: upload its initial state
+                n = d.n_particles
+                djp = np.array([m.default_Jp for m in mats], dtype=np.float32)[d.mat_idx]
+                slot.state = {
+                    "pos": torch.as_tensor(d.pos, dtype=torch.float32).to(dev),
+                    "vel": torch.as_tensor(d.vel, dtype=torch.float32).to(dev),
+                    "C": torch.zeros((n, 9), dtype=torch.float32, device=dev),
+                    "F": torch.eye(3, dtype=torch.float32, device=dev).reshape(1, 9).repeat(n, 1),
+                    "Jp": torch.as_tensor(djp).to(dev),
+                    "active": torch.ones(n, dtype=torch.bool, device=dev),
+                    "mat": torch.as_tensor(d.mat_idx.astype(np.uint8)).to(dev),
+                }
+            for k in parts:
+                v = slot.state[k]
+                parts[k].append(v.reshape(v.shape[0], -1) if k in ("C", "F") else v)
+        self.rt = MPMRuntime(specs, chunk_particles=self.chunk, sort_interval=self.sort_interval,
+                             use_graphs=self.use_graphs)
+        self.rt.load_state(torch.cat(parts["pos"]), torch.cat(parts["vel"]), torch.cat(parts["C"]),
+                           torch.cat(parts["F"]), torch.cat(parts["Jp"]), torch.cat(parts["active"]),
+                           torch.cat(parts["mat"]))
+        for slot in self.active:
+            slot.state = None
+        self.repacks += 1
+
+    def _retire(self, k):
+        """Drop rollout k from the work without repacking: its particles go inactive."""
+        slot = self.active[k]
+        slot.retired = True
+        off = self.rt.instance_offsets[k]
+        n = slot.req.scene.n_particles
+        idx = torch.arange(off, off + n, dtype=torch.int32, device=self.rt.device)
+        self.rt.set_particles_active(idx, torch.zeros(n, dtype=torch.uint8, device=self.rt.device))
+        self.queue.release(slot.bytes)
+
+    # ------------------------------------------------------------------ loop
+    def serve(self, requests, realtime: bool = True, on_result=None) -> list[Result]:
+        """Run the request stream to completion.  With realtime=True a request becomes
+        visible at its arrival time (seconds after the call starts); with realtime=False
+        all requests are visible at t=0 (throughput runs)."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        results = {r.rid: Result(r.rid, r.arrival if realtime else 0.0) for r in reqs}
+        t0 = time.perf_counter()
+        clock = lambda: time.perf_counter() - t0
+        bad = nat.MPM_STATUS_NAN | nat.MPM_STATUS_NONFINITE_VEL
+        i = 0
+        n_live = lambda: sum(1 for s in self.active if not s.retired)
+        while i < len(reqs) or self.queue.pending or n_live():
+            now = clock()
+            while i < len(reqs) and (not realtime or reqs[i].arrival <= now):
+                err = self.queue.push(reqs[i])
+                if err:
+                    results[reqs[i].rid].error = err
+                    results[reqs[i].rid].finished = now
+                i += 1
+            admitted = self.queue.pop_admissible(n_live())
+            if admitted:
+                now = clock()
+                new_slots = []
+                for req, need in admitted:
+                    results[req.rid].admitted = now
+                    new_slots.append(_Slot(req, int(req.scene.n_substeps), need))
+                self._repack(new_slots)
+            if not n_live():
+                self.rt = None
+                self.active = []
+                if i < len(reqs) and realtime:
+                    time.sleep(max(0.0, min(0.05, reqs[i].arrival - clock())))
+                continue
+            T = min(self.tick, min(s.remaining for s in self.active if not s.retired))
+            self.rt.substeps(T)
+            self.ticks += 1
+            self.particle_substeps += T * sum(s.req.scene.n_particles for s in self.active if not s.retired)
+            status = self.rt.instance_status(clear=True)  # synchronises: the tick is done
+            done = []
+            for k, s in enumerate(self.active):
+                if s.retired:
+                    continue
+                s.remaining -= T
+                if s.remaining == 0 or status[k] & bad:
+                    done.append(k)
+            if done:
+                st = self.rt.get_state(("pos", "vel")) if self.keep_results else None
+                offs = self.rt.instance_offsets
+                now = clock()
+                for k in done:
+                    s = self.active[k]
+                    r = results[s.req.rid]
+                    r.finished = now
+                    if status[k] & bad:
+                        r.error = "NaN detected in MPM states"
+                    elif st is not None:
+                        sl = slice(offs[k], offs[k] + s.req.scene.n_particles)
+                        r.pos = st["pos"][sl].cpu().numpy()
+                        r.vel = st["vel"][sl].cpu().numpy()
+                    self._retire(k)
+                    if on_result is not None:
+                        on_result(r)
+        self.rt = None
+        self.active = []
+        return [results[r.rid] for r in reqs]
+
+
+def percentile(xs, q):
+    xs = sorted(x for x in xs if x is not None)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q / 100.0
+    f, c = math.floor(k), math.ceil(k)
+    return xs[f] if f == c else xs[f] + (xs[c] - xs[f]) * (k - f)
+
+
+def sequential_timeline(requests, durations):
+    """Latencies of the plain one-request-at-a-time path under the same arrivals: each
+    request starts when it has arrived and the previous one has finished."""
+    t = 0.0
+    lat = []
+    for r, d in sorted(zip(requests, durations), key=lambda x: x[0].arrival):
+        start = max(t, r.arrival)
+        t = start + d
+        lat.append(t - r.arrival)
+    return lat

@@ -56,6 +56,7 @@ extern "C" {
 /* device status word bits (mpm_status) */
 #define MPM_STATUS_NAN 1u          /* NaN/Inf in particle positions (mpm_solver.py:451-457) */
 #define MPM_STATUS_OUT_OF_GRID 2u  /* a stencil node fell outside the grid; contribution skipped */
+#define MPM_STATUS_NONFINITE_VEL 4u /* NaN/Inf in a gathered velocity (positions stay clamped) */
 
 #define MPM_STATE_CH 25
 #define MPM_CH_X 0
@@ -229,6 +230,11 @@ int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_par
 
 /* Read (and optionally clear) the device status word; synchronises the stream. */
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
+
+/* Per-instance status words (n_instances entries, same bits as mpm_status) into host
+ * memory `out`; synchronises the stream.  Instances never share grid memory, so a NaN in
+ * one instance leaves the others' results untouched and can be handled per instance. */
+int mpm_instance_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
 
 /* Number of particles handled by the out-of-tile path since the last clear (tuning aid). */
 int mpm_fallback_count(const mpm_problem* prob, void* workspace, int32_t clear, uint64_t* out,
