@@ -554,9 +554,15 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
                 fabsf(o.mass * v[i]) + 1.5f * dx * (fabsf(A[i * 3 + 0]) + fabsf(A[i * 3 + 1]) + fabsf(A[i * 3 + 2]));
             o.bq = fmaxf(o.bq, b);
         }
+        // fmaxf drops NaN, so test the payload itself: a NaN or Inf must take the float path
+        // (where it propagates into the grid as in the reference), never the fixed-point tile
+        float chk = o.q[0] + o.q[1] + o.q[2] + o.mass;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) o.A[k] = A[k] * dx;
-        o.in_tile = tile_contains(o.base, ox, oy, oz) && isfinite(o.bq);
+        for (int k = 0; k < 9; ++k) {
+            o.A[k] = A[k] * dx;
+            chk += o.A[k];
+        }
+        o.in_tile = tile_contains(o.base, ox, oy, oz) && isfinite(o.bq) && isfinite(chk);
     } else {
         set_status(w, inst, MPM_STATUS_NAN);
     }
