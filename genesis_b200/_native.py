@@ -147,6 +147,8 @@ SIGNATURES = {
     "mpm_g2p2g": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
     "mpm_substeps": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp]),
     "mpm_substeps_noalloc": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, i64, vp]),
+    "mpm_adjoint_workspace_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
+    "mpm_substep_adjoint": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),
     "mpm_instance_status": (C.c_int, [_P(Problem), vp, i32, vp, vp]),

@@ -18,6 +18,7 @@ SOURCES = [os.path.join(CSRC, "mpm_kernels.cu")]
 DEPS = SOURCES + [
     os.path.join(CSRC, "svd3.cuh"),
     os.path.join(CSRC, "constitutive.cuh"),
+    os.path.join(CSRC, "mpm_adjoint.cuh"),
     os.path.join(ROOT, "include", "genesis_b200_mpm.h"),
 ]
 OUT = os.path.join(HERE, "libgenesis_b200_mpm.so")

@@ -1038,6 +1038,8 @@ __global__ void k_set_flag(mpm_problem prob, mpm_particles par, int n, const int
     par.pflags[s] = (uint8_t)((par.pflags[s] & ~bit) | (val[i] ? bit : 0));
 }
 
+#include "mpm_adjoint.cuh"
+
 // ---------------------------------------------------------------- host side
 
 struct DevInfo {
@@ -1368,6 +1370,47 @@ int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_par
     const bool sorts_first = sort_interval > 0 && (first_substep % sort_interval) == 0;
     if (!sorts_first && (rc = launch_sort(prob, tab, par, ws, s))) return rc;
     return substeps_impl(prob, tab, par, ws, n_substeps, sort_interval, first_substep, s);
+}
+
+// ---------------------------------------------------------------- adjoint
+int mpm_adjoint_workspace_bytes(const mpm_problem* prob, uint64_t* out) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!out) return MPM_E_INVALID;
+    uint64_t off[5];
+    *out = adj_layout(*prob, off);
+    return MPM_OK;
+}
+
+int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state, float* adj,
+                        float* lame_bar, void* workspace, void* adj_workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, state))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !adj || !lame_bar || !workspace || !adj_workspace)
+        return MPM_E_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = prob->n_particles;
+    AdjWs aw = adj_ws_of(*prob, adj_workspace);
+    Ws w = ws_of(*prob, workspace);
+    // forward recompute of the substep's grid on a scratch copy (p2g writes F and Jp)
+    if (n > 0 && cudaMemcpy2DAsync(aw.state, aw.stride * 4, state->state, state->state_stride * 4, (size_t)n * 4,
+                                   MPM_STATE_CH, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return MPM_E_CUDA;
+    mpm_particles sp = *state;
+    sp.state = aw.state;
+    sp.state_stride = aw.stride;
+    if ((rc = launch_p2g(prob, tab, &sp, workspace, s))) return rc;
+    const size_t nodes = (size_t)prob->n_blocks * BLK3;
+    if (cudaMemcpyAsync(aw.saved_mm, w.mm, nodes * 16, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return MPM_E_CUDA;
+    if ((rc = launch_grid_op(prob, tab, workspace, s))) return rc;
+    if (cudaMemsetAsync(aw.vbar, 0, nodes * 16, s) != cudaSuccess) return MPM_E_CUDA;
+    if (n > 0) {
+        k_adj_g2p<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, *state, adj, w, aw);
+        k_adj_grid<<<(int)((nodes + 255) / 256), 256, 0, s>>>(*prob, tab->instances, w, aw);
+        k_adj_p2g<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, tab->materials, *state, adj, lame_bar, aw);
+    }
+    return cuda_ok();
 }
 
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream) {

@@ -375,10 +375,21 @@ class MPMRuntime:
             self._dirty = False
 
     def substeps(self, n: int):
-        """Advance n substeps (p2g, grid op, g2p), re-sorting every sort_interval."""
-        K = max(self.sort_interval, 1)
+        """Advance n substeps (p2g, grid op, g2p), re-sorting every sort_interval
+        (sort_interval <= 0: sort once, before the first substep, and never again)."""
         n = int(n)
         stream = _cuda_stream_handle()
+        if self.sort_interval <= 0:
+            if not getattr(self, "_sorted_once", False) or self._dirty:
+                self.sort()
+                self._sorted_once = True
+                self._dirty = False
+            if n > 0:
+                self._call("mpm_substeps", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                           n, 0, self._count, stream)
+                self._count += n
+            return
+        K = max(self.sort_interval, 1)
         while n > 0:
             phase = self._count % K
             if not getattr(self, "_sorted_once", False) or (self._dirty and phase != 0):

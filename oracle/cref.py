@@ -61,6 +61,7 @@ def lib(dtype):
         path = os.path.join(BUILD, "libmpm_ref_f32.so" if key == "float32" else "libmpm_ref_f64.so")
         L = C.CDLL(path)
         L.ref_substeps.restype = C.c_int
+        L.ref_substeps_lame.restype = C.c_int
         L.ref_max_threads.restype = C.c_int
         _libs[key] = L
     return _libs[key]
@@ -70,8 +71,10 @@ def max_threads() -> int:
     return int(lib(np.float64).ref_max_threads())
 
 
-def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_threads: int = 0) -> tuple[dict, int]:
-    """Run n_substeps in C on a copy of the state; returns (new_state, status)."""
+def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_threads: int = 0,
+             mu_p=None, lam_p=None) -> tuple[dict, int]:
+    """Run n_substeps in C on a copy of the state; returns (new_state, status).  mu_p/lam_p:
+    optional per-particle Lame parameters."""
     dt = np.dtype(p.dtype)
     L = lib(dt)
     Params, Mat = _structs(dt)
@@ -109,8 +112,14 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     grid = np.zeros(4 * G, dtype=dt)
     gvel = np.zeros(3 * G, dtype=dt)
     ptr = lambda a: a.ctypes.data_as(C.c_void_p)
-    rc = L.ref_substeps(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
-                        int(n_substeps), ptr(grid), ptr(gvel), int(n_threads))
+    if mu_p is not None:
+        mu_a = np.ascontiguousarray(mu_p, dtype=dt)
+        lam_a = np.ascontiguousarray(lam_p, dtype=dt)
+        rc = L.ref_substeps_lame(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
+                                 int(n_substeps), ptr(grid), ptr(gvel), int(n_threads), ptr(mu_a), ptr(lam_a))
+    else:
+        rc = L.ref_substeps(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
+                            int(n_substeps), ptr(grid), ptr(gvel), int(n_threads))
     out = dict(st)
     out.update(x=x, v=v, C=Cm.reshape(n, 3, 3), F=F.reshape(n, 3, 3), Jp=Jp)
     return out, int(rc)

@@ -286,8 +286,19 @@ static inline int64_t gidx(const ref_params* p, int i, int j, int k) {
  * mat [n] material index, active [n] (0/1).  grid: caller scratch of 4*res^3 (momentum.xyz, mass)
  * and vel 3*res^3.  Returns 0, or 1 if a stencil left the grid, 2 if a position became NaN.
  */
+int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                      int n_threads, const REAL* mu_p, const REAL* lam_p);
+
 int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F, REAL* Jp,
                  const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel, int n_threads) {
+    return ref_substeps_lame(p, mats, n, x, v, C, F, Jp, mat, active, n_substeps, grid, gvel, n_threads, NULL, NULL);
+}
+
+/* as ref_substeps, with optional per-particle Lame parameters (NULL: the material's) */
+int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                      int n_threads, const REAL* mu_p, const REAL* lam_p) {
 #ifdef _OPENMP
     if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
@@ -314,6 +325,13 @@ int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, 
             ref_svd3(Ft, U, S, V);
             REAL J = S[0] * (S[1] * S[2]);
             const ref_material* m = &mats[mat[i]];
+            ref_material mp;
+            if (mu_p) {
+                mp = *m;
+                mp.mu = mu_p[i];
+                mp.lam = lam_p[i];
+                m = &mp;
+            }
             constitutive(m, p->eps, J, Ft, U, S, V, Jp[i], Fn, &Jpn, st);
             memcpy(Fi, Fn, 9 * sizeof(REAL));
             Jp[i] = Jpn;
