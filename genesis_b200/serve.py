@@ -73,6 +73,7 @@ class AdmissionQueue:
         self.chunk = chunk_particles
         self.pending: collections.deque = collections.deque()
         self.in_use = 0
+        self.peak_in_use = 0
 
     def push(self, req) -> str | None:
         need = estimate_bytes(req.scene, self.chunk)
@@ -86,6 +87,7 @@ class AdmissionQueue:
         while self.pending and n_active + len(out) < self.max_active and self.in_use + self.pending[0][1] <= self.budget:
             req, need = self.pending.popleft()
             self.in_use += need
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
             out.append((req, need))
         return out
 

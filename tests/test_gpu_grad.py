@@ -20,7 +20,7 @@ def _grads(d, checkpoint_every):
     tgt = torch.tensor(d.meta["target"], dtype=torch.float32, device="cuda")
     loss = ((x.mean(0) - tgt) ** 2).sum()
     loss.backward()
-    return float(loss), v0.grad.cpu().numpy().astype(np.float64), E.grad.cpu().numpy().astype(np.float64)
+    return float(loss.detach()), v0.grad.cpu().numpy().astype(np.float64), E.grad.cpu().numpy().astype(np.float64)
 
 
 def test_adjoint_matches_oracle_adjoint_small():

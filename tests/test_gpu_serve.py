@@ -60,5 +60,6 @@ def test_budget_limits_concurrency_and_nan_is_isolated():
         assert res[k].error is None
         pos, _ = _alone(reqs[k].scene)
         assert np.abs(res[k].pos - pos).max() <= 1e-5, k
-    # with room for two rollouts at a time the later ones were admitted after earlier ones left
-    assert max(r.admitted for r in res) > min(r.finished for r in res if r.error is None) - 1e-9
+    # the budget was never exceeded, so some requests had to wait for others to leave
+    assert srv.queue.peak_in_use <= srv.queue.budget
+    assert max(r.admitted for r in res) > min(r.admitted for r in res)
