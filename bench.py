@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--batch-substeps", type=int, default=100)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
+    ap.add_argument("--no-grad", action="store_true", help="skip the differentiation run")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests in the Poisson stream (2000 = the full serving config)")
     ap.add_argument("--no-cpu", action="store_true")
@@ -475,14 +476,16 @@ def run_batched(args, world, rank):
     """Batching config: 256 independent scenes (N log-uniform in [2e3, 2e5], grid density
     32/64/96, material uniform over the five, E log-uniform [1e4, 1e6]) advanced together by
     one launch sequence, against the same scenes run one at a time.  Under torchrun the
-    scenes are sharded round-robin over ranks (no data-path collective)."""
+    scenes are sharded over ranks by work (genesis_b200.shard; no data-path collective)."""
     import torch
 
     from genesis_b200 import workloads as W
     from genesis_b200.batch import BatchedScenes, run_sequential
 
+    from genesis_b200 import shard
+
     all_descs = W.batch_scenes(n_scenes=args.batch_scenes, n_substeps=args.batch_substeps)
-    descs = all_descs[rank::world]
+    descs = shard.my_shard(all_descs, rank, world)
     n_total = sum(d.n_particles for d in all_descs)
     S = args.batch_substeps
     bs = BatchedScenes(descs, tune=True, tune_cache=False)
@@ -523,7 +526,7 @@ def run_served(args, world, rank, capacity):
     measured batched capacity; continuous batching under a 150 GB HBM budget.  Reports
     p50/p99 end-to-end latency (arrival -> result on the host) and throughput, beside the plain
     one-request-at-a-time path under the same arrivals.  Under torchrun each rank serves the
-    requests with rid % world == rank."""
+    requests of its work-balanced shard (genesis_b200.shard)."""
     import torch
 
     from genesis_b200 import serve
@@ -534,7 +537,9 @@ def run_served(args, world, rank, capacity):
     work = [r.scene.n_particles * r.scene.n_substeps for r in base]
     mean_work = sum(work) / len(work)
     rate = 0.8 * capacity / mean_work  # requests per second over all ranks
-    reqs = [W.Request(r.rid, r.arrival / rate, r.scene) for r in base][rank::world]
+    from genesis_b200 import shard
+
+    reqs = shard.my_shard([W.Request(r.rid, r.arrival / rate, r.scene) for r in base], rank, world)
     my_work = sum(r.scene.n_particles * r.scene.n_substeps for r in reqs)
     srv = serve.MPMServer(budget_bytes=150e9, tick_substeps=50, keep_results=False)
     torch.cuda.synchronize()
@@ -575,6 +580,46 @@ def run_served(args, world, rank, capacity):
     }
 
 
+def run_grad(args):
+    """Differentiation config: Elastic block of 20,000 particles with per-particle E, 200
+    substeps at dt 1e-4, loss |mean(x_T) - target|^2, gradients w.r.t. v0 and E through the
+    checkpointed adjoint (checkpoints every 20 substeps); device time of forward+backward."""
+    import torch
+
+    from genesis_b200 import workloads as W
+    from genesis_b200.grad import DifferentiableRollout, rollout
+
+    d = W.diff_elastic()
+    sim = DifferentiableRollout(d, checkpoint_every=20)
+    v0 = torch.tensor(d.meta["v0"], dtype=torch.float32, device="cuda", requires_grad=True)
+    E = torch.tensor(d.E_particle, dtype=torch.float32, device="cuda", requires_grad=True)
+    tgt = torch.tensor(d.meta["target"], dtype=torch.float32, device="cuda")
+    times = []
+    for it in range(3):
+        v0.grad = None
+        E.grad = None
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x = rollout(v0, E, sim)
+        loss = ((x.mean(0) - tgt) ** 2).sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        times.append((t1 - t0, t2 - t1))
+    fwd, bwd = times[-1]
+    return {
+        "workload": "Elastic block, 20,000 particles, per-particle E, 200 substeps, checkpoints every 20",
+        "forward_s": fwd,
+        "backward_s": bwd,
+        "loss": float(loss.detach()),
+        "grad_v0": [float(g) for g in v0.grad.cpu()],
+        "grad_E_norm": float(E.grad.norm().cpu()),
+        "check": "tests/test_gpu_grad.py compares these gradients with float64 central finite differences",
+    }
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -599,6 +644,9 @@ def main():
                       "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": "gs.Scene.reset(state)+step()+get_state()"}
     if not args.no_batch:
         res["batched"] = run_batched(args, world, rank)
+        torch.cuda.empty_cache()
+    if not args.no_grad and rank == 0:
+        res["differentiation"] = run_grad(args)
         torch.cuda.empty_cache()
     if not args.no_serve:
         cap = res["batched"]["value"] if "batched" in res else res["value"]
