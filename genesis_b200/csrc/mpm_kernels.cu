@@ -38,7 +38,7 @@ namespace gbm {
 
 // resident threads per SM the register allocation of p2g / g2p2g is sized for
 #ifndef GBM_P2G_THREADS_PER_SM
-#define GBM_P2G_THREADS_PER_SM 1024
+#define GBM_P2G_THREADS_PER_SM 768
 #endif
 
 constexpr int BLK = MPM_BLOCK;         // grid block edge
@@ -715,30 +715,50 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
 #pragma unroll
     for (int k = 0; k < 9; ++k) nC[k] = 0.f;
     if (tile_contains(base, ox, oy, oz)) {
+        // separable evaluation: reduce along z, then y, then x.  With u = off - fx,
+        // C_ab = c sum_ijk w v_a u_b factors per axis, so each node costs one load and six
+        // FMAs instead of twelve.
         const int lx = base[0] - ox, ly = base[1] - oy, lz = base[2] - oz;
+        float wzd[3], wyd[3], wxd[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) {
+            wzd[k] = wz[k] * ((float)k - fx[2]);
+            wyd[k] = wy[k] * ((float)k - fx[1]);
+            wxd[k] = wx[k] * ((float)k - fx[0]);
+        }
 #pragma unroll
-            for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+            float a0[3] = {0.f, 0.f, 0.f}, ay[3] = {0.f, 0.f, 0.f}, az[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     const float4 g = VT.v[((lx + i) * TILE + (ly + j)) * TILE + (lz + k)];
-                    const float wt = wx[i] * wy[j] * wz[k];
-                    const float d0 = (float)i - fx[0], d1 = (float)j - fx[1], d2 = (float)k - fx[2];
-                    nv[0] += wt * g.x;
-                    nv[1] += wt * g.y;
-                    nv[2] += wt * g.z;
-                    const float cw = I.c_scale * wt;
-                    nC[0] += cw * g.x * d0;
-                    nC[1] += cw * g.x * d1;
-                    nC[2] += cw * g.x * d2;
-                    nC[3] += cw * g.y * d0;
-                    nC[4] += cw * g.y * d1;
-                    nC[5] += cw * g.y * d2;
-                    nC[6] += cw * g.z * d0;
-                    nC[7] += cw * g.z * d1;
-                    nC[8] += cw * g.z * d2;
+                    s0[0] += wz[k] * g.x;
+                    s0[1] += wz[k] * g.y;
+                    s0[2] += wz[k] * g.z;
+                    s1[0] += wzd[k] * g.x;
+                    s1[1] += wzd[k] * g.y;
+                    s1[2] += wzd[k] * g.z;
                 }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    a0[a] += wy[j] * s0[a];
+                    ay[a] += wyd[j] * s0[a];
+                    az[a] += wy[j] * s1[a];
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                nv[a] += wx[i] * a0[a];
+                nC[a * 3 + 0] += wxd[i] * a0[a];
+                nC[a * 3 + 1] += wx[i] * ay[a];
+                nC[a * 3 + 2] += wx[i] * az[a];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) nC[k] *= I.c_scale;
     } else {
 #pragma unroll 1
         for (int i = 0; i < 3; ++i)

@@ -177,8 +177,11 @@ def test_sort_interval_does_not_change_results():
     a.substeps(40)
     b.substeps(40)
     sa, sb = _state_np(a), _state_np(b)
-    assert np.abs(sa["pos"] - sb["pos"]).max() < 1e-6
-    assert b.fallback_count() >= 0
+    # a different binning changes only the float32 summation order; the scene holds Sand,
+    # whose float32 rounding sensitivity is ~3e-5 per 100 substeps, so the parity bar
+    # (1e-5 of the domain) applies rather than bitwise agreement
+    assert np.abs(sa["pos"] - sb["pos"]).max() < 1e-5
+    assert b.fallback_count() > 0 and a.fallback_count() == 0
 
 
 def test_graph_replay_matches_eager():
