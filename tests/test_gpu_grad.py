@@ -66,6 +66,7 @@ def test_adjoint_full_config_against_fp64_finite_differences():
         e = np.zeros(3)
         e[c] = h
         fd = (L(v0 + e, E) - L(v0 - e, E)) / (2 * h)
+        print(f"\n[accuracy] grad v0[{c}]: adjoint {gv[c]:.6e}  fp64 FD {fd:.6e}  rel {abs(gv[c] - fd) / abs(fd):.2e}")
         assert abs(gv[c] - fd) <= 2e-2 * max(abs(fd), 1e-3 * np.abs(gv).max()), (c, gv[c], fd)
     k = int(np.argmax(np.abs(gE)))
     hE = 1e-4 * E[k]
@@ -73,4 +74,5 @@ def test_adjoint_full_config_against_fp64_finite_differences():
     Ep[k] += hE
     Em[k] -= hE
     fd = (L(v0, Ep) - L(v0, Em)) / (2 * hE)
+    print(f"\n[accuracy] grad E[{k}]: adjoint {gE[k]:.6e}  fp64 FD {fd:.6e}  rel {abs(gE[k] - fd) / abs(fd):.2e}")
     assert abs(gE[k] - fd) <= 5e-2 * abs(fd), (gE[k], fd)
