@@ -40,7 +40,12 @@ namespace gbm {
 #ifndef GBM_P2G_THREADS_PER_SM
 #define GBM_P2G_THREADS_PER_SM 768
 #endif
+// unroll factor of the outermost stencil loops (3: fully unrolled, 1: rolled, smaller code)
+#ifndef GBM_OUTER_UNROLL
+#define GBM_OUTER_UNROLL 3
+#endif
 
+constexpr int kOuterUnroll = GBM_OUTER_UNROLL;
 constexpr int BLK = MPM_BLOCK;         // grid block edge
 constexpr int BLK3 = BLK * BLK * BLK;  // nodes per block
 constexpr int MARGIN = 1;              // drift margin of the shared tile (nodes)
@@ -59,14 +64,14 @@ struct Ws {
     float4* mm;          // grid momentum.xyz + mass, block-major
     float4* gv;          // grid velocity (w unused)
     uint32_t* flag;      // per grid block: 1 if active this substep
-    int2* active;        // active block list {instance, local block}
+    int2* active;        // active block list {instance, packed block coords}
     int* bin_count;      // sort histogram
     int* bin_start;      // exclusive scan of bin_count
     int* chunk_start;    // exclusive scan of chunks per bin
     int* key;            // per particle bin (global block id)
     int* rank;           // per particle rank within its bin
     int4* tile_sums;     // scan scratch
-    int4* chunks;        // work items {instance, local block, first slot, end slot}
+    int4* chunks;        // work items {instance, packed block coords, first slot, end slot}
     float* state_tmp;    // permutation scratch
     uint8_t* mat_tmp;
     uint8_t* pflags_tmp;
@@ -196,6 +201,20 @@ struct BlockCoord {
     int bx, by, bz;
 };
 
+// grid block coordinates packed 10 bits each (nblk < 1024 per axis, checked on the host):
+// work items and the active-block list carry them so kernels never divide by nblk
+__host__ __device__ __forceinline__ int pack_bc(int bx, int by, int bz) { return bx | (by << 10) | (bz << 20); }
+__device__ __forceinline__ BlockCoord unpack_bc(int p) {
+    BlockCoord c;
+    c.bx = p & 1023;
+    c.by = (p >> 10) & 1023;
+    c.bz = (p >> 20) & 1023;
+    return c;
+}
+__device__ __forceinline__ int local_block(const mpm_instance& I, int bx, int by, int bz) {
+    return (bx * I.nblk[1] + by) * I.nblk[2] + bz;
+}
+
 __device__ __forceinline__ BlockCoord block_coord(int lb, const mpm_instance& I) {
     BlockCoord c;
     c.bz = lb % I.nblk[2];
@@ -216,7 +235,7 @@ __device__ __forceinline__ void mark_block(Ws& w, int inst, const mpm_instance& 
     uint32_t* f = &w.flag[I.blk_base + lb];
     if (*((volatile uint32_t*)f) == 0u && atomicExch(f, 1u) == 0u) {
         const int i = (int)atomicAdd(&w.counters[CNT_ACTIVE], 1u);
-        w.active[i] = make_int2(inst, lb);
+        w.active[i] = make_int2(inst, pack_bc(bx, by, bz));
     }
 }
 
@@ -417,12 +436,14 @@ __global__ void k_build_chunks(mpm_problem prob, const mpm_instance* __restrict_
     const int P = prob.chunk_particles;
     const int k = find_instance_by_block(inst, prob.n_instances, b);
     const int lb = (int)(b - inst[k].blk_base);
+    const BlockCoord bc = block_coord(lb, inst[k]);
+    const int pbc = pack_bc(bc.bx, bc.by, bc.bz);
     const int start = w.bin_start[b];
     const int cs = w.chunk_start[b];
     const int nch = (cnt + P - 1) / P;
     for (int j = 0; j < nch; ++j) {
         const int s0 = start + j * P;
-        w.chunks[cs + j] = make_int4(k, lb, s0, min(s0 + P, start + cnt));
+        w.chunks[cs + j] = make_int4(k, pbc, s0, min(s0 + P, start + cnt));
     }
 }
 
@@ -568,6 +589,54 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
     }
 }
 
+// Tile node n of the 8^3 tile whose origin is (4b - 1) per axis lies in grid block b + db
+// (db in {-1, 0, 1}) at in-block offset (t + 3) & 3.  These depend only on n, so each
+// thread packs them once for the nodes it owns:
+//   bits 0-5 in-block node index, 6-7/8-9/10-11 db + 1 per axis, 12-21 shared-tile index,
+//   22-24/25-27/28-30 tile coordinates
+__device__ __forceinline__ uint32_t node_desc(int n) {
+    const int t[3] = {n >> 6, (n >> 3) & 7, n & 7};
+    uint32_t d = 0;
+    int ln = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        ln = ln * BLK + ((t[a] + 3) & 3);
+        d |= (uint32_t)((t[a] + 3) >> 2) << (6 + 2 * a);
+        d |= (uint32_t)t[a] << (22 + 3 * a);
+    }
+    d |= (uint32_t)ln;
+    d |= (uint32_t)tidx(t[0], t[1], t[2]) << 12;
+    return d;
+}
+
+// Per-chunk neighbourhood of the chunk's block: global index of block (b + db) and which
+// of the 3 offsets per axis are inside the grid.
+struct Nbhd {
+    int g0;       // global index of the chunk's own block
+    int sx, sy;   // block strides (nblk_y * nblk_z, nblk_z)
+    uint32_t vx, vy, vz;  // bit (db + 1) set if b + db is inside the grid on that axis
+};
+
+__device__ __forceinline__ Nbhd nbhd_of(const mpm_instance& I, const BlockCoord& bc) {
+    Nbhd h;
+    h.sy = I.nblk[2];
+    h.sx = I.nblk[1] * I.nblk[2];
+    h.g0 = (int)I.blk_base + bc.bx * h.sx + bc.by * h.sy + bc.bz;
+    h.vx = 2u | (bc.bx > 0 ? 1u : 0u) | (bc.bx + 1 < I.nblk[0] ? 4u : 0u);
+    h.vy = 2u | (bc.by > 0 ? 1u : 0u) | (bc.by + 1 < I.nblk[1] ? 4u : 0u);
+    h.vz = 2u | (bc.bz > 0 ? 1u : 0u) | (bc.bz + 1 < I.nblk[2] ? 4u : 0u);
+    return h;
+}
+
+// grid address of tile node d, or -1 if its block lies outside the grid
+__device__ __forceinline__ int64_t nbhd_addr(const Nbhd& h, uint32_t d) {
+    const uint32_t ex = (d >> 6) & 3, ey = (d >> 8) & 3, ez = (d >> 10) & 3;
+    if (!((h.vx >> ex) & (h.vy >> ey) & (h.vz >> ez) & 1u)) return -1;
+    const int g = h.g0 + ((int)ex - 1) * h.sx + ((int)ey - 1) * h.sy + ((int)ez - 1);
+    return ((int64_t)g << 6) + (d & 63);
+}
+
+// zero the whole tile (once per kernel; the flush re-zeroes what it touched)
 __device__ __forceinline__ void tile_zero(Tile& T, int P) {
     for (int n = threadIdx.x; n < TWORDS; n += P) {
         T.t[0][n] = 0;
@@ -586,7 +655,8 @@ __device__ __forceinline__ void tile_zero(Tile& T, int P) {
 // thread of the CTA (contains barriers); T must be zeroed and a barrier passed before.
 template <int P>
 __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const mpm_instance& I, int inst,
-                                              const BlockCoord& bc, int ox, int oy, int oz, Ws& w) {
+                                              const BlockCoord& bc, int ox, int oy, int oz, Ws& w, const Nbhd& h,
+                                              const uint32_t* nd) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const float wbq = warp_max(o.in_tile ? o.bq : 0.f);
     const float wbm = warp_max(o.in_tile ? o.mass : 0.f);
@@ -618,22 +688,26 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
             float As[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) As[k] = o.A[k] * sq;
+            // factored per axis: the (i, j) partial sums and weights are reused for the 3 k
+#pragma unroll kOuterUnroll
+            for (int i = 0; i < 3; ++i) {
+                const float wxi = sel3(wx, i), fi = (float)i;
+                const float b0 = mq0 + As[0] * fi, b1 = mq1 + As[3] * fi, b2 = mq2 + As[6] * fi;
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
+                for (int j = 0; j < 3; ++j) {
+                    const float wij = wxi * wy[j];
+                    const float c0 = b0 + As[1] * j, c1 = b1 + As[4] * j, c2 = b2 + As[7] * j;
+                    const int row = tidx(lx + i, ly + j, lz);
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const float wt = wx[i] * wy[j] * wz[k];
-                        const float ax = mq0 + (As[0] * i + As[1] * j + As[2] * k);
-                        const float ay = mq1 + (As[3] * i + As[4] * j + As[5] * k);
-                        const float az = mq2 + (As[6] * i + As[7] * j + As[8] * k);
-                        const int n = tidx(lx + i, ly + j, lz + k);
-                        atomicAdd(&T.t[0][n], fix(wt * ax));
-                        atomicAdd(&T.t[1][n], fix(wt * ay));
-                        atomicAdd(&T.t[2][n], fix(wt * az));
-                        atomicAdd(&T.t[3][n], fix(wt * ms));
+                        const float wt = wij * wz[k];
+                        atomicAdd(&T.t[0][row + k], fix(wt * (c0 + As[2] * k)));
+                        atomicAdd(&T.t[1][row + k], fix(wt * (c1 + As[5] * k)));
+                        atomicAdd(&T.t[2][row + k], fix(wt * (c2 + As[8] * k)));
+                        atomicAdd(&T.t[3][row + k], fix(wt * ms));
                     }
+                }
+            }
         } else {
             // drifted since the last sort (or a non-finite stress): bounds-checked global path
             atomicAdd((unsigned long long*)&w.counters[CNT_FALLBACK], 1ull);
@@ -658,22 +732,27 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
         }
     }
     __syncthreads();
-    // flush non-empty tile nodes, one 16-byte reduction each
+    // flush non-empty tile nodes, one 16-byte reduction each, zeroing the tile behind it
     const float iq = 1.f / sq, im = 1.f / sm;
-    for (int n = threadIdx.x; n < TN; n += P) {
-        const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
-        const int t = tidx(tx, ty, tz);
-        const int mi = T.t[3][t];
-        if (mi != 0) {
+#pragma unroll
+    for (int k = 0; k < TN / P; ++k) {
+        const uint32_t d = nd[k];
+        const int t = (d >> 12) & 1023;
+        const int mi = T.t[3][t], m0 = T.t[0][t], m1 = T.t[1][t], m2 = T.t[2][t];
+        if ((mi | m0 | m1 | m2) != 0) {
+            const int tx = (d >> 22) & 7, ty = (d >> 25) & 7, tz = (d >> 28) & 7;
             const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
-            if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+            const int64_t a = nbhd_addr(h, d);
+            if (a < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
                 set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
-                continue;
+            } else {
+                atomicAdd(&w.mm[a], make_float4((float)m0 * iq, (float)m1 * iq, (float)m2 * iq, (float)mi * im));
+                atomicOr(&T.mask, 1u << ((((d >> 6) & 3) * 9) + (((d >> 8) & 3) * 3) + ((d >> 10) & 3)));
             }
-            atomicAdd(&w.mm[node_addr(I, gx, gy, gz)],
-                      make_float4((float)T.t[0][t] * iq, (float)T.t[1][t] * iq, (float)T.t[2][t] * iq, (float)mi * im));
-            const int bit = ((gx >> 2) - bc.bx + 1) * 9 + ((gy >> 2) - bc.by + 1) * 3 + ((gz >> 2) - bc.bz + 1);
-            atomicOr(&T.mask, 1u << bit);
+            T.t[0][t] = 0;
+            T.t[1][t] = 0;
+            T.t[2][t] = 0;
+            T.t[3][t] = 0;
         }
     }
     __syncthreads();
@@ -684,15 +763,12 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
     __syncthreads();
 }
 
-__device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const mpm_instance& I, int ox, int oy, int oz,
-                                              int P) {
-    for (int n = threadIdx.x; n < TN; n += P) {
-        const int tx = n / (TILE * TILE), ty = (n / TILE) % TILE, tz = n % TILE;
-        const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
-        float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < I.res[0] && gy < I.res[1] && gz < I.res[2])
-            val = w.gv[node_addr(I, gx, gy, gz)];
-        VT.v[n] = val;
+template <int P>
+__device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const Nbhd& h, const uint32_t* nd) {
+#pragma unroll
+    for (int k = 0; k < TN / P; ++k) {
+        const int64_t a = nbhd_addr(h, nd[k]);
+        VT.v[threadIdx.x + k * P] = a >= 0 ? w.gv[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
@@ -726,7 +802,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
             wyd[k] = wy[k] * ((float)k - fx[1]);
             wxd[k] = wx[k] * ((float)k - fx[0]);
         }
-#pragma unroll
+#pragma unroll kOuterUnroll
         for (int i = 0; i < 3; ++i) {
             float a0[3] = {0.f, 0.f, 0.f}, ay[3] = {0.f, 0.f, 0.f}, az[3] = {0.f, 0.f, 0.f};
 #pragma unroll
@@ -749,12 +825,13 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
                     az[a] += wy[j] * s1[a];
                 }
             }
+            const float wxi = sel3(wx, i), wxdi = sel3(wxd, i);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                nv[a] += wx[i] * a0[a];
-                nC[a * 3 + 0] += wxd[i] * a0[a];
-                nC[a * 3 + 1] += wx[i] * ay[a];
-                nC[a * 3 + 2] += wx[i] * az[a];
+                nv[a] += wxi * a0[a];
+                nC[a * 3 + 0] += wxdi * a0[a];
+                nC[a * 3 + 1] += wxi * ay[a];
+                nC[a * 3 + 2] += wxi * az[a];
             }
         }
 #pragma unroll
@@ -812,12 +889,16 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     const float* __restrict__ S = a.par.state;
+    uint32_t nd[TN / P];
+#pragma unroll
+    for (int k = 0; k < TN / P; ++k) nd[k] = node_desc(threadIdx.x + k * P);
+    tile_zero(T, P);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
-        const BlockCoord bc = block_coord(ch.y, I);
+        const BlockCoord bc = unpack_bc(ch.y);
+        const Nbhd h = nbhd_of(I, bc);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        tile_zero(T, P);
         Payload o;
         o.live = o.in_tile = false;
         o.mass = o.bq = 0.f;
@@ -833,7 +914,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
             for (int k = 0; k < 9; ++k) C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
             particle_update(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x);
         }
-        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w);
+        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
     }
 }
 
@@ -846,12 +927,16 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     float* __restrict__ S = a.par.state;
+    uint32_t nd[TN / P];
+#pragma unroll
+    for (int k = 0; k < TN / P; ++k) nd[k] = node_desc(threadIdx.x + k * P);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
-        const BlockCoord bc = block_coord(ch.y, I);
+        const BlockCoord bc = unpack_bc(ch.y);
+        const Nbhd h = nbhd_of(I, bc);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        vel_tile_load(VT, w, I, ox, oy, oz, P);
+        vel_tile_load<P>(VT, w, h, nd);
         __syncthreads();
         const int p = ch.z + threadIdx.x;
         if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
@@ -884,13 +969,17 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     float* __restrict__ S = a.par.state;
+    uint32_t nd[TN / P];
+#pragma unroll
+    for (int k = 0; k < TN / P; ++k) nd[k] = node_desc(threadIdx.x + k * P);
+    tile_zero(T, P);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
-        const BlockCoord bc = block_coord(ch.y, I);
+        const BlockCoord bc = unpack_bc(ch.y);
+        const Nbhd h = nbhd_of(I, bc);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        vel_tile_load(VT, w, I, ox, oy, oz, P);
-        tile_zero(T, P);
+        vel_tile_load<P>(VT, w, h, nd);
         __syncthreads();
         Payload o;
         o.live = o.in_tile = false;
@@ -906,7 +995,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
                 particle_update(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x);
             }
         }
-        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w);
+        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
     }
 }
 
@@ -948,8 +1037,9 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
     for (int i = blockIdx.x * gpc + grp; i < n_active; i += gridDim.x * gpc) {
         const int2 e = w.active[i];
         const mpm_instance& I = inst[e.x];
-        const BlockCoord bc = block_coord(e.y, I);
-        const int64_t g = (I.blk_base + e.y) * BLK3 + ln;
+        const BlockCoord bc = unpack_bc(e.y);
+        const int lb = local_block(I, bc.bx, bc.by, bc.bz);
+        const int64_t g = (I.blk_base + lb) * BLK3 + ln;
         const float4 mm = w.mm[g];
         float vx = 0.f, vy = 0.f, vz = 0.f;
         if (mm.w > I.eps) {
@@ -967,7 +1057,7 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
         }
         w.gv[g] = make_float4(vx, vy, vz, 0.f);
         w.mm[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ln == 0) w.flag[I.blk_base + e.y] = 0u;
+        if (ln == 0) w.flag[I.blk_base + lb] = 0u;
     }
     // the last CTA to finish resets the active-block count for the next p2g: every CTA read
     // the count into registers before this barrier, so no fence is needed; no CTA waits on

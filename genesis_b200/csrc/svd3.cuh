@@ -19,6 +19,12 @@
 
 namespace gbm {
 
+// unroll factor of the Jacobi sweep loop (1: rolled, smaller code; 4: fully unrolled)
+#ifndef GBM_SVD_UNROLL
+#define GBM_SVD_UNROLL 1
+#endif
+constexpr int kSvdUnroll = GBM_SVD_UNROLL;
+
 // One Jacobi rotation in plane (P, Q) of the symmetric matrix a, accumulated into v.
 template <int P, int Q>
 __device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
@@ -100,7 +106,7 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* 
             a[j][i] = acc;
         }
     float v[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
-#pragma unroll
+#pragma unroll kSvdUnroll
     for (int sw = 0; sw < SWEEPS; ++sw) {
         jacobi_pq<0, 1>(a, v);
         jacobi_pq<0, 2>(a, v);

@@ -55,6 +55,8 @@ class InstanceSpec:
         pad = 3 * self.dx
         self.bnd_lo = lo + pad
         self.bnd_hi = hi - pad
+        if np.any(self.grid_res > 4 * 1023):
+            raise ValueError("grid_res above 4092 nodes per axis is not supported (10-bit block coordinates)")
 
     @property
     def nblk(self) -> np.ndarray:

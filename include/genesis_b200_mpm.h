@@ -89,7 +89,7 @@ typedef struct mpm_instance {
     int32_t p_begin;       /* first slot of this instance's particles */
     int32_t p_count;       /* number of particles */
     int32_t res[3];        /* grid_res = upper_cell - lower_cell + 1 */
-    int32_t nblk[3];       /* ceil(res / MPM_BLOCK) */
+    int32_t nblk[3];       /* ceil(res / MPM_BLOCK); at most 1023 per axis */
     int32_t lower_cell[3]; /* grid_offset */
     int32_t mat_base;      /* first entry of this instance in the material table */
     int64_t blk_base;      /* first grid block of this instance */
