@@ -1537,6 +1537,16 @@ int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t
     return MPM_OK;
 }
 
+int mpm_status_enqueue(const mpm_problem* prob, void* workspace, uint32_t* out, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!workspace || !out) return MPM_E_INVALID;
+    Ws w = ws_of(*prob, workspace);
+    if (cudaMemcpyAsync(out, &w.counters[CNT_STATUS], 4, cudaMemcpyDeviceToHost, (cudaStream_t)stream) != cudaSuccess)
+        return MPM_E_CUDA;
+    return MPM_OK;
+}
+
 int mpm_instance_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream) {
     int rc = check_problem(prob);
     if (rc) return rc;

@@ -21,6 +21,9 @@ from .entity import MPMEntity
 from .runtime import InstanceSpec, MPMRuntime
 from .states import MPMSolverState
 
+# mpm_solver.py:505-509
+NAN_MESSAGE = "NaN detected in MPM states. Try reducing the time step size or adjusting simulation parameters."
+
 log = logging.getLogger("genesis_b200")
 
 
@@ -157,9 +160,7 @@ class MPMSolver:
         """Raise if any particle position became NaN (mpm_solver.py:505-509)."""
         st = self.runtime.status(clear=False)
         if st & nat.MPM_STATUS_NAN:
-            raise GenesisException(
-                "NaN detected in MPM states. Try reducing the time step size or adjusting simulation parameters."
-            )
+            raise GenesisException(NAN_MESSAGE)
         return st
 
     # ------------------------------------------------------------------- io
@@ -196,7 +197,7 @@ class MPMSolver:
         self.runtime.set_state(
             pos=fields["pos"].reshape(B * N, 3), vel=fields["vel"].reshape(B * N, 3),
             C_=fields["C"].reshape(B * N, 9), F=fields["F"].reshape(B * N, 9),
-            Jp=fields["Jp"].reshape(B * N), active=fields["active"].reshape(B * N).to(torch.uint8),
+            Jp=fields["Jp"].reshape(B * N), active=fields["active"].reshape(B * N),
         )
 
     # ----------------------------------------------------------- properties

@@ -266,28 +266,88 @@ class MPMRuntime:
             out["active"] = out["active"].bool()
         return out
 
+    # state channels in API order: (name, dtype, values per particle)
+    _STATE_IO = (("pos", torch.float32, 3), ("vel", torch.float32, 3), ("C", torch.float32, 9),
+                 ("F", torch.float32, 9), ("Jp", torch.float32, 1), ("active", torch.uint8, 1))
+
     def set_state(self, pos=None, vel=None, C_=None, F=None, Jp=None, active=None):
-        """Overwrite any subset of the state, arrays in API order (device or host)."""
-        dev = self.device
-        keep = []
+        """Overwrite any subset of the state, arrays in API order (device or host).
 
-        def dptr(x, dtype, shape):
-            if x is None:
-                return None
-            t = torch.as_tensor(x).to(device=dev, dtype=dtype).reshape(shape).contiguous()
-            keep.append(t)
-            return t.data_ptr()
-
+        When every given array is a contiguous pinned host tensor of the channel's dtype
+        (float32; bool or uint8 for ``active``) the upload is asynchronous: the arrays are
+        copied on a side stream into a device staging buffer, and the scatter into the
+        sorted state waits for that copy on the current stream.  The host does not block,
+        so the copy overlaps whatever the device is still running."""
+        vals = dict(pos=pos, vel=vel, C=C_, F=F, Jp=Jp, active=active)
         n = self.n
         if pos is not None:
             self._dirty = True
-        self._call(
-            "mpm_set_state", C.byref(self.prob), C.byref(self.par),
-            dptr(pos, torch.float32, (n, 3)), dptr(vel, torch.float32, (n, 3)),
-            dptr(C_, torch.float32, (n, 9)), dptr(F, torch.float32, (n, 9)),
-            dptr(Jp, torch.float32, (n,)), dptr(active, torch.uint8, (n,)), _cuda_stream_handle(),
-        )
+        given = {k: v for k, v in vals.items() if v is not None}
+        if given and all(self._stageable(k, v) for k, v in given.items()):
+            return self._set_state_staged(given)
+        dev = self.device
+        keep = []
+
+        def dptr(k, dtype, width):
+            x = vals[k]
+            if x is None:
+                return None
+            t = torch.as_tensor(x).to(device=dev, dtype=dtype).reshape((n, width) if width > 1 else (n,)).contiguous()
+            keep.append(t)
+            return t.data_ptr()
+
+        self._call("mpm_set_state", C.byref(self.prob), C.byref(self.par),
+                   *[dptr(k, dt, w) for k, dt, w in self._STATE_IO], _cuda_stream_handle())
         return keep
+
+    def _stageable(self, k, v) -> bool:
+        if not isinstance(v, torch.Tensor) or v.device.type != "cpu" or not v.is_contiguous():
+            return False
+        if k == "active":
+            ok = v.dtype in (torch.bool, torch.uint8)
+        else:
+            ok = v.dtype == torch.float32
+        width = dict((a, w) for a, _, w in self._STATE_IO)[k]
+        return ok and v.numel() == self.n * width and v.is_pinned()
+
+    def _set_state_staged(self, given):
+        n = self.n
+        if getattr(self, "_staging", None) is None:
+            self._staging = torch.empty(n * 25 * 4 + n, dtype=torch.uint8, device=self.device)
+            self._copy_stream = torch.cuda.Stream(device=self.device)
+            self._staging_free = None
+        main = torch.cuda.current_stream(self.device)
+        cs = self._copy_stream
+        if self._staging_free is not None:
+            cs.wait_event(self._staging_free)  # the previous scatter has read the staging buffer
+        ptrs, off = [], 0
+        with torch.cuda.stream(cs):
+            for k, dt, w in self._STATE_IO:
+                nbytes = n * w * (4 if dt == torch.float32 else 1)
+                if k in given:
+                    dst = self._staging[off:off + nbytes]
+                    dst.copy_(given[k].reshape(-1).view(torch.uint8), non_blocking=True)
+                    ptrs.append(dst.data_ptr())
+                else:
+                    ptrs.append(None)
+                off += nbytes
+        done = torch.cuda.Event()
+        done.record(cs)
+        main.wait_event(done)
+        self._call("mpm_set_state", C.byref(self.prob), C.byref(self.par), *ptrs, _cuda_stream_handle())
+        self._staging_free = torch.cuda.Event()
+        self._staging_free.record(main)
+        return []
+
+    def status_enqueue(self):
+        """Start an asynchronous read of the status word on the current stream; returns a
+        (pinned host tensor, event) pair, valid once the event has completed."""
+        out = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        self._call("mpm_status_enqueue", C.byref(self.prob), self._ws, C.c_void_p(out.data_ptr()),
+                   _cuda_stream_handle())
+        ev = torch.cuda.Event()
+        ev.record()
+        return out, ev
 
     def _idx_call(self, name, idx, values, vdtype, vshape, with_tables=False):
         dev = self.device

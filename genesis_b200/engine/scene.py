@@ -92,7 +92,8 @@ class Scene:
         self._sim.step()
 
     def check_state(self):
-        """Explicit NaN check (one host sync)."""
+        """Explicit NaN check (one host sync); also settles the pending asynchronous checks."""
+        self._sim.poll_status(wait=True)
         return self._sim.mpm_solver.check_state()
 
     def get_state(self):
@@ -101,11 +102,13 @@ class Scene:
     def reset(self, state: SimState | None = None, envs_idx=None):
         if not self._is_built:
             raise GenesisException("Scene is not built yet.")
+        self._sim.poll_status()
         if state is None:
             state = self._init_state
         if state is not None:
             mpm_state = state.solvers_state[0] if isinstance(state, SimState) else state
             self._sim.mpm_solver.set_state(0, mpm_state, envs_idx=envs_idx)
+        self._sim._queried_states.clear()  # simulator.py:227, 238
         if envs_idx is None:
             self._sim._cur_substep_global = 0
 

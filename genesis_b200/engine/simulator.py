@@ -5,8 +5,9 @@ from __future__ import annotations
 import numpy as np
 
 from .. import _globals
+from .. import _native as nat
 from ..exceptions import GenesisException
-from .mpm_solver import LegacyCoupler, MPMSolver
+from .mpm_solver import NAN_MESSAGE, LegacyCoupler, MPMSolver
 from .states import SimState
 
 
@@ -30,6 +31,7 @@ class Simulator:
         self._coupler = LegacyCoupler(self)
         self._b200 = b200_options
         self._queried_states = []
+        self._pending_status = []  # (pinned status word, event) of steps not yet checked
 
     def build(self):
         self._B = self._scene._B
@@ -38,12 +40,29 @@ class Simulator:
     # -------------------------------------------------------------- stepping
     def step(self, in_backward=False):
         """process_input, then `substeps` substeps (simulator.py:268-292)."""
+        self.poll_status()
         self.process_input(in_backward=in_backward)
         if self.mpm_solver.is_active:
             self.mpm_solver.advance(self._substeps)
         self._cur_substep_global += self._substeps
         if self.mpm_solver.is_active and self._b200.check_nan == "step":
             self.mpm_solver.check_state()
+        elif self.mpm_solver.is_active and self._b200.check_nan == "async":
+            self._pending_status.append(self.mpm_solver.runtime.status_enqueue())
+
+    def poll_status(self, wait=False):
+        """Raise for a NaN found by an earlier step's asynchronous status read (check_nan
+        'async'); with wait=True, wait for every pending read first."""
+        while self._pending_status:
+            word, ev = self._pending_status[0]
+            if wait:
+                ev.synchronize()
+            elif not ev.query():
+                return
+            self._pending_status.pop(0)
+            if int(word[0]) & nat.MPM_STATUS_NAN:
+                self._pending_status.clear()
+                raise GenesisException(NAN_MESSAGE)
 
     def process_input(self, in_backward=False):
         if self.mpm_solver.is_active:
@@ -66,6 +85,7 @@ class Simulator:
             self.mpm_solver.substep_post_coupling(f)
 
     def get_state(self):
+        self.poll_status()
         state = SimState(self._scene, self.cur_step_global, [self.mpm_solver.get_state(self.cur_substep_local)])
         self._queried_states.append(state)
         return state

@@ -100,6 +100,9 @@ class B200Options(Options):
     chunk_particles  particles per p2g/g2p work item: 128, 256 or 512
     use_cuda_graph   replay sort_interval substeps as one captured CUDA graph
     check_nan        'step' (raise at the end of a step, one host sync per step),
+                     'async' (the step enqueues a non-blocking read of the status word;
+                     the first scene call after it has arrived raises; scene.check_state()
+                     waits for it),
                      'never' (call scene.check_state() yourself)
     """
 
@@ -108,6 +111,11 @@ class B200Options(Options):
     use_cuda_graph: bool = True
     check_nan: str = "step"
     grid_ctas: int = 0
+
+    def __init__(self, **data):
+        super().__init__(**data)
+        if self.check_nan not in ("step", "async", "never"):
+            raise GenesisException(f"check_nan must be 'step', 'async' or 'never', got {self.check_nan!r}")
 
 
 class VisOptions(Options):

@@ -245,6 +245,12 @@ int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mp
 /* Read (and optionally clear) the device status word; synchronises the stream. */
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
 
+/* Enqueue a copy of the device status word into host memory `out` on `stream` and return
+ * without waiting (the asynchronous form of the NaN check at mpm_solver.py:505-509).
+ * `*out` is valid once the stream has passed this point (event or stream sync); `out`
+ * should be pinned, otherwise the copy is synchronous. */
+int mpm_status_enqueue(const mpm_problem* prob, void* workspace, uint32_t* out, void* stream);
+
 /* Per-instance status words (n_instances entries, same bits as mpm_status) into host
  * memory `out`; synchronises the stream.  Instances never share grid memory, so a NaN in
  * one instance leaves the others' results untouched and can be handled per instance. */

@@ -74,3 +74,9 @@ def test_scene_requires_init():
             gs.Scene()
     finally:
         _globals.initialized = saved
+
+
+def test_check_nan_option_is_validated():
+    gs.options.B200Options(check_nan="async")
+    with pytest.raises(gs.GenesisException):
+        gs.options.B200Options(check_nan="sometimes")

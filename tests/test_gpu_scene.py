@@ -86,3 +86,44 @@ def test_entity_active_mask():
     scene.step()
     assert torch.equal(sand.get_particles_pos(), ps)
     assert not bool(sand.get_particles_active().any())
+
+
+def _host_state(scene, pinned):
+    st = scene.get_state()[0]
+    out = {k: getattr(st, k).cpu() for k in ("pos", "vel", "C", "F", "Jp", "active")}
+    return {k: (v.pin_memory() if pinned else v) for k, v in out.items()}
+
+
+def test_staged_upload_matches_synchronous_upload():
+    """scene.reset from pinned host tensors (asynchronous staged copy) gives the same
+    trajectory as from pageable host tensors (synchronous copy)."""
+    from genesis_b200.engine.states import MPMSolverState
+
+    res = []
+    for pinned in (False, True):
+        scene, cube, sand = _scene()
+        scene.step()
+        h = _host_state(scene, pinned)
+        h["vel"] = h["vel"] + 0.1  # a state different from the scene's current one
+        scene.step()
+        for _ in range(2):  # twice in a row: the staging buffer is reused
+            scene.reset(MPMSolverState(scene, h["pos"], h["vel"], h["C"], h["F"], h["Jp"], h["active"]))
+            scene.step()
+        res.append(scene.get_state()[0].pos.clone())
+    assert torch.equal(res[0], res[1])
+
+
+def test_async_nan_check_raises_on_a_later_call():
+    from genesis_b200.engine.states import MPMSolverState
+
+    scene, cube, sand = _scene(check_nan="async")
+    scene.step()
+    h = _host_state(scene, pinned=True)
+    h["pos"][0, 0, 0] = float("nan")
+    scene.reset(MPMSolverState(scene, h["pos"], h["vel"], h["C"], h["F"], h["Jp"], h["active"]))
+    scene.step()  # does not block; the NaN is found by a later call
+    torch.cuda.synchronize()
+    with pytest.raises(gs.GenesisException):
+        scene.get_state()
+    with pytest.raises(gs.GenesisException):
+        scene.check_state()  # the device status word stays set
