@@ -518,13 +518,23 @@ __device__ __forceinline__ bool tile_contains(const int* base, int ox, int oy, i
     return lx >= 0 && ly >= 0 && lz >= 0 && lx <= TILE - 3 && ly <= TILE - 3 && lz <= TILE - 3;
 }
 
+// per-thread shared-memory parking space for x, v, C (15 words, stride P: conflict-free);
+// 512-thread CTAs keep them in registers (their tiles leave no room under 48 KB)
+template <int P>
+constexpr bool kStash = P <= 256;
+template <int P>
+struct Stash {
+    float s[15][kStash<P> ? P : 1];
+};
+
 // compute_F_tmp + svd + return mapping + stress (mpm_solver.py:261-345) for slot p with
 // velocity v and affine C; writes F and Jp of the next frame and fills the scatter payload
 // for position x.
+template <int P>
 __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm_material* __restrict__ mats,
-                                                const mpm_particles& par, int p, const float* x, const float* v,
-                                                const float* C, int ox, int oy, int oz, Payload& o, const Ws& w,
-                                                int inst) {
+                                                const mpm_particles& par, int p, const float* x_in,
+                                                const float* v_in, const float* C_in, int ox, int oy, int oz,
+                                                Payload& o, const Ws& w, int inst, Stash<P>& sh) {
     const int64_t st = par.state_stride;
     float* __restrict__ S = par.state;
     float F[9];
@@ -545,9 +555,23 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
         for (int j = 0; j < 3; ++j) {
             float acc = F[i * 3 + j];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) acc += I.dt * C[i * 3 + k] * F[k * 3 + j];
+            for (int k = 0; k < 3; ++k) acc += I.dt * C_in[i * 3 + k] * F[k * 3 + j];
             Ft[i * 3 + j] = acc;
         }
+    // x, v and C are needed again only for the scatter payload: park them in shared
+    // memory across the SVD and return mapping, where register pressure peaks
+    // (volatile, so the compiler cannot keep them in registers instead)
+    float x[3], v[3], C[9];
+    if constexpr (kStash<P>) {
+        volatile float* sv = &sh.s[0][threadIdx.x];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            sv[k * P] = x_in[k];
+            sv[(3 + k) * P] = v_in[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sv[(6 + k) * P] = C_in[k];
+    }
     float U[9], Sg[3], V[9];
     svd3(Ft, U, Sg, V);
     const float J = Sg[0] * (Sg[1] * Sg[2]);
@@ -556,6 +580,24 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
 #pragma unroll
     for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
     S[MPM_CH_JP * st + p] = Jpn;
+    if constexpr (kStash<P>) {
+        volatile float* sv = &sh.s[0][threadIdx.x];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            x[k] = sv[k * P];
+            v[k] = sv[(3 + k) * P];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) C[k] = sv[(6 + k) * P];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            x[k] = x_in[k];
+            v[k] = v_in[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) C[k] = C_in[k];
+    }
     // affine = stress * (-dt vol 4 inv_dx^2) + mass C (mpm_solver.py:344-345)
     o.mass = m.mass;
     float A[9];
@@ -736,7 +778,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
     const float iq = 1.f / sq, im = 1.f / sm;
 #pragma unroll
     for (int k = 0; k < TN / P; ++k) {
-        const uint32_t d = nd[k];
+        const uint32_t d = nd[threadIdx.x + k * P];
         const int t = (d >> 12) & 1023;
         const int mi = T.t[3][t], m0 = T.t[0][t], m1 = T.t[1][t], m2 = T.t[2][t];
         if ((mi | m0 | m1 | m2) != 0) {
@@ -767,7 +809,7 @@ template <int P>
 __device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const Nbhd& h, const uint32_t* nd) {
 #pragma unroll
     for (int k = 0; k < TN / P; ++k) {
-        const int64_t a = nbhd_addr(h, nd[k]);
+        const int64_t a = nbhd_addr(h, nd[threadIdx.x + k * P]);
         VT.v[threadIdx.x + k * P] = a >= 0 ? w.gv[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
@@ -885,13 +927,14 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
 template <int P>
 __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a) {
     __shared__ Tile T;
+    __shared__ Stash<P> SH;
     Ws& w = a.w;
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     const float* __restrict__ S = a.par.state;
-    uint32_t nd[TN / P];
+    __shared__ uint32_t nd[TN];  // each thread reads back only the entries it wrote
 #pragma unroll
-    for (int k = 0; k < TN / P; ++k) nd[k] = node_desc(threadIdx.x + k * P);
+    for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
     tile_zero(T, P);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
@@ -912,7 +955,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
             }
 #pragma unroll
             for (int k = 0; k < 9; ++k) C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
-            particle_update(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x);
+            particle_update<P>(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x, SH);
         }
         scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
     }
@@ -927,9 +970,9 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     float* __restrict__ S = a.par.state;
-    uint32_t nd[TN / P];
+    __shared__ uint32_t nd[TN];  // each thread reads back only the entries it wrote
 #pragma unroll
-    for (int k = 0; k < TN / P; ++k) nd[k] = node_desc(threadIdx.x + k * P);
+    for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
@@ -965,13 +1008,14 @@ template <int P>
 __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs a) {
     __shared__ VelTile VT;
     __shared__ Tile T;
+    __shared__ Stash<P> SH;
     Ws& w = a.w;
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t st = a.par.state_stride;
     float* __restrict__ S = a.par.state;
-    uint32_t nd[TN / P];
+    __shared__ uint32_t nd[TN];  // each thread reads back only the entries it wrote
 #pragma unroll
-    for (int k = 0; k < TN / P; ++k) nd[k] = node_desc(threadIdx.x + k * P);
+    for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
     tile_zero(T, P);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
@@ -992,7 +1036,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
             if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
-                particle_update(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x);
+                particle_update<P>(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x, SH);
             }
         }
         scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
