@@ -404,27 +404,66 @@ __global__ void k_sort_scatter(mpm_problem prob, mpm_particles par, Ws w) {
     for (int ch = 0; ch < MPM_STATE_CH; ++ch) w.state_tmp[ch * t + dst] = par.state[ch * s + p];
     w.mat_tmp[dst] = par.mat[p];
     w.pflags_tmp[dst] = par.pflags[p];
-    const int g = par.gid[p];
-    w.gid_tmp[dst] = g;
-    par.slot[g] = dst;
+    w.gid_tmp[dst] = par.gid[p];
     if (par.mu_p) {
         w.mu_tmp[dst] = par.mu_p[p];
         w.lam_tmp[dst] = par.lam_p[p];
     }
 }
 
-__global__ void k_sort_copyback(mpm_problem prob, mpm_particles par, Ws w) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= prob.n_particles) return;
+// Second half of the sort: copy each chunk back from the scratch arrays in an order that
+// puts the particles of different cells side by side.  Within a chunk (particles of one
+// grid block), particle k of cell c goes after the first k particles of every cell and
+// after particle k of the cells before c: "round k" holds one particle of each cell that
+// has more than k.  A warp then covers up to 32 distinct cells, so the 27-node stencils of
+// its lanes fall on distinct shared-memory banks in the p2g scatter and the g2p gather
+// instead of colliding.  Also writes gid and the slot map.
+template <int P>
+__global__ void __launch_bounds__(P) k_sort_interleave(mpm_problem prob, const mpm_instance* __restrict__ inst,
+                                                       mpm_particles par, Ws w) {
+    __shared__ int cnt[BLK3];
+    const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t s = par.state_stride, t = w.tmp_stride;
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        if (threadIdx.x < BLK3) cnt[threadIdx.x] = 0;
+        __syncthreads();
+        const int4 ch = w.chunks[ci];
+        const int src = ch.z + threadIdx.x;
+        const bool live = src < ch.w;
+        int c = 0, r = 0;
+        if (live) {
+            const mpm_instance& I = inst[ch.x];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                // the cell of k_sort_keys, whose block is this chunk's block
+                const float f = floorf(w.state_tmp[(MPM_CH_X + d) * t + src] * I.inv_dx - 0.5f);
+                const int cell = isfinite(f) ? (int)fminf(fmaxf(f - (float)I.lower_cell[d], 0.f), (float)(I.res[d] - 1)) : 0;
+                c = c * BLK + (cell & (BLK - 1));
+            }
+            r = atomicAdd(&cnt[c], 1);
+        }
+        __syncthreads();
+        if (live) {
+            int pos = 0;
+#pragma unroll 8
+            for (int k = 0; k < BLK3; ++k) {
+                const int nk = cnt[k];
+                pos += min(nk, r) + ((k < c && nk > r) ? 1 : 0);
+            }
+            const int dst = ch.z + pos;
 #pragma unroll 5
-    for (int ch = 0; ch < MPM_STATE_CH; ++ch) par.state[ch * s + p] = w.state_tmp[ch * t + p];
-    par.mat[p] = w.mat_tmp[p];
-    par.pflags[p] = w.pflags_tmp[p];
-    par.gid[p] = w.gid_tmp[p];
-    if (par.mu_p) {
-        par.mu_p[p] = w.mu_tmp[p];
-        par.lam_p[p] = w.lam_tmp[p];
+            for (int q = 0; q < MPM_STATE_CH; ++q) par.state[q * s + dst] = w.state_tmp[q * t + src];
+            par.mat[dst] = w.mat_tmp[src];
+            par.pflags[dst] = w.pflags_tmp[src];
+            const int g = w.gid_tmp[src];
+            par.gid[dst] = g;
+            par.slot[g] = dst;
+            if (par.mu_p) {
+                par.mu_p[dst] = w.mu_tmp[src];
+                par.lam_p[dst] = w.lam_tmp[src];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -488,8 +527,15 @@ struct Tile {
     int cnt;
 };
 
+// Grid velocities of the 8^3 tile, float4 per node, with a y-stride of 12 nodes: a
+// quarter-warp's 8 lanes reading nodes whose (y, z) differ by (0..1, 0..3) then hit 8
+// distinct 4-bank groups (with a y-stride of 8 they would pair up).
+constexpr int VYS = 12;             // y-stride (nodes)
+constexpr int VXS = TILE * VYS;     // x-stride (96 nodes)
+__device__ __forceinline__ int vidx(int x, int y, int z) { return x * VXS + y * VYS + z; }
+
 struct VelTile {
-    float4 v[TN];
+    float4 v[TILE * VXS];
 };
 
 // Per-thread scatter payload of one particle: mass * v + affine (off - fx) dx = q + A off.
@@ -809,8 +855,9 @@ template <int P>
 __device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const Nbhd& h, const uint32_t* nd) {
 #pragma unroll
     for (int k = 0; k < TN / P; ++k) {
-        const int64_t a = nbhd_addr(h, nd[threadIdx.x + k * P]);
-        VT.v[threadIdx.x + k * P] = a >= 0 ? w.gv[a] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint32_t d = nd[threadIdx.x + k * P];
+        const int64_t a = nbhd_addr(h, d);
+        VT.v[vidx((d >> 22) & 7, (d >> 25) & 7, (d >> 28) & 7)] = a >= 0 ? w.gv[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
@@ -852,7 +899,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
                 float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    const float4 g = VT.v[((lx + i) * TILE + (ly + j)) * TILE + (lz + k)];
+                    const float4 g = VT.v[vidx(lx + i, ly + j, lz + k)];
                     s0[0] += wz[k] * g.x;
                     s0[1] += wz[k] * g.y;
                     s0[2] += wz[k] * g.z;
@@ -1279,11 +1326,21 @@ static int launch_sort(const mpm_problem* prob, const mpm_tables* tab, mpm_parti
     k_scan_reduce<<<ntiles, SCAN_T, 0, s>>>(nb, prob->chunk_particles, w);
     k_scan_tiles<<<1, SCAN_T, 0, s>>>(ntiles, w);
     k_scan_apply<<<ntiles, SCAN_T, 0, s>>>(nb, prob->chunk_particles, w);
+    k_build_chunks<<<(int)((nb + T - 1) / T), T, 0, s>>>(*prob, tab->instances, w);
     if (n > 0) {
         k_sort_scatter<<<(n + T - 1) / T, T, 0, s>>>(*prob, *par, w);
-        k_sort_copyback<<<(n + T - 1) / T, T, 0, s>>>(*prob, *par, w);
+        const DevInfo* d = dev_info();
+        if (!d) return MPM_E_CUDA;
+        const int P = prob->chunk_particles;
+        int ctas = d->sms * (2048 / P);
+        if (ctas > prob->max_chunks) ctas = prob->max_chunks > 0 ? prob->max_chunks : 1;
+        if (P == 128)
+            k_sort_interleave<128><<<ctas, 128, 0, s>>>(*prob, tab->instances, *par, w);
+        else if (P == 256)
+            k_sort_interleave<256><<<ctas, 256, 0, s>>>(*prob, tab->instances, *par, w);
+        else
+            k_sort_interleave<512><<<ctas, 512, 0, s>>>(*prob, tab->instances, *par, w);
     }
-    k_build_chunks<<<(int)((nb + T - 1) / T), T, 0, s>>>(*prob, tab->instances, w);
     return cuda_ok();
 }
 
