@@ -502,10 +502,10 @@ struct P2GArgs {
 // therefore accumulated as integers.  Each chunk picks, per channel, a power-of-two scale
 // s with max(n, 256) * b * s < 2^30, where n is the number of particles in the chunk and b
 // bounds |contribution| of any of them to any node (w <= 1, |off - fx| <= 1.5): no node
-// sum can overflow, every contribution is below 2^22 (so round-to-nearest is one float add
-// of 1.5 * 2^23, exact), and the quantisation step is 2^-22 of the chunk's largest
-// contribution, on a par with float32 accumulation.  The tile uses an x-stride of 68
-// words so the banks of a 4x4x4 block's nodes spread over all 32 banks.
+// sum can overflow, every contribution is below 2^22 (so round-to-nearest is one fused
+// multiply-add of the weight with 1.5 * 2^23), and the quantisation step is 2^-22 of the
+// chunk's largest contribution, on a par with float32 accumulation.  The tile uses an
+// x-stride of 68 words so the banks of a 4x4x4 block's nodes spread over all 32 banks.
 constexpr int TXS = TILE * TILE + 4;       // skewed x-stride of the shared tile (words)
 constexpr int TWORDS = TILE * TXS;         // words per channel (544)
 
@@ -517,8 +517,11 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// round-to-nearest float -> int for |f| < 2^22: the add leaves round(f) in the low mantissa bits
-__device__ __forceinline__ int fix(float f) { return __float_as_int(f + 12582912.0f) - 0x4B400000; }
+// round-to-nearest integer of the exact product a * b for |a * b| < 2^22: the fused add of
+// 1.5 * 2^23 leaves it in the low mantissa bits (one rounding, one instruction)
+__device__ __forceinline__ int fix_mul(float a, float b) {
+    return __float_as_int(__fmaf_rn(a, b, 12582912.0f)) - 0x4B400000;
+}
 
 struct Tile {
     int t[4][TWORDS];  // momentum x, y, z, mass
@@ -789,10 +792,10 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const float wt = wij * wz[k];
-                        atomicAdd(&T.t[0][row + k], fix(wt * (c0 + As[2] * k)));
-                        atomicAdd(&T.t[1][row + k], fix(wt * (c1 + As[5] * k)));
-                        atomicAdd(&T.t[2][row + k], fix(wt * (c2 + As[8] * k)));
-                        atomicAdd(&T.t[3][row + k], fix(wt * ms));
+                        atomicAdd(&T.t[0][row + k], fix_mul(wt, c0 + As[2] * k));
+                        atomicAdd(&T.t[1][row + k], fix_mul(wt, c1 + As[5] * k));
+                        atomicAdd(&T.t[2][row + k], fix_mul(wt, c2 + As[8] * k));
+                        atomicAdd(&T.t[3][row + k], fix_mul(wt, ms));
                     }
                 }
             }

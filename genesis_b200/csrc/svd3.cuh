@@ -32,17 +32,17 @@ __device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
     const float apq = a[P][Q];
     const float app = a[P][P];
     const float aqq = a[Q][Q];
-    float t = 0.f, c = 1.f, s = 0.f;
-    if (fabsf(apq) > 1e-30f) {
-        // approximate reciprocal / rsqrt: the rotation only needs to be orthogonal to
-        // round-off, which c = rsqrt(1 + t^2), s = t c guarantees whatever t is
-        const float tau = __fdividef(aqq - app, 2.f * apq);
-        const float at = fabsf(tau);
-        const float q = 1.f + tau * tau;
-        t = (at > 1e15f) ? __fdividef(0.5f, tau) : __fdividef(copysignf(1.f, tau), at + q * rsqrtf(q));
-        c = rsqrtf(1.f + t * t);
-        s = t * c;
-    }
+    // approximate reciprocal / rsqrt: the rotation only needs to be orthogonal to
+    // round-off, which c = rsqrt(1 + t^2), s = t c guarantees whatever t is.  Evaluated
+    // without a branch; a (numerically) zero apq selects the identity rotation t = 0,
+    // discarding whatever the division by it produced.
+    const float tau = __fdividef(aqq - app, 2.f * apq);
+    const float at = fabsf(tau);
+    const float q = 1.f + tau * tau;
+    float t = (at > 1e15f) ? __fdividef(0.5f, tau) : __fdividef(copysignf(1.f, tau), at + q * rsqrtf(q));
+    t = (fabsf(apq) > 1e-30f) ? t : 0.f;
+    const float c = rsqrtf(1.f + t * t);
+    const float s = t * c;
     a[P][P] = app - t * apq;
     a[Q][Q] = aqq + t * apq;
     a[P][Q] = 0.f;
@@ -66,14 +66,10 @@ __device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
 
 __device__ __forceinline__ void givens(float a, float b, float& c, float& s) {
     const float r2 = a * a + b * b;
-    if (r2 > 1e-30f) {
-        const float ir = rsqrtf(r2);
-        c = a * ir;
-        s = b * ir;
-    } else {
-        c = 1.f;
-        s = 0.f;
-    }
+    const bool ok = r2 > 1e-30f;  // branch-free: selects the identity for a (near) zero column
+    const float ir = rsqrtf(ok ? r2 : 1.f);
+    c = ok ? a * ir : 1.f;
+    s = ok ? b * ir : 0.f;
 }
 
 template <int I, int J>
