@@ -525,9 +525,9 @@ __device__ __forceinline__ int fix_mul(float a, float b) {
 
 struct Tile {
     int t[4][TWORDS];  // momentum x, y, z, mass
-    float red[2][32];
-    uint32_t mask;
-    int cnt;
+    float red[2][32];  // per-warp payload bounds
+    int wcnt[32];      // per-warp in-tile particle counts
+    int wreach[32];    // per-warp stencil reach into the neighbour blocks (6 bits)
 };
 
 // Grid velocities of the 8^3 tile, float4 per node, with a y-stride of 12 nodes: a
@@ -735,15 +735,13 @@ __device__ __forceinline__ void tile_zero(Tile& T, int P) {
         T.t[2][n] = 0;
         T.t[3][n] = 0;
     }
-    if (threadIdx.x == 0) {
-        T.mask = 0u;
-        T.cnt = 0;
-    }
 }
 
-// Chunk-wide fixed-point scales, the 27-node scatter, the flush of non-empty nodes to the
-// block-major grid and the marking of touched grid blocks.  Must be called by every
-// thread of the CTA (contains barriers); T must be zeroed and a barrier passed before.
+// Chunk-wide fixed-point scales, the marking of the grid blocks the chunk's stencils reach,
+// the 27-node scatter and the flush of non-empty nodes to the block-major grid.  Must be
+// called by every thread of the CTA (contains barriers); T must be zeroed and a barrier
+// passed before.  It ends without a barrier: the flush touches only the tile nodes the
+// thread owns (nd), and the next chunk writes the tile only after two more barriers.
 template <int P>
 __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const mpm_instance& I, int inst,
                                               const BlockCoord& bc, int ox, int oy, int oz, Ws& w, const Nbhd& h,
@@ -752,19 +750,46 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
     const float wbq = warp_max(o.in_tile ? o.bq : 0.f);
     const float wbm = warp_max(o.in_tile ? o.mass : 0.f);
     const unsigned nb = __ballot_sync(0xffffffffu, o.in_tile);
+    // Reach of the in-tile stencils (base .. base + 2) into the neighbour blocks, per axis:
+    // the lower block (tile coordinate 0) iff lx == 0, the upper one (>= 5) iff lx >= 3.
+    // Bits 2a / 2a+1: lower / upper neighbour on axis a.
+    uint32_t reach = 0u;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int l = o.base[a] - (a == 0 ? ox : (a == 1 ? oy : oz));
+        reach |= (__ballot_sync(0xffffffffu, o.in_tile && l == 0) ? 1u : 0u) << (2 * a);
+        reach |= (__ballot_sync(0xffffffffu, o.in_tile && l >= 3) ? 2u : 0u) << (2 * a);
+    }
     if (lane == 0) {
         T.red[0][wid] = wbq;
         T.red[1][wid] = wbm;
-        if (nb) atomicAdd(&T.cnt, __popc(nb));
+        T.wcnt[wid] = __popc(nb);
+        T.wreach[wid] = (int)reach;
     }
     __syncthreads();
     float Bq = 0.f, Bm = 0.f;
+    int cnt = 0;
+    uint32_t rch = 0u;
 #pragma unroll
     for (int i = 0; i < P / 32; ++i) {
         Bq = fmaxf(Bq, T.red[0][i]);
         Bm = fmaxf(Bm, T.red[1][i]);
+        cnt += T.wcnt[i];
+        rch |= (uint32_t)T.wreach[i];
     }
-    const float nin = (float)max(T.cnt, 256);
+    // mark the grid blocks the chunk's stencils reach (a superset of the blocks its flush
+    // writes: per axis the neighbour is included if any stencil reaches into it)
+    if (threadIdx.x < 27 && cnt > 0) {
+        const int e[3] = {threadIdx.x / 9, (threadIdx.x / 3) % 3, threadIdx.x % 3};  // db + 1 per axis
+        bool on = ((h.vx >> e[0]) & (h.vy >> e[1]) & (h.vz >> e[2]) & 1u) != 0u;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (e[a] == 0) on = on && ((rch >> (2 * a)) & 1u);
+            if (e[a] == 2) on = on && ((rch >> (2 * a + 1)) & 1u);
+        }
+        if (on) mark_block(w, inst, I, bc.bx + e[0] - 1, bc.by + e[1] - 1, bc.bz + e[2] - 1);
+    }
+    const float nin = (float)max(cnt, 256);
     // scale = 2^(29 - floor(log2(n * B))): n * B * scale < 2^30
     const float sq = Bq > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bq)))) : 1.f;
     const float sm = Bm > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bm)))) : 1.f;
@@ -838,7 +863,6 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
                 set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
             } else {
                 atomicAdd(&w.mm[a], make_float4((float)m0 * iq, (float)m1 * iq, (float)m2 * iq, (float)mi * im));
-                atomicOr(&T.mask, 1u << ((((d >> 6) & 3) * 9) + (((d >> 8) & 3) * 3) + ((d >> 10) & 3)));
             }
             T.t[0][t] = 0;
             T.t[1][t] = 0;
@@ -846,12 +870,6 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
             T.t[3][t] = 0;
         }
     }
-    __syncthreads();
-    if (threadIdx.x < 27 && ((T.mask >> threadIdx.x) & 1u)) {
-        const int t = threadIdx.x;
-        mark_block(w, inst, I, bc.bx + t / 9 - 1, bc.by + (t / 3) % 3 - 1, bc.bz + t % 3 - 1);
-    }
-    __syncthreads();
 }
 
 template <int P>
