@@ -19,6 +19,7 @@ import torch
 
 from . import _globals
 from . import materials, morphs, options
+from .engine.emitter import Emitter
 from .engine.scene import Scene
 from .exceptions import GenesisException
 
@@ -74,4 +75,4 @@ def destroy():
 EPS = _globals.EPS
 device = None
 
-__all__ = ["init", "destroy", "Scene", "GenesisException", "materials", "morphs", "options", "gpu", "cpu", "cuda"]
+__all__ = ["init", "destroy", "Scene", "Emitter", "GenesisException", "materials", "morphs", "options", "gpu", "cpu", "cuda"]

@@ -47,6 +47,7 @@ class Scene:
         self._other = other_solver_options
         self._sim = Simulator(self, self.sim_options, self.mpm_options, self.b200_options)
         self._entities = []
+        self._emitters = []
         self._is_built = False
         self._B = 1
         self._n_envs = 0
@@ -62,6 +63,26 @@ class Scene:
         ent = self._sim.mpm_solver.add_entity(len(self._entities), material, morph, surface, rng=_globals.rng)
         self._entities.append(ent)
         return ent
+
+    def add_emitter(self, material, max_particles=20000, surface=None):
+        """A particle emitter backed by a Nowhere entity of max_particles inactive particles
+        (scene.py:664-718); particles are recycled once the limit is reached."""
+        from ..morphs import Nowhere
+        from .emitter import Emitter
+
+        if self.sim_options.requires_grad:
+            raise GenesisException("Emitter is not supported in differentiable mode.")
+        if not isinstance(material, _materials.MPM.Base):
+            raise GenesisException("Non-supported material for emitter. Supported materials are: `gs.materials.MPM.Base`.")
+        emitter = Emitter(max_particles)
+        entity = self.add_entity(morph=Nowhere(n_particles=max_particles), material=material, surface=surface)
+        emitter.set_entity(entity)
+        self._emitters.append(emitter)
+        return emitter
+
+    @property
+    def emitters(self):
+        return self._emitters
 
     def build(self, n_envs=0, env_spacing=(0.0, 0.0), n_envs_per_row=None, center_envs_at_origin=True,
               compile_kernels=None):
@@ -109,6 +130,8 @@ class Scene:
             mpm_state = state.solvers_state[0] if isinstance(state, SimState) else state
             self._sim.mpm_solver.set_state(0, mpm_state, envs_idx=envs_idx)
         self._sim._queried_states.clear()  # simulator.py:227, 238
+        for emitter in self._emitters:  # scene.py:893-895
+            emitter.reset()
         if envs_idx is None:
             self._sim._cur_substep_global = 0
 
