@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -46,6 +46,7 @@ PROBF_NONFREE = 1
 MAT_ELASTIC, MAT_ELASTOPLASTIC, MAT_LIQUID, MAT_SAND, MAT_SNOW = 0, 1, 2, 3, 4
 MATF_NEOHOOKEAN = 1
 MATF_VON_MISES = 2
+MATF_MUSCLE = 4
 
 
 class NativeLibraryError(RuntimeError):
@@ -93,7 +94,7 @@ class Material(C.Structure):
         ("vm_threshold", C.c_float),
         ("sand_c1", C.c_float),
         ("sand_alpha", C.c_float),
-        ("pad0", C.c_float),
+        ("muscle_stiffness", C.c_float),
     ]
 
 
@@ -120,6 +121,8 @@ class Particles(C.Structure):
         ("slot", C.c_void_p),
         ("mu_p", C.c_void_p),
         ("lam_p", C.c_void_p),
+        ("actu", C.c_void_p),
+        ("muscle_dir", C.c_void_p),
     ]
 
 

@@ -626,6 +626,20 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
     const float J = Sg[0] * (Sg[1] * Sg[2]);
     float Fn[9], stress[9], Jpn;
     constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, stress);
+    if ((m.flags & MPM_MATF_MUSCLE) && par.actu) {
+        // muscle.py:57-65: + stiffness * actu * F_tmp d d^T F_tmp^T; a Muscle is an Elastic,
+        // whose F_new is F_tmp, so Fn stands in for F_tmp here
+        const int g = par.gid[p];
+        const float dd[3] = {par.muscle_dir[3 * g], par.muscle_dir[3 * g + 1], par.muscle_dir[3 * g + 2]};
+        const float k = m.muscle_stiffness * par.actu[g];
+        float fd[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) fd[i] = Fn[i * 3] * dd[0] + Fn[i * 3 + 1] * dd[1] + Fn[i * 3 + 2] * dd[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) stress[i * 3 + j] += k * fd[i] * fd[j];
+    }
 #pragma unroll
     for (int k = 0; k < 9; ++k) S[(MPM_CH_F + k) * st + p] = Fn[k];
     S[MPM_CH_JP * st + p] = Jpn;
@@ -1324,6 +1338,7 @@ static int check_par(const mpm_problem* p, const mpm_particles* par) {
     if (!par || !par->state || !par->mat || !par->pflags || !par->gid || !par->slot) return MPM_E_INVALID;
     if (par->state_stride < p->n_particles) return MPM_E_INVALID;
     if ((par->mu_p == nullptr) != (par->lam_p == nullptr)) return MPM_E_INVALID;
+    if ((par->actu == nullptr) != (par->muscle_dir == nullptr)) return MPM_E_INVALID;
     return MPM_OK;
 }
 

@@ -119,7 +119,7 @@ class Emitter:
                                             sampler=sampler, rng=self._rng)
         R = gu.z_up_to_R(direction) @ gu.axis_angle_to_R(np.array([0.0, 0.0, 1.0]), theta)
         positions = gu.transform_by_trans_R(positions, np.asarray(pos, dtype=np.float64), R)
-        vels = np.broadcast_to(speed * direction, positions.shape)
+        vels = np.tile(speed * direction, (len(positions), 1))
         return self._activate(positions, vels)
 
     def emit_omni(self, source_radius=0.1, pos=(0.5, 0.5, 1.0), speed=1.0, particle_size=None):

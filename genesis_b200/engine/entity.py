@@ -45,7 +45,7 @@ class MPMEntity:
         self._n_particles = len(self._particles)
         origin = np.asarray(morph.pos, dtype=np.float64)
         self._init_particles_offset = self._particles - origin
-        self._tgt = {"pos": None, "vel": None, "act": None}
+        self._tgt = {"pos": None, "vel": None, "act": None, "actu": None}
 
     # ------------------------------------------------------------ properties
     @property
@@ -169,6 +169,71 @@ class MPMEntity:
     def set_active(self, active, envs_idx=None):
         self._tgt["act"] = (_as_tensor(active, torch.uint8, self._solver.device), envs_idx)
 
+    # ---------------------------------------------------------------- muscle
+    def _assert_muscle(self):
+        from ..materials.MPM import Muscle
+
+        if not isinstance(self._material, Muscle):
+            raise GenesisException("This method is only supported by entities with a 'MPM.Muscle' material.")
+
+    def set_actuation(self, actus, envs_idx=None):
+        """Buffered per-group actuation applied at the next step (mpm_entity.py:412-427):
+        actus of shape ([M,] [n_particles,] [n_groups,]); a scalar applies to every group."""
+        self._assert_muscle()
+        a = _as_tensor(actus, torch.float32, self._solver.device)
+        if a.ndim == 0:
+            a = a.reshape((1,)).expand((self._material.n_groups,))
+        self._tgt["actu"] = (a, envs_idx)
+
+    def set_particles_actu(self, actus, particles_idx_local=None, envs_idx=None):
+        """Each particle takes the value of its muscle group (mpm_entity.py:429-451,
+        mpm_solver.py:922-934); actus of shape ([M,] [n_particles,] [n_groups,])."""
+        self._assert_muscle()
+        self._check_built()
+        idx = self._flat_idx(particles_idx_local, envs_idx)
+        G = self._material.n_groups
+        a = _as_tensor(actus, torch.float32, self._solver.device)
+        a = a.reshape(a.shape[:-1] + (G,)) if a.ndim else a.reshape(1).expand(G)
+        a = a.expand(idx.shape + (G,)).reshape(-1, G)
+        self._solver.runtime.set_actu_by_group(idx.reshape(-1), a)
+
+    def get_particles_actu(self, envs_idx=None):
+        self._assert_muscle()
+        self._check_built()
+        idx = self._flat_idx(None, envs_idx)
+        return self._squeeze(self._solver.runtime.get_actu(idx.reshape(-1)).reshape(idx.shape))
+
+    def _all_env_idx(self):
+        return self._flat_idx(None, None)  # (B, n_particles)
+
+    def set_muscle_group(self, muscle_group):
+        """Muscle group of each particle, shape (n_particles,) (mpm_entity.py:475-493)."""
+        self._assert_muscle()
+        self._check_built()
+        idx = self._all_env_idx()
+        g = _as_tensor(muscle_group, torch.int64, self._solver.device).reshape(-1).expand(idx.shape)
+        self._solver.runtime.set_muscle_group(idx.reshape(-1), g.reshape(-1))
+
+    def get_muscle_group(self):
+        self._assert_muscle()
+        self._check_built()
+        return self._solver.runtime.get_muscle_group(self._all_env_idx()[0]).to(torch.int32)
+
+    def set_muscle_direction(self, muscle_direction):
+        """Fibre direction of each particle, shape ([n_particles,] 3) (mpm_entity.py:495-517)."""
+        self._assert_muscle()
+        self._check_built()
+        idx = self._all_env_idx()
+        d = _as_tensor(muscle_direction, torch.float32, self._solver.device).reshape(-1, 3)
+        d = d.expand(idx.shape[1], 3) if d.shape[0] == 1 else d
+        self._solver.runtime.set_muscle_direction(idx.reshape(-1), d.expand(idx.shape + (3,)).reshape(-1, 3))
+
+    def set_muscle(self, muscle_group=None, muscle_direction=None):
+        if muscle_group is not None:
+            self.set_muscle_group(muscle_group)
+        if muscle_direction is not None:
+            self.set_muscle_direction(muscle_direction)
+
     def process_input(self, in_backward=False):
         # positions first: setting positions resets velocities (particle_entity.py:439-440)
         if self._tgt["pos"] is not None:
@@ -186,6 +251,9 @@ class MPMEntity:
             if v.ndim == 0:
                 v = v.expand(self._n_particles)
             self.set_particles_active(v, envs_idx=e)
+        if self._tgt.get("actu") is not None:
+            v, e = self._tgt["actu"]
+            self.set_particles_actu(v, envs_idx=e)
         for k in self._tgt:
             self._tgt[k] = None
 

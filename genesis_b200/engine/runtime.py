@@ -165,6 +165,15 @@ class MPMRuntime:
         if per_particle_lame:
             self.mu_p = torch.zeros(max(self.n, 1), dtype=torch.float32, device=dev)
             self.lam_p = torch.zeros(max(self.n, 1), dtype=torch.float32, device=dev)
+        # muscle inputs in API order (mpm_solver.py:787-788, 801: group 0, direction +z,
+        # actuation 0), allocated only when a Muscle material is present
+        self.actu = self.muscle_dir = self.muscle_group = None
+        if any(m.flags & nat.MATF_MUSCLE for m in mats):
+            nn = max(self.n, 1)
+            self.actu = torch.zeros(nn, dtype=torch.float32, device=dev)
+            self.muscle_dir = torch.zeros((nn, 3), dtype=torch.float32, device=dev)
+            self.muscle_dir[:, 2] = 1.0
+            self.muscle_group = torch.zeros(nn, dtype=torch.int64, device=dev)
         self.par = nat.Particles(
             state=self.state.data_ptr(),
             state_stride=self.stride,
@@ -174,6 +183,8 @@ class MPMRuntime:
             slot=self.slot.data_ptr(),
             mu_p=self.mu_p.data_ptr() if self.mu_p is not None else None,
             lam_p=self.lam_p.data_ptr() if self.lam_p is not None else None,
+            actu=self.actu.data_ptr() if self.actu is not None else None,
+            muscle_dir=self.muscle_dir.data_ptr() if self.muscle_dir is not None else None,
         )
         nbytes = C.c_uint64()
         nat.check("mpm_workspace_bytes", self.lib.mpm_workspace_bytes(C.byref(self.prob), C.byref(nbytes)))
@@ -195,6 +206,8 @@ class MPMRuntime:
         t = self.state.numel() * 4 + self.mat.numel() * 10 + self.workspace_bytes
         if self.mu_p is not None:
             t += self.mu_p.numel() * 8
+        if self.actu is not None:
+            t += self.actu.numel() * 24
         return int(t)
 
     # -------------------------------------------------------------- state I/O
@@ -239,6 +252,38 @@ class MPMRuntime:
         sl = self.slot[: self.n].long()
         self.mu_p[sl] = mu
         self.lam_p[sl] = lam
+
+    # ---------------------------------------------------------------- muscle
+    def _need_muscle(self):
+        if self.actu is None:
+            raise RuntimeError("runtime has no Muscle material")
+
+    def set_actu_by_group(self, idx, actus):
+        """_kernel_set_particles_actu (mpm_solver.py:922-934): particle idx[i] takes
+        actus[i, muscle_group[idx[i]]]; idx are API-order indices, actus [len(idx), n_groups]."""
+        self._need_muscle()
+        idx = torch.as_tensor(idx, dtype=torch.int64, device=self.device).reshape(-1)
+        actus = torch.as_tensor(actus, dtype=torch.float32, device=self.device).reshape(idx.numel(), -1)
+        g = self.muscle_group[idx].clamp(0, actus.shape[1] - 1)
+        self.actu[idx] = torch.gather(actus, 1, g[:, None])[:, 0]
+
+    def get_actu(self, idx):
+        self._need_muscle()
+        return self.actu[torch.as_tensor(idx, dtype=torch.int64, device=self.device).reshape(-1)]
+
+    def set_muscle_group(self, idx, group):
+        self._need_muscle()
+        idx = torch.as_tensor(idx, dtype=torch.int64, device=self.device).reshape(-1)
+        self.muscle_group[idx] = torch.as_tensor(group, dtype=torch.int64, device=self.device).reshape(-1)
+
+    def get_muscle_group(self, idx):
+        self._need_muscle()
+        return self.muscle_group[torch.as_tensor(idx, dtype=torch.int64, device=self.device).reshape(-1)]
+
+    def set_muscle_direction(self, idx, direction):
+        self._need_muscle()
+        idx = torch.as_tensor(idx, dtype=torch.int64, device=self.device).reshape(-1)
+        self.muscle_dir[idx] = torch.as_tensor(direction, dtype=torch.float32, device=self.device).reshape(-1, 3)
 
     def get_state(self, which=("pos", "vel", "C", "F", "Jp", "active")):
         """State in API order as device tensors: pos/vel [n,3], C/F [n,3,3], Jp [n], active [n] bool."""

@@ -1,7 +1,7 @@
 """gs.materials.MPM.* with the reference constructors, defaults and properties.
 
 Each class restates its reference counterpart's parameters
-(genesis/engine/materials/MPM/{base,elastic,elasto_plastic,liquid,sand,snow}.py);
+(genesis/engine/materials/MPM/{base,elastic,elasto_plastic,liquid,sand,snow,muscle}.py);
 the constitutive arithmetic itself runs in the CUDA kernel (csrc/constitutive.cuh),
 selected by ``kind`` from a device material table.
 """
@@ -70,6 +70,7 @@ class Base:
         m.vm_threshold = 0.0
         m.sand_c1 = 0.0
         m.sand_alpha = 0.0
+        m.muscle_stiffness = 0.0
         return m
 
     @property
@@ -231,4 +232,31 @@ class Snow(ElastoPlastic):
                          yield_higher=yield_higher, use_von_mises=False)
 
 
-__all__ = ["Base", "Elastic", "ElastoPlastic", "Liquid", "Sand", "Snow"]
+class Muscle(Elastic):
+    """Actuated elastic material (materials/MPM/muscle.py:8-75): the Elastic stress plus
+    stiffness * actu * F_tmp (d d^T) F_tmp^T, with stiffness = E, per-particle actuation
+    actu (set per muscle group) and fibre direction d."""
+
+    def __init__(self, E=1e6, nu=0.2, rho=1000.0, lam=None, mu=None, sampler=None, model="neohooken", n_groups=1):
+        super().__init__(E, nu, rho, lam, mu, sampler, model)
+        self._stiffness = E  # muscle.py:54: Young's modulus is the muscle stiffness
+        self._n_groups = int(n_groups)
+
+    def _native(self, p_vol):
+        m = super()._native(p_vol)
+        m.flags |= nat.MATF_MUSCLE
+        m.muscle_stiffness = float(self._stiffness)
+        return m
+
+    @property
+    def stiffness(self):
+        """Muscle stiffness."""
+        return self._stiffness
+
+    @property
+    def n_groups(self):
+        """Number of muscle groups."""
+        return self._n_groups
+
+
+__all__ = ["Base", "Elastic", "ElastoPlastic", "Liquid", "Sand", "Snow", "Muscle"]

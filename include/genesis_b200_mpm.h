@@ -32,6 +32,8 @@
  *     gid     int32[n]  original (API-order) global index of the particle in slot s
  *     slot    int32[n]  inverse of gid: slot of the particle with original index i
  *     mu_p, lam_p  float[n] optional per-particle Lame parameters (NULL: use the table)
+ *     actu, muscle_dir  optional muscle inputs in API (original) order, read through gid:
+ *             float[n] actuation and float[n][3] fibre direction; both or neither
  *   grid: block-major, MPM_BLOCK^3 nodes per block, blocks of instance k start at
  *     instances[k].blk_base; workspace-resident (see mpm_workspace_bytes).
  */
@@ -45,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 1
+#define MPM_ABI_VERSION 2
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -79,6 +81,8 @@ extern "C" {
 
 #define MPM_MATF_NEOHOOKEAN 1    /* Elastic(model="neohooken") */
 #define MPM_MATF_VON_MISES 2     /* ElastoPlastic(use_von_mises=True) */
+#define MPM_MATF_MUSCLE 4        /* Muscle: Elastic stress + muscle_stiffness * actu * (F_tmp d)(F_tmp d)^T
+                                    with fibre direction d (muscle.py:57-65) */
 
 /* problem flags */
 #define MPM_PROBF_NONFREE 1      /* some particles are non-free: run the stencil-zeroing pass after p2g */
@@ -115,7 +119,7 @@ typedef struct mpm_material {
     float vm_threshold;    /* von_mises_yield_stress / (2 mu) (elasto_plastic.py:75) */
     float sand_c1;         /* (3 lam + 2 mu) / (2 mu)         (sand.py:67) */
     float sand_alpha;      /* sqrt(2/3) * 2 sin(phi) / (3 - sin(phi)) (sand.py:47-49) */
-    float pad0;
+    float muscle_stiffness; /* Muscle: its Young's modulus (muscle.py:54) */
 } mpm_material;
 
 /* Sizes of one problem (one or many instances advanced together). */
@@ -139,6 +143,8 @@ typedef struct mpm_particles {
     int32_t* slot;
     float* mu_p;   /* optional */
     float* lam_p;  /* optional */
+    const float* actu;        /* optional, float[n] in API order: actuation (mpm_solver.py:91, 922-934) */
+    const float* muscle_dir;  /* optional, float[n][3] in API order: fibre direction (mpm_solver.py:108) */
 } mpm_particles;
 
 typedef struct mpm_tables {

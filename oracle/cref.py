@@ -46,6 +46,7 @@ def _structs(dtype):
             ("kind", C.c_int32), ("flags", C.c_int32),
             ("mu", Rt), ("lam", Rt), ("mass", Rt),
             ("clamp_lo", Rt), ("clamp_hi", Rt), ("vm_threshold", Rt), ("sand_c1", Rt), ("sand_alpha", Rt),
+            ("muscle_stiffness", Rt),
         ]
 
     return Params, Mat
@@ -62,6 +63,7 @@ def lib(dtype):
         L = C.CDLL(path)
         L.ref_substeps.restype = C.c_int
         L.ref_substeps_lame.restype = C.c_int
+        L.ref_substeps_ext.restype = C.c_int
         L.ref_max_threads.restype = C.c_int
         _libs[key] = L
     return _libs[key]
@@ -91,7 +93,7 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     marr = (Mat * len(mats))()
     for i, m in enumerate(mats):
         flags = (1 if (m.kind == R.KIND_ELASTIC and m.neohookean) else 0) | (
-            2 if (m.kind == R.KIND_ELASTOPLASTIC and m.use_von_mises) else 0)
+            2 if (m.kind == R.KIND_ELASTOPLASTIC and m.use_von_mises) else 0) | (4 if m.muscle else 0)
         marr[i].kind = m.kind
         marr[i].flags = flags
         marr[i].mu, marr[i].lam = m.mu, m.lam
@@ -100,6 +102,7 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
         marr[i].vm_threshold = m.von_mises_yield_stress / (2 * m.mu) if m.mu else 0.0
         marr[i].sand_c1 = (3 * m.lam + 2 * m.mu) / (2 * m.mu) if m.mu else 0.0
         marr[i].sand_alpha = m.alpha
+        marr[i].muscle_stiffness = m.stiffness if m.muscle else 0.0
     n = st["x"].shape[0]
     x = np.ascontiguousarray(st["x"], dtype=dt).copy()
     v = np.ascontiguousarray(st["v"], dtype=dt).copy()
@@ -112,7 +115,16 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     grid = np.zeros(4 * G, dtype=dt)
     gvel = np.zeros(3 * G, dtype=dt)
     ptr = lambda a: a.ctypes.data_as(C.c_void_p)
-    if mu_p is not None:
+    if st.get("actu") is not None:
+        actu = np.ascontiguousarray(st["actu"], dtype=dt)
+        mdir = np.ascontiguousarray(st["mdir"], dtype=dt).reshape(n, 3)
+        mu_a = np.ascontiguousarray(mu_p, dtype=dt) if mu_p is not None else None
+        lam_a = np.ascontiguousarray(lam_p, dtype=dt) if lam_p is not None else None
+        rc = L.ref_substeps_ext(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
+                                int(n_substeps), ptr(grid), ptr(gvel), int(n_threads),
+                                ptr(mu_a) if mu_a is not None else None, ptr(lam_a) if lam_a is not None else None,
+                                ptr(actu), ptr(mdir))
+    elif mu_p is not None:
         mu_a = np.ascontiguousarray(mu_p, dtype=dt)
         lam_a = np.ascontiguousarray(lam_p, dtype=dt)
         rc = L.ref_substeps_lame(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),

@@ -62,9 +62,10 @@ typedef struct {
 
 typedef struct {
     int32_t kind; /* 0 elastic 1 elastoplastic 2 liquid 3 sand 4 snow */
-    int32_t flags; /* 1 neohookean, 2 von mises */
+    int32_t flags; /* 1 neohookean, 2 von mises, 4 muscle */
     REAL mu, lam, mass;
     REAL clamp_lo, clamp_hi, vm_threshold, sand_c1, sand_alpha;
+    REAL muscle_stiffness; /* muscle.py:54 (E) */
 } ref_material;
 
 /* ---------------------------------------------------------------- SVD */
@@ -289,6 +290,9 @@ static inline int64_t gidx(const ref_params* p, int i, int j, int k) {
 int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
                       REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
                       int n_threads, const REAL* mu_p, const REAL* lam_p);
+int ref_substeps_ext(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                     REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                     int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir);
 
 int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F, REAL* Jp,
                  const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel, int n_threads) {
@@ -299,6 +303,15 @@ int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, 
 int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
                       REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
                       int n_threads, const REAL* mu_p, const REAL* lam_p) {
+    return ref_substeps_ext(p, mats, n, x, v, C, F, Jp, mat, active, n_substeps, grid, gvel, n_threads, mu_p, lam_p,
+                            NULL, NULL);
+}
+
+/* as ref_substeps_lame, with optional per-particle muscle actuation actu[n] and fibre
+ * direction mdir[n*3] (NULL: no actuation) */
+int ref_substeps_ext(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                     REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                     int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir) {
 #ifdef _OPENMP
     if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
@@ -333,6 +346,15 @@ int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL
                 m = &mp;
             }
             constitutive(m, p->eps, J, Ft, U, S, V, Jp[i], Fn, &Jpn, st);
+            if ((m->flags & 4) && actu) {
+                /* muscle.py:57-65: stress += stiffness * actu * F_tmp (d d^T) F_tmp^T */
+                const REAL* d = mdir + 3 * i;
+                REAL fd[3];
+                for (int a = 0; a < 3; ++a) fd[a] = Ft[a * 3] * d[0] + Ft[a * 3 + 1] * d[1] + Ft[a * 3 + 2] * d[2];
+                const REAL k = m->muscle_stiffness * actu[i];
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) st[a * 3 + b] += k * fd[a] * fd[b];
+            }
             memcpy(Fi, Fn, 9 * sizeof(REAL));
             Jp[i] = Jpn;
             REAL A[9];

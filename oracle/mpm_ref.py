@@ -71,6 +71,8 @@ class Material:
     yield_lower: float = 2.5e-2
     yield_higher: float = 4.5e-3
     friction_angle: float = 45.0  # Sand, degrees (sand.py:41-49)
+    muscle: bool = False  # Muscle: an Elastic with actuation stress (muscle.py:8-65)
+    stiffness: float = 0.0  # Muscle stiffness = E (muscle.py:54)
 
     @property
     def alpha(self) -> float:
@@ -87,6 +89,12 @@ def make_material(kind: str, **kw) -> Material:
     default_Jp=0 (sand.py:45).  Snow is the non-von-Mises ElastoPlastic (snow.py:50-60).
     """
     kind = kind.lower()
+    muscle = kind == "muscle"
+    if muscle:  # muscle.py:35-55: Elastic with E=1e6 and model "neohooken" by default
+        kind = "elastic"
+        kw.setdefault("E", 1e6)
+        kw.setdefault("model", "neohooken")
+        kw.pop("n_groups", None)
     viscous = kw.pop("viscous", False)
     model = kw.pop("model", "corotation")
     E = kw.pop("E", 3e5 if kind == "elastic" else 1e6)
@@ -101,6 +109,9 @@ def make_material(kind: str, **kw) -> Material:
     m = Material(kind=KIND_NAMES.index(kind), E=E, nu=nu, mu=mu, lam=lam, **kw)
     if kind == "elastic":
         m.neohookean = model == "neohooken"
+        if muscle:
+            m.muscle = True
+            m.stiffness = E
     elif kind == "liquid":
         if not viscous:
             m.mu = 0.0
@@ -242,7 +253,17 @@ def update_F_S_Jp(mat: Material, eps: float, J, F_tmp, U, S, V, Jp):
     raise ValueError(f"unknown material kind {k}")
 
 
-def update_stress(mat: Material, U, S_new, V, F_tmp, F_new, J, Jp_old):
+def update_stress(mat: Material, U, S_new, V, F_tmp, F_new, J, Jp_old, actu=None, mdir=None):
+    s = _update_stress(mat, U, S_new, V, F_tmp, F_new, J, Jp_old)
+    if mat.muscle and actu is not None:
+        # muscle.py:57-65: + stiffness * actu * F_tmp (d d^T) F_tmp^T
+        dt = F_tmp.dtype.type
+        fd = np.einsum("nij,nj->ni", F_tmp, mdir.astype(F_tmp.dtype))
+        s = s + (dt(mat.stiffness) * actu.astype(F_tmp.dtype))[:, None, None] * fd[:, :, None] * fd[:, None, :]
+    return s
+
+
+def _update_stress(mat: Material, U, S_new, V, F_tmp, F_new, J, Jp_old):
     dt = F_tmp.dtype.type
     n = F_tmp.shape[0]
     eye = np.broadcast_to(np.eye(3, dtype=F_tmp.dtype), (n, 3, 3))
@@ -337,7 +358,9 @@ def p2g(p: Params, mats: list[Material], st: dict):
         f_n, s_n, j_n = update_F_S_Jp(mat, p.eps, J[sel], F_tmp[sel], U[sel], S[sel], V[sel], Jp[act][sel])
         Fn[sel] = f_n
         Jn[sel] = j_n
-        stress[sel] = update_stress(mat, U[sel], s_n, V[sel], F_tmp[sel], f_n, J[sel], Jp[act][sel])
+        actu = st["actu"][act][sel] if st.get("actu") is not None else None
+        mdir = st["mdir"][act][sel] if st.get("mdir") is not None else None
+        stress[sel] = update_stress(mat, U[sel], s_n, V[sel], F_tmp[sel], f_n, J[sel], Jp[act][sel], actu, mdir)
         mass[sel] = particle_mass(p, mat)
     F_new[act] = Fn
     Jp_new[act] = Jn

@@ -80,3 +80,15 @@ def test_check_nan_option_is_validated():
     gs.options.B200Options(check_nan="async")
     with pytest.raises(gs.GenesisException):
         gs.options.B200Options(check_nan="sometimes")
+
+
+def test_muscle_material_follows_reference():
+    from genesis_b200 import _native as nat
+
+    m = gs.materials.MPM.Muscle()
+    assert m.E == 1e6 and m.stiffness == 1e6 and m.n_groups == 1 and m.model == "neohooken"
+    nm = m._native(1e-3)
+    assert nm.kind == nat.MAT_ELASTIC and nm.flags & nat.MATF_MUSCLE and nm.flags & nat.MATF_NEOHOOKEAN
+    assert nm.muscle_stiffness == 1e6
+    assert isinstance(m, gs.materials.MPM.Elastic)
+    assert gs.materials.MPM.Elastic()._native(1e-3).muscle_stiffness == 0.0

@@ -37,7 +37,8 @@ def test_emitted_particles_activate_and_fall():
     assert int(act.sum()) == total > 0
     pos = ent.get_particles_pos()[act]
     vel = ent.get_particles_vel()[act]
-    assert torch.isfinite(pos).all() and (pos[:, 2] < 0.6).all()
+    # droplets are emitted centred on the nozzle (z 0.59..0.61) and have moved down since
+    assert torch.isfinite(pos).all() and (pos[:, 2] < 0.61 - 1e-3).all()
     assert float(vel[:, 2].mean()) < -1.9  # launched at 2 m/s downwards, still accelerating
     assert scene.check_state() == 0
 

@@ -168,3 +168,41 @@ def test_f32_oracle_error_is_small_over_100_substeps():
     a, _ = cref.substeps(*bridge.from_desc(d, np.float64), 100)
     b, _ = cref.substeps(*bridge.from_desc(d, np.float32), 100)
     assert np.abs(a["x"] - b["x"]).max() < 1e-5
+
+
+def _muscle_case(actu_value, n_side=8, dtype=np.float64):
+    rng = np.random.default_rng(7)
+    x = W.jittered_lattice(rng, n_side, (0.45, 0.45, 0.45), 0.1 / n_side)
+    n = x.shape[0]
+    p = R.Params(grid_density=64, dt=1e-4, gravity=(0.0, 0.0, 0.0), dtype=dtype)
+    mats = [R.make_material("muscle", E=1e5)]
+    st = R.make_state(x, mats, np.zeros(n, np.int64), dtype)
+    st["actu"] = np.full(n, actu_value, dtype=dtype)
+    st["mdir"] = np.tile(np.array([0.0, 0.0, 1.0], dtype=dtype), (n, 1))
+    return p, mats, st
+
+
+def test_muscle_material_defaults_and_oracles_agree():
+    """Muscle (muscle.py:35-65): an Elastic with E=1e6 and the neo-Hookean model by default;
+    the numpy and C restatements of the actuation stress agree."""
+    m = R.make_material("muscle")
+    assert m.muscle and m.neohookean and m.stiffness == 1e6 and m.kind == R.KIND_ELASTIC
+    p, mats, st = _muscle_case(2.0)
+    o_np = R.run(p, mats, st, 5)
+    o_c, rc = cref.substeps(p, mats, st, 5)
+    assert rc == 0
+    assert np.abs(o_np["x"] - o_c["x"]).max() < 1e-12
+    assert np.abs(o_np["F"] - o_c["F"]).max() < 1e-9
+
+
+def test_muscle_actuation_contracts_along_the_fibre():
+    """A positive actuation adds tension along d = +z: the block shortens along z and not
+    along x (no gravity), while an unactuated block stays at rest."""
+    p, mats, st = _muscle_case(5.0)
+    o, _ = cref.substeps(p, mats, st, 200)
+    p0, m0, s0 = _muscle_case(0.0)
+    r, _ = cref.substeps(p0, m0, s0, 200)
+    ext = lambda a, d: a[:, d].max() - a[:, d].min()
+    assert ext(o["x"], 2) < ext(st["x"], 2) - 1e-5
+    assert abs(ext(r["x"], 2) - ext(st["x"], 2)) < 1e-9
+    assert ext(o["x"], 2) < ext(o["x"], 0)
