@@ -162,6 +162,8 @@ SIGNATURES = {
     "mpm_set_particles_vel": (C.c_int, [_P(Problem), _P(Particles), i32, vp, vp, vp]),
     "mpm_set_particles_active": (C.c_int, [_P(Problem), _P(Particles), i32, vp, vp, vp]),
     "mpm_set_particles_free": (C.c_int, [_P(Problem), _P(Particles), i32, vp, vp, vp]),
+    "mpm_update_render_fields": (C.c_int, [_P(Problem), _P(Particles), i32, i32, vp, vp, vp, i32, i32, vp, vp, vp,
+                                           vp, vp]),
     "mpm_graph_create": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp, _P(vp)]),
     "mpm_graph_launch": (C.c_int, [vp, vp]),
     "mpm_graph_destroy": (C.c_int, [vp]),

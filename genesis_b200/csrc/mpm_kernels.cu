@@ -1777,6 +1777,72 @@ int mpm_set_particles_free(const mpm_problem* prob, mpm_particles* par, int32_t 
     return cuda_ok();
 }
 
+// Render fields (mpm_solver.py:743-766).  Threads [0, n) handle particles in API order,
+// threads [n, n + n_envs * n_vverts) the visual vertices; every read goes through the
+// slot map, so the particles' sort order does not matter.
+__global__ void k_render_fields(mpm_problem prob, mpm_particles par, int n_per_env, float* rpos, float* rvel,
+                                uint8_t* ract, int n_vverts, int K, const int* sidx, const float* sw, float* vpos,
+                                uint8_t* vact) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = prob.n_particles;
+    const int64_t st = par.state_stride;
+    if (t < n) {
+        const int s = par.slot[t];
+        const bool on = par.pflags[s] & MPM_PFLAG_ACTIVE;
+        if (rpos) {
+            // gu.ti_nowhere() (utils/geom.py:1703-1705) for inactive particles
+            rpos[3 * t + 0] = on ? par.state[(MPM_CH_X + 0) * st + s] : 2333333.0f;
+            rpos[3 * t + 1] = on ? par.state[(MPM_CH_X + 1) * st + s] : 6666666.0f;
+            rpos[3 * t + 2] = on ? par.state[(MPM_CH_X + 2) * st + s] : 5201314.0f;
+        }
+        if (rvel && on) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) rvel[3 * t + d] = par.state[(MPM_CH_V + d) * st + s];
+        }
+        if (ract) ract[t] = on ? 1 : 0;
+        return;
+    }
+    const int64_t u = t - n;  // (env, vvert)
+    const int n_envs = n_per_env > 0 ? n / n_per_env : 0;
+    if (u >= (int64_t)n_envs * n_vverts) return;
+    const int e = (int)(u / n_vverts), v = (int)(u % n_vverts);
+    float acc[3] = {0.f, 0.f, 0.f};
+    int first = -1;
+    for (int j = 0; j < K; ++j) {
+        const int q = sidx[(int64_t)v * K + j];
+        if (q < 0 || q >= n_per_env) continue;  // host-computed; bounds-checked all the same
+        const int s = par.slot[e * n_per_env + q];
+        if (first < 0) first = s;
+        const float wj = sw[(int64_t)v * K + j];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) acc[d] += wj * par.state[(MPM_CH_X + d) * st + s];
+    }
+    if (vpos) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vpos[3 * u + d] = acc[d];
+    }
+    if (vact) vact[u] = (first >= 0 && (par.pflags[first] & MPM_PFLAG_ACTIVE)) ? 1 : 0;
+}
+
+int mpm_update_render_fields(const mpm_problem* prob, const mpm_particles* par, int32_t n_envs, int32_t n_per_env,
+                             float* render_pos, float* render_vel, uint8_t* render_active, int32_t n_vverts,
+                             int32_t n_supports, const int32_t* support_idx, const float* support_w, float* vvert_pos,
+                             uint8_t* vvert_active, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (n_envs < 1 || n_per_env < 0 || (int64_t)n_envs * n_per_env != prob->n_particles) return MPM_E_INVALID;
+    if (n_vverts < 0 || (n_vverts > 0 && (n_supports < 1 || !support_idx || !support_w))) return MPM_E_INVALID;
+    const int64_t total = (int64_t)prob->n_particles + (int64_t)n_envs * n_vverts;
+    if (total > 0) {
+        const int T = 256;
+        k_render_fields<<<(int)((total + T - 1) / T), T, 0, (cudaStream_t)stream>>>(
+            *prob, *par, n_per_env, render_pos, render_vel, render_active, n_vverts, n_supports, support_idx,
+            support_w, vvert_pos, vvert_active);
+    }
+    return cuda_ok();
+}
+
 struct GraphHandle {
     cudaGraph_t graph;
     cudaGraphExec_t exec;

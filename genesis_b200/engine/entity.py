@@ -17,6 +17,23 @@ def _as_tensor(x, dtype, device):
     return torch.as_tensor(np.asarray(x), dtype=dtype, device=device)
 
 
+def skinning_supports(particles, vverts, K):
+    """particle_entity.py:192-226: the K nearest particles of each visual vertex, and
+    weights b with sum 1 that reproduce the vertex from them, b[:-1] = pinv(P) (v - p_K)
+    where the columns of P are p_j - p_K.  Returns (local indices int32 [V, K], weights
+    float32 [V, K])."""
+    from scipy.spatial import cKDTree
+
+    particles = np.asarray(particles, dtype=np.float64)
+    _, idx = cKDTree(particles).query(vverts, k=K)
+    idx = np.clip(np.asarray(idx).reshape(len(vverts), K), 0, len(particles) - 1)
+    ps = particles[idx]
+    P = np.swapaxes(ps[:, :-1], -2, -1) - ps[:, -1][..., None]
+    b = np.einsum("vij,vj->vi", np.linalg.pinv(P), vverts - ps[:, -1])
+    w = np.concatenate([b, 1.0 - b.sum(axis=1, keepdims=True)], axis=1)
+    return idx.astype(np.int32), w.astype(np.float32)
+
+
 class MPMEntity:
     def __init__(self, scene, solver, material, morph, surface, particle_size, idx, particle_start, rng=None):
         self._scene = scene
@@ -43,9 +60,50 @@ class MPMEntity:
                 f"max: {self._particles.max(0)}\n"
             )
         self._n_particles = len(self._particles)
+        self._init_skinning(scene)
         origin = np.asarray(morph.pos, dtype=np.float64)
         self._init_particles_offset = self._particles - origin
         self._tgt = {"pos": None, "vel": None, "act": None, "actu": None}
+
+    # ------------------------------------------------------------ skinning
+    def _init_skinning(self, scene):
+        """Visual vertices of the morph's mesh, each a fixed affine combination of nearby
+        particles (mpm_entity.py:55-57, particle_entity.py:192-226): Liquid, Sand and Snow
+        are not skinned, nor are Nowhere entities (no mesh)."""
+        from .. import mesh as _mesh
+        from ..materials import MPM
+
+        self._vverts = np.zeros((0, 3))
+        self._vfaces = np.zeros((0, 3), dtype=np.int64)
+        self._support_idx = np.zeros((0, 0), dtype=np.int32)
+        self._support_w = np.zeros((0, 0), dtype=np.float32)
+        skinned = not isinstance(self._material, (MPM.Liquid, MPM.Sand, MPM.Snow))
+        if not skinned or isinstance(self._morph, _morphs.Nowhere):
+            return
+        if isinstance(self._morph, _morphs.Box):
+            v, f = _mesh.box_mesh(self._morph.size)
+        elif isinstance(self._morph, _morphs.Sphere):
+            v, f = _mesh.icosphere(3, self._morph.radius)
+        else:
+            return
+        R = _morphs._quat_to_R(self._morph.quat)
+        self._vverts = v @ R.T + np.asarray(self._morph.pos, dtype=np.float64)
+        self._vfaces = f
+        K = int(getattr(getattr(scene, "vis_options", None), "n_support_neighbors", 12))
+        self._support_idx, self._support_w = skinning_supports(self._particles, self._vverts, K)
+
+    @property
+    def vverts(self):
+        """Visual vertices at build time, [n_vverts, 3]."""
+        return self._vverts
+
+    @property
+    def vfaces(self):
+        return self._vfaces
+
+    @property
+    def n_vverts(self):
+        return len(self._vverts)
 
     # ------------------------------------------------------------ properties
     @property

@@ -9,6 +9,7 @@ substeps back to back (one CUDA graph per sort interval) for ``Simulator.step``.
 
 from __future__ import annotations
 
+import ctypes as C
 import logging
 
 import numpy as np
@@ -18,7 +19,7 @@ from .. import _native as nat
 from ..exceptions import GenesisException
 from .boundaries import CubeBoundary
 from .entity import MPMEntity
-from .runtime import InstanceSpec, MPMRuntime
+from .runtime import InstanceSpec, MPMRuntime, _cuda_stream_handle
 from .states import MPMSolverState
 
 # mpm_solver.py:505-509
@@ -134,6 +135,46 @@ class MPMSolver:
         mat = np.concatenate([np.full(e.n_particles, e.material.idx, dtype=np.uint8) for e in self._entities])
         act = np.concatenate([np.full(e.n_particles, e.active, dtype=bool) for e in self._entities])
         self.runtime.init_particles(np.tile(pos, (self._B, 1)), np.tile(mat, self._B), active=np.tile(act, self._B))
+        self._build_render_fields()
+
+    # ---------------------------------------------------------- render fields
+    def _build_render_fields(self):
+        """Headless render buffers (mpm_solver.py:136-157): per particle pos / vel / active
+        and per visual vertex pos / active, [B, N, ...] and [B, V, ...] device tensors."""
+        dev = self.runtime.device
+        B, N = self._B, self.n_particles
+        idx, w, start = [], [], 0
+        for e in self._entities:
+            e._vvert_start = start
+            if e.n_vverts:
+                idx.append(e._support_idx + e.particle_start)
+                w.append(e._support_w)
+                start += e.n_vverts
+        self.n_vverts = start
+        K = idx[0].shape[1] if idx else 1
+        self._vv_idx = torch.as_tensor(np.concatenate(idx) if idx else np.zeros((0, K), np.int32), device=dev)
+        self._vv_w = torch.as_tensor(np.concatenate(w) if w else np.zeros((0, K), np.float32), device=dev)
+        self.particles_render = {
+            "pos": torch.zeros((B, N, 3), dtype=torch.float32, device=dev),
+            "vel": torch.zeros((B, N, 3), dtype=torch.float32, device=dev),
+            "active": torch.zeros((B, N), dtype=torch.uint8, device=dev),
+        }
+        self.vverts_render = {
+            "pos": torch.zeros((B, self.n_vverts, 3), dtype=torch.float32, device=dev),
+            "active": torch.zeros((B, self.n_vverts), dtype=torch.uint8, device=dev),
+        }
+
+    def update_render_fields(self):
+        """_kernel_update_render_fields (mpm_solver.py:743-766) on the device."""
+        if not self.is_active:
+            return
+        rt = self.runtime
+        pr, vr = self.particles_render, self.vverts_render
+        K = int(self._vv_idx.shape[1]) if self.n_vverts else 1
+        vp = lambda t: C.c_void_p(t.data_ptr()) if t.numel() else None
+        rt._call("mpm_update_render_fields", C.byref(rt.prob), C.byref(rt.par), self._B, self.n_particles,
+                 vp(pr["pos"]), vp(pr["vel"]), vp(pr["active"]), int(self.n_vverts), K, vp(self._vv_idx),
+                 vp(self._vv_w), vp(vr["pos"]), vp(vr["active"]), _cuda_stream_handle())
 
     # -------------------------------------------------------------- stepping
     def process_input(self, in_backward=False):

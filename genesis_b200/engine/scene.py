@@ -40,6 +40,9 @@ class Scene:
         self.coupler_options = coupler_options or LegacyCouplerOptions()
         self.mpm_options = mpm_options or MPMOptions()
         self.b200_options = b200_options or B200Options()
+        from ..options import VisOptions
+
+        self.vis_options = vis_options or VisOptions()
         if self.sim_options.requires_grad:
             raise GenesisException(
                 "requires_grad scenes are served by genesis_b200.grad (checkpointed adjoint); Scene runs forward only."

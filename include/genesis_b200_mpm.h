@@ -296,6 +296,21 @@ int mpm_set_particles_active(const mpm_problem* prob, mpm_particles* par, int32_
 int mpm_set_particles_free(const mpm_problem* prob, mpm_particles* par, int32_t n, const int32_t* idx,
                            const uint8_t* free_flag, void* stream);
 
+/* ---- render fields (headless output buffers) ----------------------------
+ * _kernel_update_render_fields (mpm_solver.py:743-766).  The problem's particles are
+ * n_envs environments of n_per_env particles each (API order: env-major).  For every
+ * particle i (API order): render_pos[i] = x, or the "nowhere" point (2333333, 6666666,
+ * 5201314) when inactive; render_vel[i] = v only when active (left as is otherwise);
+ * render_active[i] = active.  For every visual vertex v of every environment e:
+ * vvert_pos[e][v] = sum_j support_w[v][j] * x(e * n_per_env + support_idx[v][j]) and
+ * vvert_active[e][v] = active of its first support.  support_idx / support_w are
+ * int32 / float [n_vverts][n_supports] (per-environment particle indices, computed on
+ * the host as particle_entity.py:192-226 does).  Any output pointer may be NULL. */
+int mpm_update_render_fields(const mpm_problem* prob, const mpm_particles* par, int32_t n_envs,
+                             int32_t n_per_env, float* render_pos, float* render_vel, uint8_t* render_active,
+                             int32_t n_vverts, int32_t n_supports, const int32_t* support_idx,
+                             const float* support_w, float* vvert_pos, uint8_t* vvert_active, void* stream);
+
 /* ---- CUDA graphs --------------------------------------------------------
  * Capture n_substeps of mpm_substeps into an executable graph (the pointers in
  * prob/tab/par/workspace are baked in and must stay valid). */
