@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -127,7 +127,32 @@ class Particles(C.Structure):
 
 
 class Tables(C.Structure):
-    _fields_ = [("instances", C.c_void_p), ("materials", C.c_void_p)]
+    _fields_ = [
+        ("instances", C.c_void_p),
+        ("materials", C.c_void_p),
+        ("colliders", C.c_void_p),
+        ("n_colliders", C.c_int32),
+        ("pad0", C.c_int32),
+        ("collider_force", C.c_void_p),
+    ]
+
+
+COLLIDER_SPHERE, COLLIDER_PLANE, COLLIDER_BOX = 0, 1, 2
+
+
+class Collider(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("instance", C.c_int32),
+        ("pos", C.c_float * 3),
+        ("rot", C.c_float * 9),
+        ("data", C.c_float * 3),
+        ("lin_vel", C.c_float * 3),
+        ("ang_vel", C.c_float * 3),
+        ("friction", C.c_float),
+        ("softness", C.c_float),
+        ("restitution", C.c_float),
+    ]
 
 
 _P = C.POINTER
@@ -191,9 +216,10 @@ def load(path: str | None = None):
             fn.argtypes = args
         if lib.mpm_abi_version() != ABI_VERSION:
             raise NativeLibraryError("ABI version mismatch between genesis_b200 and " + LIB_NAME)
-        sizes = (C.c_int32 * 4)()
+        sizes = (C.c_int32 * 6)()
         lib.mpm_struct_sizes(sizes)
-        mine = (C.sizeof(Instance), C.sizeof(Material), C.sizeof(Problem), C.sizeof(Particles))
+        mine = (C.sizeof(Instance), C.sizeof(Material), C.sizeof(Problem), C.sizeof(Particles), C.sizeof(Tables),
+                C.sizeof(Collider))
         if tuple(sizes) != mine:
             raise NativeLibraryError(f"struct layout mismatch: library {tuple(sizes)} vs binding {mine}")
         _lib = lib

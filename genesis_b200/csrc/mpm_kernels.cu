@@ -1154,7 +1154,117 @@ __global__ void k_nonfree_zero(mpm_problem prob, const mpm_instance* __restrict_
 
 // ---------------------------------------------------------------- grid op
 
-__global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w) {
+// Rigid coupling of one grid node against one kinematic collider (legacy_coupler.py:166-343):
+// signed distance and normal of the geom (utils/sdf_decomp.py:75-300), influence
+// min(exp(-sd / softness), 1), and for an approaching node (relative normal velocity < 0)
+// the frictional, restitutive projection of the relative velocity, blended by influence.
+// `mass` is the node mass without the particle-volume scale; the momentum change goes to
+// the collider as -dmv / dt (force) and (p - pos) x force (torque).
+__device__ __forceinline__ void collide_rigid(const mpm_collider& c, float eps, float dt, float mass, const float* p,
+                                              float* v, float* fout) {
+    const float q[3] = {p[0] - c.pos[0], p[1] - c.pos[1], p[2] - c.pos[2]};
+    float sd, g[3];
+    if (c.kind == MPM_COLLIDER_SPHERE) {
+        sd = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) - c.data[0];
+        const float inv = rsqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + eps);  // ti_normalize(., EPS)
+        g[0] = q[0] * inv;
+        g[1] = q[1] * inv;
+        g[2] = q[2] * inv;
+    } else {
+        float l[3], gl[3];  // geom-frame point and gradient
+#pragma unroll
+        for (int i = 0; i < 3; ++i) l[i] = c.rot[0 * 3 + i] * q[0] + c.rot[1 * 3 + i] * q[1] + c.rot[2 * 3 + i] * q[2];
+        if (c.kind == MPM_COLLIDER_PLANE) {
+            sd = l[0] * c.data[0] + l[1] * c.data[1] + l[2] * c.data[2];
+            gl[0] = c.data[0];
+            gl[1] = c.data[1];
+            gl[2] = c.data[2];
+        } else {
+            float d[3], o[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                d[i] = fabsf(l[i]) - c.data[i];
+                o[i] = fmaxf(d[i], 0.f);
+            }
+            const float out = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+            const float dm = fmaxf(d[0], fmaxf(d[1], d[2]));
+            sd = out + fminf(dm, 0.f);
+            if (out > 0.f) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) gl[i] = copysignf(o[i], l[i]) / out;
+            } else {
+                const int a = (d[0] >= d[1] && d[0] >= d[2]) ? 0 : (d[1] >= d[2] ? 1 : 2);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) gl[i] = (i == a) ? copysignf(1.f, l[i]) : 0.f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[i] = c.rot[i * 3 + 0] * gl[0] + c.rot[i * 3 + 1] * gl[1] + c.rot[i * 3 + 2] * gl[2];
+    }
+    const float influence = fminf(expf(-sd / fmaxf(1e-10f, c.softness)), 1.f);
+    if (!(influence > 0.1f)) return;
+    const float ninv = rsqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);  // sdf_func_normal_world
+    const float n[3] = {g[0] * ninv, g[1] * ninv, g[2] * ninv};
+    // velocity of the collider at p (rigid_solver_decomp.py:3413-3419)
+    const float vr[3] = {c.lin_vel[0] + c.ang_vel[1] * q[2] - c.ang_vel[2] * q[1],
+                         c.lin_vel[1] + c.ang_vel[2] * q[0] - c.ang_vel[0] * q[2],
+                         c.lin_vel[2] + c.ang_vel[0] * q[1] - c.ang_vel[1] * q[0]};
+    const float rv[3] = {v[0] - vr[0], v[1] - vr[1], v[2] - vr[2]};
+    const float rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    if (!(rn < 0.f)) return;
+    float rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
+    const float rtn = sqrtf(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
+    const float sc = fmaxf(0.f, rtn + rn * c.friction) / rtn;
+    float dv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float rnew = rt[i] * sc - n[i] * rn * c.restitution;
+        const float nvi = vr[i] + rnew * influence + rv[i] * (1.f - influence);
+        dv[i] = nvi - v[i];
+        v[i] = nvi;
+    }
+    if (fout) {
+        const float f[3] = {-mass * dv[0] / dt, -mass * dv[1] / dt, -mass * dv[2] / dt};
+        atomicAdd(&fout[0], f[0]);
+        atomicAdd(&fout[1], f[1]);
+        atomicAdd(&fout[2], f[2]);
+        atomicAdd(&fout[3], q[1] * f[2] - q[2] * f[1]);
+        atomicAdd(&fout[4], q[2] * f[0] - q[0] * f[2]);
+        atomicAdd(&fout[5], q[0] * f[1] - q[1] * f[0]);
+    }
+}
+
+// constant-velocity kinematic motion of the colliders over one substep of their instance:
+// pos += lin_vel dt, rot = exp([ang_vel] dt) rot (Rodrigues)
+__global__ void k_advance_colliders(const mpm_instance* __restrict__ inst, int n_inst, mpm_collider* cs, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    mpm_collider& c = cs[i];
+    if (c.instance < 0 || c.instance >= n_inst) return;
+    const float dt = inst[c.instance].dt;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c.pos[d] += c.lin_vel[d] * dt;
+    const float wx = c.ang_vel[0] * dt, wy = c.ang_vel[1] * dt, wz = c.ang_vel[2] * dt;
+    const float th = sqrtf(wx * wx + wy * wy + wz * wz);
+    if (th > 0.f) {
+        const float kx = wx / th, ky = wy / th, kz = wz / th, s = sinf(th), cth = cosf(th), t = 1.f - cth;
+        const float E[9] = {cth + t * kx * kx, t * kx * ky - s * kz, t * kx * kz + s * ky,
+                            t * kx * ky + s * kz, cth + t * ky * ky, t * ky * kz - s * kx,
+                            t * kx * kz - s * ky, t * ky * kz + s * kx, cth + t * kz * kz};
+        float R[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+                R[a * 3 + b] = E[a * 3 + 0] * c.rot[0 * 3 + b] + E[a * 3 + 1] * c.rot[1 * 3 + b] + E[a * 3 + 2] * c.rot[2 * 3 + b];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) c.rot[k] = R[k];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w,
+                                                 const mpm_collider* __restrict__ colliders, int n_colliders,
+                                                 float* collider_force) {
     const int n_active = (int)w.counters[CNT_ACTIVE];
     const int gpc = blockDim.x / BLK3;
     const int grp = threadIdx.x / BLK3;
@@ -1177,6 +1287,21 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
             const float px = (float)(bc.bx * BLK + lx + I.lower_cell[0]) * I.dx;
             const float py = (float)(bc.by * BLK + ly + I.lower_cell[1]) * I.dx;
             const float pz = (float)(bc.bz * BLK + lz + I.lower_cell[2]) * I.dx;
+            if (n_colliders > 0) {
+                // MPM <-> rigid (legacy_coupler.py:385-397), before the boundary; the node
+                // mass without the 1e3 particle-volume scale (legacy_coupler.py:375)
+                const float p[3] = {px, py, pz};
+                float v[3] = {vx, vy, vz};
+                const float mreal = mm.w * 1e-3f;
+                for (int k = 0; k < n_colliders; ++k) {
+                    if (colliders[k].instance != e.x) continue;
+                    collide_rigid(colliders[k], I.eps, I.dt, mreal, p, v,
+                                  collider_force ? collider_force + 6 * k : nullptr);
+                }
+                vx = v[0];
+                vy = v[1];
+                vz = v[2];
+            }
             vx = bc_vel(px, vx, I.bnd_lo[0], I.bnd_hi[0]);
             vy = bc_vel(py, vy, I.bnd_lo[1], I.bnd_hi[1]);
             vz = bc_vel(pz, vz, I.bnd_lo[2], I.bnd_hi[2]);
@@ -1410,7 +1535,11 @@ static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* 
     int ctas = prob->grid_ctas > 0 ? prob->grid_ctas : d->sms * d->occ_grid;
     const int64_t need = (prob->n_blocks + 3) / 4;
     if (ctas > need) ctas = (int)need;
-    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws));
+    if (tab->n_colliders < 0) return MPM_E_INVALID;
+    const int nc = tab->colliders ? tab->n_colliders : 0;
+    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc, tab->collider_force);
+    if (nc > 0)
+        k_advance_colliders<<<(nc + 63) / 64, 64, 0, s>>>(tab->instances, prob->n_instances, tab->colliders, nc);
     return cuda_ok();
 }
 
@@ -1453,12 +1582,14 @@ extern "C" {
 
 int mpm_abi_version(void) { return MPM_ABI_VERSION; }
 
-int mpm_struct_sizes(int32_t* out4) {
-    if (!out4) return MPM_E_INVALID;
-    out4[0] = (int32_t)sizeof(mpm_instance);
-    out4[1] = (int32_t)sizeof(mpm_material);
-    out4[2] = (int32_t)sizeof(mpm_problem);
-    out4[3] = (int32_t)sizeof(mpm_particles);
+int mpm_struct_sizes(int32_t* out6) {
+    if (!out6) return MPM_E_INVALID;
+    out6[0] = (int32_t)sizeof(mpm_instance);
+    out6[1] = (int32_t)sizeof(mpm_material);
+    out6[2] = (int32_t)sizeof(mpm_problem);
+    out6[3] = (int32_t)sizeof(mpm_particles);
+    out6[4] = (int32_t)sizeof(mpm_tables);
+    out6[5] = (int32_t)sizeof(mpm_collider);
     return MPM_OK;
 }
 
@@ -1636,6 +1767,7 @@ int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mp
     if ((rc = check_par(prob, state))) return rc;
     if (!tab || !tab->instances || !tab->materials || !adj || !lame_bar || !workspace || !adj_workspace)
         return MPM_E_INVALID;
+    if (tab->colliders && tab->n_colliders > 0) return MPM_E_INVALID;  // the adjoint has no rigid coupling
     cudaStream_t s = (cudaStream_t)stream;
     const int n = prob->n_particles;
     AdjWs aw = adj_ws_of(*prob, adj_workspace);

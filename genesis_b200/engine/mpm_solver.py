@@ -123,6 +123,8 @@ class MPMSolver:
         spec_kw["eps"] = _globals.EPS
         specs = [InstanceSpec(**spec_kw) for _ in range(self._B)]
         b = self._b200
+        rigid = list(getattr(self._scene, "_rigid_entities", []))
+        colliders = [r._collider(env) for r in rigid for env in range(self._B)]
         self.runtime = MPMRuntime(
             specs,
             device=self._sim.device,
@@ -130,7 +132,10 @@ class MPMSolver:
             sort_interval=b.sort_interval,
             grid_ctas=b.grid_ctas,
             use_graphs=b.use_cuda_graph,
+            colliders=colliders,
         )
+        for i, r in enumerate(rigid):
+            r._bind(self.runtime, [i * self._B + env for env in range(self._B)])
         pos = np.concatenate([e.init_particles for e in self._entities])
         mat = np.concatenate([np.full(e.n_particles, e.material.idx, dtype=np.uint8) for e in self._entities])
         act = np.concatenate([np.full(e.n_particles, e.active, dtype=bool) for e in self._entities])
@@ -183,6 +188,10 @@ class MPMSolver:
 
     def substep_pre_coupling(self, f):
         """compute_F_tmp + svd + p2g (mpm_solver.py:471-483); reset_grid is folded into grid op."""
+        rt = self.runtime
+        if rt.collider_force is not None and f == 0:
+            rt.collider_force.zero_()
+            rt.last_step_substeps = self._sim.substeps
         self.runtime.ensure_sorted()
         self.runtime.p2g()
 
@@ -195,7 +204,11 @@ class MPMSolver:
         self.runtime.grid_op()
 
     def advance(self, n_substeps: int):
-        self.runtime.substeps(n_substeps)
+        rt = self.runtime
+        if rt.collider_force is not None:
+            rt.collider_force.zero_()  # reaction forces are reported per step
+            rt.last_step_substeps = int(n_substeps)
+        rt.substeps(n_substeps)
 
     def check_state(self):
         """Raise if any particle position became NaN (mpm_solver.py:505-509)."""

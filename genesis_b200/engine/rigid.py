@@ -1,0 +1,154 @@
+"""Rigid entities as kinematic colliders of the MPM grid op.
+
+The reference couples MPM grid nodes to rigid geoms inside mpm_grid_op
+(genesis/engine/couplers/legacy_coupler.py:131-343, 385-397) and hands the momentum it
+removes to its rigid-body solver.  This build has no rigid-body solver: a rigid entity's
+pose and velocity are set by the caller (set_pos / set_quat / set_dofs_velocity), the
+collider moves at that velocity over the substeps, and the reaction force and torque on
+it are reported by get_coupling_force().  Sphere and Plane use the reference's analytic
+signed distance; a Box uses the exact box distance (the reference samples its SDF on a
+grid of sdf_cell_size).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from .. import morphs as _morphs
+from ..exceptions import GenesisException
+
+# float32 columns of one mpm_collider row after its two int32 fields
+_POS, _ROT, _DATA, _LIN, _ANG = slice(0, 3), slice(3, 12), slice(12, 15), slice(15, 18), slice(18, 21)
+
+
+def quat_to_R(q):
+    return _morphs._quat_to_R(np.asarray(q, dtype=np.float64))
+
+
+def R_to_quat(R):
+    """w-x-y-z quaternion of a rotation matrix (Shepperd's method)."""
+    R = np.asarray(R, dtype=np.float64)
+    tr = np.trace(R)
+    if tr > 0:
+        s = np.sqrt(tr + 1.0) * 2
+        q = [0.25 * s, (R[2, 1] - R[1, 2]) / s, (R[0, 2] - R[2, 0]) / s, (R[1, 0] - R[0, 1]) / s]
+    elif R[0, 0] > R[1, 1] and R[0, 0] > R[2, 2]:
+        s = np.sqrt(1.0 + R[0, 0] - R[1, 1] - R[2, 2]) * 2
+        q = [(R[2, 1] - R[1, 2]) / s, 0.25 * s, (R[0, 1] + R[1, 0]) / s, (R[0, 2] + R[2, 0]) / s]
+    elif R[1, 1] > R[2, 2]:
+        s = np.sqrt(1.0 + R[1, 1] - R[0, 0] - R[2, 2]) * 2
+        q = [(R[0, 2] - R[2, 0]) / s, (R[0, 1] + R[1, 0]) / s, 0.25 * s, (R[1, 2] + R[2, 1]) / s]
+    else:
+        s = np.sqrt(1.0 + R[2, 2] - R[0, 0] - R[1, 1]) * 2
+        q = [(R[1, 0] - R[0, 1]) / s, (R[0, 2] + R[2, 0]) / s, (R[1, 2] + R[2, 1]) / s, 0.25 * s]
+    q = np.asarray(q)
+    return q / np.linalg.norm(q) * (1 if q[0] >= 0 else -1)
+
+
+class KinematicRigidEntity:
+    """A gs.materials.Rigid entity with a Box, Sphere or Plane morph."""
+
+    def __init__(self, scene, idx, material, morph):
+        if isinstance(morph, _morphs.Sphere):
+            kind, data = nat.COLLIDER_SPHERE, (morph.radius, 0.0, 0.0)
+        elif isinstance(morph, _morphs.Plane):
+            kind, data = nat.COLLIDER_PLANE, morph.normal
+        elif isinstance(morph, _morphs.Box):
+            kind, data = nat.COLLIDER_BOX, tuple(np.asarray(morph.size) / 2)
+        else:
+            raise GenesisException("Rigid entities on this path take a Box, Sphere or Plane morph.")
+        self._scene = scene
+        self._idx = idx
+        self._material = material
+        self._morph = morph
+        self._kind = kind
+        self._data = np.asarray(data, dtype=np.float64)
+        self._rows = None  # collider rows in the runtime table, one per environment
+        self._rt = None
+
+    # ------------------------------------------------------------- build
+    def _collider(self, env):
+        c = nat.Collider()
+        c.kind = self._kind
+        c.instance = int(env)
+        R = quat_to_R(self._morph.quat)
+        for d in range(3):
+            c.pos[d] = float(self._morph.pos[d])
+            c.data[d] = float(self._data[d])
+        for k in range(9):
+            c.rot[k] = float(R.reshape(9)[k])
+        m = self._material
+        c.friction, c.softness, c.restitution = m.coup_friction, m.coup_softness, m.coup_restitution
+        return c
+
+    def _bind(self, runtime, rows):
+        self._rt = runtime
+        self._rows = torch.as_tensor(rows, dtype=torch.int64, device=runtime.device)
+
+    def _check_built(self):
+        if self._rt is None:
+            raise GenesisException("Scene is not built yet.")
+
+    def _sel(self, envs_idx):
+        envs = self._scene._sanitize_envs_idx(envs_idx)
+        return self._rows[envs.to(self._rows.device)]
+
+    def _set_cols(self, cols, vals, envs_idx):
+        self._check_built()
+        rows = self._sel(envs_idx)
+        v = torch.as_tensor(np.asarray(vals, dtype=np.float32), device=self._rt.device)
+        v = v.reshape(-1, cols.stop - cols.start).expand(len(rows), -1)
+        self._rt.collider_table()[rows, cols] = v
+
+    def _get_cols(self, cols, envs_idx):
+        self._check_built()
+        t = self._rt.collider_table()[self._sel(envs_idx), cols]
+        return t[0] if self._scene.n_envs == 0 else t
+
+    # ------------------------------------------------------------- API
+    @property
+    def idx(self):
+        return self._idx
+
+    @property
+    def material(self):
+        return self._material
+
+    @property
+    def morph(self):
+        return self._morph
+
+    def set_pos(self, pos, envs_idx=None):
+        self._set_cols(_POS, pos, envs_idx)
+
+    def get_pos(self, envs_idx=None):
+        return self._get_cols(_POS, envs_idx)
+
+    def set_quat(self, quat, envs_idx=None):
+        q = np.asarray(quat, dtype=np.float64).reshape(-1, 4)
+        self._set_cols(_ROT, np.stack([quat_to_R(qq).reshape(9) for qq in q]), envs_idx)
+
+    def get_quat(self, envs_idx=None):
+        R = self._get_cols(_ROT, envs_idx).cpu().numpy().reshape(-1, 3, 3)
+        q = torch.as_tensor(np.stack([R_to_quat(r) for r in R]), dtype=torch.float32)
+        return q[0] if self._scene.n_envs == 0 else q
+
+    def set_dofs_velocity(self, velocity, dofs_idx_local=None, envs_idx=None):
+        """Velocity of the free base: linear (3) then angular (3), both in the world frame."""
+        v = np.asarray(velocity, dtype=np.float64).reshape(-1, 6)
+        if dofs_idx_local is not None:
+            raise GenesisException("dofs_idx_local is not supported for kinematic colliders.")
+        self._set_cols(_LIN, v[:, :3], envs_idx)
+        self._set_cols(_ANG, v[:, 3:], envs_idx)
+
+    def get_dofs_velocity(self, envs_idx=None):
+        return torch.cat([self._get_cols(_LIN, envs_idx), self._get_cols(_ANG, envs_idx)], dim=-1)
+
+    def get_coupling_force(self, envs_idx=None):
+        """Mean force (3) and torque about the origin (3) that the MPM material exerted on
+        this collider over the last step, [6] or [n_envs, 6]."""
+        self._check_built()
+        t = self._rt.collider_force[self._sel(envs_idx)] / max(1, self._rt.last_step_substeps)
+        return t[0] if self._scene.n_envs == 0 else t

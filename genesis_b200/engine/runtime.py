@@ -91,6 +91,7 @@ class MPMRuntime:
         per_particle_lame: bool = False,
         grid_ctas: int = 0,
         use_graphs: bool = True,
+        colliders: list | None = None,
     ):
         if not torch.cuda.is_available():
             raise RuntimeError("genesis_b200 needs a CUDA device (sm_100a); there is no CPU path")
@@ -154,7 +155,24 @@ class MPMRuntime:
         dev = self.device
         self.inst_table = torch.from_numpy(nat.instances_to_bytes(insts)).to(dev)
         self.mat_table = torch.from_numpy(nat.materials_to_bytes(mats)).to(dev)
-        self.tables = nat.Tables(self.inst_table.data_ptr(), self.mat_table.data_ptr())
+        # kinematic rigid colliders of the grid op (mpm_collider rows) and their reaction
+        # force / torque accumulators
+        colliders = list(colliders or [])
+        self.n_colliders = len(colliders)
+        self.last_step_substeps = 0
+        if colliders:
+            arr = (nat.Collider * len(colliders))(*colliders)
+            self.coll_table = torch.from_numpy(np.frombuffer(bytes(arr), dtype=np.uint8).copy()).to(dev)
+            self.coll_init = self.coll_table.clone()
+            self.collider_force = torch.zeros((len(colliders), 6), dtype=torch.float32, device=dev)
+        else:
+            self.coll_table = None
+            self.collider_force = None
+        self.tables = nat.Tables(
+            self.inst_table.data_ptr(), self.mat_table.data_ptr(),
+            self.coll_table.data_ptr() if colliders else None, len(colliders), 0,
+            self.collider_force.data_ptr() if colliders else None,
+        )
 
         self.state = torch.zeros((nat.MPM_STATE_CH, self.stride), dtype=torch.float32, device=dev)
         self.mat = torch.zeros(max(self.n, 1), dtype=torch.uint8, device=dev)
@@ -252,6 +270,20 @@ class MPMRuntime:
         sl = self.slot[: self.n].long()
         self.mu_p[sl] = mu
         self.lam_p[sl] = lam
+
+    def reset_colliders(self):
+        """Back to the poses and velocities the colliders were built with."""
+        if self.coll_table is not None:
+            self.coll_table.copy_(self.coll_init)
+
+    def collider_table(self) -> torch.Tensor:
+        """The collider rows as float32 [n_colliders, 24] (pos 0:3, rot 3:12, data 12:15,
+        lin_vel 15:18, ang_vel 18:21, friction, softness, restitution), a view of the
+        device table after each row's two int32 fields; writes go straight to the table."""
+        if self.coll_table is None:
+            raise RuntimeError("runtime has no colliders")
+        stride = C.sizeof(nat.Collider) // 4
+        return self.coll_table.view(torch.float32).view(self.n_colliders, stride)[:, 2:]
 
     # ---------------------------------------------------------------- muscle
     def _need_muscle(self):

@@ -50,6 +50,7 @@ class Scene:
         self._other = other_solver_options
         self._sim = Simulator(self, self.sim_options, self.mpm_options, self.b200_options)
         self._entities = []
+        self._rigid_entities = []  # kinematic colliders of the MPM grid op
         self._emitters = []
         self._is_built = False
         self._B = 1
@@ -61,8 +62,16 @@ class Scene:
     def add_entity(self, morph, material=None, surface=None, visualize_contact=False, vis_mode=None):
         if self._is_built:
             raise GenesisException("Scene is already built.")
+        if isinstance(material, _materials.Rigid):
+            from .rigid import KinematicRigidEntity
+
+            ent = KinematicRigidEntity(self, len(self._entities), material, morph)
+            self._entities.append(ent)
+            if material.needs_coup:
+                self._rigid_entities.append(ent)
+            return ent
         if material is None or not isinstance(material, _materials.MPM.Base):
-            raise GenesisException("Only gs.materials.MPM.* entities are supported by this MPM build.")
+            raise GenesisException("Only gs.materials.MPM.* and gs.materials.Rigid entities are supported by this build.")
         ent = self._sim.mpm_solver.add_entity(len(self._entities), material, morph, surface, rng=_globals.rng)
         self._entities.append(ent)
         return ent
@@ -137,6 +146,8 @@ class Scene:
             emitter.reset()
         if envs_idx is None:
             self._sim._cur_substep_global = 0
+            if self._sim.mpm_solver.is_active:
+                self._sim.mpm_solver.runtime.reset_colliders()
 
     def save_checkpoint(self, path):
         st = self.get_state()[0]

@@ -138,4 +138,22 @@ class Nowhere(Morph):
         return np.tile(np.array([2333333.0, 6666666.0, 5201314.0]), (self.n_particles, 1))
 
 
-__all__ = ["Morph", "Box", "Sphere", "Nowhere"]
+class Plane(Morph):
+    """Infinite plane through `pos` with `normal` in its local frame (options/morphs.py:409-470);
+    only meaningful for rigid entities (a collider of the MPM grid op)."""
+
+    def __init__(self, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, normal=(0.0, 0.0, 1.0), fixed=True,
+                 plane_size=(1e3, 1e3), **kw):
+        super().__init__(pos=pos, euler=euler, quat=quat, **kw)
+        n = np.asarray(normal, dtype=np.float64)
+        if np.linalg.norm(n) < 1e-12:
+            raise GenesisException("Plane normal must be non-zero.")
+        self.normal = tuple(n / np.linalg.norm(n))
+        self.fixed = fixed
+        self.plane_size = tuple(plane_size)
+
+    def _local_particles(self, p_size, sampler, rng):
+        raise GenesisException("A Plane has no particles; use it with gs.materials.Rigid.")
+
+
+__all__ = ["Morph", "Box", "Sphere", "Nowhere", "Plane"]

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 2
+#define MPM_ABI_VERSION 3
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -147,9 +147,38 @@ typedef struct mpm_particles {
     const float* muscle_dir;  /* optional, float[n][3] in API order: fibre direction (mpm_solver.py:108) */
 } mpm_particles;
 
+/* Kinematic rigid collider coupled in the grid op (legacy_coupler.py:131-343, 385-397):
+ * a grid node with mass within its influence = min(exp(-sd / softness), 1) > 0.1 has its
+ * velocity relative to the collider's projected (friction, restitution), exactly as
+ * _func_collide_in_rigid_geom does; the momentum change is reported back as a force and a
+ * torque about `pos` (the reference hands it to its rigid solver).  The pose advances
+ * with lin_vel / ang_vel by the instance's dt after every grid op (constant-velocity
+ * kinematic motion between host updates). */
+#define MPM_COLLIDER_SPHERE 0  /* sd = |p - pos| - data[0]  (utils/sdf_decomp.py:91-92) */
+#define MPM_COLLIDER_PLANE 1   /* sd = n . R^T (p - pos), n = data (geom frame, unit) (sdf_decomp.py:94-98) */
+#define MPM_COLLIDER_BOX 2     /* half extents data[0..2]; exact box SDF (the reference samples it on a grid) */
+
+typedef struct mpm_collider {
+    int32_t kind;        /* MPM_COLLIDER_* */
+    int32_t instance;    /* instance (environment) it acts on */
+    float pos[3];        /* origin of the geom frame, world */
+    float rot[9];        /* world-from-geom rotation, row-major */
+    float data[3];       /* see MPM_COLLIDER_* */
+    float lin_vel[3];    /* velocity of the origin */
+    float ang_vel[3];    /* angular velocity, world */
+    float friction;      /* coup_friction   (materials/rigid.py:47) */
+    float softness;      /* coup_softness   (materials/rigid.py:48) */
+    float restitution;   /* coup_restitution (materials/rigid.py:49) */
+} mpm_collider;
+
 typedef struct mpm_tables {
     const mpm_instance* instances;  /* device, n_instances entries */
     const mpm_material* materials;  /* device, n_materials entries */
+    mpm_collider* colliders;        /* device, n_colliders entries (may be NULL if none) */
+    int32_t n_colliders;
+    int32_t pad0;
+    float* collider_force;          /* device, optional [n_colliders][6]: force xyz, torque xyz;
+                                       accumulated (the caller zeroes it) */
 } mpm_tables;
 
 /* ---- sizing ------------------------------------------------------------ */
@@ -157,9 +186,10 @@ typedef struct mpm_tables {
 /* ABI version of the loaded library (MPM_ABI_VERSION). */
 int mpm_abi_version(void);
 
-/* sizeof(mpm_instance), sizeof(mpm_material), sizeof(mpm_problem), sizeof(mpm_particles)
- * as compiled into the library, so a binding can verify its mirror of these structs. */
-int mpm_struct_sizes(int32_t* out4);
+/* sizeof(mpm_instance), sizeof(mpm_material), sizeof(mpm_problem), sizeof(mpm_particles),
+ * sizeof(mpm_tables), sizeof(mpm_collider) as compiled into the library, so a binding can
+ * verify its mirror of these structs. */
+int mpm_struct_sizes(int32_t* out6);
 
 /* Upper bound on the number of p2g/g2p work items for a problem. */
 int mpm_max_chunks(int32_t n_particles, int64_t n_blocks, int32_t chunk_particles, int32_t* out);

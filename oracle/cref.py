@@ -49,7 +49,14 @@ def _structs(dtype):
             ("muscle_stiffness", Rt),
         ]
 
-    return Params, Mat
+    class Coll(C.Structure):
+        _fields_ = [
+            ("kind", C.c_int32),
+            ("pos", Rt * 3), ("rot", Rt * 9), ("data", Rt * 3), ("lin_vel", Rt * 3), ("ang_vel", Rt * 3),
+            ("friction", Rt), ("softness", Rt), ("restitution", Rt),
+        ]
+
+    return Params, Mat, Coll
 
 
 _libs = {}
@@ -64,6 +71,7 @@ def lib(dtype):
         L.ref_substeps.restype = C.c_int
         L.ref_substeps_lame.restype = C.c_int
         L.ref_substeps_ext.restype = C.c_int
+        L.ref_substeps_full.restype = C.c_int
         L.ref_max_threads.restype = C.c_int
         _libs[key] = L
     return _libs[key]
@@ -79,7 +87,7 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     optional per-particle Lame parameters."""
     dt = np.dtype(p.dtype)
     L = lib(dt)
-    Params, Mat = _structs(dt)
+    Params, Mat, Coll = _structs(dt)
     P = Params()
     for d in range(3):
         P.res[d] = int(p.grid_res[d])
@@ -115,6 +123,37 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     grid = np.zeros(4 * G, dtype=dt)
     gvel = np.zeros(3 * G, dtype=dt)
     ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    if st.get("colliders"):
+        cs = st["colliders"]
+        carr = (Coll * len(cs))()
+        kinds = {"sphere": 0, "plane": 1, "box": 2}
+        for i, c in enumerate(cs):
+            carr[i].kind = kinds[c.kind]
+            for d in range(3):
+                carr[i].pos[d] = c.pos[d]
+                carr[i].data[d] = c.data[d]
+                carr[i].lin_vel[d] = c.lin_vel[d]
+                carr[i].ang_vel[d] = c.ang_vel[d]
+            for k in range(9):
+                carr[i].rot[k] = np.asarray(c.rot, dtype=np.float64).reshape(9)[k]
+            carr[i].friction, carr[i].softness, carr[i].restitution = c.friction, c.softness, c.restitution
+        forces = np.zeros((len(cs), 6), dtype=dt)
+        actu = np.ascontiguousarray(st["actu"], dtype=dt) if st.get("actu") is not None else None
+        mdir = np.ascontiguousarray(st["mdir"], dtype=dt).reshape(n, 3) if st.get("mdir") is not None else None
+        mu_a = np.ascontiguousarray(mu_p, dtype=dt) if mu_p is not None else None
+        lam_a = np.ascontiguousarray(lam_p, dtype=dt) if lam_p is not None else None
+        opt = lambda a: ptr(a) if a is not None else None
+        rc = L.ref_substeps_full(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
+                                 int(n_substeps), ptr(grid), ptr(gvel), int(n_threads), opt(mu_a), opt(lam_a),
+                                 opt(actu), opt(mdir), carr, len(cs), ptr(forces))
+        moved = []
+        for i, c in enumerate(cs):
+            moved.append(R.Collider(c.kind, np.array(carr[i].pos[:]), np.array(carr[i].rot[:]).reshape(3, 3),
+                                    np.asarray(c.data), np.asarray(c.lin_vel), np.asarray(c.ang_vel), c.friction,
+                                    c.softness, c.restitution))
+        out = dict(st)
+        out.update(x=x, v=v, C=Cm.reshape(n, 3, 3), F=F.reshape(n, 3, 3), Jp=Jp, colliders=moved, forces=forces)
+        return out, int(rc)
     if st.get("actu") is not None:
         actu = np.ascontiguousarray(st["actu"], dtype=dt)
         mdir = np.ascontiguousarray(st["mdir"], dtype=dt).reshape(n, 3)

@@ -39,6 +39,8 @@
 #define RABS(x) fabsf(x)
 #define RMAX(a, b) fmaxf(a, b)
 #define RMIN(a, b) fminf(a, b)
+#define R_SIN(x) sinf(x)
+#define R_COS(x) cosf(x)
 #else
 #define R_SQRT(x) sqrt(x)
 #define RLOG(x) log(x)
@@ -48,6 +50,8 @@
 #define RABS(x) fabs(x)
 #define RMAX(a, b) fmax(a, b)
 #define RMIN(a, b) fmin(a, b)
+#define R_SIN(x) sin(x)
+#define R_COS(x) cos(x)
 #endif
 
 typedef struct {
@@ -67,6 +71,14 @@ typedef struct {
     REAL clamp_lo, clamp_hi, vm_threshold, sand_c1, sand_alpha;
     REAL muscle_stiffness; /* muscle.py:54 (E) */
 } ref_material;
+
+/* kinematic rigid collider of the grid op (legacy_coupler.py:131-343); kind 0 sphere
+ * (data[0] radius), 1 plane (data = unit normal, geom frame), 2 box (data = half extents) */
+typedef struct {
+    int32_t kind;
+    REAL pos[3], rot[9], data[3], lin_vel[3], ang_vel[3];
+    REAL friction, softness, restitution;
+} ref_collider;
 
 /* ---------------------------------------------------------------- SVD */
 
@@ -293,6 +305,10 @@ int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL
 int ref_substeps_ext(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
                      int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir);
+int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                      int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir,
+                      ref_collider* colliders, int n_colliders, REAL* forces);
 
 int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F, REAL* Jp,
                  const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel, int n_threads) {
@@ -312,6 +328,101 @@ int ref_substeps_lame(const ref_params* p, const ref_material* mats, int n, REAL
 int ref_substeps_ext(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
                      int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir) {
+    return ref_substeps_full(p, mats, n, x, v, C, F, Jp, mat, active, n_substeps, grid, gvel, n_threads, mu_p, lam_p,
+                             actu, mdir, NULL, 0, NULL);
+}
+
+/* legacy_coupler.py:166-343 for one node against one collider; adds the reaction force
+ * and torque (about c->pos) to f[6] */
+static void collide_rigid(const ref_collider* c, REAL eps, REAL dt, REAL mass, const REAL* pos, REAL* v, REAL* f) {
+    REAL q[3] = {pos[0] - c->pos[0], pos[1] - c->pos[1], pos[2] - c->pos[2]};
+    REAL sd, g[3];
+    if (c->kind == 0) {
+        sd = R_SQRT(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) - c->data[0];
+        REAL nn = R_SQRT(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + eps);
+        for (int i = 0; i < 3; ++i) g[i] = q[i] / nn;
+    } else {
+        REAL l[3], gl[3];
+        for (int i = 0; i < 3; ++i) l[i] = c->rot[0 * 3 + i] * q[0] + c->rot[1 * 3 + i] * q[1] + c->rot[2 * 3 + i] * q[2];
+        if (c->kind == 1) {
+            sd = l[0] * c->data[0] + l[1] * c->data[1] + l[2] * c->data[2];
+            for (int i = 0; i < 3; ++i) gl[i] = c->data[i];
+        } else {
+            REAL d[3], o[3];
+            for (int i = 0; i < 3; ++i) {
+                d[i] = (l[i] < 0 ? -l[i] : l[i]) - c->data[i];
+                o[i] = d[i] > 0 ? d[i] : 0;
+            }
+            REAL out = R_SQRT(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+            REAL dm = d[0] > d[1] ? (d[0] > d[2] ? d[0] : d[2]) : (d[1] > d[2] ? d[1] : d[2]);
+            sd = out + (dm < 0 ? dm : 0);
+            if (out > 0) {
+                for (int i = 0; i < 3; ++i) gl[i] = (l[i] < 0 ? -o[i] : o[i]) / out;
+            } else {
+                int a = (d[0] >= d[1] && d[0] >= d[2]) ? 0 : (d[1] >= d[2] ? 1 : 2);
+                for (int i = 0; i < 3; ++i) gl[i] = (i == a) ? (l[i] < 0 ? -1 : 1) : 0;
+            }
+        }
+        for (int i = 0; i < 3; ++i) g[i] = c->rot[i * 3 + 0] * gl[0] + c->rot[i * 3 + 1] * gl[1] + c->rot[i * 3 + 2] * gl[2];
+    }
+    REAL soft = c->softness > (REAL)1e-10 ? c->softness : (REAL)1e-10;
+    REAL infl = RMIN(REXP(-sd / soft), (REAL)1);
+    if (!(infl > (REAL)0.1)) return;
+    REAL gn = R_SQRT(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);
+    REAL n[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
+    const REAL* w = c->ang_vel;
+    REAL vr[3] = {c->lin_vel[0] + w[1] * q[2] - w[2] * q[1], c->lin_vel[1] + w[2] * q[0] - w[0] * q[2],
+                  c->lin_vel[2] + w[0] * q[1] - w[1] * q[0]};
+    REAL rv[3] = {v[0] - vr[0], v[1] - vr[1], v[2] - vr[2]};
+    REAL rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    if (!(rn < 0)) return;
+    REAL rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
+    REAL rtn = R_SQRT(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
+    REAL sc = rtn + rn * c->friction;
+    sc = (sc > 0 ? sc : 0) / rtn;
+    REAL dv[3];
+    for (int i = 0; i < 3; ++i) {
+        REAL rnew = rt[i] * sc - n[i] * rn * c->restitution;
+        REAL nv = vr[i] + rnew * infl + rv[i] * (1 - infl);
+        dv[i] = nv - v[i];
+        v[i] = nv;
+    }
+    if (f) {
+        REAL fo[3] = {-mass * dv[0] / dt, -mass * dv[1] / dt, -mass * dv[2] / dt};
+        REAL to[3] = {q[1] * fo[2] - q[2] * fo[1], q[2] * fo[0] - q[0] * fo[2], q[0] * fo[1] - q[1] * fo[0]};
+        for (int i = 0; i < 3; ++i) {
+#pragma omp atomic
+            f[i] += fo[i];
+#pragma omp atomic
+            f[3 + i] += to[i];
+        }
+    }
+}
+
+/* constant-velocity kinematic motion over one substep */
+static void advance_collider(ref_collider* c, REAL dt) {
+    for (int d = 0; d < 3; ++d) c->pos[d] += c->lin_vel[d] * dt;
+    REAL wx = c->ang_vel[0] * dt, wy = c->ang_vel[1] * dt, wz = c->ang_vel[2] * dt;
+    REAL th = R_SQRT(wx * wx + wy * wy + wz * wz);
+    if (th > 0) {
+        REAL kx = wx / th, ky = wy / th, kz = wz / th, s = R_SIN(th), co = R_COS(th), t = 1 - co;
+        REAL E[9] = {co + t * kx * kx, t * kx * ky - s * kz, t * kx * kz + s * ky, t * kx * ky + s * kz, co + t * ky * ky,
+                     t * ky * kz - s * kx, t * kx * kz - s * ky, t * ky * kz + s * kx, co + t * kz * kz};
+        REAL R[9];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                R[a * 3 + b] = E[a * 3 + 0] * c->rot[0 * 3 + b] + E[a * 3 + 1] * c->rot[1 * 3 + b] + E[a * 3 + 2] * c->rot[2 * 3 + b];
+        memcpy(c->rot, R, sizeof(R));
+    }
+}
+
+/* as ref_substeps_ext, with kinematic rigid colliders coupled in the grid op
+ * (legacy_coupler.py:385-397); forces (optional, [n_colliders][6]) accumulate the
+ * reaction force and torque over all substeps; the colliders' poses advance in place */
+int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                      int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir,
+                      ref_collider* colliders, int n_colliders, REAL* forces) {
 #ifdef _OPENMP
     if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
@@ -402,13 +513,19 @@ int ref_substeps_ext(const ref_params* p, const ref_material* mats, int n, REAL*
                 int ii = (int)(g / ((int64_t)p->res[1] * p->res[2]));
                 int I[3] = {ii, j, k};
                 REAL inv = 1 / cell[3];
+                REAL vel[3], pos[3];
                 for (int d = 0; d < 3; ++d) {
-                    REAL vel = inv * cell[d] + p->dt * p->gravity[d];
-                    REAL pos = (REAL)(I[d] + p->lower_cell[d]) * p->dx;
-                    out[d] = bc_vel(pos, vel, p->bnd_lo[d], p->bnd_hi[d]);
+                    vel[d] = inv * cell[d] + p->dt * p->gravity[d];
+                    pos[d] = (REAL)(I[d] + p->lower_cell[d]) * p->dx;
                 }
+                /* MPM <-> rigid (legacy_coupler.py:385-397), node mass without the 1e3 volume scale */
+                for (int k = 0; k < n_colliders; ++k)
+                    collide_rigid(&colliders[k], p->eps, p->dt, cell[3] / (REAL)1e3, pos, vel,
+                                  forces ? forces + 6 * k : NULL);
+                for (int d = 0; d < 3; ++d) out[d] = bc_vel(pos[d], vel[d], p->bnd_lo[d], p->bnd_hi[d]);
             }
         }
+        for (int k = 0; k < n_colliders; ++k) advance_collider(&colliders[k], p->dt);
         /* g2p (mpm_solver.py:391-449) */
 #pragma omp parallel for schedule(static) reduction(| : status)
         for (int i = 0; i < n; ++i) {

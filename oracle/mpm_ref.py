@@ -402,8 +402,89 @@ def p2g(p: Params, mats: list[Material], st: dict):
     return gm.astype(dt), gp.astype(dt), F_new, Jp_new
 
 
-def grid_op(p: Params, gm, gp):
-    """MPM core of LegacyCoupler.mpm_grid_op (legacy_coupler.py:364-375, 495-496)."""
+@dataclass
+class Collider:
+    """A kinematic rigid geom coupled in the grid op (legacy_coupler.py:131-343): kind
+    'sphere' (data[0] = radius), 'plane' (data = unit normal, geom frame) or 'box' (data =
+    half extents); pose (pos, rot world-from-geom), velocity (lin_vel of pos, ang_vel) and
+    the Rigid material's coupling parameters (materials/rigid.py:46-49)."""
+
+    kind: str
+    pos: np.ndarray
+    rot: np.ndarray
+    data: np.ndarray
+    lin_vel: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    ang_vel: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    friction: float = 0.1
+    softness: float = 0.002
+    restitution: float = 0.0
+
+
+def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
+    """_func_collide_with_rigid_geom + _func_collide_in_rigid_geom for grid nodes at pos
+    (legacy_coupler.py:166-343); sphere and plane SDFs as utils/sdf_decomp.py:91-98, the
+    box's exact.  Returns (new velocity, force, torque about c.pos)."""
+    dt = vel.dtype.type
+    q = pos - np.asarray(c.pos, dtype=dt)
+    R = np.asarray(c.rot, dtype=dt)
+    data = np.asarray(c.data, dtype=dt)
+    if c.kind == "sphere":
+        sd = np.linalg.norm(q, axis=1) - data[0]
+        g = q / np.sqrt((q * q).sum(1) + dt(eps))[:, None]
+    else:
+        l = q @ R  # geom frame: R^T q per row
+        if c.kind == "plane":
+            sd = l @ data
+            gl = np.broadcast_to(data, l.shape)
+        else:
+            d = np.abs(l) - data
+            o = np.maximum(d, 0)
+            out = np.sqrt((o * o).sum(1))
+            sd = out + np.minimum(d.max(1), 0)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                g_out = np.copysign(o, l) / out[:, None]
+            a = d.argmax(1)
+            g_in = np.zeros_like(l)
+            g_in[np.arange(len(l)), a] = np.copysign(dt(1), l[np.arange(len(l)), a])
+            gl = np.where((out > 0)[:, None], g_out, g_in)
+        g = gl @ R.T
+    with np.errstate(over="ignore"):
+        infl = np.minimum(np.exp(-sd / max(1e-10, c.softness)), dt(1)).astype(dt)
+    n = g / np.sqrt((g * g).sum(1) + dt(eps))[:, None]
+    vr = np.asarray(c.lin_vel, dtype=dt)[None, :] + np.cross(np.asarray(c.ang_vel, dtype=dt)[None, :], q)
+    rv = vel - vr
+    rn = (rv * n).sum(1)
+    hit = (infl > 0.1) & (rn < 0)
+    rt = rv - rn[:, None] * n
+    rtn = np.sqrt((rt * rt).sum(1) + dt(eps))
+    sc = np.maximum(dt(0), rtn + rn * dt(c.friction)) / rtn
+    rnew = rt * sc[:, None] - n * (rn * dt(c.restitution))[:, None]
+    nv = vr + rnew * infl[:, None] + rv * (dt(1) - infl)[:, None]
+    out_v = np.where(hit[:, None], nv, vel)
+    f = -(mass[:, None] * (out_v - vel)) / dt(sdt)
+    return out_v, f.sum(0), np.cross(q, f).sum(0)
+
+
+def advance_colliders(p: Params, colliders):
+    """Constant-velocity kinematic motion over one substep (pos += v dt, rot = exp(w dt) rot)."""
+    out = []
+    for c in colliders:
+        w = np.asarray(c.ang_vel, dtype=np.float64) * p.dt
+        th = np.linalg.norm(w)
+        R = np.asarray(c.rot, dtype=np.float64)
+        if th > 0:
+            k = w / th
+            K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+            R = (np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K) @ R
+        out.append(Collider(c.kind, np.asarray(c.pos) + np.asarray(c.lin_vel) * p.dt, R, c.data, c.lin_vel, c.ang_vel,
+                            c.friction, c.softness, c.restitution))
+    return out
+
+
+def grid_op(p: Params, gm, gp, colliders=None, forces=None):
+    """MPM core of LegacyCoupler.mpm_grid_op (legacy_coupler.py:364-375, 495-496), with the
+    rigid coupling of :385-397 for kinematic colliders (forces, if a list, receives one
+    (force, torque) pair per collider)."""
     dt = p.dtype
     res = gm.shape
     vel = np.zeros(res + (3,), dtype=dt)
@@ -413,6 +494,10 @@ def grid_op(p: Params, gm, gp):
     v = v + dt(p.dt) * np.asarray(p.gravity, dtype=dt)[None, :]
     idx = np.argwhere(act)
     pos = (idx + p.lower_cell[None, :]).astype(dt) * dt(p.dx)
+    for c in colliders or []:
+        v, f, t = collide_rigid(c, p.eps, p.dt, pos, v, (m / dt(1e3)).astype(dt))
+        if forces is not None:
+            forces.append((f, t))
     _, v = boundary(p, pos, v)
     vel[act] = v
     return vel
@@ -460,10 +545,13 @@ def g2p(p: Params, st: dict, vel):
 def substep(p: Params, mats: list[Material], st: dict, return_grid: bool = False):
     """One full substep: p2g, grid op, g2p.  ``st`` is not modified."""
     gm, gp, F_new, Jp_new = p2g(p, mats, st)
-    vel = grid_op(p, gm, gp)
+    colliders = st.get("colliders")
+    vel = grid_op(p, gm, gp, colliders)
     xn, vn, Cn = g2p(p, st, vel)
     out = dict(st)
     out.update(x=xn, v=vn, C=Cn, F=F_new, Jp=Jp_new)
+    if colliders:
+        out["colliders"] = advance_colliders(p, colliders)
     if np.isnan(xn).any():
         raise FloatingPointError("NaN detected in MPM states (mpm_solver.py:505-509)")
     if return_grid:

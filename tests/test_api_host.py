@@ -92,3 +92,19 @@ def test_muscle_material_follows_reference():
     assert nm.muscle_stiffness == 1e6
     assert isinstance(m, gs.materials.MPM.Elastic)
     assert gs.materials.MPM.Elastic()._native(1e-3).muscle_stiffness == 0.0
+
+
+def test_rigid_material_and_plane_follow_reference():
+    m = gs.materials.Rigid()
+    assert (m.coup_friction, m.coup_softness, m.coup_restitution, m.needs_coup) == (0.1, 0.002, 0.0, True)
+    for bad in (dict(coup_friction=-1), dict(coup_softness=-1), dict(coup_restitution=2), dict(friction=10.0),
+                dict(sdf_min_res=8)):
+        with pytest.raises(gs.GenesisException):
+            gs.materials.Rigid(**bad)
+    p = gs.morphs.Plane(normal=(0, 0, 2))
+    assert np.allclose(p.normal, (0, 0, 1))
+    from genesis_b200.engine.rigid import R_to_quat, quat_to_R
+
+    q = np.array([0.9, 0.1, -0.3, 0.2])
+    q /= np.linalg.norm(q)
+    assert np.allclose(R_to_quat(quat_to_R(q)), q)

@@ -206,3 +206,80 @@ def test_muscle_actuation_contracts_along_the_fibre():
     assert ext(o["x"], 2) < ext(st["x"], 2) - 1e-5
     assert abs(ext(r["x"], 2) - ext(st["x"], 2)) < 1e-9
     assert ext(o["x"], 2) < ext(o["x"], 0)
+
+
+def _block_over(collider, n_side=10, z0=0.35, v0=(0.0, 0.0, -1.0), substeps=300, dtype=np.float64):
+    rng = np.random.default_rng(11)
+    x = W.jittered_lattice(rng, n_side, (0.45, 0.45, z0), 0.1 / n_side)
+    n = x.shape[0]
+    p = R.Params(grid_density=64, dt=1e-4, dtype=dtype)
+    mats = [R.make_material("elastic", E=2e4)]
+    st = R.make_state(x, mats, np.zeros(n, np.int64), dtype, v=np.tile(v0, (n, 1)))
+    st["colliders"] = [collider]
+    out, rc = cref.substeps(p, mats, st, substeps)
+    assert rc == 0
+    return out, st
+
+
+def test_rigid_colliders_numpy_and_c_agree():
+    """The two restatements of the grid-op rigid coupling agree (sphere, tilted box,
+    moving plane), including the reaction force and the advanced pose."""
+    th = np.deg2rad(20)
+    Rt = np.array([[np.cos(th), 0, np.sin(th)], [0, 1, 0], [-np.sin(th), 0, np.cos(th)]])
+    cases = [
+        R.Collider("sphere", np.array([0.5, 0.5, 0.3]), np.eye(3), np.array([0.05, 0, 0]), friction=0.5),
+        R.Collider("box", np.array([0.5, 0.5, 0.3]), Rt, np.array([0.2, 0.2, 0.04]), ang_vel=np.array([0, 0, 2.0])),
+        R.Collider("plane", np.array([0.5, 0.5, 0.33]), np.eye(3), np.array([0, 0, 1.0]), lin_vel=np.array([0, 0, 0.3])),
+    ]
+    for c in cases:
+        rng = np.random.default_rng(5)
+        x = W.jittered_lattice(rng, 6, (0.45, 0.45, 0.345), 0.06 / 6)
+        n = x.shape[0]
+        p = R.Params(grid_density=64, dt=1e-4, dtype=np.float64)
+        mats = [R.make_material("elastic", E=2e4)]
+        st = R.make_state(x, mats, np.zeros(n, np.int64), np.float64, v=np.tile([0.0, 0.0, -2.0], (n, 1)))
+        st["colliders"] = [c]
+        a = R.run(p, mats, st, 8)
+        b, rc = cref.substeps(p, mats, st, 8)
+        assert rc == 0
+        assert np.abs(a["x"] - b["x"]).max() < 1e-12, c.kind
+        assert np.allclose(a["colliders"][0].pos, b["colliders"][0].pos)
+        assert np.allclose(a["colliders"][0].rot, b["colliders"][0].rot)
+
+
+def test_rigid_sphere_collider_stops_a_falling_block():
+    """legacy_coupler.py:166-343: a block thrown down onto a fixed sphere does not pass
+    through it; without the collider it falls below the sphere's top."""
+    c = R.Collider("sphere", np.array([0.5, 0.5, 0.25]), np.eye(3), np.array([0.06, 0, 0]))
+    out, st = _block_over(c, v0=(0, 0, -3.0), substeps=400)
+    r = np.linalg.norm(out["x"] - c.pos, axis=1)
+    assert r.min() > 0.06 - 1.5 / 64  # penetration bounded by the grid resolution
+    assert out["forces"][0][2] < 0  # the block pushes the sphere down
+    free, _ = _block_over(R.Collider("sphere", np.array([0.5, 0.5, -5.0]), np.eye(3), np.array([0.06, 0, 0])),
+                          v0=(0, 0, -3.0), substeps=400)
+    assert free["x"][:, 2].min() < 0.25
+
+
+def test_rigid_collider_forms_agree():
+    """A plane with normal +z through z=0.3 and a box whose top face is at z=0.3 stop a
+    falling block at the same height; a tilted frictionless plane lets it slide."""
+    plane = R.Collider("plane", np.array([0.5, 0.5, 0.3]), np.eye(3), np.array([0.0, 0.0, 1.0]))
+    box = R.Collider("box", np.array([0.5, 0.5, 0.2]), np.eye(3), np.array([0.3, 0.3, 0.1]))
+    a, _ = _block_over(plane, v0=(0, 0, -2.0))
+    b, _ = _block_over(box, v0=(0, 0, -2.0))
+    assert abs(a["x"][:, 2].min() - b["x"][:, 2].min()) < 2e-3
+    assert 0.3 - 1.5 / 64 < a["x"][:, 2].min() < 0.31
+    th = np.deg2rad(30)
+    Rt = np.array([[np.cos(th), 0, np.sin(th)], [0, 1, 0], [-np.sin(th), 0, np.cos(th)]])
+    slope = R.Collider("plane", np.array([0.5, 0.5, 0.3]), Rt, np.array([0.0, 0.0, 1.0]), friction=0.0)
+    c, st = _block_over(slope, z0=0.33, v0=(0, 0, -1.0), substeps=600)
+    assert c["x"][:, 0].mean() > st["x"][:, 0].mean() + 0.005  # slid down-slope (+x)
+
+
+def test_kinematic_collider_motion():
+    p = R.Params(grid_density=64, dt=1e-4, dtype=np.float64)
+    c = R.Collider("sphere", np.array([0.5, 0.5, 0.4]), np.eye(3), np.array([0.05, 0, 0]),
+                   lin_vel=np.array([0.0, 0.0, 0.5]), ang_vel=np.array([0.0, 0.0, 3.0]))
+    c2 = R.advance_colliders(p, [c])[0]
+    assert np.allclose(c2.pos, [0.5, 0.5, 0.4 + 0.5e-4])
+    assert np.allclose(c2.rot @ c2.rot.T, np.eye(3)) and np.isclose(np.arctan2(c2.rot[1, 0], c2.rot[0, 0]), 3e-4)
