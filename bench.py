@@ -104,18 +104,60 @@ def ncu_traffic():
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+    """SM clock and clock-event reasons sampled every 10 ms during the timed region, through
+    NVML in a background thread (read-only queries); nvidia-smi at 200 ms if NVML is
+    unavailable."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
+        self.samples = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
         self.proc = None
         self.path = None
 
     def start(self):
+        try:
+            import threading
+
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = None
+            try:  # the CUDA device's own GPU, whatever CUDA_VISIBLE_DEVICES renumbered
+                import torch
+
+                h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(torch.cuda.get_device_properties(self.gpu).uuid))
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            masks = [(name, getattr(pynvml, attr, 0)) for name, attr in self.REASONS]
+            self._stop = threading.Event()
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        mhz = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                        r = int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                        self.samples.append((mhz, [n for n, m in masks if m and (r & m)]))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+
+            self._thread = threading.Thread(target=run, daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            self._thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -126,6 +168,16 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
+            if not self.samples:
+                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"], "source": "nvml"}
+            sm = [m for m, _ in self.samples]
+            loaded = [x for x in sm if x > 0.5 * (self.max_mhz or max(sm))] or sm
+            reasons = sorted({r for _, rs in self.samples for r in rs})
+            return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(self.samples), "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -147,7 +199,7 @@ class Clocks:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 def dist_setup(args):
