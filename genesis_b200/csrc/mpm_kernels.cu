@@ -794,7 +794,8 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
     // mark the grid blocks the chunk's stencils reach (a superset of the blocks its flush
     // writes: per axis the neighbour is included if any stencil reaches into it)
     if (threadIdx.x < 27 && cnt > 0) {
-        const int e[3] = {threadIdx.x / 9, (threadIdx.x / 3) % 3, threadIdx.x % 3};  // db + 1 per axis
+        const int t = (int)threadIdx.x;
+        const int e[3] = {t / 9, (t / 3) % 3, t % 3};  // db + 1 per axis
         bool on = ((h.vx >> e[0]) & (h.vy >> e[1]) & (h.vz >> e[2]) & 1u) != 0u;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
