@@ -11,7 +11,6 @@ scene B times.
 
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 from . import autotune

@@ -9,7 +9,6 @@ the grid block-major inside one workspace blob.
 from __future__ import annotations
 
 import ctypes as C
-import math
 from dataclasses import dataclass, field
 
 import numpy as np

@@ -2,8 +2,6 @@
 
 from __future__ import annotations
 
-import torch
-
 
 class MPMSolverState:
     """Dynamic state of the MPM solver: pos/vel [B,N,3], C/F [B,N,3,3], Jp [B,N], active [B,N] bool."""

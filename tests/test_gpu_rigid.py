@@ -7,7 +7,6 @@ import pytest
 import torch
 
 import genesis_b200 as gs
-from genesis_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 

@@ -1,6 +1,5 @@
 """End-to-end through the public API (gs.init / gs.Scene / entities), on the GPU."""
 
-import numpy as np
 import pytest
 import torch
 

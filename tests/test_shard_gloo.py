@@ -4,7 +4,6 @@ by work, each 'processes' its shard, and the gathered results cover every scene 
 import os
 
 import numpy as np
-import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
