@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 MPM_OK = 0
 MPM_E_INVALID = -1

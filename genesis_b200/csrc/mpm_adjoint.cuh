@@ -228,8 +228,35 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
     svd3(Ft, U, Sg, V);
     uvt(U, V, Rm);
     const float J = Sg[0] * (Sg[1] * Sg[2]);
+    const bool neo = (m.flags & MPM_MATF_NEOHOOKEAN) != 0;
+    // muscle actuation (muscle.py:57-65): + ka g g^T with g = F_tmp d, ka = stiffness * actu
+    const bool musc = (m.flags & MPM_MATF_MUSCLE) && par.actu;
+    float dd[3] = {0.f, 0.f, 0.f}, g[3] = {0.f, 0.f, 0.f}, ka = 0.f;
+    if (musc) {
+        const int gi = par.gid[s];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) dd[a] = par.muscle_dir[3 * gi + a];
+        ka = m.muscle_stiffness * par.actu[gi];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) g[a] = Ft[a * 3 + 0] * dd[0] + Ft[a * 3 + 1] * dd[1] + Ft[a * 3 + 2] * dd[2];
+    }
     float P[9];
-    corotated(mu, lam, J, Ft, Rm, P);
+    if (neo) {
+        // mu F_tmp F_tmp^T + (lam log J - mu) I   (elastic.py:78-81)
+        const float dg = lam * logf(J) - mu;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                P[i * 3 + j] = mu * (Ft[i * 3 + 0] * Ft[j * 3 + 0] + Ft[i * 3 + 1] * Ft[j * 3 + 1] +
+                                     Ft[i * 3 + 2] * Ft[j * 3 + 2]) + (i == j ? dg : 0.f);
+    } else {
+        corotated(mu, lam, J, Ft, Rm, P);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) P[i * 3 + j] += ka * g[i] * g[j];
     const float mass = m.mass;
     float A[9];
 #pragma unroll
@@ -275,11 +302,55 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
         Pb[k] = I.stress_scale * Ab[k];
         Cbn[k] = mass * Ab[k];
     }
+    float Ftb[9];
+    float mub = 0.f, lamb = 0.f;
+    if (musc) {
+        // P += ka g g^T: gb = ka (Pb + Pb^T) g, Ftb += gb d^T, dL/dactu = stiffness g^T Pb g
+        float gb[3], gPg = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            gb[a] = 0.f;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                gb[a] += ka * (Pb[a * 3 + b] + Pb[b * 3 + a]) * g[b];
+                gPg += g[a] * Pb[a * 3 + b] * g[b];
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) Ftb[a * 3 + b] = gb[a] * dd[b];
+        lame_bar[2 * st + s] += m.muscle_stiffness * gPg;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Ftb[k] = 0.f;
+    }
+    if (neo) {
+        // P = mu F F^T + (lam log J - mu) I: Ftb += mu (Pb + Pb^T) F + lam tr(Pb) / J dJ/dF
+        const float trP = Pb[0] + Pb[4] + Pb[8];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                float acc = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) acc += (Pb[i * 3 + k] + Pb[k * 3 + i]) * Ft[k * 3 + j];
+                Ftb[i * 3 + j] += mu * acc;
+                mub += Pb[i * 3 + j] * (Ft[i * 3 + 0] * Ft[j * 3 + 0] + Ft[i * 3 + 1] * Ft[j * 3 + 1] +
+                                        Ft[i * 3 + 2] * Ft[j * 3 + 2]);
+            }
+        mub -= trP;
+        lamb = trP * logf(J);
+        float K[9];
+        cofactor(Ft, K);
+        const float Jb = lam * trP / J;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Ftb[k] += Jb * K[k];
+    } else {
     // P = 2 mu (Ft - R) Ft^T + lam J (J - 1) I
     float D[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) D[k] = Ft[k] - Rm[k];
-    float mub = 0.f;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -289,8 +360,8 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
         }
     mub *= 2.f;
     const float trP = Pb[0] + Pb[4] + Pb[8];
-    const float lamb = trP * J * (J - 1.f);
-    float Ftb[9], Rb[9];
+    lamb = trP * J * (J - 1.f);
+    float Rb[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -302,7 +373,7 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
                 a2 += Pb[k * 3 + i] * D[k * 3 + j];   // (Pb^T D)_ij
             }
             a3 = a1;
-            Ftb[i * 3 + j] = 2.f * mu * (a1 + a2);
+            Ftb[i * 3 + j] += 2.f * mu * (a1 + a2);
             Rb[i * 3 + j] = -2.f * mu * a3;
         }
     const float Jb = lam * (2.f * J - 1.f) * trP;
@@ -341,6 +412,7 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
                 for (int b = 0; b < 3; ++b) acc += U[i * 3 + a] * X[a * 3 + b] * V[j * 3 + b];
             Ftb[i * 3 + j] += acc;
         }
+    }
     // F_new = F_tmp (Elastic): the incoming F adjoint adds to F_tmp's
     float* xo = adj + (int64_t)MPM_CH_X * st;
     float* vo = adj + (int64_t)MPM_CH_V * st;

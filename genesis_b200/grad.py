@@ -7,10 +7,12 @@ reverse: it restores a segment's checkpoint, recomputes the states inside it, an
 the adjoint of each substep (mpm_substep_adjoint) from the last to the first.  Memory is
 one state per checkpoint plus one segment of states, instead of every substep.
 
-Supported: Elastic (corotated) scenes with per-particle Young's modulus; gradients with
-respect to a uniform initial velocity v0 (3,) and per-particle E (N,).  This replaces the
-reference's requires_grad path (simulator.py:294-303, mpm_solver.py:485-517, with the
-gstaichi autodiff kernels and backward_svd at mpm_solver.py:1112-1129) for this case.
+Supported: Elastic scenes (corotated or neo-Hookean) and Muscle scenes, with per-particle
+Young's modulus; gradients with respect to a uniform initial velocity v0 (3,), per-particle
+E (N,) and, for Muscle, per-particle actuation (N,) (mpm_solver.py:922-949: the reference's
+actuation gradients).  This replaces the reference's requires_grad path
+(simulator.py:294-303, mpm_solver.py:485-517, with the gstaichi autodiff kernels and
+backward_svd at mpm_solver.py:1112-1129) for these cases.
 """
 
 from __future__ import annotations
@@ -27,8 +29,9 @@ from .exceptions import GenesisException
 class DifferentiableRollout:
     def __init__(self, desc, checkpoint_every: int = 20, nu: float | None = None):
         kinds = {k for k, _ in desc.materials}
-        if kinds != {"elastic"} or any(kw.get("model", "corotation") != "corotation" for _, kw in desc.materials):
-            raise GenesisException("the adjoint supports Elastic (corotated) scenes only")
+        if not kinds <= {"elastic", "muscle"} or len(desc.materials) != 1:
+            raise GenesisException("the adjoint supports one Elastic or Muscle material per scene")
+        self.muscle = kinds == {"muscle"}
         self.desc = desc
         self.k = int(checkpoint_every)
         self.T = int(desc.n_substeps)
@@ -42,19 +45,27 @@ class DifferentiableRollout:
         nat.check("mpm_adjoint_workspace_bytes", lib.mpm_adjoint_workspace_bytes(C.byref(self.rt.prob), C.byref(nbytes)))
         self.adj_ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.rt.device)
         self.adj = torch.zeros_like(self.rt.state)
-        self.lame_bar = torch.zeros((2, self.rt.stride), dtype=torch.float32, device=self.rt.device)
+        # dL/dmu, dL/dlam and (Muscle) dL/dactu per slot
+        self.lame_bar = torch.zeros((3, self.rt.stride), dtype=torch.float32, device=self.rt.device)
+        if self.muscle:
+            mdir = desc.meta.get("muscle_dir")
+            if mdir is not None:
+                self.rt.muscle_dir[: self.rt.n] = torch.as_tensor(mdir, dtype=torch.float32, device=self.rt.device)
         self.checkpoints: list[torch.Tensor] = []
 
     def _lame(self, E):
         nu = self.nu
         return E / (2.0 * (1.0 + nu)), E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
 
-    def forward(self, v0: torch.Tensor, E: torch.Tensor) -> torch.Tensor:
+    def forward(self, v0: torch.Tensor, E: torch.Tensor, actu: torch.Tensor | None = None) -> torch.Tensor:
         rt, d = self.rt, self.desc
         n = rt.n
         dev = rt.device
         v0 = v0.detach().to(dev, torch.float32).reshape(1, 3)
         E = E.detach().to(dev, torch.float32).reshape(n)
+        if self.muscle:
+            a = torch.zeros(n, device=dev) if actu is None else actu.detach().to(dev, torch.float32).reshape(n)
+            rt.actu[:n] = a
         mats = torch.zeros(n, dtype=torch.uint8, device=dev)
         rt.load_state(
             torch.as_tensor(d.pos, dtype=torch.float32, device=dev),
@@ -82,13 +93,16 @@ class DifferentiableRollout:
         rt = self.rt
         par = nat.Particles(
             state=state.data_ptr(), state_stride=rt.stride, mat=rt.mat.data_ptr(), pflags=rt.pflags.data_ptr(),
-            gid=rt.gid.data_ptr(), slot=rt.slot.data_ptr(), mu_p=rt.mu_p.data_ptr(), lam_p=rt.lam_p.data_ptr())
+            gid=rt.gid.data_ptr(), slot=rt.slot.data_ptr(), mu_p=rt.mu_p.data_ptr(), lam_p=rt.lam_p.data_ptr(),
+            actu=rt.actu.data_ptr() if self.muscle else None,
+            muscle_dir=rt.muscle_dir.data_ptr() if self.muscle else None)
         nat.check("mpm_substep_adjoint", rt.lib.mpm_substep_adjoint(
             C.byref(rt.prob), C.byref(rt.tables), C.byref(par), C.c_void_p(self.adj.data_ptr()),
             C.c_void_p(self.lame_bar.data_ptr()), rt._ws, C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
 
     def backward(self, pos_grad: torch.Tensor):
-        """pos_grad: dL/dx_final [N,3] in API order -> (dL/dv0 [3], dL/dE [N])."""
+        """pos_grad: dL/dx_final [N,3] in API order -> (dL/dv0 [3], dL/dE [N], dL/dactu [N] or
+        None)."""
         rt = self.rt
         n = rt.n
         slot = rt.slot[:n].long()
@@ -115,21 +129,28 @@ class DifferentiableRollout:
         Ebar_slot = self.lame_bar[0, :n] / (2.0 * (1.0 + nu)) + self.lame_bar[1, :n] * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
         Ebar = torch.empty(n, dtype=torch.float32, device=rt.device)
         Ebar[gid] = Ebar_slot
-        return vbar, Ebar
+        abar = None
+        if self.muscle:
+            abar = torch.empty(n, dtype=torch.float32, device=rt.device)
+            abar[gid] = self.lame_bar[2, :n]
+        return vbar, Ebar, abar
 
 
 class _RolloutFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, v0, E, sim):
+    def forward(ctx, v0, E, actu, sim):
         ctx.sim = sim
-        return sim.forward(v0, E)
+        return sim.forward(v0, E, actu)
 
     @staticmethod
     def backward(ctx, grad_pos):
-        v0b, Eb = ctx.sim.backward(grad_pos)
-        return v0b, Eb, None
+        v0b, Eb, ab = ctx.sim.backward(grad_pos)
+        return v0b, Eb, ab, None
 
 
-def rollout(v0: torch.Tensor, E: torch.Tensor, sim: DifferentiableRollout) -> torch.Tensor:
-    """Final particle positions [N,3] of the rollout, differentiable w.r.t. v0 and E."""
-    return _RolloutFunction.apply(v0, E, sim)
+def rollout(v0: torch.Tensor, E: torch.Tensor, sim: DifferentiableRollout, actu: torch.Tensor | None = None):
+    """Final particle positions [N,3] of the rollout, differentiable w.r.t. v0, E and (for a
+    Muscle scene) the per-particle actuation."""
+    if sim.muscle and actu is None:
+        actu = torch.zeros(sim.rt.n, device=sim.rt.device)
+    return _RolloutFunction.apply(v0, E, actu, sim)

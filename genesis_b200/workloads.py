@@ -216,5 +216,6 @@ def make_materials(scene: SceneDesc, module):
         "liquid": module.Liquid,
         "sand": module.Sand,
         "snow": module.Snow,
+        "muscle": module.Muscle,
     }
     return [cls[k](**kw) for k, kw in scene.materials]

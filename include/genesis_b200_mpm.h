@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 3
+#define MPM_ABI_VERSION 4
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -264,15 +264,17 @@ int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* 
 int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par,
                          int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
 
-/* ---- differentiation (Elastic, corotated) ----------------------------------
- * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with elastic.py:70-75;
+/* ---- differentiation (Elastic corotated / neo-Hookean, Muscle) --------------
+ * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with elastic.py:62-83 and
+ * muscle.py:57-65; every material of the problem must be an Elastic or a Muscle;
  * replaces the gstaichi autodiff of substep_post_coupling_grad / couple_grad /
  * substep_pre_coupling_grad, mpm_solver.py:485-517, legacy_coupler.py:996-1017).
  * `state` is the particle state at the START of the substep (unchanged by the call; the
  * particles must still be in the slot order the last mpm_sort_particles produced).
  * `adj` (float[25][state_stride], same planar layout as the state) holds on entry the
  * adjoint of the substep's output x, v, C, F and on return the adjoint of its input;
- * `lame_bar` (float[2][state_stride]) accumulates dL/dmu and dL/dlam per particle.
+ * `lame_bar` (float[3][state_stride]) accumulates per slot dL/dmu, dL/dlam and, when
+ * `state->actu` is set (Muscle), dL/dactu (row 2 is untouched otherwise).
  * The caller allocates adj_workspace (mpm_adjoint_workspace_bytes). */
 int mpm_adjoint_workspace_bytes(const mpm_problem* prob, uint64_t* out);
 int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state, float* adj,

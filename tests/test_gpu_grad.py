@@ -76,3 +76,81 @@ def test_adjoint_full_config_against_fp64_finite_differences():
     fd = (L(v0, Ep) - L(v0, Em)) / (2 * hE)
     print(f"\n[accuracy] grad E[{k}]: adjoint {gE[k]:.6e}  fp64 FD {fd:.6e}  rel {abs(gE[k] - fd) / abs(fd):.2e}")
     assert abs(gE[k] - fd) <= 5e-2 * abs(fd), (gE[k], fd)
+
+
+def _fd_setup(d, actu=None, mdir=None):
+    from oracle import bridge, cref
+    from oracle import mpm_adjoint as AD
+
+    p, mats, st = bridge.from_desc(d, np.float64)
+    n = d.n_particles
+    tgt = d.meta["target"]
+
+    def L(v, Ev, a=None):
+        s = dict(st)
+        s["v"] = np.tile(v, (n, 1))
+        if a is not None:
+            s["actu"] = a
+            s["mdir"] = mdir
+        mu, lam = AD.lame_of_E(Ev, 0.3)
+        out, rc = cref.substeps(p, mats, s, d.n_substeps, mu_p=mu, lam_p=lam)
+        assert rc == 0
+        return float(((out["x"].mean(0) - tgt) ** 2).sum())
+
+    return L
+
+
+def test_neo_hookean_adjoint_against_fp64_finite_differences():
+    d = W.diff_elastic(n=2000, n_substeps=120)
+    d.materials = [("elastic", dict(E=1e5, nu=0.3, rho=1000.0, model="neohooken"))]
+    loss, gv, gE = _grads(d, checkpoint_every=20)
+    L = _fd_setup(d)
+    v0, E = d.meta["v0"], d.E_particle
+    h = 1e-4
+    for c in (0, 2):
+        e = np.zeros(3)
+        e[c] = h
+        fd = (L(v0 + e, E) - L(v0 - e, E)) / (2 * h)
+        print(f"\n[accuracy] neo-Hookean grad v0[{c}]: adjoint {gv[c]:.6e}  fp64 FD {fd:.6e}")
+        assert abs(gv[c] - fd) <= 2e-2 * max(abs(fd), 1e-3 * np.abs(gv).max()), (c, gv[c], fd)
+    k = int(np.argmax(np.abs(gE)))
+    hE = 1e-4 * E[k]
+    Ep, Em = E.copy(), E.copy()
+    Ep[k] += hE
+    Em[k] -= hE
+    fd = (L(v0, Ep) - L(v0, Em)) / (2 * hE)
+    print(f"\n[accuracy] neo-Hookean grad E[{k}]: adjoint {gE[k]:.6e}  fp64 FD {fd:.6e}")
+    assert abs(gE[k] - fd) <= 5e-2 * abs(fd), (gE[k], fd)
+
+
+def test_muscle_actuation_adjoint_against_fp64_finite_differences():
+    """Muscle (neo-Hookean) block with two actuation groups along different fibres:
+    dL/d(group actuation) = sum of the per-particle actuation adjoints of the group."""
+    from genesis_b200.grad import DifferentiableRollout, rollout
+
+    d = W.diff_elastic(n=2000, n_substeps=120)
+    d.materials = [("muscle", dict(E=1e5, nu=0.3, rho=1000.0))]
+    n = d.n_particles
+    group = (d.pos[:, 0] > np.median(d.pos[:, 0])).astype(np.int64)
+    mdir = np.where(group[:, None] == 0, [0.0, 0.0, 1.0], [0.0, 0.6, 0.8])
+    d.meta["muscle_dir"] = mdir
+    a_grp = np.array([0.3, -0.2])
+    sim = DifferentiableRollout(d, checkpoint_every=20)
+    v0 = torch.tensor(d.meta["v0"], dtype=torch.float32, device="cuda")
+    E = torch.tensor(d.E_particle, dtype=torch.float32, device="cuda")
+    a = torch.tensor(a_grp[group], dtype=torch.float32, device="cuda", requires_grad=True)
+    x = rollout(v0, E, sim, actu=a)
+    tgt = torch.tensor(d.meta["target"], dtype=torch.float32, device="cuda")
+    ((x.mean(0) - tgt) ** 2).sum().backward()
+    ga = a.grad.cpu().numpy().astype(np.float64)
+    g_grp = np.array([ga[group == 0].sum(), ga[group == 1].sum()])
+    L = _fd_setup(d, mdir=mdir)
+    h = 1e-3
+    for gi in range(2):
+        ap, am = a_grp.copy(), a_grp.copy()
+        ap[gi] += h
+        am[gi] -= h
+        fd = (L(d.meta["v0"], d.E_particle, ap[group]) - L(d.meta["v0"], d.E_particle, am[group])) / (2 * h)
+        print(f"\n[accuracy] muscle grad actu[group {gi}]: adjoint {g_grp[gi]:.6e}  fp64 FD {fd:.6e}")
+        assert abs(g_grp[gi] - fd) <= 3e-2 * max(abs(fd), 1e-3 * np.abs(g_grp).max()), (gi, g_grp[gi], fd)
+    assert n == 2000
