@@ -579,7 +579,9 @@ struct Stash {
 // compute_F_tmp + svd + return mapping + stress (mpm_solver.py:261-345) for slot p with
 // velocity v and affine C; writes F and Jp of the next frame and fills the scatter payload
 // for position x.
-template <int P>
+// MUSCLE: compiled with the Muscle actuation term (a separate instantiation, so problems
+// without muscles pay no registers for it)
+template <int P, bool MUSCLE>
 __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm_material* __restrict__ mats,
                                                 const mpm_particles& par, int p, const float* x_in,
                                                 const float* v_in, const float* C_in, int ox, int oy, int oz,
@@ -626,7 +628,7 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
     const float J = Sg[0] * (Sg[1] * Sg[2]);
     float Fn[9], stress[9], Jpn;
     constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, stress);
-    if ((m.flags & MPM_MATF_MUSCLE) && par.actu) {
+    if (MUSCLE && (m.flags & MPM_MATF_MUSCLE) && par.actu) {
         // muscle.py:57-65: + stiffness * actu * F_tmp d d^T F_tmp^T; a Muscle is an Elastic,
         // whose F_new is F_tmp, so Fn stands in for F_tmp here
         const int g = par.gid[p];
@@ -1007,7 +1009,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
 
 // ---------------------------------------------------------------- p2g
 
-template <int P>
+template <int P, bool MUSCLE>
 __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a) {
     __shared__ Tile T;
     __shared__ Stash<P> SH;
@@ -1038,7 +1040,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
             }
 #pragma unroll
             for (int k = 0; k < 9; ++k) C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
-            particle_update<P>(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x, SH);
+            particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x, SH);
         }
         scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
     }
@@ -1087,7 +1089,7 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
 
 // g2p of substep n fused with p2g of substep n+1: the new v and C never leave registers
 // (they are recomputed from the grid by the next gather), only x, F and Jp are stored.
-template <int P>
+template <int P, bool MUSCLE>
 __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs a) {
     __shared__ VelTile VT;
     __shared__ Tile T;
@@ -1119,7 +1121,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
             if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
-                particle_update<P>(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x, SH);
+                particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x, SH);
             }
         }
         scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
@@ -1430,15 +1432,15 @@ static const DevInfo* dev_info() {
     if (d.sms == 0) {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        d.occ_p2g[0] = occ_of<128>(k_p2g<128>);
-        d.occ_p2g[1] = occ_of<256>(k_p2g<256>);
-        d.occ_p2g[2] = occ_of<512>(k_p2g<512>);
+        d.occ_p2g[0] = occ_of<128>(k_p2g<128, false>);
+        d.occ_p2g[1] = occ_of<256>(k_p2g<256, false>);
+        d.occ_p2g[2] = occ_of<512>(k_p2g<512, false>);
         d.occ_g2p[0] = occ_of<128>(k_g2p<128>);
         d.occ_g2p[1] = occ_of<256>(k_g2p<256>);
         d.occ_g2p[2] = occ_of<512>(k_g2p<512>);
-        d.occ_g2p2g[0] = occ_of<128>(k_g2p2g<128>);
-        d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256>);
-        d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512>);
+        d.occ_g2p2g[0] = occ_of<128>(k_g2p2g<128, false>);
+        d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256, false>);
+        d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512, false>);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op, 256, 0);
         d.occ_grid = n > 0 ? n : 1;
@@ -1520,10 +1522,26 @@ static int launch_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_partic
     P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
     const int pi = p_index(prob->chunk_particles);
     const int ctas = persistent_ctas(prob, d->occ_p2g[pi]);
+    const bool muscle = par->actu != nullptr;
     switch (prob->chunk_particles) {
-        case 128: k_p2g<128><<<ctas, 128, 0, s>>>(a); break;
-        case 256: k_p2g<256><<<ctas, 256, 0, s>>>(a); break;
-        case 512: k_p2g<512><<<ctas, 512, 0, s>>>(a); break;
+        case 128:
+            if (muscle)
+                k_p2g<128, true><<<ctas, 128, 0, s>>>(a);
+            else
+                k_p2g<128, false><<<ctas, 128, 0, s>>>(a);
+            break;
+        case 256:
+            if (muscle)
+                k_p2g<256, true><<<ctas, 256, 0, s>>>(a);
+            else
+                k_p2g<256, false><<<ctas, 256, 0, s>>>(a);
+            break;
+        case 512:
+            if (muscle)
+                k_p2g<512, true><<<ctas, 512, 0, s>>>(a);
+            else
+                k_p2g<512, false><<<ctas, 512, 0, s>>>(a);
+            break;
     }
     if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
         k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);
@@ -1565,10 +1583,26 @@ static int launch_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_part
     P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
     const int pi = p_index(prob->chunk_particles);
     const int ctas = persistent_ctas(prob, d->occ_g2p2g[pi]);
+    const bool muscle = par->actu != nullptr;
     switch (prob->chunk_particles) {
-        case 128: k_g2p2g<128><<<ctas, 128, 0, s>>>(a); break;
-        case 256: k_g2p2g<256><<<ctas, 256, 0, s>>>(a); break;
-        case 512: k_g2p2g<512><<<ctas, 512, 0, s>>>(a); break;
+        case 128:
+            if (muscle)
+                k_g2p2g<128, true><<<ctas, 128, 0, s>>>(a);
+            else
+                k_g2p2g<128, false><<<ctas, 128, 0, s>>>(a);
+            break;
+        case 256:
+            if (muscle)
+                k_g2p2g<256, true><<<ctas, 256, 0, s>>>(a);
+            else
+                k_g2p2g<256, false><<<ctas, 256, 0, s>>>(a);
+            break;
+        case 512:
+            if (muscle)
+                k_g2p2g<512, true><<<ctas, 512, 0, s>>>(a);
+            else
+                k_g2p2g<512, false><<<ctas, 512, 0, s>>>(a);
+            break;
     }
     if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
         k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);
