@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--batch-substeps", type=int, default=100)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
     ap.add_argument("--no-grad", action="store_true", help="skip the differentiation run")
-    ap.add_argument("--serve-requests", type=int, default=200,
+    ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests in the Poisson stream (2000 = the full serving config)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-run", action="store_true", help="short run for ncu launch lists")
