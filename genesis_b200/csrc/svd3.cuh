@@ -12,9 +12,10 @@
 //      the singular values on the diagonal of R; only the last one can be negative
 //      (det A < 0).
 // Unlike the paper's quaternion "approximate Givens" rotations, the Jacobi step uses
-// exact rotations (Golub & Van Loan, Alg. 8.4.2) with a fixed count of 4 sweeps, which
-// keeps the kernel branch-light: 4 cyclic sweeps leave relative off-diagonal residue
-// below 1e-20 for F = I + E with |E| up to 0.5 (3 sweeps: ~6e-6), i.e. float32 round-off.
+// exact rotations (Golub & Van Loan, Alg. 8.4.2) with at most 4 sweeps: 4 cyclic sweeps
+// leave relative off-diagonal residue below 1e-20 for F = I + E with |E| up to 0.5
+// (3 sweeps: ~6e-6), i.e. float32 round-off; a warp stops earlier once all its lanes have
+// converged to that level (quadratic convergence: typically after 2-3 sweeps).
 #pragma once
 
 namespace gbm {
@@ -104,6 +105,13 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* 
     float v[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
 #pragma unroll kSvdUnroll
     for (int sw = 0; sw < SWEEPS; ++sw) {
+        // Early exit, decided per warp: once every active lane's off-diagonal mass is below
+        // 1e-7 of its diagonal, a further rotation moves the diagonal by O(1e-14) and V by
+        // O(1e-7), i.e. float32 round-off (and when eigenvalues nearly coincide, a rotation
+        // inside that eigenspace leaves U S V^T, and every isotropic function of F, unchanged).
+        const float off = fabsf(a[0][1]) + fabsf(a[0][2]) + fabsf(a[1][2]);
+        const float diag = fabsf(a[0][0]) + fabsf(a[1][1]) + fabsf(a[2][2]);
+        if (__all_sync(__activemask(), !(off > 1e-7f * diag))) break;
         jacobi_pq<0, 1>(a, v);
         jacobi_pq<0, 2>(a, v);
         jacobi_pq<1, 2>(a, v);
