@@ -94,3 +94,17 @@ def test_missing_library_fails_loudly(tmp_path):
             nat.load(str(tmp_path / "nope.so"))
         finally:
             nat._lib = saved
+
+
+def test_block_count_above_the_scan_limit_is_refused(lib):
+    """More grid blocks than the single-pass scan covers (4096 x 4096) -> MPM_E_CAPACITY."""
+    mc = C.c_int32()
+    assert lib.mpm_max_chunks(1000, 4096 * 4096, 128, C.byref(mc)) == 0
+    ok = nat.Problem(n_instances=1, n_particles=1000, n_blocks=4096 * 4096, n_materials=1, chunk_particles=128,
+                     max_chunks=mc.value, grid_ctas=0, flags=0)
+    b = C.c_uint64()
+    assert lib.mpm_workspace_bytes(C.byref(ok), C.byref(b)) == 0
+    assert lib.mpm_max_chunks(1000, 4096 * 4096 + 1, 128, C.byref(mc)) == 0
+    big = nat.Problem(n_instances=1, n_particles=1000, n_blocks=4096 * 4096 + 1, n_materials=1, chunk_particles=128,
+                      max_chunks=mc.value, grid_ctas=0, flags=0)
+    assert lib.mpm_workspace_bytes(C.byref(big), C.byref(b)) == nat.MPM_E_CAPACITY
