@@ -84,6 +84,8 @@ class MPMEntity:
             v, f = _mesh.box_mesh(self._morph.size)
         elif isinstance(self._morph, _morphs.Sphere):
             v, f = _mesh.icosphere(3, self._morph.radius)
+        elif isinstance(self._morph, _morphs.Mesh):
+            v, f = self._morph.vertices, self._morph.faces
         else:
             return
         R = _morphs._quat_to_R(self._morph.quat)

@@ -48,3 +48,95 @@ def icosphere(subdivisions=3, radius=1.0):
             nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
         f = nf
     return np.asarray(verts) * radius, np.asarray(f, dtype=np.int64)
+
+
+# ---------------------------------------------------------------- mesh files
+
+def load_obj(path):
+    """Vertices [V, 3] and triangles [F, 3] of a Wavefront OBJ file ('v' and 'f' records;
+    polygons are fanned into triangles, 'f' indices may carry /vt/vn and be negative)."""
+    verts, faces = [], []
+    with open(path) as fh:
+        for line in fh:
+            parts = line.split()
+            if not parts:
+                continue
+            if parts[0] == "v" and len(parts) >= 4:
+                verts.append([float(parts[1]), float(parts[2]), float(parts[3])])
+            elif parts[0] == "f" and len(parts) >= 4:
+                idx = []
+                for tok in parts[1:]:
+                    i = int(tok.split("/")[0])
+                    idx.append(i - 1 if i > 0 else len(verts) + i)
+                for k in range(1, len(idx) - 1):
+                    faces.append([idx[0], idx[k], idx[k + 1]])
+    if not verts or not faces:
+        raise ValueError(f"{path}: no vertices or faces")
+    return np.asarray(verts, dtype=np.float64), np.asarray(faces, dtype=np.int64)
+
+
+def _ray_crossings(tri, oy, oz):
+    """x of the crossings of the lines {(t, oy[r], oz[r])} with the triangles tri [T, 3, 3]:
+    a list of sorted arrays, one per line.  Triangles are binned by their y-z bounding box
+    on a coarse grid so each line is tested only against the triangles of its cell."""
+    y0, z0 = tri[:, :, 1], tri[:, :, 2]
+    lo = np.array([min(y0.min(), oy.min()), min(z0.min(), oz.min())])
+    hi = np.array([max(y0.max(), oy.max()), max(z0.max(), oz.max())])
+    G = int(np.clip(np.sqrt(len(tri)) / 2, 1, 128))
+    cell = (hi - lo) / G + 1e-12
+    tminy = np.floor((y0.min(1) - lo[0]) / cell[0]).astype(int).clip(0, G - 1)
+    tmaxy = np.floor((y0.max(1) - lo[0]) / cell[0]).astype(int).clip(0, G - 1)
+    tminz = np.floor((z0.min(1) - lo[1]) / cell[1]).astype(int).clip(0, G - 1)
+    tmaxz = np.floor((z0.max(1) - lo[1]) / cell[1]).astype(int).clip(0, G - 1)
+    buckets = [[[] for _ in range(G)] for _ in range(G)]
+    for t in range(len(tri)):
+        for a in range(tminy[t], tmaxy[t] + 1):
+            for b in range(tminz[t], tmaxz[t] + 1):
+                buckets[a][b].append(t)
+    ly = np.floor((oy - lo[0]) / cell[0]).astype(int).clip(0, G - 1)
+    lz = np.floor((oz - lo[1]) / cell[1]).astype(int).clip(0, G - 1)
+    out = [None] * len(oy)
+    key = ly * G + lz
+    for k in np.unique(key):
+        rays = np.nonzero(key == k)[0]
+        ts = buckets[k // G][k % G]
+        if not ts:
+            for r in rays:
+                out[r] = np.zeros(0)
+            continue
+        T = tri[ts]  # [t, 3, 3]
+        a, b, c = T[:, 0], T[:, 1], T[:, 2]
+        # 2-D barycentrics of (oy, oz) in the y-z projection of each triangle
+        d = (b[:, 1] - a[:, 1]) * (c[:, 2] - a[:, 2]) - (c[:, 1] - a[:, 1]) * (b[:, 2] - a[:, 2])
+        py = oy[rays][:, None] - a[None, :, 1]
+        pz = oz[rays][:, None] - a[None, :, 2]
+        dd = np.where(d == 0, 1.0, d)[None, :]  # triangles seen edge-on never count as hit
+        u = (py * (c[None, :, 2] - a[None, :, 2]) - (c[None, :, 1] - a[None, :, 1]) * pz) / dd
+        v = ((b[None, :, 1] - a[None, :, 1]) * pz - py * (b[None, :, 2] - a[None, :, 2])) / dd
+        hit = (d[None, :] != 0) & (u >= 0) & (v >= 0) & (u + v <= 1)
+        x = a[None, :, 0] + u * (b[None, :, 0] - a[None, :, 0]) + v * (c[None, :, 0] - a[None, :, 0])
+        for i, r in enumerate(rays):
+            out[r] = np.sort(x[i][hit[i]])
+    return out
+
+
+def points_inside(verts, faces, pts):
+    """Even-odd ray test (rays along +x) of points against a closed triangle mesh.  The rays
+    are shifted by an irrational sub-tolerance offset so none passes exactly through an
+    edge or a vertex."""
+    tri = np.asarray(verts, dtype=np.float64)[np.asarray(faces)]
+    ext = float(np.ptp(verts, axis=0).max()) or 1.0
+    oy = pts[:, 1] + 1e-9 * ext * np.sqrt(2.0)
+    oz = pts[:, 2] + 1e-9 * ext * np.sqrt(3.0)
+    # points sharing a ray (a regular lattice) are tested once per ray
+    keys, inv = np.unique(np.stack([oy, oz], 1), axis=0, return_inverse=True)
+    xs = _ray_crossings(tri, keys[:, 0], keys[:, 1])
+    inside = np.zeros(len(pts), dtype=bool)
+    inv = np.asarray(inv).reshape(-1)
+    order = np.argsort(inv, kind="stable")
+    starts = np.searchsorted(inv[order], np.arange(len(keys) + 1))
+    for r, x in enumerate(xs):
+        sel = order[starts[r]:starts[r + 1]]
+        n_after = len(x) - np.searchsorted(x, pts[sel, 0], side="right")
+        inside[sel] = (n_after % 2) == 1
+    return inside

@@ -1,4 +1,4 @@
-"""gs.morphs used by MPM entities: Box, Sphere and Nowhere.
+"""gs.morphs used by MPM entities: Box, Sphere, Mesh and Nowhere.
 
 Particle sampling follows the reference's simple samplers
 (genesis/utils/particle.py:174-202, ``_box_to_particles``): 'regular' places
@@ -138,6 +138,52 @@ class Nowhere(Morph):
         return np.tile(np.array([2333333.0, 6666666.0, 5201314.0]), (self.n_particles, 1))
 
 
+class Mesh(Morph):
+    """Morph loaded from a Wavefront OBJ file (options/morphs.py:603-760, ``Mesh``).
+
+    The vertices are scaled in the file's frame, then rotated by ``quat``/``euler`` and moved
+    to ``pos`` (engine/mesh.py:342, particle_entity.py:265-268).  Particles are sampled the
+    way the reference's ``trimesh_to_particles_simple`` does (utils/particle.py:42-76): a
+    box lattice over the scaled mesh's bounds, of which the points inside the closed mesh are
+    kept; inside is an exact even-odd ray test here (the reference keeps points with a
+    negative winding-number signed distance, which is the same set for a closed mesh).
+    Fields of the reference's Mesh that only matter to rigid bodies or to the renderer
+    (decimate, convexify, coacd_options, group_by_material, ...) are accepted and ignored."""
+
+    def __init__(self, file, scale=1.0, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, **kw):
+        super().__init__(pos=pos, euler=euler, quat=quat, **kw)
+        from . import mesh as _mesh
+
+        self.file = str(file)
+        if not self.file.lower().endswith(".obj"):
+            raise GenesisException(f"Unsupported mesh file (only .obj is read): {self.file}")
+        try:
+            v, f = _mesh.load_obj(self.file)
+        except (OSError, ValueError) as e:
+            raise GenesisException(f"Cannot load mesh {self.file}: {e}") from e
+        sc = np.broadcast_to(np.asarray(scale, dtype=np.float64), (3,))
+        if np.any(sc <= 0):
+            raise GenesisException("Mesh scale must be positive.")
+        self.scale = float(sc[0]) if np.all(sc == sc[0]) else tuple(float(x) for x in sc)
+        self.vertices = v * sc  # local (scaled, untransformed) frame
+        self.faces = f
+
+    def _local_particles(self, p_size, sampler, rng):
+        from . import mesh as _mesh
+
+        lo, hi = self.vertices.min(0), self.vertices.max(0)
+        size, center = hi - lo, (hi + lo) / 2
+        if sampler == "random":
+            pts = rng.uniform(low=lo, high=hi, size=(n_particles_3D(p_size, size), 3))
+        elif sampler == "regular":
+            axes = [np.linspace(center[d] - size[d] / 2 + 0.5 * p_size, center[d] + size[d] / 2 - 0.5 * p_size,
+                                n_particles_1D(p_size, size[d])) for d in range(3)]
+            pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+        else:
+            raise GenesisException(f"Unsupported sampler method: {sampler}.")
+        return pts[_mesh.points_inside(self.vertices, self.faces, pts)]
+
+
 class Plane(Morph):
     """Infinite plane through `pos` with `normal` in its local frame (options/morphs.py:409-470);
     only meaningful for rigid entities (a collider of the MPM grid op)."""
@@ -156,4 +202,4 @@ class Plane(Morph):
         raise GenesisException("A Plane has no particles; use it with gs.materials.Rigid.")
 
 
-__all__ = ["Morph", "Box", "Sphere", "Nowhere", "Plane"]
+__all__ = ["Morph", "Box", "Sphere", "Mesh", "Nowhere", "Plane"]

@@ -126,3 +126,33 @@ def test_async_nan_check_raises_on_a_later_call():
         scene.get_state()
     with pytest.raises(gs.GenesisException):
         scene.check_state()  # the device status word stays set
+
+
+def test_mesh_morph_entity_matches_box(tmp_path):
+    """A box loaded from an OBJ file steps like the Box primitive of the same size and pose
+    (same lattice up to round-off), and its file mesh is skinned."""
+    hx = 0.5
+    v = [[x, y, z] for x in (-hx, hx) for y in (-hx, hx) for z in (-hx, hx)]
+    q = [[0, 1, 3, 2], [4, 6, 7, 5], [0, 4, 5, 1], [2, 3, 7, 6], [0, 2, 6, 4], [1, 5, 7, 3]]
+    obj = tmp_path / "cube.obj"
+    obj.write_text("".join(f"v {a} {b} {c}\n" for a, b, c in v) + "".join(
+        "f " + " ".join(str(i + 1) for i in f) + "\n" for f in q))
+
+    def run(morph):
+        gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+        scene = gs.Scene(
+            sim_options=gs.options.SimOptions(dt=1e-3, substeps=10, gravity=(0, 0, -9.8)),
+            mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
+                                              particle_size=0.0125),
+        )
+        e = scene.add_entity(morph, material=gs.materials.MPM.Elastic(E=1e5, nu=0.3))
+        scene.build()
+        for _ in range(5):
+            scene.step()
+        return e, e.get_particles_pos().cpu()
+
+    em, pm = run(gs.morphs.Mesh(file=str(obj), scale=0.2, pos=(0.5, 0.5, 0.5), euler=(0, 0, 20)))
+    eb, pb = run(gs.morphs.Box(size=(0.2, 0.2, 0.2), pos=(0.5, 0.5, 0.5), euler=(0, 0, 20)))
+    assert em.n_particles == eb.n_particles == 16**3
+    assert torch.allclose(pm, pb, atol=1e-5)
+    assert em.n_vverts == 8

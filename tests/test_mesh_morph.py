@@ -1,0 +1,100 @@
+"""gs.morphs.Mesh on the host: the OBJ reader, the inside test and the box-lattice sampler
+(utils/particle.py:42-76, ``trimesh_to_particles_simple``).  No GPU."""
+
+import numpy as np
+import pytest
+
+from genesis_b200 import mesh
+from genesis_b200.exceptions import GenesisException
+from genesis_b200.morphs import Box, Mesh
+
+
+def _write_obj(path, v, f, quads=None):
+    with open(path, "w") as fh:
+        fh.write("# generated\no body\n")
+        for p in v:
+            fh.write(f"v {p[0]:.9f} {p[1]:.9f} {p[2]:.9f}\n")
+        fh.write("vn 0 0 1\n")
+        for t in f:
+            fh.write("f " + " ".join(f"{i + 1}//1" for i in t) + "\n")
+        for q in quads or []:
+            fh.write("f " + " ".join(str(i - len(v)) for i in q) + "\n")  # negative indices
+
+
+def _box_quads(size):
+    """A box written as six quads (fanned into triangles by the reader)."""
+    hx, hy, hz = np.asarray(size) / 2
+    v = np.array([[x, y, z] for x in (-hx, hx) for y in (-hy, hy) for z in (-hz, hz)])
+    q = [[0, 1, 3, 2], [4, 6, 7, 5], [0, 4, 5, 1], [2, 3, 7, 6], [0, 2, 6, 4], [1, 5, 7, 3]]
+    return v, q
+
+
+def test_obj_reader(tmp_path):
+    v, q = _box_quads((0.2, 0.1, 0.3))
+    p = tmp_path / "box.obj"
+    _write_obj(p, v, [], quads=q)
+    rv, rf = mesh.load_obj(str(p))
+    assert np.allclose(rv, v) and rf.shape == (12, 3)
+    with pytest.raises(ValueError):
+        mesh.load_obj(str(_write_empty(tmp_path)))
+
+
+def _write_empty(tmp_path):
+    p = tmp_path / "empty.obj"
+    p.write_text("# nothing\n")
+    return p
+
+
+def test_inside_exact_on_box_and_sphere():
+    rng = np.random.default_rng(1)
+    bv, bf = mesh.box_mesh((0.2, 0.1, 0.3))
+    q = rng.uniform(-0.2, 0.2, size=(4000, 3))
+    assert (mesh.points_inside(bv, bf, q) == (np.abs(q) < [0.1, 0.05, 0.15]).all(1)).all()
+    sv, sf = mesh.icosphere(3, 0.1)
+    p = rng.uniform(-0.12, 0.12, size=(8000, 3))
+    r = np.linalg.norm(p, axis=1)
+    ins = mesh.points_inside(sv, sf, p)
+    # the icosphere lies between radius 0.1*cos(edge angle) and 0.1
+    assert not ins[r > 0.1].any() and ins[r < 0.098].all()
+
+
+def test_mesh_morph_matches_box_lattice(tmp_path):
+    v, q = _box_quads((1.0, 1.0, 1.0))
+    p = tmp_path / "unit.obj"
+    _write_obj(p, v, [], quads=q)
+    m = Mesh(file=str(p), scale=(0.2, 0.1, 0.3), pos=(0.5, 0.4, 0.3), euler=(0, 0, 30))
+    b = Box(size=(0.2, 0.1, 0.3), pos=(0.5, 0.4, 0.3), euler=(0, 0, 30))
+    pm, pb = m.sample(0.01, "regular"), b.sample(0.01, "regular")
+    assert pm.shape == pb.shape
+    assert np.allclose(np.sort(pm, axis=0), np.sort(pb, axis=0), atol=1e-12)
+
+
+def test_mesh_morph_sphere_counts(tmp_path):
+    sv, sf = mesh.icosphere(3, 1.0)
+    p = tmp_path / "ball.obj"
+    _write_obj(p, sv, sf)
+    m = Mesh(file=str(p), scale=0.1, pos=(0.5, 0.5, 0.5))
+    pts = m.sample(0.01, "regular")
+    t = m.vertices[m.faces]
+    vol = np.einsum("ij,ij->i", t[:, 0], np.cross(t[:, 1], t[:, 2])).sum() / 6.0  # enclosed volume
+    size = np.ptp(m.vertices, axis=0)
+    n = np.round(size / 0.01)
+    cell = np.prod((size - 0.01) / (n - 1))  # the lattice spacing the sampler used per axis
+    assert abs(len(pts) * cell / vol - 1.0) < 0.02
+    assert (np.linalg.norm(pts - 0.5, axis=1) <= 0.1).all()
+    rnd = m.sample(0.01, "random", rng=np.random.default_rng(0))
+    expect = np.prod(n) * vol / np.prod(size)  # the bounds-box sample times the inside share
+    assert abs(len(rnd) / expect - 1.0) < 0.05
+    assert (np.linalg.norm(rnd - 0.5, axis=1) <= 0.1).all()
+    pbs = m.sample(0.01, "pbs")
+    assert pbs.shape == pts.shape
+
+
+def test_mesh_morph_errors(tmp_path):
+    with pytest.raises(GenesisException):
+        Mesh(file=str(tmp_path / "missing.obj"))
+    with pytest.raises(GenesisException):
+        Mesh(file=str(tmp_path / "a.stl"))
+    p = _write_empty(tmp_path)
+    with pytest.raises(GenesisException):
+        Mesh(file=str(p))
