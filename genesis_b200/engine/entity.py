@@ -3,6 +3,8 @@
 
 from __future__ import annotations
 
+import uuid
+
 import numpy as np
 import torch
 
@@ -44,6 +46,7 @@ class MPMEntity:
         self._surface = surface
         self._particle_size = particle_size
         self._idx = idx
+        self._uid = uuid.uuid4().hex[:7]
         self._particle_start = particle_start
         sampler = material.sampler
         self.sampler = sampler
@@ -84,6 +87,8 @@ class MPMEntity:
             v, f = _mesh.box_mesh(self._morph.size)
         elif isinstance(self._morph, _morphs.Sphere):
             v, f = _mesh.icosphere(3, self._morph.radius)
+        elif isinstance(self._morph, _morphs.Cylinder):
+            v, f = _mesh.cylinder_mesh(self._morph.radius, self._morph.height)
         elif isinstance(self._morph, _morphs.Mesh):
             v, f = self._morph.vertices, self._morph.faces
         else:
@@ -102,6 +107,37 @@ class MPMEntity:
     @property
     def vfaces(self):
         return self._vfaces
+
+    @property
+    def n_vfaces(self):
+        return len(self._vfaces)
+
+    def _v_offsets(self):
+        """(first visual vertex, first visual face) of this entity in the solver's
+        concatenation of the entities' visual meshes, in the order they were added."""
+        vv = vf = 0
+        for e in self._solver.entities:
+            if e is self:
+                return vv, vf
+            vv += e.n_vverts
+            vf += e.n_vfaces
+        return vv, vf
+
+    @property
+    def vvert_start(self):
+        return self._v_offsets()[0]
+
+    @property
+    def vvert_end(self):
+        return self.vvert_start + self.n_vverts
+
+    @property
+    def vface_start(self):
+        return self._v_offsets()[1]
+
+    @property
+    def vface_end(self):
+        return self.vface_start + self.n_vfaces
 
     @property
     def n_vverts(self):
@@ -135,6 +171,10 @@ class MPMEntity:
     @property
     def idx(self):
         return self._idx
+
+    @property
+    def uid(self):
+        return self._uid
 
     @property
     def n_particles(self):
@@ -215,6 +255,12 @@ class MPMEntity:
         vals = self._values(free, (), idx.shape[0], idx.shape[1], torch.uint8)
         self._solver.runtime.set_particles_free(idx.reshape(-1), vals)
 
+    def get_free(self):
+        """Free (True) or fixed (False) flag of each particle, shape (n_particles,)
+        (mpm_entity.py:571-583)."""
+        self._check_built()
+        return self._solver.runtime.get_particles_free(self._flat_idx(None, None)[0])
+
     # buffered targets applied at the next step (particle_entity.py:418-458, 503-578)
     def set_position(self, value, envs_idx=None):
         poss = _as_tensor(value, torch.float32, self._solver.device)
@@ -227,7 +273,17 @@ class MPMEntity:
         self._tgt["vel"] = (_as_tensor(vels, torch.float32, self._solver.device), envs_idx)
 
     def set_active(self, active, envs_idx=None):
-        self._tgt["act"] = (_as_tensor(active, torch.uint8, self._solver.device), envs_idx)
+        a = _as_tensor(active, torch.uint8, self._solver.device)
+        self._tgt["act"] = (a, envs_idx)
+        self.active = bool((a != 0).any())
+
+    def activate(self):
+        """Every particle of the entity takes part in the next step (particle_entity.py:639-644)."""
+        self.set_active(1)
+
+    def deactivate(self):
+        """Every particle of the entity is frozen from the next step on (particle_entity.py:646-651)."""
+        self.set_active(0)
 
     # ---------------------------------------------------------------- muscle
     def _assert_muscle(self):
@@ -342,6 +398,20 @@ class MPMEntity:
 
     def get_particles_active(self, envs_idx=None):
         return self._squeeze(self._get(("active",), envs_idx)["active"])
+
+    def find_closest_particle(self, pos, envs_idx=None):
+        """Local index of the particle closest to pos ([M,] 3) per environment
+        (particle_entity.py:709-738); a scalar tensor without environments."""
+        self._check_built()
+        p = _as_tensor(pos, torch.float32, self._solver.device)
+        envs = self._envs(envs_idx)
+        if p.ndim == 1:
+            p = p.reshape(1, 3).expand(len(envs), 3)
+        if p.shape != (len(envs), 3):
+            raise GenesisException(f"Invalid tensor shape {tuple(p.shape)} (expected ({len(envs)}, 3)).")
+        cur = self._get(("pos",), envs_idx)["pos"]
+        idx = torch.argmin(torch.linalg.norm(cur - p[:, None], dim=-1), dim=-1).to(torch.int32)
+        return idx[0] if self._scene.n_envs == 0 else idx
 
     def get_state(self):
         st = self._get(("pos", "vel", "C", "F", "Jp", "active"), None)

@@ -447,6 +447,11 @@ class MPMRuntime:
     def set_particles_active(self, idx, active):
         return self._idx_call("mpm_set_particles_active", idx, active, torch.uint8, ())
 
+    def get_particles_free(self, idx):
+        """Free flags (bool) of API-order particles idx."""
+        idx = torch.as_tensor(idx, dtype=torch.int64, device=self.device).reshape(-1)
+        return (self.pflags[self.slot[idx].long()] & nat.PFLAG_FREE) != 0
+
     def set_particles_free(self, idx, free):
         keep = self._idx_call("mpm_set_particles_free", idx, free, torch.uint8, ())
         if not bool(torch.as_tensor(free).bool().all()):

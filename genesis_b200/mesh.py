@@ -2,6 +2,7 @@
 them with trimesh: genesis/engine/mesh.py:369-381, utils/mesh.py:706-723, 823-880).
 
 box_mesh: the 8 corners and 12 triangles of an axis-aligned box.
+cylinder_mesh: a closed polygonal cylinder along z (trimesh.creation.cylinder's layout).
 icosphere: the unit icosahedron with every triangle split into four `subdivisions`
 times and the new vertices pushed onto the sphere (subdivisions=3: 642 vertices,
 1280 faces, as trimesh.creation.icosphere gives).
@@ -48,6 +49,22 @@ def icosphere(subdivisions=3, radius=1.0):
             nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
         f = nf
     return np.asarray(verts) * radius, np.asarray(f, dtype=np.int64)
+
+
+def cylinder_mesh(radius=0.5, height=1.0, sections=32):
+    """Closed cylinder along z centred on the origin: `sections` vertices per rim plus the
+    two cap centres (2 * sections + 2 vertices, 4 * sections outward-wound triangles)."""
+    a = 2.0 * np.pi * np.arange(sections) / sections
+    ring = np.stack([radius * np.cos(a), radius * np.sin(a)], 1)
+    h = height / 2.0
+    v = np.concatenate([np.c_[ring, np.full(sections, -h)], np.c_[ring, np.full(sections, h)],
+                        [[0.0, 0.0, -h], [0.0, 0.0, h]]])
+    lo, hi = 2 * sections, 2 * sections + 1
+    f = []
+    for i in range(sections):
+        j = (i + 1) % sections
+        f += [(i, j, sections + j), (i, sections + j, sections + i), (lo, j, i), (hi, sections + i, sections + j)]
+    return v, np.asarray(f, dtype=np.int64)
 
 
 # ---------------------------------------------------------------- mesh files

@@ -1,4 +1,4 @@
-"""gs.morphs used by MPM entities: Box, Sphere, Mesh and Nowhere.
+"""gs.morphs used by MPM entities: Box, Sphere, Cylinder, Mesh and Nowhere.
 
 Particle sampling follows the reference's simple samplers
 (genesis/utils/particle.py:174-202, ``_box_to_particles``): 'regular' places
@@ -121,6 +121,31 @@ class Sphere(Morph):
         return g[np.linalg.norm(g, axis=1) <= r]
 
 
+class Cylinder(Morph):
+    """Cylinder along the local z axis, centred on pos (options/morphs.py:278-343).  Sampled as
+    the box [2r, 2r, h] cut to the points within r of the axis (utils/particle.py:225-246)."""
+
+    def __init__(self, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, height=1.0, radius=0.5, **kw):
+        super().__init__(pos=pos, euler=euler, quat=quat, **kw)
+        self.height = float(height)
+        self.radius = float(radius)
+        if self.height <= 0 or self.radius <= 0:
+            raise GenesisException("Cylinder height and radius must be positive.")
+
+    def _local_particles(self, p_size, sampler, rng):
+        r, h = self.radius, self.height
+        size = np.array([2 * r, 2 * r, h])
+        if sampler == "random":
+            pts = rng.uniform(low=-size / 2, high=size / 2, size=(n_particles_3D(p_size, size), 3))
+        elif sampler == "regular":
+            axes = [np.linspace(-size[d] / 2 + 0.5 * p_size, size[d] / 2 - 0.5 * p_size,
+                                n_particles_1D(p_size, size[d])) for d in range(3)]
+            pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+        else:
+            raise GenesisException(f"Unsupported sampler method: {sampler}.")
+        return pts[np.linalg.norm(pts[:, :2], axis=1) <= r]
+
+
 class Nowhere(Morph):
     """Inactive particles parked far away, activated later by an emitter (options/morphs.py: Nowhere)."""
 
@@ -202,4 +227,4 @@ class Plane(Morph):
         raise GenesisException("A Plane has no particles; use it with gs.materials.Rigid.")
 
 
-__all__ = ["Morph", "Box", "Sphere", "Mesh", "Nowhere", "Plane"]
+__all__ = ["Morph", "Box", "Sphere", "Cylinder", "Mesh", "Nowhere", "Plane"]

@@ -156,3 +156,59 @@ def test_mesh_morph_entity_matches_box(tmp_path):
     assert em.n_particles == eb.n_particles == 16**3
     assert torch.allclose(pm, pb, atol=1e-5)
     assert em.n_vverts == 8
+
+
+def test_entity_utilities():
+    """activate/deactivate, get_free, find_closest_particle and the visual-mesh ranges
+    (particle_entity.py:639-651, 709-738; mpm_entity.py:571-583)."""
+    scene, cube, sand = _scene(substeps=5)
+    assert cube.uid != sand.uid and len(cube.uid) == 7
+    assert cube.vvert_start == 0 and cube.vvert_end == cube.n_vverts == 8 and cube.n_vfaces == 12
+    assert sand.n_vverts == 0 and sand.vvert_start == sand.vvert_end == 8  # Sand is not skinned
+    assert bool(cube.get_free().all()) and cube.get_free().shape == (cube.n_particles,)
+    cube.set_free(torch.zeros(cube.n_particles, dtype=torch.bool))
+    assert not bool(cube.get_free().any()) and bool(sand.get_free().all())
+    cube.set_free(torch.ones(cube.n_particles, dtype=torch.bool))
+    p = cube.get_particles_pos()
+    k = 123
+    i = cube.find_closest_particle(p[k] + 1e-4)
+    assert i.ndim == 0 and int(i) == k
+    cube.deactivate()
+    p0 = cube.get_particles_pos().clone()
+    scene.step()
+    assert not bool(cube.get_particles_active().any())
+    assert torch.equal(cube.get_particles_pos(), p0)  # inactive particles are copied through
+    cube.activate()
+    scene.step()
+    assert bool(cube.get_particles_active().all())
+    assert float((cube.get_particles_pos()[:, 2] - p0[:, 2]).mean()) < 0
+
+
+def test_find_closest_particle_batched():
+    scene, cube, sand = _scene(n_envs=2, substeps=5)
+    p = cube.get_particles_pos()
+    i = cube.find_closest_particle(torch.stack([p[0, 7], p[1, 99]]))
+    assert i.shape == (2,) and i.tolist() == [7, 99]
+
+
+def test_cylinder_entity_steps_and_skins():
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=1e-3, substeps=10, gravity=(0, 0, -9.8)),
+        mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
+                                          particle_size=0.0125),
+    )
+    cyl = scene.add_entity(gs.morphs.Cylinder(pos=(0.5, 0.5, 0.3), radius=0.1, height=0.2),
+                           material=gs.materials.MPM.Elastic(E=1e5, nu=0.3))
+    scene.build()
+    z0 = float(cyl.get_particles_pos()[:, 2].mean())
+    for _ in range(5):
+        scene.step()
+    assert float(cyl.get_particles_pos()[:, 2].mean()) < z0
+    assert cyl.n_vverts == 66 and cyl.n_vfaces == 128
+    solver = cyl.solver
+    solver.update_render_fields()
+    vv = solver.vverts_render["pos"][0].cpu().double()
+    # the skinned rim stays around the particles' centre of mass
+    c = cyl.get_particles_pos().cpu().double().mean(0)
+    assert float((vv.mean(0) - c).norm()) < 0.02

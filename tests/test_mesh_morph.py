@@ -98,3 +98,26 @@ def test_mesh_morph_errors(tmp_path):
     p = _write_empty(tmp_path)
     with pytest.raises(GenesisException):
         Mesh(file=str(p))
+
+
+def test_cylinder_morph_and_mesh():
+    from genesis_b200.morphs import Cylinder
+
+    c = Cylinder(pos=(0.5, 0.5, 0.4), radius=0.1, height=0.2, euler=(90, 0, 0))
+    pts = c.sample(0.01, "regular")
+    # regular lattice of 20 x 20 x 20 cut to the disc: pi/4 of the columns
+    assert abs(len(pts) / (20**3 * np.pi / 4) - 1.0) < 0.03
+    R = np.array([[1, 0, 0], [0, 0, -1], [0, 1, 0]])  # 90 degrees about x
+    local = (pts - [0.5, 0.5, 0.4]) @ R
+    assert (np.linalg.norm(local[:, :2], axis=1) <= 0.1 + 1e-12).all() and (np.abs(local[:, 2]) < 0.1).all()
+    v, f = mesh.cylinder_mesh(0.1, 0.2, sections=32)
+    assert v.shape == (66, 3) and f.shape == (128, 3)
+    n = np.cross(v[f][:, 1] - v[f][:, 0], v[f][:, 2] - v[f][:, 0])
+    assert (np.einsum("ij,ij->i", n, v[f].mean(1)) > 0).all()  # outward winding
+    q = np.random.default_rng(3).uniform(-0.12, 0.12, size=(3000, 3))
+    ins = mesh.points_inside(v, f, q)
+    r = np.linalg.norm(q[:, :2], axis=1)
+    assert not ins[(r > 0.1) | (np.abs(q[:, 2]) > 0.1)].any()
+    assert ins[(r < 0.1 * np.cos(np.pi / 32)) & (np.abs(q[:, 2]) < 0.1)].all()
+    with pytest.raises(GenesisException):
+        Cylinder(radius=0.0)
