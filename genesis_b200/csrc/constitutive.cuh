@@ -47,6 +47,19 @@ __device__ __forceinline__ void corotated(float mu, float lam, float J, const fl
         }
 }
 
+// Logarithms, exponentials and quotients of the return mappings use the MUFU-based forms,
+// as the reference's kernels do (they are compiled with fast_math, genesis/__init__.py:265):
+// their error (absolute ~1e-7 in log, relative ~1e-7 in exp) is that of the singular values
+// they are applied to.
+__device__ __forceinline__ float flog(float x) { return __logf(x); }
+__device__ __forceinline__ float fexp(float x) { return __expf(x); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
+// Inviscid Liquid needs only J from the SVD (its stress is lam J (J - 1) I).
+__device__ __forceinline__ bool needs_uv(const mpm_material& m, float mu) {
+    return !(m.kind == MPM_MAT_LIQUID && mu == 0.f);
+}
+
 // Return mapping + stress for one particle.
 //   in : material m (mu/lam possibly overridden per particle), eps = gs.EPS,
 //        J = det(S), F_tmp, U, S, V, Jp (previous frame)
@@ -62,7 +75,7 @@ __device__ __forceinline__ void constitutive(const mpm_material& m, float mu, fl
             Jp_new = Jp;
             if (m.flags & MPM_MATF_NEOHOOKEAN) {
                 // mu F_tmp F_tmp^T + (lam log J - mu) I   (elastic.py:78-81)
-                const float d = lam * logf(J) - mu;
+                const float d = lam * flog(J) - mu;
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -77,13 +90,20 @@ __device__ __forceinline__ void constitutive(const mpm_material& m, float mu, fl
             break;
         }
         case MPM_MAT_LIQUID: {
-            // F_new = J^(1/3) I (liquid.py:52); pow keeps the NaN of a negative J
-            const float c = powf(J, 1.f / 3.f);
+            // F_new = J^(1/3) I (liquid.py:52); pow(J, 1/3) is NaN for a negative J
+            const float c = J >= 0.f ? cbrtf(J) : __int_as_float(0x7fc00000);
 #pragma unroll
             for (int k = 0; k < 9; ++k) F_new[k] = (k % 4 == 0) ? c : 0.f;
             Jp_new = Jp;
-            uvt(U, V, R);
-            corotated(mu, lam, J, Ft, R, stress);  // liquid.py:60 uses F_tmp
+            if (mu == 0.f) {
+                // liquid.py:47-48: mu is 0 unless viscous, so 2 mu (F_tmp - R) F_tmp^T vanishes
+                const float diag = lam * J * (J - 1.f);
+#pragma unroll
+                for (int k = 0; k < 9; ++k) stress[k] = (k % 4 == 0) ? diag : 0.f;
+            } else {
+                uvt(U, V, R);
+                corotated(mu, lam, J, Ft, R, stress);  // liquid.py:60 uses F_tmp
+            }
             break;
         }
         case MPM_MAT_ELASTOPLASTIC: {
@@ -92,15 +112,15 @@ __device__ __forceinline__ void constitutive(const mpm_material& m, float mu, fl
                 // elasto_plastic.py:71-84
                 float e[3];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) e[d] = logf(fmaxf(S[d], 0.05f));
-                const float mean = (e[0] + e[1] + e[2]) / 3.f;
+                for (int d = 0; d < 3; ++d) e[d] = flog(fmaxf(S[d], 0.05f));
+                const float mean = (e[0] + e[1] + e[2]) * (1.f / 3.f);
                 float eh[3] = {e[0] - mean, e[1] - mean, e[2] - mean};
                 const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
                 const float dg = ehn - m.vm_threshold * (m.mu / mu);
                 if (dg > 0.f) {
-                    const float r = dg / ehn;
+                    const float r = fdiv(dg, ehn);
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) Sn[d] = expf(e[d] - r * eh[d]);
+                    for (int d = 0; d < 3; ++d) Sn[d] = fexp(e[d] - r * eh[d]);
                     usvt(U, Sn, V, F_new);
                 } else {
 #pragma unroll
@@ -122,12 +142,12 @@ __device__ __forceinline__ void constitutive(const mpm_material& m, float mu, fl
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 Sn[d] = fminf(fmaxf(S[d], m.clamp_lo), m.clamp_hi);
-                jp = jp * (S[d] / Sn[d]);
+                jp = jp * fdiv(S[d], Sn[d]);
             }
             Jp_new = jp;
             usvt(U, Sn, V, F_new);
             // snow.py:75-79: hardening from the previous Jp
-            const float h = expf(10.f * (1.f - Jp));
+            const float h = fexp(10.f * (1.f - Jp));
             uvt(U, V, R);
             corotated(mu * h, lam * h, J, F_new, R, stress);
             break;
@@ -135,32 +155,37 @@ __device__ __forceinline__ void constitutive(const mpm_material& m, float mu, fl
         case MPM_MAT_SAND:
         default: {
             // sand.py:52-77
-            float e[3], Sn[3];
+            // ls = log S_new: S_new = exp(ls) is built from its logarithm, so sand.py:82's
+            // log(S_new) is ls itself (0 when the return mapping projects to the tip)
+            float e[3], Sn[3], ls[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) e[d] = logf(fmaxf(fabsf(S[d]), 1e-4f));
+            for (int d = 0; d < 3; ++d) e[d] = flog(fmaxf(fabsf(S[d]), 1e-4f));
             const float tr = e[0] + e[1] + e[2] + Jp;
-            float eh[3] = {e[0] - tr / 3.f, e[1] - tr / 3.f, e[2] - tr / 3.f};
+            const float t3 = tr * (1.f / 3.f);
+            float eh[3] = {e[0] - t3, e[1] - t3, e[2] - t3};
             const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
             if (tr >= 0.f) {
                 Jp_new = tr;
                 Sn[0] = Sn[1] = Sn[2] = 1.f;
+                ls[0] = ls[1] = ls[2] = 0.f;
             } else {
                 Jp_new = 0.f;
-                const float c1 = (3.f * lam + 2.f * mu) / (2.f * mu);
+                const float c1 = fdiv(3.f * lam + 2.f * mu, 2.f * mu);
                 const float dg = ehn + c1 * tr * m.sand_alpha;
-                const float r = fmaxf(0.f, dg) / ehn;
+                const float r = fdiv(fmaxf(0.f, dg), ehn);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) Sn[d] = expf(e[d] - r * eh[d]);
+                for (int d = 0; d < 3; ++d) {
+                    ls[d] = e[d] - r * eh[d];
+                    Sn[d] = fexp(ls[d]);
+                }
             }
             usvt(U, Sn, V, F_new);
             // sand.py:80-88 with S = S_new
             float center[3];
-            const float l0 = logf(Sn[0]), l1 = logf(Sn[1]), l2 = logf(Sn[2]);
-            const float lsum = l0 + l1 + l2;
-            const float ls[3] = {l0, l1, l2};
+            const float lsum = ls[0] + ls[1] + ls[2];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                const float inv = 1.f / Sn[d];
+                const float inv = fdiv(1.f, Sn[d]);
                 center[d] = 2.f * mu * ls[d] * inv + lam * lsum * inv;
             }
             float M[9];

@@ -624,7 +624,7 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
         for (int k = 0; k < 9; ++k) sv[(6 + k) * P] = C_in[k];
     }
     float U[9], Sg[3], V[9];
-    svd3(Ft, U, Sg, V);
+    svd3(Ft, U, Sg, V, needs_uv(m, mu));
     const float J = Sg[0] * (Sg[1] * Sg[2]);
     float Fn[9], stress[9], Jpn;
     constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, stress);

@@ -90,8 +90,10 @@ __device__ __forceinline__ void swap_cols_neg(float (&b)[3][3], float (&v)[3][3]
 }
 
 // A (row-major, 9 floats) = U diag(S) V^T with U, V proper rotations (row-major).
+// need_uv = false: the caller uses only the product S0 S1 S2 (= det A, which the QR
+// below yields whatever V is), so this lane does not hold up the warp's Jacobi sweeps.
 template <int SWEEPS = 4>
-__device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* V) {
+__device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* V, bool need_uv = true) {
     float a[3][3];
     // A^T A
 #pragma unroll
@@ -111,7 +113,7 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* 
         // inside that eigenspace leaves U S V^T, and every isotropic function of F, unchanged).
         const float off = fabsf(a[0][1]) + fabsf(a[0][2]) + fabsf(a[1][2]);
         const float diag = fabsf(a[0][0]) + fabsf(a[1][1]) + fabsf(a[2][2]);
-        if (__all_sync(__activemask(), !(off > 1e-7f * diag))) break;
+        if (__all_sync(__activemask(), !need_uv || !(off > 1e-7f * diag))) break;
         jacobi_pq<0, 1>(a, v);
         jacobi_pq<0, 2>(a, v);
         jacobi_pq<1, 2>(a, v);
