@@ -412,43 +412,91 @@ __global__ void k_sort_scatter(mpm_problem prob, mpm_particles par, Ws w) {
 }
 
 // Second half of the sort: copy each chunk back from the scratch arrays in an order that
-// puts the particles of different cells side by side.  Within a chunk (particles of one
-// grid block), particle k of cell c goes after the first k particles of every cell and
-// after particle k of the cells before c: "round k" holds one particle of each cell that
-// has more than k.  A warp then covers up to 32 distinct cells, so the 27-node stencils of
-// its lanes fall on distinct shared-memory banks in the p2g scatter and the g2p gather
-// instead of colliding.  Also writes gid and the slot map.
+// spreads the chunk's particles over the shared-memory banks.  A particle in in-block cell
+// (cx, cy, cz) scatters into tile words whose bank is (4 cx + 8 cy + cz + const) mod 32
+// for every stencil node (x-stride 68, y-stride 8), so its bank class
+// b = (4 cx + 8 cy + cz) mod 32 (two cells per class) decides its atomics' conflicts: a
+// warp costs as many shared-memory wavefronts per atomic as its most repeated class.
+//   1. Order: the r-th of the n_b particles of class b gets the key ((2r + 1) / (2 n_b), b)
+//      and the chunk is laid out by key, so every class is spread evenly over the chunk
+//      and each warp holds about 32 n_b / n of class b (the fewest repeats any split into
+//      warps can have, up to rounding).  The position of a particle is the number of
+//      smaller keys, summed per class in exact integer arithmetic.
+//   2. Deal: inside a full warp, lanes are re-dealt so that the four 8-lane phases of the
+//      gather's 16-byte loads (velocity tile slot = b mod 8) each see distinct slots where
+//      the warp's classes allow: the warp's particles ranked by (b mod 8, position) go to
+//      lane (i mod 4) * 8 + i / 4.
+// Also writes gid and the slot map.
 template <int P>
 __global__ void __launch_bounds__(P) k_sort_interleave(mpm_problem prob, const mpm_instance* __restrict__ inst,
                                                        mpm_particles par, Ws w) {
-    __shared__ int cnt[BLK3];
+    __shared__ int cnt[32];
+    __shared__ unsigned char s_slot[P];
     const int n_chunks = (int)w.counters[CNT_CHUNKS];
     const int64_t s = par.state_stride, t = w.tmp_stride;
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
-        if (threadIdx.x < BLK3) cnt[threadIdx.x] = 0;
+        if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
         __syncthreads();
         const int4 ch = w.chunks[ci];
         const int src = ch.z + threadIdx.x;
+        const int n = ch.w - ch.z;
         const bool live = src < ch.w;
-        int c = 0, r = 0;
+        int b = 0, r = 0;
         if (live) {
             const mpm_instance& I = inst[ch.x];
+            int c[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 // the cell of k_sort_keys, whose block is this chunk's block
                 const float f = floorf(w.state_tmp[(MPM_CH_X + d) * t + src] * I.inv_dx - 0.5f);
                 const int cell = isfinite(f) ? (int)fminf(fmaxf(f - (float)I.lower_cell[d], 0.f), (float)(I.res[d] - 1)) : 0;
-                c = c * BLK + (cell & (BLK - 1));
+                c[d] = cell & (BLK - 1);
             }
-            r = atomicAdd(&cnt[c], 1);
+            b = (4 * c[0] + 8 * c[1] + c[2]) & 31;
+            r = atomicAdd(&cnt[b], 1);
+        }
+        __syncthreads();
+        int pos = 0;
+        if (live) {
+            // #{(b', r') : (2r' + 1) n_b < (2r + 1) n_b', or equal and b' < b}
+            const int nb = cnt[b], two_n = 2 * nb;
+            const float inv = 1.f / (float)two_n;
+#pragma unroll 8
+            for (int k = 0; k < 32; ++k) {
+                const int nk = cnt[k];
+                const int q = (2 * r + 1) * nk - nb;
+                int cc;
+                if (k == b) {
+                    cc = r;
+                } else if (q < 0) {
+                    cc = 0;
+                } else {
+                    // q / (2 n_b) to the nearest integer: q < 2^20 and 2 n_b <= 1024, so the
+                    // quotient is an integer or at least 1/1024 away from one, far above the
+                    // float rounding of q * (1 / (2 n_b)) (below 1e-4 here)
+                    const int m = (int)floorf((float)q * inv + 0.5f);
+                    if (m * two_n == q)
+                        cc = m + ((k < b && m < nk) ? 1 : 0);
+                    else
+                        cc = m * two_n > q ? m : m + 1;
+                    cc = min(cc, nk);
+                }
+                pos += cc;
+            }
+            s_slot[pos] = (unsigned char)(b & 7);
         }
         __syncthreads();
         if (live) {
-            int pos = 0;
+            const int wb = pos & ~31;
+            if (wb + 32 <= n) {
+                const int sl = b & 7, me = pos & 31;
+                int i = 0;
 #pragma unroll 8
-            for (int k = 0; k < BLK3; ++k) {
-                const int nk = cnt[k];
-                pos += min(nk, r) + ((k < c && nk > r) ? 1 : 0);
+                for (int j = 0; j < 32; ++j) {
+                    const int o = s_slot[wb + j];
+                    i += (o < sl || (o == sl && j < me)) ? 1 : 0;
+                }
+                pos = wb + (i & 3) * 8 + (i >> 2);
             }
             const int dst = ch.z + pos;
 #pragma unroll 5
@@ -530,11 +578,12 @@ struct Tile {
     int wreach[32];    // per-warp stencil reach into the neighbour blocks (6 bits)
 };
 
-// Grid velocities of the 8^3 tile, float4 per node, with a y-stride of 12 nodes: a
-// quarter-warp's 8 lanes reading nodes whose (y, z) differ by (0..1, 0..3) then hit 8
-// distinct 4-bank groups (with a y-stride of 8 they would pair up).
-constexpr int VYS = 12;             // y-stride (nodes)
-constexpr int VXS = TILE * VYS;     // x-stride (96 nodes)
+// Grid velocities of the 8^3 tile, float4 per node, laid out like the atomic tile
+// (x-stride 68 nodes, y-stride 8): the 16-byte slot of a lane's every stencil node is then
+// (4 cx + cz + const) mod 8, i.e. its bank class mod 8, which the sort's lane deal keeps
+// distinct within each 8-lane phase of a 16-byte load.
+constexpr int VYS = TILE;           // y-stride (nodes)
+constexpr int VXS = TXS;            // x-stride (68 nodes)
 __device__ __forceinline__ int vidx(int x, int y, int z) { return x * VXS + y * VYS + z; }
 
 struct VelTile {
