@@ -181,6 +181,7 @@ SIGNATURES = {
     "mpm_status_enqueue": (C.c_int, [_P(Problem), vp, vp, vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),
     "mpm_instance_status": (C.c_int, [_P(Problem), vp, i32, vp, vp]),
+    "mpm_instance_status_enqueue": (C.c_int, [_P(Problem), vp, i32, vp, vp]),
     "mpm_get_state": (C.c_int, [_P(Problem), _P(Particles), vp, vp, vp, vp, vp, vp, vp]),
     "mpm_set_state": (C.c_int, [_P(Problem), _P(Particles), vp, vp, vp, vp, vp, vp, vp]),
     "mpm_set_particles_pos": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, vp, vp, vp]),

@@ -1707,7 +1707,15 @@ int mpm_workspace_init(const mpm_problem* prob, void* workspace, void* stream) {
     int rc = check_problem(prob);
     if (rc) return rc;
     if (!workspace) return MPM_E_INVALID;
-    if (cudaMemsetAsync(workspace, 0, layout_of(*prob).total, (cudaStream_t)stream) != cudaSuccess) return MPM_E_CUDA;
+    // Only what is read before it is written needs zeros: the grids (mm accumulates; gv of
+    // blocks no particle reached is read as zero velocity), the block flags, the counters
+    // and the per-instance statuses.  The sort scratch between them (keys, ranks, chunk
+    // table, permutation arrays: ~110 B per particle) is always written first.
+    const Layout L = layout_of(*prob);
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* b = (unsigned char*)workspace;
+    if (cudaMemsetAsync(b, 0, L.off[3], s) != cudaSuccess) return MPM_E_CUDA;  // mm, gv, flag
+    if (cudaMemsetAsync(b + L.off[17], 0, L.total - L.off[17], s) != cudaSuccess) return MPM_E_CUDA;
     return MPM_OK;
 }
 
@@ -1909,6 +1917,19 @@ int mpm_instance_status(const mpm_problem* prob, void* workspace, int32_t clear,
     const size_t bytes = (size_t)prob->n_instances * 4;
     if (cudaMemcpyAsync(out, w.inst_status, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPM_E_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return MPM_E_CUDA;
+    if (clear && cudaMemsetAsync(w.inst_status, 0, bytes, s) != cudaSuccess) return MPM_E_CUDA;
+    return MPM_OK;
+}
+
+int mpm_instance_status_enqueue(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out,
+                                void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!workspace || !out) return MPM_E_INVALID;
+    Ws w = ws_of(*prob, workspace);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = (size_t)prob->n_instances * 4;
+    if (cudaMemcpyAsync(out, w.inst_status, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPM_E_CUDA;
     if (clear && cudaMemsetAsync(w.inst_status, 0, bytes, s) != cudaSuccess) return MPM_E_CUDA;
     return MPM_OK;
 }

@@ -582,6 +582,16 @@ class MPMRuntime:
                    out.ctypes.data_as(C.c_void_p), _cuda_stream_handle())
         return out
 
+    def instance_status_enqueue(self, clear: bool = False):
+        """Enqueue the read of the per-instance status words: returns (pinned uint32 host
+        tensor, event), valid once the event has completed."""
+        out = torch.zeros(max(len(self._insts), 1), dtype=torch.int32, pin_memory=True)
+        self._call("mpm_instance_status_enqueue", C.byref(self.prob), self._ws, int(clear),
+                   C.c_void_p(out.data_ptr()), _cuda_stream_handle())
+        ev = torch.cuda.Event()
+        ev.record()
+        return out, ev
+
     def load_state(self, pos, vel, C_, F, Jp, active, mat):
         """Overwrite the whole particle state from device tensors in API order
         (pos/vel [n,3], C/F [n,9] or [n,3,3], Jp [n], active [n] bool, mat [n] uint8) and

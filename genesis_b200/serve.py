@@ -40,6 +40,20 @@ def estimate_bytes(desc, chunk_particles: int = 128) -> int:
     return int(n * per_particle + blocks * per_block + chunks)
 
 
+def _upload(a, dtype, dev):
+    """Host array -> device tensor through pinned memory, without waiting for the stream
+    (a copy from pageable memory would block the host until the GPU reaches it)."""
+    h = torch.as_tensor(np.asarray(a)).to(dtype).pin_memory()
+    return h.to(dev, non_blocking=True)
+
+
+def _download(t):
+    """Device tensor -> pinned host tensor, enqueued on the current stream."""
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    return h
+
+
 @dataclasses.dataclass
 class Result:
     rid: int
@@ -62,6 +76,8 @@ class _Slot:
     bytes: int
     state: dict | None = None  # device tensors in API order while being repacked
     retired: bool = False  # finished or evicted; a hole until the next repack
+    spec: object = None  # InstanceSpec, built once at admission
+    mats: list | None = None
 
 
 class AdmissionQueue:
@@ -98,8 +114,16 @@ class AdmissionQueue:
 class MPMServer:
     def __init__(self, budget_bytes: float = 150e9, tick_substeps: int = 50, max_active: int = 512,
                  chunk_particles: int = 128, sort_interval: int = 50, keep_results: bool = True,
-                 use_graphs: bool = False):
+                 use_graphs: bool = False, admit_wait: float = 0.2, admit_ratio: float = 0.25,
+                 min_live_particles: int = 2_000_000):
+        """admit_wait > 0 batches admissions: while at least min_live_particles are being
+        advanced, queued requests join (which costs a repack of every live rollout) only
+        once their particles reach admit_ratio of the live ones or the oldest has waited
+        admit_wait seconds.  admit_wait = 0 admits at every tick."""
         self.tick = int(tick_substeps)
+        self.admit_wait = float(admit_wait)
+        self.admit_ratio = float(admit_ratio)
+        self.min_live_particles = int(min_live_particles)
         self.queue = AdmissionQueue(budget_bytes, max_active, chunk_particles)
         self.chunk = chunk_particles
         self.sort_interval = sort_interval
@@ -130,19 +154,22 @@ class MPMServer:
         parts = {k: [] for k in ("pos", "vel", "C", "F", "Jp", "active", "mat")}
         for slot in self.active:
             d = slot.req.scene
-            mats = W.make_materials(d, MPM)
-            specs.append(spec_from_desc(d, mats))
+            if slot.spec is None:
+                slot.mats = W.make_materials(d, MPM)
+                slot.spec = spec_from_desc(d, slot.mats)
+            mats = slot.mats
+            specs.append(slot.spec)
             if slot.state is None:  # newly admitted: upload its initial state
                 n = d.n_particles
                 djp = np.array([m.default_Jp for m in mats], dtype=np.float32)[d.mat_idx]
                 slot.state = {
-                    "pos": torch.as_tensor(d.pos, dtype=torch.float32).to(dev),
-                    "vel": torch.as_tensor(d.vel, dtype=torch.float32).to(dev),
+                    "pos": _upload(d.pos, torch.float32, dev),
+                    "vel": _upload(d.vel, torch.float32, dev),
                     "C": torch.zeros((n, 9), dtype=torch.float32, device=dev),
                     "F": torch.eye(3, dtype=torch.float32, device=dev).reshape(1, 9).repeat(n, 1),
-                    "Jp": torch.as_tensor(djp).to(dev),
+                    "Jp": _upload(djp, torch.float32, dev),
                     "active": torch.ones(n, dtype=torch.bool, device=dev),
-                    "mat": torch.as_tensor(d.mat_idx.astype(np.uint8)).to(dev),
+                    "mat": _upload(d.mat_idx, torch.uint8, dev),
                 }
             for k in parts:
                 v = slot.state[k]
@@ -170,7 +197,14 @@ class MPMServer:
     def serve(self, requests, realtime: bool = True, on_result=None) -> list[Result]:
         """Run the request stream to completion.  With realtime=True a request becomes
         visible at its arrival time (seconds after the call starts); with realtime=False
-        all requests are visible at t=0 (throughput runs)."""
+        all requests are visible at t=0 (throughput runs).
+
+        The loop is pipelined: a tick's substeps, the read of its per-instance statuses and
+        of the results of the rollouts it completes are enqueued first; retiring those
+        rollouts, admitting queued requests and repacking (all stream-ordered after the
+        tick) then run on the host while the GPU works, and only then does the host wait
+        for the tick.  A rollout whose status shows NaN is evicted from whatever layout it
+        is in by then."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         results = {r.rid: Result(r.rid, r.arrival if realtime else 0.0) for r in reqs}
         t0 = time.perf_counter()
@@ -178,7 +212,9 @@ class MPMServer:
         bad = nat.MPM_STATUS_NAN | nat.MPM_STATUS_NONFINITE_VEL
         i = 0
         n_live = lambda: sum(1 for s in self.active if not s.retired)
-        while i < len(reqs) or self.queue.pending or n_live():
+
+        def push_arrivals():
+            nonlocal i
             now = clock()
             while i < len(reqs) and (not realtime or reqs[i].arrival <= now):
                 err = self.queue.push(reqs[i])
@@ -186,49 +222,78 @@ class MPMServer:
                     results[reqs[i].rid].error = err
                     results[reqs[i].rid].finished = now
                 i += 1
+
+        def admit():
+            if not self.queue.pending:
+                return False
+            if self.admit_wait > 0.0 and n_live():
+                live_p = sum(s.req.scene.n_particles for s in self.active if not s.retired)
+                if live_p >= self.min_live_particles:
+                    pend_p = sum(r.scene.n_particles for r, _ in self.queue.pending)
+                    oldest = self.queue.pending[0][0]
+                    waited = clock() - (oldest.arrival if realtime else 0.0)
+                    if pend_p < self.admit_ratio * live_p and waited < self.admit_wait:
+                        return False
             admitted = self.queue.pop_admissible(n_live())
-            if admitted:
-                now = clock()
-                new_slots = []
-                for req, need in admitted:
-                    results[req.rid].admitted = now
-                    new_slots.append(_Slot(req, int(req.scene.n_substeps), need))
-                self._repack(new_slots)
-            if not n_live():
+            if not admitted:
+                return False
+            now = clock()
+            new_slots = []
+            for req, need in admitted:
+                results[req.rid].admitted = now
+                new_slots.append(_Slot(req, int(req.scene.n_substeps), need))
+            self._repack(new_slots)
+            return True
+
+        while i < len(reqs) or self.queue.pending or n_live():
+            push_arrivals()
+            if not n_live() and not admit():
                 self.rt = None
                 self.active = []
                 if i < len(reqs) and realtime:
                     time.sleep(max(0.0, min(0.05, reqs[i].arrival - clock())))
                 continue
-            T = min(self.tick, min(s.remaining for s in self.active if not s.retired))
+            # ---- enqueue one tick, the read of its statuses and of its finished results
+            tick_slots = [s for s in self.active if not s.retired]
+            T = min(self.tick, min(s.remaining for s in tick_slots))
             self.rt.substeps(T)
             self.ticks += 1
-            self.particle_substeps += T * sum(s.req.scene.n_particles for s in self.active if not s.retired)
-            status = self.rt.instance_status(clear=True)  # synchronises: the tick is done
-            done = []
-            for k, s in enumerate(self.active):
-                if s.retired:
-                    continue
+            self.particle_substeps += T * sum(s.req.scene.n_particles for s in tick_slots)
+            tick_index = {id(s): k for k, s in enumerate(self.active)}
+            for s in tick_slots:
                 s.remaining -= T
-                if s.remaining == 0 or status[k] & bad:
-                    done.append(k)
-            if done:
-                st = self.rt.get_state(("pos", "vel")) if self.keep_results else None
+            finishing = [s for s in tick_slots if s.remaining == 0]
+            fin_host = {}
+            if finishing and self.keep_results:
+                st = self.rt.get_state(("pos", "vel"))
                 offs = self.rt.instance_offsets
-                now = clock()
-                for k in done:
-                    s = self.active[k]
-                    r = results[s.req.rid]
-                    r.finished = now
-                    if status[k] & bad:
-                        r.error = "NaN detected in MPM states"
-                    elif st is not None:
-                        sl = slice(offs[k], offs[k] + s.req.scene.n_particles)
-                        r.pos = st["pos"][sl].cpu().numpy()
-                        r.vel = st["vel"][sl].cpu().numpy()
-                    self._retire(k)
-                    if on_result is not None:
-                        on_result(r)
+                for s in finishing:
+                    k = tick_index[id(s)]
+                    sl = slice(offs[k], offs[k] + s.req.scene.n_particles)
+                    fin_host[id(s)] = tuple(_download(st[key][sl]) for key in ("pos", "vel"))
+            status_host, status_ev = self.rt.instance_status_enqueue(clear=True)
+            # ---- host work while the tick runs (all GPU work it issues is stream-ordered)
+            for s in finishing:
+                self._retire(tick_index[id(s)])
+            push_arrivals()
+            admit()
+            # ---- wait for the tick
+            status_ev.synchronize()
+            status = status_host.numpy().view(np.uint32)
+            now = clock()
+            for s in tick_slots:
+                if not status[tick_index[id(s)]] & bad and s.remaining:
+                    continue
+                r = results[s.req.rid]
+                r.finished = now
+                if status[tick_index[id(s)]] & bad:
+                    r.error = "NaN detected in MPM states"
+                    if not s.retired:  # evict it from the current layout
+                        self._retire(next(k for k, o in enumerate(self.active) if o is s))
+                elif id(s) in fin_host:
+                    r.pos, r.vel = (t.numpy() for t in fin_host[id(s)])
+                if on_result is not None:
+                    on_result(r)
         self.rt = None
         self.active = []
         return [results[r.rid] for r in reqs]

@@ -294,6 +294,13 @@ int mpm_status_enqueue(const mpm_problem* prob, void* workspace, uint32_t* out, 
  * one instance leaves the others' results untouched and can be handled per instance. */
 int mpm_instance_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
 
+/* Enqueue the copy of the per-instance status words into host memory `out` (pinned, for the
+ * copy to be asynchronous) and, with clear != 0, their reset, on `stream`; returns without
+ * waiting.  `out` is valid once the stream has passed this point.  Used by the serving loop
+ * to read a tick's statuses while it prepares the next tick. */
+int mpm_instance_status_enqueue(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out,
+                                void* stream);
+
 /* Number of particles handled by the out-of-tile path since the last clear (tuning aid). */
 int mpm_fallback_count(const mpm_problem* prob, void* workspace, int32_t clear, uint64_t* out,
                        void* stream);

@@ -63,3 +63,18 @@ def test_budget_limits_concurrency_and_nan_is_isolated():
     # the budget was never exceeded, so some requests had to wait for others to leave
     assert srv.queue.peak_in_use <= srv.queue.budget
     assert max(r.admitted for r in res) > min(r.admitted for r in res)
+
+
+def test_batched_admission_keeps_results():
+    """Admissions held back while enough particles are live (every repack re-lays out all live
+    rollouts): a rollout's result does not depend on when it joined."""
+    reqs = _stream(6, seed=3, spacing=0.0)
+    srv = serve.MPMServer(budget_bytes=80e9, tick_substeps=16, max_active=2, admit_wait=10.0, admit_ratio=1e9,
+                          min_live_particles=1)
+    res = srv.serve(reqs, realtime=False)
+    # with two slots and the hold-back rule, waiting requests join only once nothing is live
+    assert srv.repacks == 3
+    for r, q in zip(res, reqs):
+        assert r.error is None, r.error
+        pos, _ = _alone(q.scene)
+        assert np.abs(r.pos - pos).max() <= 1e-5, r.rid
