@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -42,6 +42,7 @@ MPM_BLOCK = 4
 PFLAG_ACTIVE = 1
 PFLAG_FREE = 2
 PROBF_NONFREE = 1
+PROBF_CPIC = 2
 
 MAT_ELASTIC, MAT_ELASTOPLASTIC, MAT_LIQUID, MAT_SAND, MAT_SNOW = 0, 1, 2, 3, 4
 MATF_NEOHOOKEAN = 1
@@ -123,6 +124,8 @@ class Particles(C.Structure):
         ("lam_p", C.c_void_p),
         ("actu", C.c_void_p),
         ("muscle_dir", C.c_void_p),
+        ("cpic_normal", C.c_void_p),
+        ("cpic_sep", C.c_void_p),
     ]
 
 

@@ -534,6 +534,120 @@ __global__ void k_build_chunks(mpm_problem prob, const mpm_instance* __restrict_
     }
 }
 
+// ---------------------------------------------------------------- rigid colliders
+
+// signed distance sd of the geom at p (utils/sdf_decomp.py:75-300), its world gradient g
+// (unnormalised for the sphere) and q = p - the geom's origin
+__device__ __forceinline__ void sdf_grad(const mpm_collider& c, const float* p, float& sd, float* g, float* q) {
+    q[0] = p[0] - c.pos[0];
+    q[1] = p[1] - c.pos[1];
+    q[2] = p[2] - c.pos[2];
+    if (c.kind == MPM_COLLIDER_SPHERE) {
+        sd = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) - c.data[0];
+        g[0] = q[0];
+        g[1] = q[1];
+        g[2] = q[2];
+    } else {
+        float l[3], gl[3];  // geom-frame point and gradient
+#pragma unroll
+        for (int i = 0; i < 3; ++i) l[i] = c.rot[0 * 3 + i] * q[0] + c.rot[1 * 3 + i] * q[1] + c.rot[2 * 3 + i] * q[2];
+        if (c.kind == MPM_COLLIDER_PLANE) {
+            sd = l[0] * c.data[0] + l[1] * c.data[1] + l[2] * c.data[2];
+            gl[0] = c.data[0];
+            gl[1] = c.data[1];
+            gl[2] = c.data[2];
+        } else {
+            float d[3], o[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                d[i] = fabsf(l[i]) - c.data[i];
+                o[i] = fmaxf(d[i], 0.f);
+            }
+            const float out = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+            const float dm = fmaxf(d[0], fmaxf(d[1], d[2]));
+            sd = out + fminf(dm, 0.f);
+            if (out > 0.f) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) gl[i] = copysignf(o[i], l[i]) / out;
+            } else {
+                const int a = (d[0] >= d[1] && d[0] >= d[2]) ? 0 : (d[1] >= d[2] ? 1 : 2);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) gl[i] = (i == a) ? copysignf(1.f, l[i]) : 0.f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[i] = c.rot[i * 3 + 0] * gl[0] + c.rot[i * 3 + 1] * gl[1] + c.rot[i * 3 + 2] * gl[2];
+    }
+}
+
+// unit outward normal (sdf_func_normal_world); the sphere's gradient is q / sqrt(|q|^2 + eps)
+// before the normalisation, as ti_normalize(q, EPS) gives it
+__device__ __forceinline__ void unit_normal(const mpm_collider& c, float eps, float* g, float* n) {
+    if (c.kind == MPM_COLLIDER_SPHERE) {
+        const float inv = rsqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);
+        g[0] *= inv;
+        g[1] *= inv;
+        g[2] *= inv;
+    }
+    const float ninv = rsqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);
+    n[0] = g[0] * ninv;
+    n[1] = g[1] * ninv;
+    n[2] = g[2] * ninv;
+}
+
+__device__ __forceinline__ void collider_normal(const mpm_collider& c, float eps, const float* p, float* n) {
+    float sd, g[3], q[3];
+    sdf_grad(c, p, sd, g, q);
+    unit_normal(c, eps, g, n);
+}
+
+// legacy_coupler.py:297-341 (_func_collide_in_rigid_geom) for a point at q from the collider
+// origin with outward normal n and influence infl: v relative to the collider's velocity at
+// the point loses its inward normal part (restitution) and is slowed tangentially
+// (friction); the momentum change goes to fout[6] as force and torque about the origin
+__device__ __forceinline__ void rigid_respond(const mpm_collider& c, float eps, float dt, float mass, const float* q,
+                                              const float* n, float infl, float* v, float* fout) {
+    // velocity of the collider at p (rigid_solver_decomp.py:3413-3419)
+    const float vr[3] = {c.lin_vel[0] + c.ang_vel[1] * q[2] - c.ang_vel[2] * q[1],
+                         c.lin_vel[1] + c.ang_vel[2] * q[0] - c.ang_vel[0] * q[2],
+                         c.lin_vel[2] + c.ang_vel[0] * q[1] - c.ang_vel[1] * q[0]};
+    const float rv[3] = {v[0] - vr[0], v[1] - vr[1], v[2] - vr[2]};
+    const float rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    if (!(rn < 0.f)) return;
+    float rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
+    const float rtn = sqrtf(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
+    const float sc = fmaxf(0.f, rtn + rn * c.friction) / rtn;
+    float dv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float rnew = rt[i] * sc - n[i] * rn * c.restitution;
+        const float nvi = vr[i] + rnew * infl + rv[i] * (1.f - infl);
+        dv[i] = nvi - v[i];
+        v[i] = nvi;
+    }
+    if (fout) {
+        const float f[3] = {-mass * dv[0] / dt, -mass * dv[1] / dt, -mass * dv[2] / dt};
+        atomicAdd(&fout[0], f[0]);
+        atomicAdd(&fout[1], f[1]);
+        atomicAdd(&fout[2], f[2]);
+        atomicAdd(&fout[3], q[1] * f[2] - q[2] * f[1]);
+        atomicAdd(&fout[4], q[2] * f[0] - q[0] * f[2]);
+        atomicAdd(&fout[5], q[0] * f[1] - q[1] * f[0]);
+    }
+}
+
+// the grid op's coupling of one node (legacy_coupler.py:166-343): influence
+// min(exp(-sd / softness), 1), acting above 0.1
+__device__ __forceinline__ void collide_rigid(const mpm_collider& c, float eps, float dt, float mass, const float* p,
+                                              float* v, float* fout) {
+    float sd, g[3], q[3], n[3];
+    sdf_grad(c, p, sd, g, q);
+    const float influence = fminf(expf(-sd / fmaxf(1e-10f, c.softness)), 1.f);
+    if (!(influence > 0.1f)) return;
+    unit_normal(c, eps, g, n);
+    rigid_respond(c, eps, dt, mass, q, n, influence, v, fout);
+}
+
 // ---------------------------------------------------------------- p2g
 
 struct P2GArgs {
@@ -542,6 +656,9 @@ struct P2GArgs {
     const mpm_material* mats;
     mpm_particles par;
     Ws w;
+    const mpm_collider* cols;  // CPIC variants only
+    int n_cols;
+    float* cforce;
 };
 
 // Shared tile in int32 fixed point.  On sm_100 shared-memory float atomicAdd is not a
@@ -596,6 +713,7 @@ struct Payload {
     float mass, bq;
     int base[3];
     bool live, in_tile;
+    int slot, gid;  // CPIC variants only (-1: no particle)
 };
 
 // element i of a 3-array without dynamic indexing (keeps it in registers in rolled loops)
@@ -745,6 +863,104 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
     }
 }
 
+// ---------------------------------------------------------------- CPIC
+// mpm_solver.py:357-379, 412-427 and legacy_coupler.py:498-525, against the colliders.
+
+// coupler.preprocess: the particle (API id g, at x) takes each collider's normal at x unless it
+// points against the one it remembers, i.e. unless it has crossed the collider
+__device__ __forceinline__ void cpic_update_normals(const P2GArgs& a, int inst, const mpm_instance& I, int g,
+                                                    const float* x) {
+    const int64_t st = a.par.state_stride;
+    for (int k = 0; k < a.n_cols; ++k) {
+        const mpm_collider& c = a.cols[k];
+        if (c.instance != inst) continue;
+        float n[3];
+        collider_normal(c, I.eps, x, n);
+        float* o = a.par.cpic_normal + (int64_t)(3 * k) * st + g;
+        if (n[0] * o[0] + n[1] * o[st] + n[2] * o[2 * st] >= 0.f) {
+            o[0] = n[0];
+            o[st] = n[1];
+            o[2 * st] = n[2];
+        }
+    }
+}
+
+// 1 + the first collider whose normal at grid node (gx, gy, gz) points against the one
+// particle g remembers (it separates them), or 0
+__device__ __forceinline__ uint32_t cpic_separating(const P2GArgs& a, int inst, const mpm_instance& I, int g, int gx,
+                                                    int gy, int gz) {
+    const float pos[3] = {(float)(gx + I.lower_cell[0]) * I.dx, (float)(gy + I.lower_cell[1]) * I.dx,
+                          (float)(gz + I.lower_cell[2]) * I.dx};
+    const int64_t st = a.par.state_stride;
+    for (int k = 0; k < a.n_cols; ++k) {
+        const mpm_collider& c = a.cols[k];
+        if (c.instance != inst) continue;
+        float n[3];
+        collider_normal(c, I.eps, pos, n);
+        const float* o = a.par.cpic_normal + (int64_t)(3 * k) * st + g;
+        if (n[0] * o[0] + n[1] * o[st] + n[2] * o[2 * st] < 0.f) return (uint32_t)(k + 1);
+    }
+    return 0u;
+}
+
+// the separated nodes' byte codes of one particle (slot p) for the g2p that follows; byte 27
+// flags that there is at least one
+__device__ __forceinline__ void cpic_store(const P2GArgs& a, int p, uint32_t* sw) {
+    const int64_t st = a.par.state_stride;
+    if (sw[0] | sw[1] | sw[2] | sw[3] | sw[4] | sw[5] | sw[6]) sw[6] |= 1u << 24;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) a.par.cpic_sep[q * st + p] = sw[q];
+}
+
+// g2p of the separated nodes: instead of the grid velocity, the particle's own velocity after
+// the rigid response along the normal it remembers (influence 1, mass m w / 1e3; the
+// reaction goes to the collider's force)
+__device__ __forceinline__ void cpic_correct(const P2GArgs& a, const VelTile* VT, const Ws& w, const mpm_instance& I,
+                                             int p, const float* x, const int* base, const float* fx, const float* wx,
+                                             const float* wy, const float* wz, bool tile, int ox, int oy, int oz,
+                                             float* nv, float* nC) {
+    const int64_t st = a.par.state_stride;
+    const uint32_t w6 = a.par.cpic_sep[6 * st + p];
+    if (!(w6 >> 24)) return;
+    uint32_t sw[7];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sw[q] = a.par.cpic_sep[q * st + p];
+    sw[6] = w6;
+    const int g = a.par.gid[p];
+    const float mass = a.mats[I.mat_base + a.par.mat[p]].mass;
+    const float v0[3] = {a.par.state[(MPM_CH_V + 0) * st + p], a.par.state[(MPM_CH_V + 1) * st + p],
+                         a.par.state[(MPM_CH_V + 2) * st + p]};
+#pragma unroll 1
+    for (int nidx = 0; nidx < 27; ++nidx) {
+        const uint32_t sg = (sw[nidx >> 2] >> (8 * (nidx & 3))) & 255u;
+        if (!sg) continue;
+        const int i = nidx / 9, j = (nidx / 3) % 3, k = nidx % 3;
+        const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
+        float4 gvn;
+        if (tile) {
+            gvn = VT->v[vidx(gx - ox, gy - oy, gz - oz)];
+        } else {
+            if (gx < 0 || gy < 0 || gz < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) continue;
+            gvn = w.gv[node_addr(I, gx, gy, gz)];
+        }
+        const mpm_collider& c = a.cols[sg - 1];
+        const float wt = sel3(wx, i) * sel3(wy, j) * sel3(wz, k);
+        float vs[3] = {v0[0], v0[1], v0[2]};
+        const float q[3] = {x[0] - c.pos[0], x[1] - c.pos[1], x[2] - c.pos[2]};
+        const float* on = a.par.cpic_normal + (int64_t)(3 * (sg - 1)) * st + g;
+        const float n[3] = {on[0], on[st], on[2 * st]};
+        rigid_respond(c, I.eps, I.dt, mass * wt / 1e3f, q, n, 1.f, vs, a.cforce ? a.cforce + 6 * (sg - 1) : nullptr);
+        const float dv[3] = {vs[0] - gvn.x, vs[1] - gvn.y, vs[2] - gvn.z};
+        const float off[3] = {(float)i - fx[0], (float)j - fx[1], (float)k - fx[2]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            nv[d] += wt * dv[d];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) nC[d * 3 + e] += I.c_scale * wt * dv[d] * off[e];
+        }
+    }
+}
+
 // Tile node n of the 8^3 tile whose origin is (4b - 1) per axis lies in grid block b + db
 // (db in {-1, 0, 1}) at in-block offset (t + 3) & 3.  These depend only on n, so each
 // thread packs them once for the nodes it owns:
@@ -807,10 +1023,10 @@ __device__ __forceinline__ void tile_zero(Tile& T, int P) {
 // called by every thread of the CTA (contains barriers); T must be zeroed and a barrier
 // passed before.  It ends without a barrier: the flush touches only the tile nodes the
 // thread owns (nd), and the next chunk writes the tile only after two more barriers.
-template <int P>
+template <int P, bool CPIC = false>
 __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const mpm_instance& I, int inst,
                                               const BlockCoord& bc, int ox, int oy, int oz, Ws& w, const Nbhd& h,
-                                              const uint32_t* nd) {
+                                              const uint32_t* nd, const P2GArgs* cp = nullptr) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const float wbq = warp_max(o.in_tile ? o.bq : 0.f);
     const float wbm = warp_max(o.in_tile ? o.mass : 0.f);
@@ -859,6 +1075,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
     // scale = 2^(29 - floor(log2(n * B))): n * B * scale < 2^30
     const float sq = Bq > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bq)))) : 1.f;
     const float sm = Bm > 0.f ? ldexpf(1.f, max(-120, min(120, 29 - ilogbf(nin * Bm)))) : 1.f;
+    uint32_t sw[7] = {0u, 0u, 0u, 0u, 0u, 0u, 0u};  // CPIC: separated nodes
     if (o.live) {
         float wx[3], wy[3], wz[3];
         bspline(o.fx[0], wx);
@@ -883,6 +1100,15 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const float wt = wij * wz[k];
+                        if constexpr (CPIC) {
+                            const uint32_t sg =
+                                cpic_separating(*cp, inst, I, o.gid, o.base[0] + i, o.base[1] + j, o.base[2] + k);
+                            if (sg) {
+                                const int nidx = i * 9 + j * 3 + k;
+                                sw[nidx >> 2] |= sg << (8 * (nidx & 3));
+                                continue;
+                            }
+                        }
                         atomicAdd(&T.t[0][row + k], fix_mul(wt, c0 + As[2] * k));
                         atomicAdd(&T.t[1][row + k], fix_mul(wt, c1 + As[5] * k));
                         atomicAdd(&T.t[2][row + k], fix_mul(wt, c2 + As[8] * k));
@@ -904,6 +1130,14 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
                             set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
                             continue;
                         }
+                        if constexpr (CPIC) {
+                            const uint32_t sg = cpic_separating(*cp, inst, I, o.gid, gx, gy, gz);
+                            if (sg) {
+                                const int nidx = i * 9 + j * 3 + k;
+                                sw[nidx >> 2] |= sg << (8 * (nidx & 3));
+                                continue;
+                            }
+                        }
                         const float wt = sel3(wx, i) * sel3(wy, j) * sel3(wz, k);
                         const float ax = o.q[0] + (o.A[0] * i + o.A[1] * j + o.A[2] * k);
                         const float ay = o.q[1] + (o.A[3] * i + o.A[4] * j + o.A[5] * k);
@@ -912,6 +1146,9 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
                         mark_block(w, inst, I, gx >> 2, gy >> 2, gz >> 2);
                     }
         }
+    }
+    if constexpr (CPIC) {
+        if (o.slot >= 0) cpic_store(*cp, o.slot, sw);
     }
     __syncthreads();
     // flush non-empty tile nodes, one 16-byte reduction each, zeroing the tile behind it
@@ -951,8 +1188,10 @@ __device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const Nb
 // g2p gather (mpm_solver.py:396-431): v = sum w v_i, C = 4 inv_dx sum w v_i (off - fx)^T;
 // then x += dt v and the boundary (mpm_solver.py:434-437).  Returns false if nothing
 // could be gathered (non-finite x).
+template <bool CPIC = false>
 __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm_instance& I, int inst, float* x,
-                                       float* nv, float* nC, int ox, int oy, int oz) {
+                                       float* nv, float* nC, int ox, int oy, int oz, const P2GArgs* cp = nullptr,
+                                       int p = 0) {
     if (!finite3(x[0], x[1], x[2])) {
         set_status(w, inst, MPM_STATUS_NAN);
         return false;
@@ -1042,6 +1281,8 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
                     nC[8] += cw * g.z * d2;
                 }
     }
+    if constexpr (CPIC)
+        cpic_correct(*cp, &VT, w, I, p, x, base, fx, wx, wy, wz, tile_contains(base, ox, oy, oz), ox, oy, oz, nv, nC);
     // a non-finite velocity is flagged separately: the boundary clamp (fminf/fmaxf, like
     // ti.min/ti.max) maps a NaN position back onto the wall, so the reference's
     // position-only check would not see it
@@ -1058,7 +1299,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
 
 // ---------------------------------------------------------------- p2g
 
-template <int P, bool MUSCLE>
+template <int P, bool MUSCLE, bool CPIC>
 __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a) {
     __shared__ Tile T;
     __shared__ Stash<P> SH;
@@ -1079,6 +1320,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
         Payload o;
         o.live = o.in_tile = false;
         o.mass = o.bq = 0.f;
+        o.slot = -1;
         const int p = ch.z + threadIdx.x;
         if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
             float x[3], v[3], C[9];
@@ -1089,15 +1331,20 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
             }
 #pragma unroll
             for (int k = 0; k < 9; ++k) C[k] = __ldg(&S[(MPM_CH_C + k) * st + p]);
+            if constexpr (CPIC) {
+                o.slot = p;
+                o.gid = a.par.gid[p];
+                cpic_update_normals(a, ch.x, I, o.gid, x);
+            }
             particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x, SH);
         }
-        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
+        scatter_flush<P, CPIC>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd, &a);
     }
 }
 
 // ---------------------------------------------------------------- g2p
 
-template <int P>
+template <int P, bool CPIC>
 __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
     __shared__ VelTile VT;
     Ws& w = a.w;
@@ -1120,7 +1367,7 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
             float x[3], nv[3], nC[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
+            if (gather<CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     S[(MPM_CH_X + d) * st + p] = x[d];
@@ -1138,7 +1385,7 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
 
 // g2p of substep n fused with p2g of substep n+1: the new v and C never leave registers
 // (they are recomputed from the grid by the next gather), only x, F and Jp are stored.
-template <int P, bool MUSCLE>
+template <int P, bool MUSCLE, bool CPIC>
 __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs a) {
     __shared__ VelTile VT;
     __shared__ Tile T;
@@ -1162,18 +1409,28 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
         Payload o;
         o.live = o.in_tile = false;
         o.mass = o.bq = 0.f;
+        o.slot = -1;
         const int p = ch.z + threadIdx.x;
         if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
             float x[3], nv[3], nC[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
+            if constexpr (CPIC) o.slot = p;  // a particle with a non-finite x leaves no separated nodes
+            if (gather<CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
+                if constexpr (CPIC) {
+                    // the next g2p's rigid response needs this substep's velocity, and the
+                    // normals follow the particle after its gather (coupler.preprocess)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) S[(MPM_CH_V + d) * st + p] = nv[d];
+                    o.gid = a.par.gid[p];
+                    cpic_update_normals(a, ch.x, I, o.gid, x);
+                }
                 particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x, SH);
             }
         }
-        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
+        scatter_flush<P, CPIC>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd, &a);
     }
 }
 
@@ -1207,85 +1464,6 @@ __global__ void k_nonfree_zero(mpm_problem prob, const mpm_instance* __restrict_
 // ---------------------------------------------------------------- grid op
 
 // Rigid coupling of one grid node against one kinematic collider (legacy_coupler.py:166-343):
-// signed distance and normal of the geom (utils/sdf_decomp.py:75-300), influence
-// min(exp(-sd / softness), 1), and for an approaching node (relative normal velocity < 0)
-// the frictional, restitutive projection of the relative velocity, blended by influence.
-// `mass` is the node mass without the particle-volume scale; the momentum change goes to
-// the collider as -dmv / dt (force) and (p - pos) x force (torque).
-__device__ __forceinline__ void collide_rigid(const mpm_collider& c, float eps, float dt, float mass, const float* p,
-                                              float* v, float* fout) {
-    const float q[3] = {p[0] - c.pos[0], p[1] - c.pos[1], p[2] - c.pos[2]};
-    float sd, g[3];
-    if (c.kind == MPM_COLLIDER_SPHERE) {
-        sd = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) - c.data[0];
-        const float inv = rsqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + eps);  // ti_normalize(., EPS)
-        g[0] = q[0] * inv;
-        g[1] = q[1] * inv;
-        g[2] = q[2] * inv;
-    } else {
-        float l[3], gl[3];  // geom-frame point and gradient
-#pragma unroll
-        for (int i = 0; i < 3; ++i) l[i] = c.rot[0 * 3 + i] * q[0] + c.rot[1 * 3 + i] * q[1] + c.rot[2 * 3 + i] * q[2];
-        if (c.kind == MPM_COLLIDER_PLANE) {
-            sd = l[0] * c.data[0] + l[1] * c.data[1] + l[2] * c.data[2];
-            gl[0] = c.data[0];
-            gl[1] = c.data[1];
-            gl[2] = c.data[2];
-        } else {
-            float d[3], o[3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                d[i] = fabsf(l[i]) - c.data[i];
-                o[i] = fmaxf(d[i], 0.f);
-            }
-            const float out = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
-            const float dm = fmaxf(d[0], fmaxf(d[1], d[2]));
-            sd = out + fminf(dm, 0.f);
-            if (out > 0.f) {
-#pragma unroll
-                for (int i = 0; i < 3; ++i) gl[i] = copysignf(o[i], l[i]) / out;
-            } else {
-                const int a = (d[0] >= d[1] && d[0] >= d[2]) ? 0 : (d[1] >= d[2] ? 1 : 2);
-#pragma unroll
-                for (int i = 0; i < 3; ++i) gl[i] = (i == a) ? copysignf(1.f, l[i]) : 0.f;
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) g[i] = c.rot[i * 3 + 0] * gl[0] + c.rot[i * 3 + 1] * gl[1] + c.rot[i * 3 + 2] * gl[2];
-    }
-    const float influence = fminf(expf(-sd / fmaxf(1e-10f, c.softness)), 1.f);
-    if (!(influence > 0.1f)) return;
-    const float ninv = rsqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);  // sdf_func_normal_world
-    const float n[3] = {g[0] * ninv, g[1] * ninv, g[2] * ninv};
-    // velocity of the collider at p (rigid_solver_decomp.py:3413-3419)
-    const float vr[3] = {c.lin_vel[0] + c.ang_vel[1] * q[2] - c.ang_vel[2] * q[1],
-                         c.lin_vel[1] + c.ang_vel[2] * q[0] - c.ang_vel[0] * q[2],
-                         c.lin_vel[2] + c.ang_vel[0] * q[1] - c.ang_vel[1] * q[0]};
-    const float rv[3] = {v[0] - vr[0], v[1] - vr[1], v[2] - vr[2]};
-    const float rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
-    if (!(rn < 0.f)) return;
-    float rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
-    const float rtn = sqrtf(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
-    const float sc = fmaxf(0.f, rtn + rn * c.friction) / rtn;
-    float dv[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const float rnew = rt[i] * sc - n[i] * rn * c.restitution;
-        const float nvi = vr[i] + rnew * influence + rv[i] * (1.f - influence);
-        dv[i] = nvi - v[i];
-        v[i] = nvi;
-    }
-    if (fout) {
-        const float f[3] = {-mass * dv[0] / dt, -mass * dv[1] / dt, -mass * dv[2] / dt};
-        atomicAdd(&fout[0], f[0]);
-        atomicAdd(&fout[1], f[1]);
-        atomicAdd(&fout[2], f[2]);
-        atomicAdd(&fout[3], q[1] * f[2] - q[2] * f[1]);
-        atomicAdd(&fout[4], q[2] * f[0] - q[0] * f[2]);
-        atomicAdd(&fout[5], q[0] * f[1] - q[1] * f[0]);
-    }
-}
-
 // constant-velocity kinematic motion of the colliders over one substep of their instance:
 // pos += lin_vel dt, rot = exp([ang_vel] dt) rot (Rodrigues)
 __global__ void k_advance_colliders(const mpm_instance* __restrict__ inst, int n_inst, mpm_collider* cs, int n) {
@@ -1481,15 +1659,15 @@ static const DevInfo* dev_info() {
     if (d.sms == 0) {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        d.occ_p2g[0] = occ_of<128>(k_p2g<128, false>);
-        d.occ_p2g[1] = occ_of<256>(k_p2g<256, false>);
-        d.occ_p2g[2] = occ_of<512>(k_p2g<512, false>);
-        d.occ_g2p[0] = occ_of<128>(k_g2p<128>);
-        d.occ_g2p[1] = occ_of<256>(k_g2p<256>);
-        d.occ_g2p[2] = occ_of<512>(k_g2p<512>);
-        d.occ_g2p2g[0] = occ_of<128>(k_g2p2g<128, false>);
-        d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256, false>);
-        d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512, false>);
+        d.occ_p2g[0] = occ_of<128>(k_p2g<128, false, false>);
+        d.occ_p2g[1] = occ_of<256>(k_p2g<256, false, false>);
+        d.occ_p2g[2] = occ_of<512>(k_p2g<512, false, false>);
+        d.occ_g2p[0] = occ_of<128>(k_g2p<128, false>);
+        d.occ_g2p[1] = occ_of<256>(k_g2p<256, false>);
+        d.occ_g2p[2] = occ_of<512>(k_g2p<512, false>);
+        d.occ_g2p2g[0] = occ_of<128>(k_g2p2g<128, false, false>);
+        d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256, false, false>);
+        d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512, false, false>);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op, 256, 0);
         d.occ_grid = n > 0 ? n : 1;
@@ -1565,32 +1743,52 @@ static int persistent_ctas(const mpm_problem* prob, int occ) {
     return ctas;
 }
 
+// launch helpers: one kernel per chunk size, muscle term and CPIC
+template <int P>
+static void run_p2g(bool m, bool cp, int ctas, cudaStream_t s, const P2GArgs& a) {
+    if (m)
+        cp ? k_p2g<P, true, true><<<ctas, P, 0, s>>>(a) : k_p2g<P, true, false><<<ctas, P, 0, s>>>(a);
+    else
+        cp ? k_p2g<P, false, true><<<ctas, P, 0, s>>>(a) : k_p2g<P, false, false><<<ctas, P, 0, s>>>(a);
+}
+template <int P>
+static void run_g2p2g(bool m, bool cp, int ctas, cudaStream_t s, const P2GArgs& a) {
+    if (m)
+        cp ? k_g2p2g<P, true, true><<<ctas, P, 0, s>>>(a) : k_g2p2g<P, true, false><<<ctas, P, 0, s>>>(a);
+    else
+        cp ? k_g2p2g<P, false, true><<<ctas, P, 0, s>>>(a) : k_g2p2g<P, false, false><<<ctas, P, 0, s>>>(a);
+}
+template <int P>
+static void run_g2p(bool cp, int ctas, cudaStream_t s, const P2GArgs& a) {
+    cp ? k_g2p<P, true><<<ctas, P, 0, s>>>(a) : k_g2p<P, false><<<ctas, P, 0, s>>>(a);
+}
+
+// the kernels' arguments; CPIC runs when the problem asks for it and the instance has
+// colliders (MPM_E_INVALID if its buffers are missing or there are more than 254 colliders,
+// the limit of its one-byte node codes)
+static int p2g_args(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* par, void* ws, P2GArgs& a,
+                    bool& cpic) {
+    const int nc = tab->colliders ? tab->n_colliders : 0;
+    cpic = (prob->flags & MPM_PROBF_CPIC) && nc > 0;
+    if (cpic && (!par->cpic_normal || !par->cpic_sep || nc > 254)) return MPM_E_INVALID;
+    a = P2GArgs{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws), tab->colliders, nc, tab->collider_force};
+    return MPM_OK;
+}
+
 static int launch_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, cudaStream_t s) {
     const DevInfo* d = dev_info();
     if (!d) return MPM_E_CUDA;
-    P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
+    P2GArgs a;
+    bool cpic;
+    int rc = p2g_args(prob, tab, par, ws, a, cpic);
+    if (rc) return rc;
     const int pi = p_index(prob->chunk_particles);
     const int ctas = persistent_ctas(prob, d->occ_p2g[pi]);
     const bool muscle = par->actu != nullptr;
     switch (prob->chunk_particles) {
-        case 128:
-            if (muscle)
-                k_p2g<128, true><<<ctas, 128, 0, s>>>(a);
-            else
-                k_p2g<128, false><<<ctas, 128, 0, s>>>(a);
-            break;
-        case 256:
-            if (muscle)
-                k_p2g<256, true><<<ctas, 256, 0, s>>>(a);
-            else
-                k_p2g<256, false><<<ctas, 256, 0, s>>>(a);
-            break;
-        case 512:
-            if (muscle)
-                k_p2g<512, true><<<ctas, 512, 0, s>>>(a);
-            else
-                k_p2g<512, false><<<ctas, 512, 0, s>>>(a);
-            break;
+        case 128: run_p2g<128>(muscle, cpic, ctas, s, a); break;
+        case 256: run_p2g<256>(muscle, cpic, ctas, s, a); break;
+        case 512: run_p2g<512>(muscle, cpic, ctas, s, a); break;
     }
     if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
         k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);
@@ -1614,13 +1812,16 @@ static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* 
 static int launch_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, cudaStream_t s) {
     const DevInfo* d = dev_info();
     if (!d) return MPM_E_CUDA;
-    P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
+    P2GArgs a;
+    bool cpic;
+    int rc = p2g_args(prob, tab, par, ws, a, cpic);
+    if (rc) return rc;
     const int pi = p_index(prob->chunk_particles);
     const int ctas = persistent_ctas(prob, d->occ_g2p[pi]);
     switch (prob->chunk_particles) {
-        case 128: k_g2p<128><<<ctas, 128, 0, s>>>(a); break;
-        case 256: k_g2p<256><<<ctas, 256, 0, s>>>(a); break;
-        case 512: k_g2p<512><<<ctas, 512, 0, s>>>(a); break;
+        case 128: run_g2p<128>(cpic, ctas, s, a); break;
+        case 256: run_g2p<256>(cpic, ctas, s, a); break;
+        case 512: run_g2p<512>(cpic, ctas, s, a); break;
     }
     return cuda_ok();
 }
@@ -1629,29 +1830,17 @@ static int launch_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_part
                         cudaStream_t s) {
     const DevInfo* d = dev_info();
     if (!d) return MPM_E_CUDA;
-    P2GArgs a{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws)};
+    P2GArgs a;
+    bool cpic;
+    int rc = p2g_args(prob, tab, par, ws, a, cpic);
+    if (rc) return rc;
     const int pi = p_index(prob->chunk_particles);
     const int ctas = persistent_ctas(prob, d->occ_g2p2g[pi]);
     const bool muscle = par->actu != nullptr;
     switch (prob->chunk_particles) {
-        case 128:
-            if (muscle)
-                k_g2p2g<128, true><<<ctas, 128, 0, s>>>(a);
-            else
-                k_g2p2g<128, false><<<ctas, 128, 0, s>>>(a);
-            break;
-        case 256:
-            if (muscle)
-                k_g2p2g<256, true><<<ctas, 256, 0, s>>>(a);
-            else
-                k_g2p2g<256, false><<<ctas, 256, 0, s>>>(a);
-            break;
-        case 512:
-            if (muscle)
-                k_g2p2g<512, true><<<ctas, 512, 0, s>>>(a);
-            else
-                k_g2p2g<512, false><<<ctas, 512, 0, s>>>(a);
-            break;
+        case 128: run_g2p2g<128>(muscle, cpic, ctas, s, a); break;
+        case 256: run_g2p2g<256>(muscle, cpic, ctas, s, a); break;
+        case 512: run_g2p2g<512>(muscle, cpic, ctas, s, a); break;
     }
     if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
         k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);

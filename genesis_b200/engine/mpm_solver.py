@@ -133,6 +133,7 @@ class MPMSolver:
             grid_ctas=b.grid_ctas,
             use_graphs=b.use_cuda_graph,
             colliders=colliders,
+            cpic=self._enable_CPIC,  # active only with rigid colliders, as in the reference
         )
         for i, r in enumerate(rigid):
             r._bind(self.runtime, [i * self._B + env for env in range(self._B)])

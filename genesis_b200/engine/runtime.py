@@ -91,6 +91,7 @@ class MPMRuntime:
         grid_ctas: int = 0,
         use_graphs: bool = True,
         colliders: list | None = None,
+        cpic: bool = False,
     ):
         if not torch.cuda.is_available():
             raise RuntimeError("genesis_b200 needs a CUDA device (sm_100a); there is no CPU path")
@@ -191,6 +192,13 @@ class MPMRuntime:
             self.muscle_dir = torch.zeros((nn, 3), dtype=torch.float32, device=dev)
             self.muscle_dir[:, 2] = 1.0
             self.muscle_group = torch.zeros(nn, dtype=torch.int64, device=dev)
+        # CPIC (with colliders only): the collider-side normal each particle remembers, per
+        # collider in API order, and the separated stencil nodes of the last p2g, per slot
+        self.cpic_normal = self.cpic_sep = None
+        if cpic and colliders:
+            self.cpic_normal = torch.zeros((3 * len(colliders), self.stride), dtype=torch.float32, device=dev)
+            self.cpic_sep = torch.zeros((7, self.stride), dtype=torch.int32, device=dev)
+            self.prob.flags |= nat.PROBF_CPIC
         self.par = nat.Particles(
             state=self.state.data_ptr(),
             state_stride=self.stride,
@@ -202,6 +210,8 @@ class MPMRuntime:
             lam_p=self.lam_p.data_ptr() if self.lam_p is not None else None,
             actu=self.actu.data_ptr() if self.actu is not None else None,
             muscle_dir=self.muscle_dir.data_ptr() if self.muscle_dir is not None else None,
+            cpic_normal=self.cpic_normal.data_ptr() if self.cpic_normal is not None else None,
+            cpic_sep=self.cpic_sep.data_ptr() if self.cpic_sep is not None else None,
         )
         nbytes = C.c_uint64()
         nat.check("mpm_workspace_bytes", self.lib.mpm_workspace_bytes(C.byref(self.prob), C.byref(nbytes)))
@@ -271,9 +281,19 @@ class MPMRuntime:
         self.lam_p[sl] = lam
 
     def reset_colliders(self):
-        """Back to the poses and velocities the colliders were built with."""
+        """Back to the poses and velocities the colliders were built with; the particles
+        forget their CPIC sides (legacy_coupler.py:120-123)."""
         if self.coll_table is not None:
             self.coll_table.copy_(self.coll_init)
+        if self.cpic_normal is not None:
+            self.cpic_normal.zero_()
+            self.cpic_sep.zero_()
+
+    def get_cpic_normals(self) -> torch.Tensor:
+        """The remembered collider-side normals, [n_colliders, n, 3] in API order."""
+        if self.cpic_normal is None:
+            raise RuntimeError("runtime has no CPIC state")
+        return self.cpic_normal[:, : self.n].reshape(-1, 3, self.n).permute(0, 2, 1)
 
     def collider_table(self) -> torch.Tensor:
         """The collider rows as float32 [n_colliders, 24] (pos 0:3, rot 3:12, data 12:15,

@@ -89,8 +89,6 @@ class MPMOptions(Options):
             raise GenesisException("Invalid pair of upper_bound and lower_bound.")
         if self.particle_size is None:
             self.particle_size = 0.01 * 64.0 / self.grid_density
-        if self.enable_CPIC:
-            raise GenesisException("CPIC needs the rigid solver, which is not part of this MPM-only build.")
 
 
 class B200Options(Options):

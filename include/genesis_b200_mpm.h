@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 4
+#define MPM_ABI_VERSION 5
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -86,6 +86,7 @@ extern "C" {
 
 /* problem flags */
 #define MPM_PROBF_NONFREE 1      /* some particles are non-free: run the stencil-zeroing pass after p2g */
+#define MPM_PROBF_CPIC 2         /* CPIC against the colliders (mpm_particles.cpic_normal/cpic_sep required) */
 
 /* One simulated scene (one environment).  Mirrors the derived constants of
  * MPMSolver.__init__ (mpm_solver.py:31-78) and Simulator (simulator.py:110). */
@@ -145,6 +146,15 @@ typedef struct mpm_particles {
     float* lam_p;  /* optional */
     const float* actu;        /* optional, float[n] in API order: actuation (mpm_solver.py:91, 922-934) */
     const float* muscle_dir;  /* optional, float[n][3] in API order: fibre direction (mpm_solver.py:108) */
+    /* CPIC (MPM_PROBF_CPIC; mpm_solver.py:357-379, 412-427, legacy_coupler.py:498-525),
+     * both zero-initialised by the caller:
+     *   cpic_normal  float[n_colliders * 3][state_stride], indexed by API particle id: the
+     *                collider-side normal each particle remembers (mpm_rigid_normal);
+     *   cpic_sep     uint32[7][state_stride], indexed by slot: byte j < 27 of a particle's
+     *                7 words is 1 + the collider separating it from stencil node j in the last
+     *                p2g (0: none), byte 27 is nonzero if any is. */
+    float* cpic_normal;
+    uint32_t* cpic_sep;
 } mpm_particles;
 
 /* Kinematic rigid collider coupled in the grid op (legacy_coupler.py:131-343, 385-397):

@@ -72,6 +72,7 @@ def lib(dtype):
         L.ref_substeps_lame.restype = C.c_int
         L.ref_substeps_ext.restype = C.c_int
         L.ref_substeps_full.restype = C.c_int
+        L.ref_substeps_cpic.restype = C.c_int
         L.ref_max_threads.restype = C.c_int
         _libs[key] = L
     return _libs[key]
@@ -143,9 +144,12 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
         mu_a = np.ascontiguousarray(mu_p, dtype=dt) if mu_p is not None else None
         lam_a = np.ascontiguousarray(lam_p, dtype=dt) if lam_p is not None else None
         opt = lambda a: ptr(a) if a is not None else None
-        rc = L.ref_substeps_full(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
+        # CPIC: st["cpic_normal"] [n_colliders, n, 3] (zeros at the start) switches it on
+        rn = st.get("cpic_normal")
+        rn = np.ascontiguousarray(rn, dtype=dt).copy() if rn is not None else None
+        rc = L.ref_substeps_cpic(C.byref(P), marr, n, ptr(x), ptr(v), ptr(Cm), ptr(F), ptr(Jp), ptr(mat), ptr(act),
                                  int(n_substeps), ptr(grid), ptr(gvel), int(n_threads), opt(mu_a), opt(lam_a),
-                                 opt(actu), opt(mdir), carr, len(cs), ptr(forces))
+                                 opt(actu), opt(mdir), carr, len(cs), ptr(forces), opt(rn))
         moved = []
         for i, c in enumerate(cs):
             moved.append(R.Collider(c.kind, np.array(carr[i].pos[:]), np.array(carr[i].rot[:]).reshape(3, 3),
@@ -153,6 +157,8 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
                                     c.softness, c.restitution))
         out = dict(st)
         out.update(x=x, v=v, C=Cm.reshape(n, 3, 3), F=F.reshape(n, 3, 3), Jp=Jp, colliders=moved, forces=forces)
+        if rn is not None:
+            out["cpic_normal"] = rn
         return out, int(rc)
     if st.get("actu") is not None:
         actu = np.ascontiguousarray(st["actu"], dtype=dt)

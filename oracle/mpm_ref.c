@@ -309,6 +309,10 @@ int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL
                       REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
                       int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir,
                       ref_collider* colliders, int n_colliders, REAL* forces);
+int ref_substeps_cpic(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                      int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir,
+                      ref_collider* colliders, int n_colliders, REAL* forces, REAL* rnormal);
 
 int ref_substeps(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F, REAL* Jp,
                  const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel, int n_threads) {
@@ -332,11 +336,11 @@ int ref_substeps_ext(const ref_params* p, const ref_material* mats, int n, REAL*
                              actu, mdir, NULL, 0, NULL);
 }
 
-/* legacy_coupler.py:166-343 for one node against one collider; adds the reaction force
- * and torque (about c->pos) to f[6] */
-static void collide_rigid(const ref_collider* c, REAL eps, REAL dt, REAL mass, const REAL* pos, REAL* v, REAL* f) {
-    REAL q[3] = {pos[0] - c->pos[0], pos[1] - c->pos[1], pos[2] - c->pos[2]};
-    REAL sd, g[3];
+/* signed distance sd and (unnormalised) world gradient g of the collider at pos, q = pos -
+ * collider centre (utils/sdf_decomp.py: the analytic sphere/plane/box SDFs) */
+static void sdf_grad(const ref_collider* c, REAL eps, const REAL* pos, REAL* sd_out, REAL* g, REAL* q) {
+    REAL sd;
+    for (int i = 0; i < 3; ++i) q[i] = pos[i] - c->pos[i];
     if (c->kind == 0) {
         sd = R_SQRT(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) - c->data[0];
         REAL nn = R_SQRT(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + eps);
@@ -365,11 +369,22 @@ static void collide_rigid(const ref_collider* c, REAL eps, REAL dt, REAL mass, c
         }
         for (int i = 0; i < 3; ++i) g[i] = c->rot[i * 3 + 0] * gl[0] + c->rot[i * 3 + 1] * gl[1] + c->rot[i * 3 + 2] * gl[2];
     }
-    REAL soft = c->softness > (REAL)1e-10 ? c->softness : (REAL)1e-10;
-    REAL infl = RMIN(REXP(-sd / soft), (REAL)1);
-    if (!(infl > (REAL)0.1)) return;
+    *sd_out = sd;
+}
+
+/* sdf_func_normal_world: the unit outward normal of the collider at pos */
+static void sdf_normal(const ref_collider* c, REAL eps, const REAL* pos, REAL* n) {
+    REAL sd, g[3], q[3];
+    sdf_grad(c, eps, pos, &sd, g, q);
     REAL gn = R_SQRT(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);
-    REAL n[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
+    for (int i = 0; i < 3; ++i) n[i] = g[i] / gn;
+}
+
+/* the collision response of legacy_coupler.py:297-341 (_func_collide_in_rigid_geom) for a
+ * point at q from the collider centre with outward normal n and influence infl; adds the
+ * reaction force and torque (about the centre) to f[6] */
+static void rigid_respond(const ref_collider* c, REAL eps, REAL dt, REAL mass, const REAL* q, const REAL* n, REAL infl,
+                          REAL* v, REAL* f) {
     const REAL* w = c->ang_vel;
     REAL vr[3] = {c->lin_vel[0] + w[1] * q[2] - w[2] * q[1], c->lin_vel[1] + w[2] * q[0] - w[0] * q[2],
                   c->lin_vel[2] + w[0] * q[1] - w[1] * q[0]};
@@ -399,6 +414,19 @@ static void collide_rigid(const ref_collider* c, REAL eps, REAL dt, REAL mass, c
     }
 }
 
+/* legacy_coupler.py:166-343 for one node against one collider (the grid op's coupling):
+ * influence min(exp(-sd / softness), 1), acting above 0.1 */
+static void collide_rigid(const ref_collider* c, REAL eps, REAL dt, REAL mass, const REAL* pos, REAL* v, REAL* f) {
+    REAL sd, g[3], q[3];
+    sdf_grad(c, eps, pos, &sd, g, q);
+    REAL soft = c->softness > (REAL)1e-10 ? c->softness : (REAL)1e-10;
+    REAL infl = RMIN(REXP(-sd / soft), (REAL)1);
+    if (!(infl > (REAL)0.1)) return;
+    REAL gn = R_SQRT(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + eps);
+    REAL n[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
+    rigid_respond(c, eps, dt, mass, q, n, infl, v, f);
+}
+
 /* constant-velocity kinematic motion over one substep */
 static void advance_collider(ref_collider* c, REAL dt) {
     for (int d = 0; d < 3; ++d) c->pos[d] += c->lin_vel[d] * dt;
@@ -423,6 +451,31 @@ int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL
                       REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
                       int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir,
                       ref_collider* colliders, int n_colliders, REAL* forces) {
+    return ref_substeps_cpic(p, mats, n, x, v, C, F, Jp, mat, active, n_substeps, grid, gvel, n_threads, mu_p, lam_p,
+                             actu, mdir, colliders, n_colliders, forces, NULL);
+}
+
+/* as ref_substeps_full, with CPIC (mpm_solver.py:357-379, 412-427; legacy_coupler.py:498-525)
+ * when rnormal ([n_colliders][n][3], the particles' remembered collider-side normals, zero
+ * at the start) is given: at the start of each substep every active particle takes the
+ * collider's normal at its position unless that points against the one it remembers (it has
+ * crossed the collider); p2g skips the stencil nodes whose normal points against the
+ * particle's for some collider (the first such collider separates them), and g2p takes for
+ * those nodes, instead of the grid velocity, the particle's own velocity after the rigid
+ * response along its remembered normal (influence 1; the reaction goes to forces).  The
+ * normals and p2g see the colliders' poses at the start of the substep, g2p the advanced
+ * ones. */
+int ref_substeps_cpic(const ref_params* p, const ref_material* mats, int n, REAL* x, REAL* v, REAL* C, REAL* F,
+                      REAL* Jp, const int32_t* mat, const uint8_t* active, int n_substeps, REAL* grid, REAL* gvel,
+                      int n_threads, const REAL* mu_p, const REAL* lam_p, const REAL* actu, const REAL* mdir,
+                      ref_collider* colliders, int n_colliders, REAL* forces, REAL* rnormal) {
+    signed char* sep = NULL;
+    if (rnormal && n_colliders > 0) {
+        sep = (signed char*)malloc((size_t)n * 27);
+        if (!sep) return 4;
+    } else {
+        rnormal = NULL;
+    }
 #ifdef _OPENMP
     if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
@@ -432,6 +485,23 @@ int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL
 #pragma omp parallel for schedule(static)
         for (int64_t g = 0; g < G; ++g) {
             grid[4 * g + 0] = grid[4 * g + 1] = grid[4 * g + 2] = grid[4 * g + 3] = 0;
+        }
+        if (rnormal) {
+            /* coupler.preprocess -> mpm_surface_to_particle (legacy_coupler.py:498-525) */
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; ++i) {
+                if (!active[i]) continue;
+                for (int k = 0; k < n_colliders; ++k) {
+                    REAL nn[3];
+                    REAL* o = rnormal + 3 * ((int64_t)k * n + i);
+                    sdf_normal(&colliders[k], p->eps, x + 3 * i, nn);
+                    if (nn[0] * o[0] + nn[1] * o[1] + nn[2] * o[2] >= 0) {
+                        o[0] = nn[0];
+                        o[1] = nn[1];
+                        o[2] = nn[2];
+                    }
+                }
+            }
         }
         /* p2g (mpm_solver.py:290-389) */
 #pragma omp parallel for schedule(static) reduction(| : status)
@@ -488,6 +558,21 @@ int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL
                         if (gi < 0 || gj < 0 || gk < 0 || gi >= p->res[0] || gj >= p->res[1] || gk >= p->res[2]) {
                             status |= 1;
                             continue;
+                        }
+                        if (sep) {
+                            /* mpm_solver.py:357-379: is the node on the other side of a collider? */
+                            const REAL cp[3] = {(REAL)(gi + p->lower_cell[0]) * p->dx,
+                                                (REAL)(gj + p->lower_cell[1]) * p->dx,
+                                                (REAL)(gk + p->lower_cell[2]) * p->dx};
+                            int sg = -1;
+                            for (int k = 0; k < n_colliders && sg < 0; ++k) {
+                                REAL nc[3];
+                                const REAL* np_ = rnormal + 3 * ((int64_t)k * n + i);
+                                sdf_normal(&colliders[k], p->eps, cp, nc);
+                                if (np_[0] * nc[0] + np_[1] * nc[1] + np_[2] * nc[2] < 0) sg = k;
+                            }
+                            sep[(int64_t)i * 27 + a * 9 + b * 3 + c] = (signed char)sg;
+                            if (sg >= 0) continue;
                         }
                         REAL wt = w[a][0] * w[b][1] * w[c][2];
                         REAL dp[3] = {(a - fx[0]) * p->dx, (b - fx[1]) * p->dx, (c - fx[2]) * p->dx};
@@ -552,6 +637,21 @@ int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL
                         }
                         REAL wt = w[a][0] * w[b][1] * w[c][2];
                         const REAL* gv = gvel + 3 * gidx(p, gi, gj, gk);
+                        REAL vs[3];
+                        const int sg = sep ? sep[(int64_t)i * 27 + a * 9 + b * 3 + c] : -1;
+                        if (sg >= 0) {
+                            /* mpm_solver.py:412-427: the particle's own velocity after the rigid
+                             * response along its remembered normal, mass m w / 1e3 */
+                            const ref_collider* cs = &colliders[sg];
+                            REAL q[3];
+                            for (int d = 0; d < 3; ++d) {
+                                q[d] = x[3 * i + d] - cs->pos[d];
+                                vs[d] = v[3 * i + d];
+                            }
+                            rigid_respond(cs, p->eps, p->dt, mats[mat[i]].mass * wt / (REAL)1e3, q,
+                                          rnormal + 3 * ((int64_t)sg * n + i), 1, vs, forces ? forces + 6 * sg : NULL);
+                            gv = vs;
+                        }
                         REAL dp[3] = {a - fx[0], b - fx[1], c - fx[2]};
                         for (int d = 0; d < 3; ++d) {
                             nv[d] += wt * gv[d];
@@ -569,6 +669,7 @@ int ref_substeps_full(const ref_params* p, const ref_material* mats, int n, REAL
             memcpy(C + 9 * i, nC, 9 * sizeof(REAL));
         }
     }
+    free(sep);
     return status;
 }
 

@@ -283,3 +283,40 @@ def test_kinematic_collider_motion():
     c2 = R.advance_colliders(p, [c])[0]
     assert np.allclose(c2.pos, [0.5, 0.5, 0.4 + 0.5e-4])
     assert np.allclose(c2.rot @ c2.rot.T, np.eye(3)) and np.isclose(np.arctan2(c2.rot[1, 0], c2.rot[0, 0]), 3e-4)
+
+
+def _block_cpic(collider, cpic, n_side=10, z0=0.33, v0=(0.0, 0.0, -2.0), substeps=400, n_threads=0):
+    rng = np.random.default_rng(12)
+    x = W.jittered_lattice(rng, n_side, (0.45, 0.45, z0), 0.1 / n_side)
+    n = x.shape[0]
+    p = R.Params(grid_density=64, dt=1e-4, dtype=np.float64)
+    mats = [R.make_material("elastic", E=2e4)]
+    st = R.make_state(x, mats, np.zeros(n, np.int64), np.float64, v=np.tile(v0, (n, 1)))
+    st["colliders"] = [collider]
+    if cpic:
+        st["cpic_normal"] = np.zeros((1, n, 3))
+    out, rc = cref.substeps(p, mats, st, substeps, n_threads=n_threads)
+    assert rc == 0
+    return out
+
+
+def test_cpic_thin_slab_separates_its_sides():
+    """mpm_solver.py:357-379, 412-427: a fixed slab far thinner than a grid cell (0.002 m
+    against dx = 0.0156 m).  The grid-op coupling alone reaches only the nodes within its
+    influence band, so a falling block passes through; with CPIC the nodes under the slab are
+    cut off from the particles above it, which stay on their side."""
+    slab = R.Collider("box", np.array([0.5, 0.5, 0.3]), np.eye(3), np.array([0.3, 0.3, 0.001]))
+    leak = _block_cpic(slab, cpic=False)
+    assert leak["x"][:, 2].min() < 0.28
+    kept = _block_cpic(slab, cpic=True)
+    assert kept["x"][:, 2].min() > 0.3 - 1.5 / 64
+    assert (kept["cpic_normal"][0][:, 2] > 0.99).all()  # every particle remembers the upper side
+    assert kept["forces"][0][2] < 0  # the block pushes the slab down
+
+
+def test_cpic_without_crossing_is_the_plain_coupling():
+    """Far from any collider nothing is separated: CPIC changes nothing."""
+    far = R.Collider("sphere", np.array([0.5, 0.5, 0.1]), np.eye(3), np.array([0.03, 0, 0]))
+    a = _block_cpic(far, cpic=False, substeps=100, n_threads=1)  # one thread: a fixed summation order
+    b = _block_cpic(far, cpic=True, substeps=100, n_threads=1)
+    assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["v"], b["v"])
