@@ -76,3 +76,24 @@ def test_cpic_keeps_the_block_on_its_side():
     for _ in range(30):
         leak.step()
     assert float(lblock.get_particles_pos()[:, 2].min()) < 0.28  # without CPIC it passes through
+
+
+def test_cpic_per_environment():
+    """Each environment's particles see only their own slab (collider.instance): with two
+    environments both keep the block on top, identically."""
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=1e-3, substeps=10, gravity=(0, 0, -9.8)),
+        mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
+                                          particle_size=0.01, enable_CPIC=True),
+    )
+    block = scene.add_entity(gs.morphs.Box(lower=(0.45, 0.45, 0.31), upper=(0.55, 0.55, 0.41)),
+                             material=gs.materials.MPM.Elastic(E=2e4))
+    scene.add_entity(gs.morphs.Box(**SLAB), material=gs.materials.Rigid())
+    scene.build(n_envs=2)
+    block.set_particles_vel(torch.tensor([0.0, 0.0, -2.0]).expand(2, block.n_particles, 3))
+    for _ in range(20):
+        scene.step()
+    z = block.get_particles_pos()[..., 2]
+    assert z.shape[0] == 2 and float(z.min()) > 0.3 - 1.5 / 64
+    assert torch.allclose(z[0], z[1], atol=1e-6)
