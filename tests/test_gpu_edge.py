@@ -101,3 +101,39 @@ def test_513_cubed_grid_free_fall_is_exact():
     assert np.abs(x[:, :2] - pos[:, :2]).max() < 2e-6
     assert np.abs((pos[:, 2] - x[:, 2]) - drop).max() < 2e-6, drop
     assert rt.status() == 0
+
+
+def _empty_like(desc):
+    import dataclasses
+
+    return dataclasses.replace(desc, pos=np.zeros((0, 3)), vel=np.zeros((0, 3)), mat_idx=np.zeros(0, dtype=np.int64),
+                               name="empty")
+
+
+def test_empty_scene_in_a_batch_and_alone():
+    """A scene without particles: alone it steps as a no-op (status clean), and between two
+    others in one batch it changes nothing of theirs (ragged instance table with a zero
+    particle range)."""
+    from genesis_b200 import workloads as W
+    from genesis_b200.engine.runtime import runtime_from_descs
+
+    a = W.elastic_cube(n_side=12, n_substeps=20)
+    b = W.mixed_500k(n_side=10, n_substeps=20)
+    empty = _empty_like(a)
+    rt0 = runtime_from_descs([empty])
+    rt0.substeps(5)
+    torch.cuda.synchronize()
+    assert rt0.status() == 0 and rt0.n == 0
+    alone = []
+    for d in (a, b):
+        rt = runtime_from_descs([d])
+        rt.substeps(20)
+        alone.append(rt.get_state(("pos",))["pos"].cpu().numpy())
+    rt = runtime_from_descs([a, empty, b])
+    rt.substeps(20)
+    pos = rt.get_state(("pos",))["pos"].cpu().numpy()
+    offs = rt.instance_offsets
+    assert offs[1] == offs[2] == a.n_particles
+    assert np.abs(pos[: a.n_particles] - alone[0]).max() <= 1e-5  # float atomics: summation order
+    assert np.abs(pos[a.n_particles:] - alone[1]).max() <= 1e-5
+    assert (rt.instance_status() == 0).all()
