@@ -231,16 +231,23 @@ int mpm_sort_particles(const mpm_problem* prob, const mpm_tables* tab, mpm_parti
 
 /* compute_F_tmp + svd + material return mapping + stress + p2g scatter
  * (mpm_solver.py:261-389).  Writes F and Jp of the next frame in place and leaves
- * grid mass/momentum in the workspace. */
+ * grid mass/momentum in the workspace.  With MPM_PROBF_CPIC and colliders it first does
+ * coupler.preprocess (legacy_coupler.py:498-525: par->cpic_normal) and leaves out, per
+ * stencil node, the particles a collider separates from it (mpm_solver.py:357-379,
+ * recorded in par->cpic_sep for the g2p that follows). */
 int mpm_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
             void* stream);
 
 /* Grid update of LegacyCoupler.mpm_grid_op, MPM core (legacy_coupler.py:364-375, 495-496):
- * momentum -> velocity, gravity, CubeBoundary.  Clears mass/momentum after reading. */
+ * momentum -> velocity, gravity, the coupling with tab->colliders (legacy_coupler.py:385-397,
+ * reaction into tab->collider_force), CubeBoundary; then the colliders advance by one
+ * substep.  Clears mass/momentum after reading. */
 int mpm_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* workspace, void* stream);
 
 /* g2p (mpm_solver.py:391-449) with the NaN check of _is_state_valid folded into a
- * device status bit.  Updates x, v, C in place. */
+ * device status bit.  Updates x, v, C in place.  With MPM_PROBF_CPIC the nodes p2g
+ * recorded as separated contribute the particle's rigid-response velocity instead of the
+ * grid's (mpm_solver.py:412-427). */
 int mpm_g2p(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
             void* stream);
 
