@@ -89,6 +89,12 @@ class MPMEntity:
             v, f = _mesh.icosphere(3, self._morph.radius)
         elif isinstance(self._morph, _morphs.Cylinder):
             v, f = _mesh.cylinder_mesh(self._morph.radius, self._morph.height)
+        elif isinstance(self._morph, _morphs.MeshSet):
+            v, f = self._morph.visual_mesh()  # already placed
+            self._vverts, self._vfaces = v, f
+            K = int(getattr(getattr(scene, "vis_options", None), "n_support_neighbors", 12))
+            self._support_idx, self._support_w = skinning_supports(self._particles, self._vverts, K)
+            return
         elif isinstance(self._morph, _morphs.Mesh):
             v, f = self._morph.vertices, self._morph.faces
         else:
@@ -98,6 +104,11 @@ class MPMEntity:
         self._vfaces = f
         K = int(getattr(getattr(scene, "vis_options", None), "n_support_neighbors", 12))
         self._support_idx, self._support_w = skinning_supports(self._particles, self._vverts, K)
+
+    @property
+    def mesh_set_group_ids(self):
+        """For a MeshSet entity, the index of the mesh each particle came from."""
+        return getattr(self._morph, "group_ids", None)
 
     @property
     def vverts(self):

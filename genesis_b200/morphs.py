@@ -209,6 +209,50 @@ class Mesh(Morph):
         return pts[_mesh.points_inside(self.vertices, self.faces, pts)]
 
 
+class MeshSet(Mesh):
+    """Several OBJ meshes sampled into one entity (options/morphs.py:720-723).  As the
+    reference's particle entity does (particle_entity.py:239-262), every mesh is scaled and
+    sampled in its own frame and its particles are moved by its entry of `poss`; `eulers`
+    orient only the visual meshes (particle_entity.py:280-286).  `group_ids` gives each
+    particle the index of its mesh (the entity's mesh_set_group_ids)."""
+
+    def __init__(self, files, poss=None, eulers=None, scale=1.0, **kw):
+        files = list(files)
+        if not files:
+            raise GenesisException("MeshSet needs at least one file.")
+        poss = [tuple(p) for p in (poss if poss is not None else [(0.0, 0.0, 0.0)] * len(files))]
+        eulers = [tuple(e) for e in (eulers if eulers is not None else [(0.0, 0.0, 0.0)] * len(files))]
+        if len(poss) != len(files) or len(eulers) != len(files):
+            raise GenesisException("MeshSet: `files`, `poss` and `eulers` must have the same length.")
+        super().__init__(file=files[0], scale=scale, **kw)
+        self.files = [str(f) for f in files]
+        self.poss, self.eulers = poss, eulers
+        self.parts = [Mesh(file=f, scale=scale) for f in self.files]
+        self.group_ids = np.zeros(0, dtype=np.int64)
+
+    def sample(self, p_size, sampler, rng=None):
+        rng = rng or np.random.default_rng()
+        if sampler.startswith("pbs"):
+            sampler = "regular"
+        out, gid = [], []
+        for i, (m, pos) in enumerate(zip(self.parts, self.poss)):
+            pts = m._local_particles(p_size, sampler, rng) + np.asarray(pos, dtype=np.float64)
+            out.append(pts)
+            gid.append(np.full(len(pts), i, dtype=np.int64))
+        self.group_ids = np.concatenate(gid)
+        return np.concatenate(out).astype(np.float64)
+
+    def visual_mesh(self):
+        """The meshes placed by poss and eulers, concatenated (vertices, faces)."""
+        vs, fs, off = [], [], 0
+        for m, pos, eul in zip(self.parts, self.poss, self.eulers):
+            R = _quat_to_R(_euler_to_quat(eul))
+            vs.append(m.vertices @ R.T + np.asarray(pos, dtype=np.float64))
+            fs.append(m.faces + off)
+            off += len(m.vertices)
+        return np.concatenate(vs), np.concatenate(fs)
+
+
 class Plane(Morph):
     """Infinite plane through `pos` with `normal` in its local frame (options/morphs.py:409-470);
     only meaningful for rigid entities (a collider of the MPM grid op)."""
@@ -227,4 +271,4 @@ class Plane(Morph):
         raise GenesisException("A Plane has no particles; use it with gs.materials.Rigid.")
 
 
-__all__ = ["Morph", "Box", "Sphere", "Cylinder", "Mesh", "Nowhere", "Plane"]
+__all__ = ["Morph", "Box", "Sphere", "Cylinder", "Mesh", "MeshSet", "Nowhere", "Plane"]

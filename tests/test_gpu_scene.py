@@ -212,3 +212,30 @@ def test_cylinder_entity_steps_and_skins():
     # the skinned rim stays around the particles' centre of mass
     c = cyl.get_particles_pos().cpu().double().mean(0)
     assert float((vv.mean(0) - c).norm()) < 0.02
+
+
+def test_mesh_set_entity(tmp_path):
+    """Two OBJ cubes in one MeshSet entity: each keeps its particles' group id and both fall."""
+    hx = 0.5
+    v = [[x, y, z] for x in (-hx, hx) for y in (-hx, hx) for z in (-hx, hx)]
+    q = [[0, 1, 3, 2], [4, 6, 7, 5], [0, 4, 5, 1], [2, 3, 7, 6], [0, 2, 6, 4], [1, 5, 7, 3]]
+    obj = tmp_path / "cube.obj"
+    obj.write_text("".join(f"v {a} {b} {c}\n" for a, b, c in v) + "".join(
+        "f " + " ".join(str(i + 1) for i in f) + "\n" for f in q))
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=1e-3, substeps=10, gravity=(0, 0, -9.8)),
+        mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
+                                          particle_size=0.0125),
+    )
+    e = scene.add_entity(gs.morphs.MeshSet(files=[str(obj), str(obj)], poss=[(0.3, 0.5, 0.5), (0.7, 0.5, 0.5)],
+                                           scale=0.1), material=gs.materials.MPM.Elastic(E=1e5, nu=0.3))
+    scene.build()
+    g = e.mesh_set_group_ids
+    assert g.shape == (e.n_particles,) and (g == 0).sum() == (g == 1).sum() == 8**3
+    z0 = e.get_particles_pos()[:, 2].clone()
+    for _ in range(5):
+        scene.step()
+    dz = (e.get_particles_pos()[:, 2] - z0).cpu().numpy()
+    assert dz[g == 0].mean() < 0 and dz[g == 1].mean() < 0
+    assert e.n_vverts == 16

@@ -121,3 +121,25 @@ def test_cylinder_morph_and_mesh():
     assert ins[(r < 0.1 * np.cos(np.pi / 32)) & (np.abs(q[:, 2]) < 0.1)].all()
     with pytest.raises(GenesisException):
         Cylinder(radius=0.0)
+
+
+def test_mesh_set_samples_each_mesh_at_its_position(tmp_path):
+    from genesis_b200.morphs import MeshSet
+
+    v, q = _box_quads((1.0, 1.0, 1.0))
+    a, b = tmp_path / "a.obj", tmp_path / "b.obj"
+    _write_obj(a, v, [], quads=q)
+    sv, sf = mesh.icosphere(2, 1.0)
+    _write_obj(b, sv, sf)
+    ms = MeshSet(files=[str(a), str(b)], poss=[(0.3, 0.5, 0.5), (0.7, 0.5, 0.5)], eulers=[(0, 0, 0), (0, 0, 45)],
+                 scale=0.1)
+    pts = ms.sample(0.01, "regular")
+    g = ms.group_ids
+    assert pts.shape[0] == g.shape[0] and set(g.tolist()) == {0, 1}
+    assert np.allclose(pts[g == 0].mean(0), [0.3, 0.5, 0.5], atol=1e-9)  # 10^3 lattice of the cube
+    assert (g == 0).sum() == 1000
+    assert (np.linalg.norm(pts[g == 1] - [0.7, 0.5, 0.5], axis=1) <= 0.1).all()
+    vv, vf = ms.visual_mesh()
+    assert vv.shape[0] == 8 + len(sv) and vf.max() == vv.shape[0] - 1
+    with pytest.raises(GenesisException):
+        MeshSet(files=[str(a)], poss=[(0, 0, 0), (1, 1, 1)])
