@@ -8,9 +8,11 @@ the adjoint of each substep (mpm_substep_adjoint) from the last to the first.  M
 one state per checkpoint plus one segment of states, instead of every substep.
 
 Supported: Elastic scenes (corotated or neo-Hookean) and Muscle scenes, with per-particle
-Young's modulus; gradients with respect to a uniform initial velocity v0 (3,), per-particle
-E (N,) and, for Muscle, per-particle actuation (N,) (mpm_solver.py:922-949: the reference's
-actuation gradients).  This replaces the reference's requires_grad path
+Young's modulus; gradients with respect to the initial velocity (a uniform v0 (3,), as
+entity.set_velocity sets it, or per particle (N, 3)), the initial positions (an offset (3,) of
+the scene's positions, as entity.set_position moves an entity, or absolute positions (N, 3)),
+per-particle E (N,) and, for Muscle, per-particle actuation (N,) (mpm_solver.py:922-949: the
+reference's actuation gradients; particle_entity.py:415-481: its state-input gradients).  This replaces the reference's requires_grad path
 (simulator.py:294-303, mpm_solver.py:485-517, with the gstaichi autodiff kernels and
 backward_svd at mpm_solver.py:1112-1129) for these cases.
 """
@@ -57,19 +59,25 @@ class DifferentiableRollout:
         nu = self.nu
         return E / (2.0 * (1.0 + nu)), E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
 
-    def forward(self, v0: torch.Tensor, E: torch.Tensor, actu: torch.Tensor | None = None) -> torch.Tensor:
+    def forward(self, v0: torch.Tensor, E: torch.Tensor, actu: torch.Tensor | None = None,
+                x0: torch.Tensor | None = None) -> torch.Tensor:
         rt, d = self.rt, self.desc
         n = rt.n
         dev = rt.device
-        v0 = v0.detach().to(dev, torch.float32).reshape(1, 3)
+        v0 = v0.detach().to(dev, torch.float32)
+        v0 = v0.reshape(1, 3).expand(n, 3) if v0.numel() == 3 else v0.reshape(n, 3)
+        pos = torch.as_tensor(d.pos, dtype=torch.float32, device=dev)
+        if x0 is not None:
+            x0 = x0.detach().to(dev, torch.float32)
+            pos = pos + x0.reshape(1, 3) if x0.numel() == 3 else x0.reshape(n, 3)
         E = E.detach().to(dev, torch.float32).reshape(n)
         if self.muscle:
             a = torch.zeros(n, device=dev) if actu is None else actu.detach().to(dev, torch.float32).reshape(n)
             rt.actu[:n] = a
         mats = torch.zeros(n, dtype=torch.uint8, device=dev)
         rt.load_state(
-            torch.as_tensor(d.pos, dtype=torch.float32, device=dev),
-            v0.expand(n, 3).contiguous(),
+            pos.contiguous(),
+            v0.contiguous(),
             torch.zeros((n, 9), device=dev),
             torch.eye(3, device=dev).reshape(1, 9).repeat(n, 1),
             torch.ones(n, device=dev),
@@ -102,7 +110,8 @@ class DifferentiableRollout:
 
     def backward(self, pos_grad: torch.Tensor):
         """pos_grad: dL/dx_final [N,3] in API order -> (dL/dv0 [3], dL/dE [N], dL/dactu [N] or
-        None)."""
+        None).  The per-particle gradients of the initial positions and velocities, [N,3] in API
+        order, are left in x0_grad and v0_grad."""
         rt = self.rt
         n = rt.n
         slot = rt.slot[:n].long()
@@ -124,6 +133,10 @@ class DifferentiableRollout:
             t_end = t0
         rt.state.copy_(final)
         gid = rt.gid[:n].long()
+        self.x0_grad = torch.empty((n, 3), dtype=torch.float32, device=rt.device)
+        self.x0_grad[gid] = self.adj[0:3, :n].t()
+        self.v0_grad = torch.empty((n, 3), dtype=torch.float32, device=rt.device)
+        self.v0_grad[gid] = self.adj[3:6, :n].t()
         vbar = self.adj[3:6, :n].sum(dim=1)
         nu = self.nu
         Ebar_slot = self.lame_bar[0, :n] / (2.0 * (1.0 + nu)) + self.lame_bar[1, :n] * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
@@ -138,19 +151,29 @@ class DifferentiableRollout:
 
 class _RolloutFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, v0, E, actu, sim):
+    def forward(ctx, v0, E, actu, x0, sim):
         ctx.sim = sim
-        return sim.forward(v0, E, actu)
+        ctx.v0_per_particle = v0.numel() != 3
+        ctx.x0_shape = None if x0 is None else tuple(x0.shape)
+        return sim.forward(v0, E, actu, x0)
 
     @staticmethod
     def backward(ctx, grad_pos):
-        v0b, Eb, ab = ctx.sim.backward(grad_pos)
-        return v0b, Eb, ab, None
+        sim = ctx.sim
+        v0b, Eb, ab = sim.backward(grad_pos)
+        if ctx.v0_per_particle:
+            v0b = sim.v0_grad
+        x0b = None
+        if ctx.x0_shape is not None:
+            x0b = sim.x0_grad.sum(0).reshape(ctx.x0_shape) if len(ctx.x0_shape) < 2 else sim.x0_grad
+        return v0b, Eb, ab, x0b, None
 
 
-def rollout(v0: torch.Tensor, E: torch.Tensor, sim: DifferentiableRollout, actu: torch.Tensor | None = None):
-    """Final particle positions [N,3] of the rollout, differentiable w.r.t. v0, E and (for a
-    Muscle scene) the per-particle actuation."""
+def rollout(v0: torch.Tensor, E: torch.Tensor, sim: DifferentiableRollout, actu: torch.Tensor | None = None,
+            x0: torch.Tensor | None = None):
+    """Final particle positions [N,3] of the rollout, differentiable w.r.t. the initial velocity
+    v0 ((3,) uniform or (N,3)), the initial positions x0 (None: the scene's; (3,): an offset of
+    them; (N,3): absolute), E and (for a Muscle scene) the per-particle actuation."""
     if sim.muscle and actu is None:
         actu = torch.zeros(sim.rt.n, device=sim.rt.device)
-    return _RolloutFunction.apply(v0, E, actu, sim)
+    return _RolloutFunction.apply(v0, E, actu, x0, sim)

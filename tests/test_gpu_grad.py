@@ -154,3 +154,53 @@ def test_muscle_actuation_adjoint_against_fp64_finite_differences():
         print(f"\n[accuracy] muscle grad actu[group {gi}]: adjoint {g_grp[gi]:.6e}  fp64 FD {fd:.6e}")
         assert abs(g_grp[gi] - fd) <= 3e-2 * max(abs(fd), 1e-3 * np.abs(g_grp).max()), (gi, g_grp[gi], fd)
     assert n == 2000
+
+
+def test_position_and_per_particle_velocity_gradients_against_fp64_fd():
+    """dL/d(position offset) (entity.set_position) and per-particle dL/dv0 from the adjoint,
+    against float64 central differences of the C restatement (particle_entity.py:415-481)."""
+    from oracle import bridge, cref
+    from oracle import mpm_adjoint as AD
+
+    from genesis_b200.grad import DifferentiableRollout, rollout
+
+    d = W.diff_elastic(n=2000, n_substeps=80)
+    sim = DifferentiableRollout(d, checkpoint_every=20)
+    n = d.n_particles
+    v0 = torch.tensor(np.tile(d.meta["v0"], (n, 1)), dtype=torch.float32, device="cuda", requires_grad=True)
+    off = torch.zeros(3, dtype=torch.float32, device="cuda", requires_grad=True)
+    E = torch.tensor(d.E_particle, dtype=torch.float32, device="cuda")
+    tgt = torch.tensor(d.meta["target"], dtype=torch.float32, device="cuda")
+    x = rollout(v0, E, sim, x0=off)
+    ((x.mean(0) - tgt) ** 2).sum().backward()
+    g_off = off.grad.cpu().numpy().astype(np.float64)
+    g_v = v0.grad.cpu().numpy().astype(np.float64)
+    assert g_v.shape == (n, 3)
+
+    p, mats, st = bridge.from_desc(d, np.float64)
+    mu, lam = AD.lame_of_E(d.E_particle, 0.3)
+
+    def L(dx=np.zeros(3), dv=None):
+        s = dict(st)
+        s["x"] = st["x"] + dx
+        v = np.tile(d.meta["v0"], (n, 1))
+        if dv is not None:
+            v = v + dv
+        s["v"] = v
+        out, rc = cref.substeps(p, mats, s, d.n_substeps, mu_p=mu, lam_p=lam)
+        assert rc == 0
+        return float(((out["x"].mean(0) - d.meta["target"]) ** 2).sum())
+
+    h = 1e-5
+    for c in range(3):
+        e = np.zeros(3)
+        e[c] = h
+        fd = (L(dx=e) - L(dx=-e)) / (2 * h)
+        print(f"\n[accuracy] grad position offset[{c}]: adjoint {g_off[c]:.6e}  fp64 FD {fd:.6e}")
+        assert abs(g_off[c] - fd) <= 2e-2 * max(abs(fd), 1e-3 * np.abs(g_off).max()), (c, g_off[c], fd)
+    k = int(np.argmax(np.abs(g_v[:, 2])))
+    dv = np.zeros((n, 3))
+    dv[k, 2] = 1e-3
+    fd = (L(dv=dv) - L(dv=-dv)) / 2e-3
+    print(f"\n[accuracy] grad v0[particle {k}, z]: adjoint {g_v[k, 2]:.6e}  fp64 FD {fd:.6e}")
+    assert abs(g_v[k, 2] - fd) <= 5e-2 * abs(fd), (g_v[k, 2], fd)
