@@ -54,14 +54,22 @@ class DifferentiableRollout:
             if mdir is not None:
                 self.rt.muscle_dir[: self.rt.n] = torch.as_tensor(mdir, dtype=torch.float32, device=self.rt.device)
         self.checkpoints: list[torch.Tensor] = []
+        self.generation = 0  # forwards so far: a backward must follow its own forward
 
     def _lame(self, E):
         nu = self.nu
         return E / (2.0 * (1.0 + nu)), E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
 
     def forward(self, v0: torch.Tensor, E: torch.Tensor, actu: torch.Tensor | None = None,
-                x0: torch.Tensor | None = None) -> torch.Tensor:
+                x0: torch.Tensor | None = None, record=None) -> torch.Tensor:
+        """Final positions [N,3]; with record (substep counts in [0, T]) the positions after each
+        of them, [len(record), N, 3] (a loss over a trajectory, as the reference's scripts build
+        from get_state() every step)."""
         rt, d = self.rt, self.desc
+        self.generation += 1
+        self.record = None if record is None else [int(r) for r in record]
+        if self.record is not None and any(r < 0 or r > self.T for r in self.record):
+            raise GenesisException(f"record substeps must lie in [0, {self.T}]")
         n = rt.n
         dev = rt.device
         v0 = v0.detach().to(dev, torch.float32)
@@ -89,13 +97,24 @@ class DifferentiableRollout:
         rt._count = 0
         rt.ensure_sorted()  # fixes the slot order for the whole rollout and its adjoint
         self.checkpoints = []
+        rec = {}
+        if self.record is not None and 0 in self.record:
+            rec[0] = rt.get_state(("pos",))["pos"]
         t = 0
         while t < self.T:
             m = min(self.k, self.T - t)
             self.checkpoints.append(rt.state.clone())
-            rt.substeps(m)
-            t += m
-        return rt.get_state(("pos",))["pos"]
+            # split at the recorded substeps (the same results: this runtime never re-sorts, and a
+            # fused g2p + p2g equals a g2p followed by a p2g)
+            stops = sorted({r for r in (self.record or []) if t < r < t + m} | {t + m})
+            for r in stops:
+                rt.substeps(r - t)
+                t = r
+                if self.record is not None and r in self.record:
+                    rec[r] = rt.get_state(("pos",))["pos"]
+        if self.record is None:
+            return rt.get_state(("pos",))["pos"]
+        return torch.stack([rec[r] for r in self.record])
 
     def _adjoint_substep(self, state: torch.Tensor):
         rt = self.rt
@@ -109,15 +128,29 @@ class DifferentiableRollout:
             C.c_void_p(self.lame_bar.data_ptr()), rt._ws, C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
 
     def backward(self, pos_grad: torch.Tensor):
-        """pos_grad: dL/dx_final [N,3] in API order -> (dL/dv0 [3], dL/dE [N], dL/dactu [N] or
-        None).  The per-particle gradients of the initial positions and velocities, [N,3] in API
-        order, are left in x0_grad and v0_grad."""
+        """pos_grad: dL/dx_final [N,3] in API order (or, after a forward with record,
+        [len(record), N, 3]) -> (dL/dv0 [3], dL/dE [N], dL/dactu [N] or None).  The per-particle
+        gradients of the initial positions and velocities, [N,3] in API order, are left in
+        x0_grad and v0_grad."""
         rt = self.rt
         n = rt.n
         slot = rt.slot[:n].long()
         self.adj.zero_()
         self.lame_bar.zero_()
-        self.adj[0:3, slot] = pos_grad.to(rt.device, torch.float32).reshape(n, 3).t()
+        g = pos_grad.to(rt.device, torch.float32)
+        # dL/dx at each recorded substep, added to the adjoint when the walk back reaches it
+        inject = {}
+        if self.record is None:
+            inject[self.T] = g.reshape(n, 3)
+        else:
+            for i, r in enumerate(self.record):
+                inject[r] = inject[r] + g[i].reshape(n, 3) if r in inject else g[i].reshape(n, 3)
+
+        def add(r):
+            if r in inject:
+                self.adj[0:3, slot] += inject[r].t()
+
+        add(self.T)
         final = rt.state.clone()
         t_end = self.T
         for ci in range(len(self.checkpoints) - 1, -1, -1):
@@ -129,8 +162,11 @@ class DifferentiableRollout:
                 states.append(rt.state.clone())
                 rt.substeps(1)
             for j in range(m - 1, -1, -1):
+                if t0 + j + 1 != self.T:
+                    add(t0 + j + 1)
                 self._adjoint_substep(states[j])
             t_end = t0
+        add(0)
         rt.state.copy_(final)
         gid = rt.gid[:n].long()
         self.x0_grad = torch.empty((n, 3), dtype=torch.float32, device=rt.device)
@@ -151,29 +187,34 @@ class DifferentiableRollout:
 
 class _RolloutFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, v0, E, actu, x0, sim):
+    def forward(ctx, v0, E, actu, x0, sim, record):
         ctx.sim = sim
+        ctx.generation = sim.generation + 1
         ctx.v0_per_particle = v0.numel() != 3
         ctx.x0_shape = None if x0 is None else tuple(x0.shape)
-        return sim.forward(v0, E, actu, x0)
+        return sim.forward(v0, E, actu, x0, record)
 
     @staticmethod
     def backward(ctx, grad_pos):
         sim = ctx.sim
+        if sim.generation != ctx.generation:
+            raise GenesisException("this rollout's checkpoints were replaced by a later forward of the same "
+                                   "DifferentiableRollout; call backward before the next forward")
         v0b, Eb, ab = sim.backward(grad_pos)
         if ctx.v0_per_particle:
             v0b = sim.v0_grad
         x0b = None
         if ctx.x0_shape is not None:
             x0b = sim.x0_grad.sum(0).reshape(ctx.x0_shape) if len(ctx.x0_shape) < 2 else sim.x0_grad
-        return v0b, Eb, ab, x0b, None
+        return v0b, Eb, ab, x0b, None, None
 
 
 def rollout(v0: torch.Tensor, E: torch.Tensor, sim: DifferentiableRollout, actu: torch.Tensor | None = None,
-            x0: torch.Tensor | None = None):
-    """Final particle positions [N,3] of the rollout, differentiable w.r.t. the initial velocity
-    v0 ((3,) uniform or (N,3)), the initial positions x0 (None: the scene's; (3,): an offset of
+            x0: torch.Tensor | None = None, record=None):
+    """Final particle positions [N,3] of the rollout (or, with record, the positions after each
+    listed substep count, [len(record), N, 3]), differentiable w.r.t. the initial velocity v0
+    ((3,) uniform or (N,3)), the initial positions x0 (None: the scene's; (3,): an offset of
     them; (N,3): absolute), E and (for a Muscle scene) the per-particle actuation."""
     if sim.muscle and actu is None:
         actu = torch.zeros(sim.rt.n, device=sim.rt.device)
-    return _RolloutFunction.apply(v0, E, actu, x0, sim)
+    return _RolloutFunction.apply(v0, E, actu, x0, sim, record)

@@ -204,3 +204,60 @@ def test_position_and_per_particle_velocity_gradients_against_fp64_fd():
     fd = (L(dv=dv) - L(dv=-dv)) / 2e-3
     print(f"\n[accuracy] grad v0[particle {k}, z]: adjoint {g_v[k, 2]:.6e}  fp64 FD {fd:.6e}")
     assert abs(g_v[k, 2] - fd) <= 5e-2 * abs(fd), (g_v[k, 2], fd)
+
+
+def test_trajectory_loss_gradient_against_fp64_fd():
+    """A loss over the positions after every 20 substeps (the reference's scripts sum a loss
+    over get_state() each step): the recorded states' gradients enter the adjoint at their
+    substeps; dL/dv0 and dL/dE against float64 central differences."""
+    from oracle import bridge, cref
+    from oracle import mpm_adjoint as AD
+
+    from genesis_b200.grad import DifferentiableRollout, rollout
+
+    d = W.diff_elastic(n=2000, n_substeps=80)
+    sim = DifferentiableRollout(d, checkpoint_every=30)  # record points fall inside segments
+    rec = [0, 20, 40, 60, 80]
+    v0 = torch.tensor(d.meta["v0"], dtype=torch.float32, device="cuda", requires_grad=True)
+    E = torch.tensor(d.E_particle, dtype=torch.float32, device="cuda", requires_grad=True)
+    tgt = torch.tensor(d.meta["target"], dtype=torch.float32, device="cuda")
+    xs = rollout(v0, E, sim, record=rec)
+    assert xs.shape == (len(rec), d.n_particles, 3)
+    ((xs.mean(1) - tgt) ** 2).sum().backward()
+    gv, gE = v0.grad.cpu().numpy().astype(np.float64), E.grad.cpu().numpy().astype(np.float64)
+    final = rollout(v0.detach(), E.detach(), sim)
+    # splitting the substep calls changes nothing but the order of the grid's float atomics
+    assert torch.allclose(xs[-1], final, atol=1e-6)
+    stale = rollout(v0, E, sim, record=rec)
+    rollout(v0.detach(), E.detach(), sim)  # a later forward replaces the checkpoints
+    with pytest.raises(Exception, match="backward before the next forward"):
+        stale.sum().backward()
+
+    p, mats, st = bridge.from_desc(d, np.float64)
+    n = d.n_particles
+
+    def L(v, Ev):
+        s = dict(st)
+        s["v"] = np.tile(v, (n, 1))
+        mu, lam = AD.lame_of_E(Ev, 0.3)
+        loss = float(((s["x"].mean(0) - d.meta["target"]) ** 2).sum())
+        for _ in range(4):
+            s, rc = cref.substeps(p, mats, s, 20, mu_p=mu, lam_p=lam)
+            assert rc == 0
+            loss += float(((s["x"].mean(0) - d.meta["target"]) ** 2).sum())
+        return loss
+
+    h = 1e-4
+    for c in range(3):
+        e = np.zeros(3)
+        e[c] = h
+        fd = (L(d.meta["v0"] + e, d.E_particle) - L(d.meta["v0"] - e, d.E_particle)) / (2 * h)
+        print(f"\n[accuracy] trajectory grad v0[{c}]: adjoint {gv[c]:.6e}  fp64 FD {fd:.6e}")
+        assert abs(gv[c] - fd) <= 2e-2 * max(abs(fd), 1e-3 * np.abs(gv).max()), (c, gv[c], fd)
+    k = int(np.argmax(np.abs(gE)))
+    Ep, Em = d.E_particle.copy(), d.E_particle.copy()
+    Ep[k] *= 1 + 1e-4
+    Em[k] *= 1 - 1e-4
+    fd = (L(d.meta["v0"], Ep) - L(d.meta["v0"], Em)) / (2e-4 * d.E_particle[k])
+    print(f"\n[accuracy] trajectory grad E[{k}]: adjoint {gE[k]:.6e}  fp64 FD {fd:.6e}")
+    assert abs(gE[k] - fd) <= 5e-2 * abs(fd), (gE[k], fd)
