@@ -272,8 +272,54 @@ class MPMEntity:
         self._check_built()
         return self._solver.runtime.get_particles_free(self._flat_idx(None, None)[0])
 
-    # buffered targets applied at the next step (particle_entity.py:418-458, 503-578)
+    # buffered targets applied at the next step (particle_entity.py:418-458, 503-578); in a
+    # differentiable scene they go to the scene's tape, which applies them at the next step and
+    # hands back their gradients (particle_entity.py:460-481)
+    def _tape(self):
+        return getattr(self._solver, "tape", None) if self._scene.requires_grad else None
+
+    def _input_map(self, kind, value, envs_idx):
+        """What a set_position / set_velocity / set_actuation value writes, per environment and
+        particle (differentiable in value): positions / velocities [n_envs, n, 3], actuation
+        [n_envs, n]."""
+        n_envs, n = len(self._envs(envs_idx)), self._n_particles
+        if kind == "pos":
+            v = value
+            if v.ndim == 1 or (v.ndim == 2 and v.shape[0] != n):
+                off = torch.as_tensor(self._init_particles_offset, dtype=torch.float32, device=v.device)
+                v = off + v[..., None, :]
+            return v.expand(n_envs, n, 3)
+        if kind == "vel":
+            return value.expand(n_envs, n, 3)
+        G = self._material.n_groups
+        a = value.reshape(value.shape[:-1] + (G,)) if value.ndim else value.reshape(1).expand(G)
+        a = a.expand(n_envs, n, G)
+        idx = self._flat_idx(None, envs_idx)
+        grp = self._solver.runtime.muscle_group[idx.reshape(-1)].reshape(n_envs, n, 1)
+        return torch.gather(a, 2, grp).squeeze(2)
+
+    def _input_grad(self, kind, shape, g, envs_idx):
+        """dL/d(value) of a set_* input from dL/d(what it wrote) g."""
+        with torch.enable_grad():
+            a = torch.zeros(shape, dtype=torch.float32, device=g.device, requires_grad=True)
+            out = self._input_map(kind, a, envs_idx)
+            (ga,) = torch.autograd.grad(out, a, grad_outputs=g.reshape(out.shape), allow_unused=True)
+        return torch.zeros(shape, device=g.device) if ga is None else ga
+
+    def _apply_position(self, value, envs_idx):
+        self.set_particles_pos(self._input_map("pos", value, envs_idx), envs_idx=envs_idx)
+
+    def _apply_velocity(self, value, envs_idx):
+        self.set_particles_vel(self._input_map("vel", value, envs_idx), envs_idx=envs_idx)
+
+    def _apply_actuation(self, value, envs_idx):
+        idx = self._flat_idx(None, envs_idx)
+        self._solver.runtime.actu[idx.reshape(-1)] = self._input_map("actu", value, envs_idx).reshape(-1)
+
     def set_position(self, value, envs_idx=None):
+        if self._tape() is not None:
+            self._tape().record_input(self, "pos", value, envs_idx)
+            return
         poss = _as_tensor(value, torch.float32, self._solver.device)
         if poss.ndim == 1 or (poss.ndim == 2 and poss.shape[0] != self._n_particles):
             off = torch.as_tensor(self._init_particles_offset, dtype=torch.float32, device=poss.device)
@@ -281,6 +327,9 @@ class MPMEntity:
         self._tgt["pos"] = (poss, envs_idx)
 
     def set_velocity(self, vels, envs_idx=None):
+        if self._tape() is not None:
+            self._tape().record_input(self, "vel", vels, envs_idx)
+            return
         self._tgt["vel"] = (_as_tensor(vels, torch.float32, self._solver.device), envs_idx)
 
     def set_active(self, active, envs_idx=None):
@@ -307,6 +356,9 @@ class MPMEntity:
         """Buffered per-group actuation applied at the next step (mpm_entity.py:412-427):
         actus of shape ([M,] [n_particles,] [n_groups,]); a scalar applies to every group."""
         self._assert_muscle()
+        if self._tape() is not None:
+            self._tape().record_input(self, "actu", actus, envs_idx)
+            return
         a = _as_tensor(actus, torch.float32, self._solver.device)
         if a.ndim == 0:
             a = a.reshape((1,)).expand((self._material.n_groups,))
@@ -388,6 +440,9 @@ class MPMEntity:
     def _get(self, keys, envs_idx):
         self._check_built()
         envs = self._envs(envs_idx)
+        if self._tape() is not None:  # differentiable: slices of a query node of the tape
+            full = self._solver.get_state()
+            return {k: getattr(full, k)[envs, self._particle_start : self.particle_end] for k in keys}
         st = self._solver.runtime.get_state(keys)
         B, N = self._solver.B, self._solver.n_particles
         out = {}

@@ -1,0 +1,187 @@
+"""Scene-level differentiation: `SimOptions(requires_grad=True)` scenes.
+
+Replaces the reference's differentiable scene (simulator.py:294-344 `_step_grad` /
+`sub_step_grad`, scene.py:1267-1281 `_backward`, grad/tensor.py:73-79 `gs.Tensor.backward`,
+particle_entity.py:415-481 `process_input_grad`, mpm_entity.py:245-264) with torch autograd
+nodes over the checkpointed CUDA adjoint (mpm_substep_adjoint):
+
+* every `scene.step()` is one `_Step` node.  Its inputs are the previous step's handle (a
+  one-element tensor that only orders the nodes) and the tensors given to the entities'
+  `set_position` / `set_velocity` / `set_actuation` for that step; it saves the particle state
+  after those inputs as its checkpoint and returns the next handle;
+* every `scene.get_state()` (or entity `get_state()` / `get_particles_*`) is a `_Query` node on
+  the current handle whose outputs are the state tensors.
+
+`loss.backward()` then needs no scene call: autograd runs every query of a state and the step
+that consumes it before the step that produced it, so when `_Step.backward` of step s runs, the
+adjoint buffer holds dL/d(state after step s) minus the queries of that state, which it adds;
+it recomputes the step's substeps from its checkpoint, runs their adjoints in reverse, reads
+the gradients of the step's inputs (undoing them in reverse order: the state components an
+input overwrote get a zero adjoint) and leaves dL/d(state before step s) for the step before.
+Actuation persists until it is set again, so its gradient accumulates across steps and is
+consumed by the step that set it.
+
+Scope (the adjoint's): Elastic (corotated / neo-Hookean) and Muscle materials, no rigid
+colliders, no emitters; positions may be set only before the first step (setting them later
+re-bins the particles, which would change the slot order the adjoint walks in).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from .. import _native as nat
+from ..exceptions import GenesisException
+from .runtime import _cuda_stream_handle
+
+_KIND_ORDER = {"pos": 0, "vel": 1, "actu": 2}  # the order entity.process_input applies them in
+
+
+class SceneTape:
+    def __init__(self, solver):
+        self.solver = solver
+        rt = solver.runtime
+        self.rt = rt
+        if rt.mu_p is None:
+            raise GenesisException("the differentiable runtime needs per-particle Lame parameters")
+        nbytes = C.c_uint64()
+        nat.check("mpm_adjoint_workspace_bytes", rt.lib.mpm_adjoint_workspace_bytes(C.byref(rt.prob), C.byref(nbytes)))
+        self.adj_ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=rt.device)
+        self.adj = torch.zeros_like(rt.state)  # dL/d(state), slot order
+        self.lame_bar = torch.zeros((3, rt.stride), dtype=torch.float32, device=rt.device)
+        self.muscle = rt.actu is not None
+        self.reset()
+
+    def reset(self):
+        self.handle = torch.zeros(1, device=self.rt.device, requires_grad=True)
+        self.n_steps = 0
+        self.pending = []  # (entity, kind, value, envs_idx) for the next step
+        self.inject = {}  # state index -> dL/d(state) of its queries, slot order
+        self.cursor = None  # the state index the adjoint buffer currently stands for
+
+    # ------------------------------------------------------------------ forward
+    def record_input(self, entity, kind, value, envs_idx):
+        if kind == "pos" and self.n_steps > 0:
+            raise GenesisException("In a differentiable scene, positions can be set only before the first step.")
+        if not isinstance(value, torch.Tensor):
+            value = torch.as_tensor(value, dtype=torch.float32)
+        self.pending.append((entity, kind, value.to(self.rt.device, torch.float32), envs_idx))
+
+    def step(self):
+        inputs = sorted(self.pending, key=lambda t: (_KIND_ORDER[t[1]], t[0].idx))
+        self.pending = []
+        meta = [(e, k, envs) for e, k, _, envs in inputs]
+        self.handle = _Step.apply(self, self.n_steps, meta, self.handle, *[v for _, _, v, _ in inputs])
+        self.n_steps += 1
+
+    def query(self):
+        return _Query.apply(self, self.n_steps, self.handle)
+
+    # ------------------------------------------------------------------ helpers
+    def _apply(self, entity, kind, value, envs):
+        if kind == "pos":
+            entity._apply_position(value, envs)
+        elif kind == "vel":
+            entity._apply_velocity(value, envs)
+        else:
+            entity._apply_actuation(value, envs)
+
+    def _adjoint_substep(self, state):
+        rt = self.rt
+        par = nat.Particles(
+            state=state.data_ptr(), state_stride=rt.stride, mat=rt.mat.data_ptr(), pflags=rt.pflags.data_ptr(),
+            gid=rt.gid.data_ptr(), slot=rt.slot.data_ptr(), mu_p=rt.mu_p.data_ptr(), lam_p=rt.lam_p.data_ptr(),
+            actu=rt.actu.data_ptr() if self.muscle else None,
+            muscle_dir=rt.muscle_dir.data_ptr() if self.muscle else None)
+        nat.check("mpm_substep_adjoint", rt.lib.mpm_substep_adjoint(
+            C.byref(rt.prob), C.byref(rt.tables), C.byref(par), C.c_void_p(self.adj.data_ptr()),
+            C.c_void_p(self.lame_bar.data_ptr()), rt._ws, C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
+
+
+class _Step(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, tape, s, meta, handle, *values):
+        rt, solver = tape.rt, tape.solver
+        for (entity, kind, envs), v in zip(meta, values):
+            tape._apply(entity, kind, v.detach(), envs)
+        solver.process_input()  # the non-differentiable targets (activeness) as usual
+        if not getattr(rt, "_sorted_once", False) or rt._dirty:  # the slot order is fixed from here on
+            rt.sort()
+            rt._sorted_once = True
+            rt._dirty = False
+        ctx.tape, ctx.s, ctx.meta = tape, s, meta
+        ctx.shapes = [tuple(v.shape) for v in values]
+        ctx.ckpt = rt.state.clone()
+        ctx.actu = rt.actu.clone() if tape.muscle else None
+        solver.advance(solver._sim.substeps)
+        return handle.new_zeros(1)
+
+    @staticmethod
+    def backward(ctx, g_handle):
+        tape, rt, s = ctx.tape, ctx.tape.rt, ctx.s
+        if tape.cursor != s + 1:  # the latest step of this backward pass
+            tape.adj.zero_()
+            tape.lame_bar.zero_()
+        inj = tape.inject.pop(s + 1, None)
+        if inj is not None:
+            tape.adj += inj
+        live = rt.state.clone()
+        live_actu = rt.actu.clone() if tape.muscle else None
+        rt.state.copy_(ctx.ckpt)
+        if tape.muscle:
+            rt.actu.copy_(ctx.actu)
+        states = []
+        for _ in range(tape.solver._sim.substeps):  # recompute the step, one state per substep
+            states.append(rt.state.clone())
+            rt.substeps(1)
+        for st in reversed(states):
+            tape._adjoint_substep(st)
+        rt.state.copy_(live)
+        if tape.muscle:
+            rt.actu.copy_(live_actu)
+        grads = [None] * len(ctx.meta)
+        for i in range(len(ctx.meta) - 1, -1, -1):  # undo the inputs, the last applied first
+            entity, kind, envs = ctx.meta[i]
+            idx = entity._flat_idx(None, envs)  # [n_envs, n_particles] runtime ids
+            slots = rt.slot[idx.reshape(-1)].long()
+            if kind == "actu":
+                g = tape.lame_bar[2, slots].reshape(idx.shape)  # dL/dactu per particle
+                tape.lame_bar[2, slots] = 0.0
+            else:
+                rows = slice(0, 3) if kind == "pos" else slice(3, 6)
+                g = tape.adj[rows, slots].t().reshape(idx.shape + (3,))
+                if kind == "pos":
+                    tape.adj[:, slots] = 0.0  # set_particles_pos resets v, C, F and Jp as well
+                else:
+                    tape.adj[3:6, slots] = 0.0
+            grads[i] = entity._input_grad(kind, ctx.shapes[i], g, envs)
+        tape.cursor = s
+        return (None, None, None, torch.zeros_like(g_handle), *grads)
+
+
+class _Query(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, tape, s, handle):
+        rt, solver = tape.rt, tape.solver
+        st = rt.get_state(("pos", "vel", "C", "F", "Jp"))
+        B, N = solver._B, solver.n_particles
+        ctx.tape, ctx.s = tape, s
+        return (st["pos"].reshape(B, N, 3), st["vel"].reshape(B, N, 3), st["C"].reshape(B, N, 3, 3),
+                st["F"].reshape(B, N, 3, 3), st["Jp"].reshape(B, N))
+
+    @staticmethod
+    def backward(ctx, g_pos, g_vel, g_C, g_F, g_Jp):
+        tape = ctx.tape
+        rt = tape.rt
+        n = rt.n
+        slot = rt.slot[:n].long()
+        inj = torch.zeros_like(rt.state)
+        for g, rows, w in ((g_pos, slice(0, 3), 3), (g_vel, slice(3, 6), 3), (g_C, slice(6, 15), 9),
+                           (g_F, slice(15, 24), 9), (g_Jp, slice(24, 25), 1)):
+            if g is not None:
+                inj[rows, slot] = g.reshape(n, w).t().to(torch.float32)
+        prev = tape.inject.get(ctx.s)
+        tape.inject[ctx.s] = inj if prev is None else prev + inj
+        return None, None, torch.zeros(1, device=rt.device)

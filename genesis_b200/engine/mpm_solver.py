@@ -42,6 +42,7 @@ class MPMSolver:
         self._upper_bound = np.array(options.upper_bound, dtype=np.float64)
         self._lower_bound = np.array(options.lower_bound, dtype=np.float64)
         self._enable_CPIC = options.enable_CPIC
+        self.tape = None  # the differentiable scene's tape (grad_tape.SceneTape), built in build()
         # mpm_solver.py:43-61
         self._particle_volume_real = float(self._particle_size**3)
         self._particle_volume_scale = 1e3
@@ -125,15 +126,24 @@ class MPMSolver:
         b = self._b200
         rigid = list(getattr(self._scene, "_rigid_entities", []))
         colliders = [r._collider(env) for r in rigid for env in range(self._B)]
+        grad = self._sim.requires_grad
+        if grad:
+            from ..materials import MPM
+
+            bad = [type(m).__name__ for m in self.unique_materials if not isinstance(m, (MPM.Elastic, MPM.Muscle))]
+            if bad or rigid:
+                raise GenesisException("A differentiable scene supports MPM.Elastic and MPM.Muscle entities only "
+                                       f"(got {', '.join(bad) or 'rigid colliders'}).")
         self.runtime = MPMRuntime(
             specs,
             device=self._sim.device,
             chunk_particles=b.chunk_particles,
-            sort_interval=b.sort_interval,
+            sort_interval=0 if grad else b.sort_interval,  # the adjoint walks one fixed slot order
             grid_ctas=b.grid_ctas,
-            use_graphs=b.use_cuda_graph,
+            use_graphs=b.use_cuda_graph and not grad,
             colliders=colliders,
             cpic=self._enable_CPIC,  # active only with rigid colliders, as in the reference
+            per_particle_lame=grad,
         )
         for i, r in enumerate(rigid):
             r._bind(self.runtime, [i * self._B + env for env in range(self._B)])
@@ -141,6 +151,14 @@ class MPMSolver:
         mat = np.concatenate([np.full(e.n_particles, e.material.idx, dtype=np.uint8) for e in self._entities])
         act = np.concatenate([np.full(e.n_particles, e.active, dtype=bool) for e in self._entities])
         self.runtime.init_particles(np.tile(pos, (self._B, 1)), np.tile(mat, self._B), active=np.tile(act, self._B))
+        self.tape = None
+        if grad:
+            from .grad_tape import SceneTape
+
+            mu = np.concatenate([np.full(e.n_particles, e.material.mu) for e in self._entities])
+            lam = np.concatenate([np.full(e.n_particles, e.material.lam) for e in self._entities])
+            self.runtime.set_lame(np.tile(mu, self._B), np.tile(lam, self._B))
+            self.tape = SceneTape(self)
         self._build_render_fields()
 
     # ---------------------------------------------------------- render fields
@@ -222,8 +240,12 @@ class MPMSolver:
     def get_state(self, f=None):
         if not self.is_active:
             return None
-        st = self.runtime.get_state()
         B, N = self._B, self.n_particles
+        if self.tape is not None:  # differentiable: a query node of the scene's tape
+            pos, vel, C_, F, Jp = self.tape.query()
+            act = self.runtime.get_state(("active",))["active"].reshape(B, N)
+            return MPMSolverState(self._scene, pos, vel, C_, F, Jp, act)
+        st = self.runtime.get_state()
         return MPMSolverState(
             self._scene,
             st["pos"].reshape(B, N, 3),

@@ -42,10 +42,6 @@ class Scene:
         from ..options import VisOptions
 
         self.vis_options = vis_options or VisOptions()
-        if self.sim_options.requires_grad:
-            raise GenesisException(
-                "requires_grad scenes are served by genesis_b200.grad (checkpointed adjoint); Scene runs forward only."
-            )
         self._other = other_solver_options
         self._sim = Simulator(self, self.sim_options, self.mpm_options, self.b200_options)
         self._entities = []
@@ -147,6 +143,8 @@ class Scene:
             self._sim._cur_substep_global = 0
             if self._sim.mpm_solver.is_active:
                 self._sim.mpm_solver.runtime.reset_colliders()
+                if self._sim.mpm_solver.tape is not None:
+                    self._sim.mpm_solver.tape.reset()  # a new differentiable rollout
 
     def save_checkpoint(self, path):
         st = self.get_state()[0]

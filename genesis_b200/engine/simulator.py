@@ -41,9 +41,12 @@ class Simulator:
     def step(self, in_backward=False):
         """process_input, then `substeps` substeps (simulator.py:268-292)."""
         self.poll_status()
-        self.process_input(in_backward=in_backward)
-        if self.mpm_solver.is_active:
-            self.mpm_solver.advance(self._substeps)
+        if self.mpm_solver.is_active and self.mpm_solver.tape is not None:
+            self.mpm_solver.tape.step()  # inputs, substeps and their checkpoint as one autograd node
+        else:
+            self.process_input(in_backward=in_backward)
+            if self.mpm_solver.is_active:
+                self.mpm_solver.advance(self._substeps)
         self._cur_substep_global += self._substeps
         if self.mpm_solver.is_active and self._b200.check_nan == "step":
             self.mpm_solver.check_state()
