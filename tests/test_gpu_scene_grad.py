@@ -132,3 +132,33 @@ def test_differentiable_scene_limits():
     s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.3), size=(0.1, 0.1, 0.1)), material=gs.materials.MPM.Sand())
     with pytest.raises(gs.GenesisException):
         s2.build()
+
+
+def test_gradients_with_environments():
+    """Two identical environments and one velocity input applied to both: the loss sums the two,
+    so the gradient is twice the one-environment gradient (the tape addresses particles through
+    the environments' runtime ids)."""
+
+    def run(n_envs):
+        gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+        scene = gs.Scene(
+            sim_options=gs.options.SimOptions(dt=DT, substeps=SUB, gravity=(0, 0, -9.8), requires_grad=True),
+            mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
+                                              particle_size=P_SIZE),
+        )
+        ent = scene.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.15), size=(0.08, 0.08, 0.08)),
+                               material=gs.materials.MPM.Elastic(E=2e4))
+        scene.build(n_envs=n_envs)
+        v = torch.tensor([0.3, -0.2, -1.0], device="cuda", requires_grad=True)
+        ent.set_velocity(v)
+        goal = torch.tensor(GOAL, dtype=torch.float32, device="cuda")
+        loss = 0.0
+        for _ in range(4):
+            scene.step()
+            pos = scene.get_state().solvers_state[0].pos  # [B, N, 3]
+            loss = loss + ((pos.mean(1) - goal) ** 2).sum()
+        loss.backward()
+        return v.grad.cpu().numpy()
+
+    g1, g2 = run(0), run(2)
+    assert np.allclose(g2, 2 * g1, rtol=1e-4, atol=1e-9), (g1, g2)
