@@ -22,6 +22,8 @@ from . import materials, morphs, options, surfaces
 from .engine.emitter import Emitter
 from .engine.scene import Scene
 from .exceptions import GenesisException
+from .creation_ops import *  # noqa: F401,F403  gs.tensor, gs.zeros, ... (genesis/grad/creation_ops.py)
+from .creation_ops import from_torch
 
 __version__ = "0.1.0"
 

@@ -59,7 +59,7 @@ def test_position_and_velocity_inputs_with_a_trajectory_loss():
     mat_kw = dict(E=2e4, nu=0.3, rho=1000.0)
     scene, ent = _scene(gs.materials.MPM.Elastic(**mat_kw))
     offsets = ent.init_particles - np.asarray(ent.morph.pos)
-    pos = torch.tensor([0.5, 0.5, 0.15], device="cuda", requires_grad=True)
+    pos = gs.tensor([0.5, 0.5, 0.15], requires_grad=True)  # as the reference's scripts create inputs
     v0 = torch.tensor([0.3, -0.2, -1.0], device="cuda", requires_grad=True)
     v3 = torch.tensor([-0.4, 0.1, 0.5], device="cuda", requires_grad=True)
     ent.set_position(pos)
