@@ -162,3 +162,27 @@ def test_gradients_with_environments():
 
     g1, g2 = run(0), run(2)
     assert np.allclose(g2, 2 * g1, rtol=1e-4, atol=1e-9), (g1, g2)
+
+
+def test_reset_between_optimisation_iterations():
+    """forward, backward, scene.reset(), forward, backward (an optimisation loop): the second
+    iteration with the same input gives the same gradient, and a changed input a different one."""
+    scene, ent = _scene(gs.materials.MPM.Elastic(E=2e4))
+    goal = torch.tensor(GOAL, dtype=torch.float32, device="cuda")
+
+    def iteration(v):
+        vv = gs.tensor(v, requires_grad=True)
+        ent.set_velocity(vv)
+        loss = 0.0
+        for _ in range(3):
+            scene.step()
+            loss = loss + ((ent.get_particles_pos().mean(0) - goal) ** 2).sum()
+        loss.backward()
+        scene.reset()
+        return vv.grad.cpu().numpy(), float(loss.detach())
+
+    g1, l1 = iteration([0.2, 0.0, -0.5])
+    g2, l2 = iteration([0.2, 0.0, -0.5])
+    g3, _ = iteration([0.0, 0.4, 0.5])
+    assert np.allclose(g1, g2, rtol=1e-5, atol=1e-9) and abs(l1 - l2) <= 1e-6 * l1
+    assert not np.allclose(g1, g3, rtol=1e-3)
