@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--sort-interval", type=int, default=50)
     ap.add_argument("--chunk", type=int, default=128)
     ap.add_argument("--n-side", type=int, default=50, help="particles per box edge (50 -> 500k)")
+    ap.add_argument("--grid-density", type=int, default=128,
+                    help="grid nodes per metre (128 -> 129^3; with --n-side 100 / 200, 256 / 512 keep the "
+                         "particles per cell of the default scene)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential comparison")
     ap.add_argument("--batch-scenes", type=int, default=256)
@@ -85,6 +88,15 @@ def peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def workload_name(args, d):
+    """The default scene's name, or the same mix at another size."""
+    if args.n_side == 50 and args.grid_density == 128:
+        return WORKLOAD
+    return (f"mixed_{d.n_particles}: 4 x {d.n_particles // 4:,} particles (Liquid, Sand, Snow, ElastoPlastic), "
+            f"grid_density {args.grid_density} ({d.grid_res}^3 nodes), dt 5e-5, {args.substeps_per_step} "
+            "substeps per step")
 
 
 def ncu_traffic():
@@ -266,7 +278,7 @@ def run_reference(args, world, rank):
     from genesis_b200 import workloads as W
     from oracle import bridge, cref
 
-    d = W.mixed_500k(n_side=args.n_side)
+    d = W.mixed_500k(n_side=args.n_side, grid_density=args.grid_density)
     threads = os.cpu_count() or 1
     p, mats, st = bridge.from_desc(d, np.float32)
     sub = 2  # substeps per reference step: a bounded sample of the 100-substep step
@@ -294,7 +306,7 @@ def run_reference(args, world, rank):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": d.n_particles, "grid": "129^3",
+        "config": {"workload": workload_name(args, d), "particles": d.n_particles, "grid": f"{d.grid_res}^3",
                    "substeps_per_step": sub, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -441,7 +453,7 @@ def run_ours(args, world, rank, local):
     from genesis_b200.engine.runtime import runtime_from_descs
 
     S = args.substeps_per_step
-    d = W.mixed_500k(n_side=args.n_side)
+    d = W.mixed_500k(n_side=args.n_side, grid_density=args.grid_density)
     rt = runtime_from_descs([d], sort_interval=args.sort_interval, chunk_particles=args.chunk)
     for _ in range(args.warmup):
         rt.substeps(S)
@@ -480,7 +492,8 @@ def run_ours(args, world, rank, local):
     t_dom = kb[dom][0] * 1e-3
     achieved = alg / t_dom / 1e9
     tr = ncu_traffic()
-    traffic = tr.get(f"{dom}_dram_bytes_per_launch")
+    # the committed ncu figure is the default scene's; other sizes report none
+    traffic = tr.get(f"{dom}_dram_bytes_per_launch") if workload_name(args, d) == WORKLOAD else None
     nsub = 3 * args.sort_interval
     sub_ms = sum(kb[k][0] * kb[k][1] for k in kb) / nsub
     sub_alg = SUBSTEP_BYTES[0] * d.n_particles + SUBSTEP_BYTES[1] * n_act
@@ -503,9 +516,9 @@ def run_ours(args, world, rank, local):
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": WORKLOAD,
+            "workload": workload_name(args, d),
             "particles": d.n_particles,
-            "grid": "129^3",
+            "grid": f"{d.grid_res}^3",
             "substeps_per_step": S,
             "sort_interval": args.sort_interval,
             "chunk_particles": args.chunk,
