@@ -479,6 +479,16 @@ class MPMEntity:
         idx = torch.argmin(torch.linalg.norm(cur - p[:, None], dim=-1), dim=-1).to(torch.int32)
         return idx[0] if self._scene.n_envs == 0 else idx
 
+    def get_frame(self, f, pos, vel, C, F, Jp, active):
+        """Copy the entity's state into the given tensors (mpm_entity.py:293-340): pos/vel
+        [B, n, 3], C/F [B, n, 3, 3], Jp/active [B, n].  Only the current frame is kept here, so
+        f must be the current local substep (sim.cur_substep_local)."""
+        if int(f) != self._sim.cur_substep_local:
+            raise GenesisException(f"Only the current frame ({self._sim.cur_substep_local}) is kept, not {f}.")
+        st = self._get(("pos", "vel", "C", "F", "Jp", "active"), None)
+        for dst, key in ((pos, "pos"), (vel, "vel"), (C, "C"), (F, "F"), (Jp, "Jp"), (active, "active")):
+            dst.copy_(st[key].to(dst.device, dst.dtype).reshape(dst.shape))
+
     def get_state(self):
         st = self._get(("pos", "vel", "C", "F", "Jp", "active"), None)
         return MPMEntityState(self, self._sim.cur_step_global, st["pos"], st["vel"], st["C"], st["F"], st["Jp"],

@@ -239,3 +239,16 @@ def test_mesh_set_entity(tmp_path):
     dz = (e.get_particles_pos()[:, 2] - z0).cpu().numpy()
     assert dz[g == 0].mean() < 0 and dz[g == 1].mean() < 0
     assert e.n_vverts == 16
+
+
+def test_get_frame_fills_given_tensors():
+    scene, cube, sand = _scene(substeps=5)
+    scene.step()
+    B, n = 1, cube.n_particles
+    bufs = [torch.zeros(B, n, 3), torch.zeros(B, n, 3), torch.zeros(B, n, 3, 3), torch.zeros(B, n, 3, 3),
+            torch.zeros(B, n), torch.zeros(B, n, dtype=torch.bool)]
+    cube.get_frame(scene.sim.cur_substep_local, *bufs)
+    st = cube.get_state()
+    assert torch.equal(bufs[0], st.pos.cpu()) and torch.equal(bufs[3], st.F.cpu()) and bool(bufs[5].all())
+    with pytest.raises(gs.GenesisException):
+        cube.get_frame(scene.sim.cur_substep_local + 1, *bufs)
