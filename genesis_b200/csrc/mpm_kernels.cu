@@ -38,7 +38,7 @@ namespace gbm {
 
 // resident threads per SM the register allocation of p2g / g2p2g is sized for
 #ifndef GBM_P2G_THREADS_PER_SM
-#define GBM_P2G_THREADS_PER_SM 768
+#define GBM_P2G_THREADS_PER_SM 896
 #endif
 // unroll factor of the outermost stencil loops (3: fully unrolled, 1: rolled, smaller code)
 #ifndef GBM_OUTER_UNROLL
