@@ -57,6 +57,8 @@ class Scene:
     def add_entity(self, morph, material=None, surface=None, visualize_contact=False, vis_mode=None):
         if self._is_built:
             raise GenesisException("Scene is already built.")
+        if material is None:  # scene.py:355-356: a Rigid entity by default
+            material = _materials.Rigid()
         if isinstance(material, _materials.Rigid):
             from .rigid import KinematicRigidEntity
 

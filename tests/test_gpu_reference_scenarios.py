@@ -1,0 +1,68 @@
+"""The reference's own MPM test scenarios run through this package, with their assertions
+(the parts that involve only MPM and rigid colliders; the PBD cloth, SPH water and FEM box of
+the same scenes belong to other solvers)."""
+
+import numpy as np
+import pytest
+import torch
+
+import genesis_b200 as gs
+
+pytestmark = pytest.mark.gpu
+
+
+def test_deformable_parallel_mpm_cube():
+    """tests/test_deformable_physics.py:110-222 (test_deformable_parallel), its MPM cube: an
+    Elastic cube (rho 200) dropped on a frictionless coupled ground plane in two environments,
+    1,500 steps of 10 substeps; it moves, stays above the ground and comes to rest."""
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=2e-3, substeps=10),
+        mpm_options=gs.options.MPMOptions(lower_bound=(0.5, -0.1, -0.05), upper_bound=(0.7, 0.1, 0.3)),
+    )
+    scene.add_entity(morph=gs.morphs.Plane(), material=gs.materials.Rigid(needs_coup=True, coup_friction=0.0))
+    cube = scene.add_entity(morph=gs.morphs.Box(pos=(0.6, 0.0, 0.1), size=(0.1, 0.1, 0.1)),
+                            material=gs.materials.MPM.Elastic(rho=200),
+                            surface=gs.surfaces.Default(color=(0.9, 0.8, 0.2, 1.0)))
+    scene.build(n_envs=2)
+    init = cube.get_particles_pos().clone()
+    scene.get_state()
+    for _ in range(1500):
+        scene.step()
+    final = cube.get_particles_pos()
+    assert float((init - final).abs().sum()) > 0.1
+    assert float(final[..., 2].min()) > -1e-5
+    vel = cube.get_particles_vel()
+    print(f"\n[reference scenario] max |v| after 1500 steps: {float(vel.abs().max()):.2e}")
+    assert torch.allclose(vel, torch.zeros_like(vel), atol=1e-4)
+
+
+@pytest.mark.parametrize("material_type", [gs.materials.MPM.Liquid, gs.materials.MPM.Sand, gs.materials.MPM.Snow,
+                                           gs.materials.MPM.Elastic])
+def test_fluid_emitter_mpm(material_type):
+    """tests/test_hybrid.py:86-154 (test_fluid_emitter) with its MPM materials and two
+    environments: a ground plane added without a material (a Rigid entity by default), an
+    emitter of 5,000 particles, emit_omni, then five circular droplets with a step after each.
+    The reference asserts only that this runs; here the emitted particles also stay finite and
+    inside the domain."""
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=4e-3, substeps=10),
+        mpm_options=gs.options.MPMOptions(lower_bound=(0.0, -1.5, 0.0), upper_bound=(1.0, 1.5, 4.0)),
+    )
+    scene.add_entity(gs.morphs.Plane())
+    emitter = scene.add_emitter(material=material_type(), max_particles=5000,
+                                surface=gs.surfaces.Glass(color=(0.7, 0.85, 1.0, 0.7)))
+    scene.build(n_envs=2)
+    emitter.emit_omni()
+    for _ in range(5):
+        emitter.emit(droplet_shape="circle", droplet_size=0.25)
+        scene.step()
+    scene.step()
+    ent = emitter.entity
+    act = ent.get_particles_active()
+    pos = ent.get_particles_pos()
+    assert act.shape[0] == 2 and int(act[0].sum()) > 0 and torch.equal(act[0], act[1])
+    live = pos[act]
+    assert bool(torch.isfinite(live).all())
+    assert float(live[:, 2].min()) >= 0.0 and float(live[:, 0].max()) <= 1.0
