@@ -66,3 +66,37 @@ def test_fluid_emitter_mpm(material_type):
     live = pos[act]
     assert bool(torch.isfinite(live).all())
     assert float(live[:, 2].min()) >= 0.0 and float(live[:, 0].max()) <= 1.0
+
+
+def _legacy_coupling(substeps):
+    substep_dt, horizon_substeps = 4e-4, 100
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=substep_dt * substeps, substeps=substeps),
+        mpm_options=gs.options.MPMOptions(lower_bound=(-0.5, -1.0, 0.0), upper_bound=(0.5, 1.0, 1)),
+    )
+    scene.add_entity(morph=gs.morphs.Plane())
+    box = scene.add_entity(material=gs.materials.Rigid(rho=1.0), morph=gs.morphs.Box(pos=(0.0, -0.25, 0.1),
+                                                                                     size=(0.2, 0.2, 0.2)))
+    liquid = scene.add_entity(material=gs.materials.MPM.Liquid(), morph=gs.morphs.Box(pos=(0.0, 0.0, 0.2),
+                                                                                      size=(0.3, 0.3, 0.3)))
+    scene.build()
+    impulse = torch.zeros(3, device="cuda")
+    for _ in range(horizon_substeps // substeps):
+        scene.step()
+        impulse += box.get_coupling_force()[:3] * substep_dt * substeps  # mean force over the step x its time
+    return liquid.get_particles_pos(), impulse.cpu().numpy()
+
+
+def test_rigid_mpm_legacy_coupling():
+    """tests/test_hybrid.py:285-360 (test_rigid_mpm_legacy_coupling) for a kinematic box: the
+    reference checks that the liquid pushes the box along -y and that the result does not depend
+    on how the same substep dt is grouped into steps.  The box here does not move (no rigid
+    dynamics), so the push is read as the impulse the liquid gave it, and the grouping check is
+    made on the liquid's particles and that impulse."""
+    p1, j1 = _legacy_coupling(1)
+    p10, j10 = _legacy_coupling(10)
+    print(f"\n[reference scenario] impulse on the box: substeps 1 {j1}, substeps 10 {j10}")
+    assert j1[1] < 0 and j10[1] < 0  # pushed along -y
+    assert torch.allclose(p1, p10, atol=1e-5)
+    assert np.allclose(j1, j10, rtol=1e-3, atol=1e-6)
