@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from . import _globals
-from . import materials, morphs, options, surfaces
+from . import materials, morphs, options, surfaces, textures
 from .engine.emitter import Emitter
 from .engine.scene import Scene
 from .exceptions import GenesisException
@@ -77,4 +77,4 @@ def destroy():
 EPS = _globals.EPS
 device = None
 
-__all__ = ["init", "destroy", "Scene", "Emitter", "GenesisException", "materials", "morphs", "options", "surfaces", "gpu", "cpu", "cuda"]
+__all__ = ["init", "destroy", "Scene", "Emitter", "GenesisException", "materials", "morphs", "options", "surfaces", "textures", "gpu", "cpu", "cuda"]

@@ -278,6 +278,19 @@ class MPMEntity:
     def _tape(self):
         return getattr(self._solver, "tape", None) if self._scene.requires_grad else None
 
+    def _actu_groups(self, a, n_envs, n):
+        """Per-group actuation values of shape ([M,] [n_particles,] [n_groups,]) broadcast to
+        [n_envs, n, n_groups] (mpm_entity.py:412-451): a 2-D value is per environment when
+        the scene is batched and its first dimension matches the environments, else per
+        particle."""
+        G = self._material.n_groups
+        if a.ndim == 0:
+            a = a.reshape(1).expand(G)
+        a = a.reshape(a.shape[:-1] + (G,))
+        if a.ndim == 2 and self._scene.n_envs > 0 and a.shape[0] == n_envs and a.shape[0] != n:
+            a = a[:, None, :]
+        return a.expand(n_envs, n, G)
+
     def _input_map(self, kind, value, envs_idx):
         """What a set_position / set_velocity / set_actuation value writes, per environment and
         particle (differentiable in value): positions / velocities [n_envs, n, 3], actuation
@@ -291,9 +304,7 @@ class MPMEntity:
             return v.expand(n_envs, n, 3)
         if kind == "vel":
             return value.expand(n_envs, n, 3)
-        G = self._material.n_groups
-        a = value.reshape(value.shape[:-1] + (G,)) if value.ndim else value.reshape(1).expand(G)
-        a = a.expand(n_envs, n, G)
+        a = self._actu_groups(value, n_envs, n)
         idx = self._flat_idx(None, envs_idx)
         grp = self._solver.runtime.muscle_group[idx.reshape(-1)].reshape(n_envs, n, 1)
         return torch.gather(a, 2, grp).squeeze(2)
@@ -372,8 +383,7 @@ class MPMEntity:
         idx = self._flat_idx(particles_idx_local, envs_idx)
         G = self._material.n_groups
         a = _as_tensor(actus, torch.float32, self._solver.device)
-        a = a.reshape(a.shape[:-1] + (G,)) if a.ndim else a.reshape(1).expand(G)
-        a = a.expand(idx.shape + (G,)).reshape(-1, G)
+        a = self._actu_groups(a, idx.shape[0], idx.shape[1]).reshape(-1, G)
         self._solver.runtime.set_actu_by_group(idx.reshape(-1), a)
 
     def get_particles_actu(self, envs_idx=None):

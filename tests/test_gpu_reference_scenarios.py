@@ -100,3 +100,59 @@ def test_rigid_mpm_legacy_coupling():
     assert j1[1] < 0 and j10[1] < 0  # pushed along -y
     assert torch.allclose(p1, p10, atol=1e-5)
     assert np.allclose(j1, j10, rtol=1e-3, atol=1e-6)
+
+
+@pytest.mark.parametrize("n_envs", [0, 2])
+def test_muscle_worm(n_envs, tmp_path):
+    """tests/test_deformable_physics.py:15-107 (test_muscle) with MPM.Muscle: a worm on a
+    high-friction coupled plane, four muscle groups (upper/lower x fore/hind) along +y, 200
+    steps with the hind-lower group actuated sinusoidally.  The reference's worm mesh is an
+    asset file; an elongated ellipsoid of the same footprint written by the test stands in.
+    The reference only runs it; here the worm also stays finite and above the plane, and its
+    actuated groups move relative to an unactuated copy."""
+    from genesis_b200 import mesh
+
+    v, f = mesh.icosphere(3, 1.0)
+    v = v * np.array([0.6, 2.0, 0.5])  # scaled by 0.1 below: 0.12 x 0.4 x 0.1 m
+    obj = tmp_path / "worm.obj"
+    obj.write_text("".join(f"v {a} {b} {c}\n" for a, b, c in v) + "".join(f"f {i+1} {j+1} {k+1}\n" for i, j, k in f))
+
+    def run(actuate):
+        gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+        scene = gs.Scene(
+            sim_options=gs.options.SimOptions(dt=5e-4, substeps=10, gravity=(0, 0, -9.8)),
+            mpm_options=gs.options.MPMOptions(lower_bound=(-1.0, -1.0, -0.2), upper_bound=(1.0, 1.0, 1.0)),
+        )
+        scene.add_entity(morph=gs.morphs.Plane(), material=gs.materials.Rigid(coup_friction=5.0))
+        worm = scene.add_entity(
+            morph=gs.morphs.Mesh(file=str(obj), pos=(0.3, 0.3, 0.051), scale=0.1),
+            material=gs.materials.MPM.Muscle(E=5e5, nu=0.45, rho=10000.0, n_groups=4),
+            surface=gs.surfaces.Default(diffuse_texture=gs.textures.ImageTexture(image_path="worm.png")),
+        )
+        scene.build(n_envs=n_envs) if n_envs > 0 else scene.build()
+        pos = worm.get_state().pos[0].cpu().numpy()
+        n_units = worm.n_particles
+        pmax, pmin = pos.max(0), pos.min(0)
+        rng_ = pmax - pmin
+        upper = pos[:, 2] > pmin[2] + rng_[2] * 0.3
+        fore = pos[:, 1] < pmin[1] + rng_[1] * 0.6
+        group = np.zeros(n_units, dtype=int)
+        group[upper & ~fore] = 1
+        group[~upper & fore] = 2
+        group[~upper & ~fore] = 3
+        worm.set_muscle(muscle_group=group, muscle_direction=np.array([[0.0, 1.0, 0.0]] * n_units, dtype=np.float32))
+        scene.reset()
+        for i in range(200):
+            a = np.array([0.0, 0.0, 0.0, (1.0 * (0.5 + np.sin(0.005 * np.pi * i))) if actuate else 0.0])
+            worm.set_actuation(np.tile(a, (n_envs, 1)) if n_envs > 1 else a)
+            scene.step()
+        return worm.get_particles_pos(), group
+
+    p_act, group = run(True)
+    p_rest, _ = run(False)
+    p_act = p_act if n_envs == 0 else p_act[0]
+    p_rest = p_rest if n_envs == 0 else p_rest[0]
+    assert bool(torch.isfinite(p_act).all()) and float(p_act[:, 2].min()) > -1e-5
+    moved = (p_act - p_rest).norm(dim=1).cpu().numpy()
+    print(f"\n[reference scenario] worm: mean displacement by actuation, group 3 {moved[group == 3].mean():.2e} m")
+    assert moved[group == 3].mean() > 1e-4
