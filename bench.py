@@ -408,7 +408,7 @@ def run_e2e(d, S, K, W_):
     import torch
 
     scene = build_scene(d, S, check_nan="async")
-    st = scene.get_state()[0]
+    st = scene.get_state()[3]
     host = {k: getattr(st, k).cpu().pin_memory() for k in ("pos", "vel", "C", "F", "Jp", "active")}
     from genesis_b200.engine.states import MPMSolverState
 
@@ -423,7 +423,7 @@ def run_e2e(d, S, K, W_):
         s = MPMSolverState(scene, host["pos"], host["vel"], host["C"], host["F"], host["Jp"], host["active"])
         scene.reset(s)
         scene.step()
-        cur = scene.get_state()[0]
+        cur = scene.get_state()[3]
         d2h_stream.wait_stream(main)
         with torch.cuda.stream(d2h_stream):
             out_pos.copy_(cur.pos, non_blocking=True)

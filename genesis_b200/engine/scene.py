@@ -11,7 +11,7 @@ from .. import materials as _materials
 from ..exceptions import GenesisException
 from ..options import B200Options, LegacyCouplerOptions, MPMOptions, SimOptions
 from .simulator import Simulator
-from .states import SimState
+from .states import MPM_INDEX, SimState
 
 log = logging.getLogger("genesis_b200")
 
@@ -136,7 +136,7 @@ class Scene:
         if state is None:
             state = self._init_state
         if state is not None:
-            mpm_state = state.solvers_state[0] if isinstance(state, SimState) else state
+            mpm_state = state.solvers_state[MPM_INDEX] if isinstance(state, SimState) else state
             self._sim.mpm_solver.set_state(0, mpm_state, envs_idx=envs_idx)
         self._sim._queried_states.clear()  # simulator.py:227, 238
         for emitter in self._emitters:  # scene.py:893-895
@@ -149,7 +149,7 @@ class Scene:
                     self._sim.mpm_solver.tape.reset()  # a new differentiable rollout
 
     def save_checkpoint(self, path):
-        st = self.get_state()[0]
+        st = self.get_state()[MPM_INDEX]
         torch.save({k: getattr(st, k).cpu() for k in ("pos", "vel", "C", "F", "Jp", "active")} |
                    {"cur_substep_global": self._sim.cur_substep_global}, path)
 

@@ -8,7 +8,7 @@ from .. import _globals
 from .. import _native as nat
 from ..exceptions import GenesisException
 from .mpm_solver import NAN_MESSAGE, LegacyCoupler, MPMSolver
-from .states import SimState
+from .states import MPM_INDEX, SOLVER_NAMES, SimState
 
 
 class Simulator:
@@ -89,7 +89,9 @@ class Simulator:
 
     def get_state(self):
         self.poll_status()
-        state = SimState(self._scene, self.cur_step_global, [self.mpm_solver.get_state(self.cur_substep_local)])
+        slots = [None] * len(SOLVER_NAMES)
+        slots[MPM_INDEX] = self.mpm_solver.get_state(self.cur_substep_local)
+        state = SimState(self._scene, self.cur_step_global, slots)
         self._queried_states.append(state)
         return state
 

@@ -61,8 +61,15 @@ class MPMEntityState(MPMSolverState):
         return self._s_global
 
 
+# the reference's solver order (simulator.py:129-140): a scene's state has one entry per solver,
+# None for the solvers that are not active; only the MPM solver exists here
+SOLVER_NAMES = ("tool", "rigid", "avatar", "mpm", "sph", "pbd", "fem", "sf")
+MPM_INDEX = SOLVER_NAMES.index("mpm")
+
+
 class SimState:
-    """Scene-level state: one entry per solver; only the MPM solver exists here (states/solvers.py:5-45)."""
+    """Scene-level state: one entry per solver, in the reference's order, so the MPM state is
+    solvers_state[3] as scripts written for the reference index it (states/solvers.py:5-45)."""
 
     def __init__(self, scene, s_global, solvers_state):
         self._scene = scene

@@ -65,7 +65,7 @@ def test_scene_with_emitted_particles_matches_oracle():
         # a sphere ignores the droplet length, but a positive one is needed to emit at all
         em.emit("sphere", 0.08, droplet_length=0.08, pos=(0.6, 0.55, 0.5), speed=1.0, direction=(1, 0, -1))
         scene.step()
-    s0 = scene.get_state()[0]
+    s0 = scene.get_state()[3]
     host = {k: getattr(s0, k)[0].cpu().numpy() for k in ("pos", "vel", "C", "F", "Jp", "active")}
     n_sand = sand.n_particles
     mat = np.concatenate([np.zeros(n_sand, np.int64), np.ones(em.entity.n_particles, np.int64)])
@@ -77,7 +77,7 @@ def test_scene_with_emitted_particles_matches_oracle():
     o, rc = cref.substeps(p, mats, st, 10)
     assert rc == 0
     scene.step()
-    g = scene.get_state()[0]
+    g = scene.get_state()[3]
     gx = g.pos[0].cpu().numpy()
     act = host["active"].astype(bool)
     assert act.sum() > n_sand

@@ -34,7 +34,7 @@ def test_render_fields_match_host_arithmetic():
         scene.step()
     solver = scene.sim.mpm_solver
     solver.update_render_fields()
-    st = scene.get_state()[0]
+    st = scene.get_state()[3]
     pos, vel, act = st.pos.cpu().numpy(), st.vel.cpu().numpy(), st.active.cpu().numpy()
     pr = {k: v.cpu().numpy() for k, v in solver.particles_render.items()}
     nowhere = np.array([2333333.0, 6666666.0, 5201314.0], dtype=np.float32)

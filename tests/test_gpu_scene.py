@@ -36,7 +36,7 @@ def test_scene_step_state_shapes_and_fall():
     for _ in range(3):
         scene.step()
     st = scene.get_state()
-    s = st.solvers_state[0]
+    s = st.solvers_state[3]
     assert s.pos.shape == (1, N, 3) and s.F.shape == (1, N, 3, 3) and s.Jp.shape == (1, N)
     assert s.active.dtype == torch.bool and bool(s.active.all())
     p1 = cube.get_particles_pos()
@@ -50,12 +50,12 @@ def test_envs_identical_and_reset():
     s0 = scene.get_state()
     for _ in range(2):
         scene.step()
-    s = scene.get_state()[0]
+    s = scene.get_state()[3]
     assert s.pos.shape[0] == 3
     assert torch.allclose(s.pos[0], s.pos[1], atol=1e-6) and torch.allclose(s.pos[0], s.pos[2], atol=1e-6)
     scene.reset()
-    r = scene.get_state()[0]
-    assert torch.equal(r.pos, s0[0].pos.to(r.pos.device))
+    r = scene.get_state()[3]
+    assert torch.equal(r.pos, s0[3].pos.to(r.pos.device))
 
 
 def test_plugin_substeps_match_fused_step():
@@ -65,7 +65,7 @@ def test_plugin_substeps_match_fused_step():
     for f in range(10):
         a.sim.substep(0)
     b.step()
-    pa, pb = a.get_state()[0].pos, b.get_state()[0].pos
+    pa, pb = a.get_state()[3].pos, b.get_state()[3].pos
     assert torch.allclose(pa, pb, atol=1e-6)
 
 
@@ -88,7 +88,7 @@ def test_entity_active_mask():
 
 
 def _host_state(scene, pinned):
-    st = scene.get_state()[0]
+    st = scene.get_state()[3]
     out = {k: getattr(st, k).cpu() for k in ("pos", "vel", "C", "F", "Jp", "active")}
     return {k: (v.pin_memory() if pinned else v) for k, v in out.items()}
 
@@ -108,7 +108,7 @@ def test_staged_upload_matches_synchronous_upload():
         for _ in range(2):  # twice in a row: the staging buffer is reused
             scene.reset(MPMSolverState(scene, h["pos"], h["vel"], h["C"], h["F"], h["Jp"], h["active"]))
             scene.step()
-        res.append(scene.get_state()[0].pos.clone())
+        res.append(scene.get_state()[3].pos.clone())
     assert torch.equal(res[0], res[1])
 
 

@@ -70,7 +70,7 @@ def test_position_and_velocity_inputs_with_a_trajectory_loss():
         if s == 3:
             ent.set_velocity(v3)  # an input in the middle of the rollout
         scene.step()
-        st = scene.get_state().solvers_state[0]
+        st = scene.get_state().solvers_state[3]
         loss = loss + ((st.pos[0].mean(0) - goal) ** 2).sum()
     loss.backward()
     vals = {"pos": pos.detach().cpu().numpy().astype(np.float64), "v0": v0.detach().cpu().numpy().astype(np.float64),
@@ -155,7 +155,7 @@ def test_gradients_with_environments():
         loss = 0.0
         for _ in range(4):
             scene.step()
-            pos = scene.get_state().solvers_state[0].pos  # [B, N, 3]
+            pos = scene.get_state().solvers_state[3].pos  # [B, N, 3]
             loss = loss + ((pos.mean(1) - goal) ** 2).sum()
         loss.backward()
         return v.grad.cpu().numpy()
