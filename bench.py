@@ -71,13 +71,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential comparison")
     ap.add_argument("--batch-scenes", type=int, default=256)
-    ap.add_argument("--batch-substeps", type=int, default=100)
+    ap.add_argument("--batch-substeps", type=int, default=500, help="substeps per scene (500 = the batching config)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
     ap.add_argument("--no-grad", action="store_true", help="skip the differentiation run")
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests in the Poisson stream (2000 = the full serving config)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--profile-run", action="store_true", help="short run for ncu launch lists")
     return ap.parse_args()
 
 
@@ -576,8 +575,8 @@ def run_batched(args, world, rank):
     b.record()
     torch.cuda.synchronize()
     t_b = reduce_max(world, a.elapsed_time(b) * 1e-3)
-    n_local = bs.n_particles
     status = bs.rt.status()
+    split = kernel_breakdown(bs.rt, n_substeps=2 * K)
     del bs
     torch.cuda.empty_cache()
     t_s = reduce_max(world, run_sequential(descs, S))
@@ -592,6 +591,7 @@ def run_batched(args, world, rank):
         "sequential_value": n_total * S / t_s,
         "speedup_vs_sequential": t_s / t_b,
         "tuning": tuning,
+        "kernel_ms": {k: round(v[0], 5) for k, v in split.items()},
         "status_word": status,
     }
 
