@@ -108,3 +108,25 @@ def test_rigid_material_and_plane_follow_reference():
     q = np.array([0.9, 0.1, -0.3, 0.2])
     q /= np.linalg.norm(q)
     assert np.allclose(R_to_quat(quat_to_R(q)), q)
+
+
+def test_sim_state_solver_order():
+    """A scene's state holds one entry per solver in the reference's order
+    (simulator.py:129-140), so scripts find the MPM state at solvers_state[3]."""
+    import torch
+
+    from genesis_b200.engine.states import MPM_INDEX, SOLVER_NAMES, MPMSolverState, SimState
+
+    assert SOLVER_NAMES == ("tool", "rigid", "avatar", "mpm", "sph", "pbd", "fem", "sf")
+    assert MPM_INDEX == 3
+    z = torch.zeros
+    mpm = MPMSolverState(None, z(1, 2, 3), z(1, 2, 3), z(1, 2, 3, 3), z(1, 2, 3, 3), z(1, 2), torch.ones(1, 2, dtype=torch.bool))
+    slots = [None] * len(SOLVER_NAMES)
+    slots[MPM_INDEX] = mpm
+    s = SimState(None, 7, slots)
+    assert s.solvers_state[3] is mpm and s[3] is mpm
+    assert [i for i, st in enumerate(s) if st is not None] == [3]
+    assert s.s_global == 7
+    assert bool((s.solvers_state[3].active == 1).all())
+    s.serializable()
+    assert s.scene is None
