@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -137,10 +137,11 @@ class Tables(C.Structure):
         ("n_colliders", C.c_int32),
         ("pad0", C.c_int32),
         ("collider_force", C.c_void_p),
+        ("sdf_voxels", C.c_void_p),
     ]
 
 
-COLLIDER_SPHERE, COLLIDER_PLANE, COLLIDER_BOX = 0, 1, 2
+COLLIDER_SPHERE, COLLIDER_PLANE, COLLIDER_BOX, COLLIDER_TOOL = 0, 1, 2, 3
 
 
 class Collider(C.Structure):
@@ -155,6 +156,11 @@ class Collider(C.Structure):
         ("friction", C.c_float),
         ("softness", C.c_float),
         ("restitution", C.c_float),
+        ("sdf_res", C.c_int32),
+        ("sdf_pad", C.c_int32),
+        ("sdf_offset", C.c_int64),
+        ("sdf_scale", C.c_float * 3),
+        ("floor", C.c_float),
     ]
 
 
@@ -193,6 +199,7 @@ SIGNATURES = {
     "mpm_set_particles_free": (C.c_int, [_P(Problem), _P(Particles), i32, vp, vp, vp]),
     "mpm_update_render_fields": (C.c_int, [_P(Problem), _P(Particles), i32, i32, vp, vp, vp, i32, i32, vp, vp, vp,
                                            vp, vp]),
+    "mpm_sdf_voxelize": (C.c_int, [vp, i32, vp, i32, i32, C.c_float, vp, vp]),
     "mpm_graph_create": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp, _P(vp)]),
     "mpm_graph_launch": (C.c_int, [vp, vp]),
     "mpm_graph_destroy": (C.c_int, [vp]),

@@ -648,6 +648,116 @@ __device__ __forceinline__ void collide_rigid(const mpm_collider& c, float eps, 
     rigid_respond(c, eps, dt, mass, q, n, influence, v, fout);
 }
 
+// ---------------------------------------------------------------- tool entities
+// engine/entities/tool_entity/mesh.py:80-176 (Tool.collide), coupled by
+// legacy_coupler.py:346-350 before the rigid geoms.
+
+// E = exp([w] dt) (Rodrigues), the rotation of one substep at angular velocity w; the
+// quaternion product of tool_entity.py:183-186 and the rigid colliders' motion are this
+// rotation applied in the world frame (E R)
+__device__ __forceinline__ void rot_step(const float* w, float dt, float* E) {
+    const float wx = w[0] * dt, wy = w[1] * dt, wz = w[2] * dt;
+    const float th = sqrtf(wx * wx + wy * wy + wz * wz);
+    if (!(th > 0.f)) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) E[k] = (k % 4 == 0) ? 1.f : 0.f;
+        return;
+    }
+    const float kx = wx / th, ky = wy / th, kz = wz / th, s = sinf(th), c = cosf(th), t = 1.f - c;
+    E[0] = c + t * kx * kx;
+    E[1] = t * kx * ky - s * kz;
+    E[2] = t * kx * kz + s * ky;
+    E[3] = t * kx * ky + s * kz;
+    E[4] = c + t * ky * ky;
+    E[5] = t * ky * kz - s * kx;
+    E[6] = t * kx * kz - s * ky;
+    E[7] = t * ky * kz + s * kx;
+    E[8] = c + t * kz * kz;
+}
+
+// mesh.py:89-104: trilinear sample of the voxel grid at voxel coordinate pv; 1 outside it
+__device__ __forceinline__ float tool_sdf_at(const float* __restrict__ vox, int res, const float* pv) {
+    const float f0 = floorf(pv[0]), f1 = floorf(pv[1]), f2 = floorf(pv[2]);
+    if (!(f0 >= 0.f && f1 >= 0.f && f2 >= 0.f && f0 < (float)(res - 1) && f1 < (float)(res - 1) &&
+          f2 < (float)(res - 1)))
+        return 1.f;
+    const int b0 = (int)f0, b1 = (int)f1, b2 = (int)f2;
+    float sd = 0.f;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+        const float w = (1.f - fabsf(pv[0] - (float)(b0 + i))) * (1.f - fabsf(pv[1] - (float)(b1 + j))) *
+                        (1.f - fabsf(pv[2] - (float)(b2 + k)));
+        sd += w * vox[((int64_t)(b0 + i) * res + (b1 + j)) * res + (b2 + k)];
+    }
+    return sd;
+}
+
+// Tool.collide for a grid node at p with velocity v (mesh.py:147-176)
+__device__ __forceinline__ void collide_tool(const mpm_collider& c, const float* __restrict__ sdf_voxels, float eps,
+                                             float dt, const float* p, float* v) {
+    if (!sdf_voxels || c.sdf_res < 2) return;
+    const float q[3] = {p[0] - c.pos[0], p[1] - c.pos[1], p[2] - c.pos[2]};
+    const float half = 0.5f * (float)(c.sdf_res - 1);
+    float pv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        pv[i] = c.sdf_scale[i] * (c.rot[0 * 3 + i] * q[0] + c.rot[1 * 3 + i] * q[1] + c.rot[2 * 3 + i] * q[2]) + half;
+    const float* vox = sdf_voxels + c.sdf_offset;
+    const float sd = tool_sdf_at(vox, c.sdf_res, pv);
+    const float influence = fminf(expf(-sd / fmaxf(eps, c.softness)), 1.f);
+    if (!(sd <= 0.f || influence > 0.1f)) return;
+    // vel_collider (mesh.py:139-145): where the body point at p is one substep later, minus p,
+    // over dt.  Written as ((E - I) q + dpos) / dt with (E - I) q = sin(th) k x q +
+    // 2 sin^2(th / 2) k x (k x q), so the difference of the two poses loses no digits
+    float vc[3];
+    {
+        const float wx = c.ang_vel[0] * dt, wy = c.ang_vel[1] * dt, wz = c.ang_vel[2] * dt;
+        const float th = sqrtf(wx * wx + wy * wy + wz * wz);
+        float d[3] = {0.f, 0.f, 0.f};
+        if (th > 0.f) {
+            const float k[3] = {wx / th, wy / th, wz / th};
+            const float kq[3] = {k[1] * q[2] - k[2] * q[1], k[2] * q[0] - k[0] * q[2], k[0] * q[1] - k[1] * q[0]};
+            const float kkq[3] = {k[1] * kq[2] - k[2] * kq[1], k[2] * kq[0] - k[0] * kq[2], k[0] * kq[1] - k[1] * kq[0]};
+            const float sh = sinf(0.5f * th), s = sinf(th), t = 2.f * sh * sh;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) d[i] = s * kq[i] + t * kkq[i];
+        }
+        float dz = c.lin_vel[2] * dt;
+        if (c.pos[2] + dz < c.floor) dz = c.floor - c.pos[2];  // FloorBoundary.impose_pos of the origin
+        vc[0] = (d[0] + c.lin_vel[0] * dt) / dt;
+        vc[1] = (d[1] + c.lin_vel[1] * dt) / dt;
+        vc[2] = (d[2] + dz) / dt;
+    }
+    const float rv[3] = {v[0] - vc[0], v[1] - vc[1], v[2] - vc[2]};
+    // normal (mesh.py:107-137): central differences of 1e-2 voxel, normalised, mapped to the
+    // mesh frame by the inverse voxel scale and to the world by the pose, normalised again
+    float nv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float a[3] = {pv[0], pv[1], pv[2]}, b[3] = {pv[0], pv[1], pv[2]};
+        a[i] += 1e-2f;
+        b[i] -= 1e-2f;
+        nv[i] = (tool_sdf_at(vox, c.sdf_res, a) - tool_sdf_at(vox, c.sdf_res, b)) / 2e-2f;
+    }
+    float inv = rsqrtf(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2] + eps);
+    const float nm[3] = {nv[0] * inv / c.sdf_scale[0], nv[1] * inv / c.sdf_scale[1], nv[2] * inv / c.sdf_scale[2]};
+    float n[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n[i] = c.rot[i * 3 + 0] * nm[0] + c.rot[i * 3 + 1] * nm[1] + c.rot[i * 3 + 2] * nm[2];
+    inv = rsqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] + eps);
+    n[0] *= inv;
+    n[1] *= inv;
+    n[2] *= inv;
+    const float rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    if (!(rn < 0.f)) return;
+    const float rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
+    const float rtn = sqrtf(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
+    const float sc = fmaxf(0.f, rtn + rn * c.friction) / rtn;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = vc[i] + rt[i] * sc * influence + rv[i] * (1.f - influence);
+}
+
 // ---------------------------------------------------------------- p2g
 
 struct P2GArgs {
@@ -873,7 +983,7 @@ __device__ __forceinline__ void cpic_update_normals(const P2GArgs& a, int inst, 
     const int64_t st = a.par.state_stride;
     for (int k = 0; k < a.n_cols; ++k) {
         const mpm_collider& c = a.cols[k];
-        if (c.instance != inst) continue;
+        if (c.instance != inst || c.kind == MPM_COLLIDER_TOOL) continue;  // CPIC: rigid geoms only
         float n[3];
         collider_normal(c, I.eps, x, n);
         float* o = a.par.cpic_normal + (int64_t)(3 * k) * st + g;
@@ -894,7 +1004,7 @@ __device__ __forceinline__ uint32_t cpic_separating(const P2GArgs& a, int inst, 
     const int64_t st = a.par.state_stride;
     for (int k = 0; k < a.n_cols; ++k) {
         const mpm_collider& c = a.cols[k];
-        if (c.instance != inst) continue;
+        if (c.instance != inst || c.kind == MPM_COLLIDER_TOOL) continue;  // CPIC: rigid geoms only
         float n[3];
         collider_normal(c, I.eps, pos, n);
         const float* o = a.par.cpic_normal + (int64_t)(3 * k) * st + g;
@@ -1463,9 +1573,9 @@ __global__ void k_nonfree_zero(mpm_problem prob, const mpm_instance* __restrict_
 
 // ---------------------------------------------------------------- grid op
 
-// Rigid coupling of one grid node against one kinematic collider (legacy_coupler.py:166-343):
 // constant-velocity kinematic motion of the colliders over one substep of their instance:
-// pos += lin_vel dt, rot = exp([ang_vel] dt) rot (Rodrigues)
+// pos += lin_vel dt (a tool's origin then clamped to its floor, tool_entity.py:178-189),
+// rot = exp([ang_vel] dt) rot
 __global__ void k_advance_colliders(const mpm_instance* __restrict__ inst, int n_inst, mpm_collider* cs, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1474,14 +1584,10 @@ __global__ void k_advance_colliders(const mpm_instance* __restrict__ inst, int n
     const float dt = inst[c.instance].dt;
 #pragma unroll
     for (int d = 0; d < 3; ++d) c.pos[d] += c.lin_vel[d] * dt;
-    const float wx = c.ang_vel[0] * dt, wy = c.ang_vel[1] * dt, wz = c.ang_vel[2] * dt;
-    const float th = sqrtf(wx * wx + wy * wy + wz * wz);
-    if (th > 0.f) {
-        const float kx = wx / th, ky = wy / th, kz = wz / th, s = sinf(th), cth = cosf(th), t = 1.f - cth;
-        const float E[9] = {cth + t * kx * kx, t * kx * ky - s * kz, t * kx * kz + s * ky,
-                            t * kx * ky + s * kz, cth + t * ky * ky, t * ky * kz - s * kx,
-                            t * kx * kz - s * ky, t * ky * kz + s * kx, cth + t * kz * kz};
-        float R[9];
+    if (c.kind == MPM_COLLIDER_TOOL) c.pos[2] = fmaxf(c.pos[2], c.floor);
+    if (c.ang_vel[0] != 0.f || c.ang_vel[1] != 0.f || c.ang_vel[2] != 0.f) {
+        float E[9], R[9];
+        rot_step(c.ang_vel, dt, E);
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -1492,9 +1598,10 @@ __global__ void k_advance_colliders(const mpm_instance* __restrict__ inst, int n
     }
 }
 
-__global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w,
+// at most 64 registers (4 CTAs per SM): the collider responses, rare, may spill instead
+__global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w,
                                                  const mpm_collider* __restrict__ colliders, int n_colliders,
-                                                 float* collider_force) {
+                                                 float* collider_force, const float* __restrict__ sdf_voxels) {
     const int n_active = (int)w.counters[CNT_ACTIVE];
     const int gpc = blockDim.x / BLK3;
     const int grp = threadIdx.x / BLK3;
@@ -1523,8 +1630,12 @@ __global__ void __launch_bounds__(256) k_grid_op(mpm_problem prob, const mpm_ins
                 const float p[3] = {px, py, pz};
                 float v[3] = {vx, vy, vz};
                 const float mreal = mm.w * 1e-3f;
+                for (int k = 0; k < n_colliders; ++k) {  // MPM <-> Tool (legacy_coupler.py:381-383)
+                    if (colliders[k].instance != e.x || colliders[k].kind != MPM_COLLIDER_TOOL) continue;
+                    collide_tool(colliders[k], sdf_voxels, I.eps, I.dt, p, v);
+                }
                 for (int k = 0; k < n_colliders; ++k) {
-                    if (colliders[k].instance != e.x) continue;
+                    if (colliders[k].instance != e.x || colliders[k].kind == MPM_COLLIDER_TOOL) continue;
                     collide_rigid(colliders[k], I.eps, I.dt, mreal, p, v,
                                   collider_force ? collider_force + 6 * k : nullptr);
                 }
@@ -1803,7 +1914,8 @@ static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* 
     if (ctas > need) ctas = (int)need;
     if (tab->n_colliders < 0) return MPM_E_INVALID;
     const int nc = tab->colliders ? tab->n_colliders : 0;
-    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc, tab->collider_force);
+    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc, tab->collider_force,
+                                    tab->sdf_voxels);
     if (nc > 0)
         k_advance_colliders<<<(nc + 63) / 64, 64, 0, s>>>(tab->instances, prob->n_instances, tab->colliders, nc);
     return cuda_ok();
@@ -1850,6 +1962,129 @@ static int launch_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_part
 }  // namespace gbm
 
 using namespace gbm;
+
+// ---------------------------------------------------------------- tool SDF voxels
+// compute_sdf_data (utils/mesh.py:179-201): the signed distance of every voxel centre of a
+// res^3 lattice over [-radius, radius]^3 to a triangle mesh.  Each CTA stages the mesh in
+// tiles of 256 triangles in shared memory; every thread owns one voxel and keeps the nearest
+// squared distance and the winding number.
+
+// squared distance from p to triangle (a, b, c): the closest point by the Voronoi region of
+// p (Ericson, Real-Time Collision Detection, 5.1.5)
+__device__ __forceinline__ float tri_dist2(const float* p, const float* a, const float* b, const float* c) {
+    float ab[3], ac[3], ap[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        ab[i] = b[i] - a[i];
+        ac[i] = c[i] - a[i];
+        ap[i] = p[i] - a[i];
+    }
+    auto dot = [](const float* u, const float* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+    float q[3];
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.f && d2 <= 0.f) {
+        q[0] = a[0], q[1] = a[1], q[2] = a[2];
+    } else {
+        float bp[3], cp[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            bp[i] = p[i] - b[i];
+            cp[i] = p[i] - c[i];
+        }
+        const float d3 = dot(ab, bp), d4 = dot(ac, bp), d5 = dot(ab, cp), d6 = dot(ac, cp);
+        const float vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
+        if (d3 >= 0.f && d4 <= d3) {
+            q[0] = b[0], q[1] = b[1], q[2] = b[2];
+        } else if (d6 >= 0.f && d5 <= d6) {
+            q[0] = c[0], q[1] = c[1], q[2] = c[2];
+        } else if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+            const float t = d1 / (d1 - d3);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) q[i] = a[i] + t * ab[i];
+        } else if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+            const float t = d2 / (d2 - d6);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) q[i] = a[i] + t * ac[i];
+        } else if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+            const float t = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+#pragma unroll
+            for (int i = 0; i < 3; ++i) q[i] = b[i] + t * (c[i] - b[i]);
+        } else {
+            const float den = 1.f / (va + vb + vc);
+            const float v = vb * den, w = vc * den;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) q[i] = a[i] + ab[i] * v + ac[i] * w;
+        }
+    }
+    const float d[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+    return d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+}
+
+// solid angle of triangle (a, b, c) seen from p, signed by the triangle's orientation
+// (Van Oosterom & Strackee 1983): tan(omega / 2) = det[r_a r_b r_c] /
+// (|r_a||r_b||r_c| + (r_a.r_b)|r_c| + (r_a.r_c)|r_b| + (r_b.r_c)|r_a|)
+__device__ __forceinline__ float tri_solid_angle(const float* p, const float* a, const float* b, const float* c) {
+    const float ra[3] = {a[0] - p[0], a[1] - p[1], a[2] - p[2]};
+    const float rb[3] = {b[0] - p[0], b[1] - p[1], b[2] - p[2]};
+    const float rc[3] = {c[0] - p[0], c[1] - p[1], c[2] - p[2]};
+    const float la = sqrtf(ra[0] * ra[0] + ra[1] * ra[1] + ra[2] * ra[2]);
+    const float lb = sqrtf(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
+    const float lc = sqrtf(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2]);
+    const float det = ra[0] * (rb[1] * rc[2] - rb[2] * rc[1]) - ra[1] * (rb[0] * rc[2] - rb[2] * rc[0]) +
+                      ra[2] * (rb[0] * rc[1] - rb[1] * rc[0]);
+    const float den = la * lb * lc + (ra[0] * rb[0] + ra[1] * rb[1] + ra[2] * rb[2]) * lc +
+                      (ra[0] * rc[0] + ra[1] * rc[1] + ra[2] * rc[2]) * lb +
+                      (rb[0] * rc[0] + rb[1] * rc[1] + rb[2] * rc[2]) * la;
+    return 2.f * atan2f(det, den);
+}
+
+constexpr int SDF_T = 256;
+
+__global__ void __launch_bounds__(SDF_T) k_sdf_voxelize(const float* __restrict__ V, int nv, const int* __restrict__ Fc,
+                                                        int nf, int res, float radius, float* __restrict__ out) {
+    __shared__ float tri[SDF_T][9];
+    const int64_t n = (int64_t)res * res * res;
+    const int64_t vid = (int64_t)blockIdx.x * SDF_T + threadIdx.x;
+    const int i = (int)(vid / ((int64_t)res * res)), j = (int)((vid / res) % res), k = (int)(vid % res);
+    const float step = 2.f * radius / (float)(res - 1);
+    const float p[3] = {-radius + step * (float)i, -radius + step * (float)j, -radius + step * (float)k};
+    float d2 = 3.402823466e38f, wind = 0.f;
+    for (int f0 = 0; f0 < nf; f0 += SDF_T) {
+        const int f = f0 + threadIdx.x;
+        bool ok = false;
+        if (f < nf) {
+            const int ia = Fc[3 * f], ib = Fc[3 * f + 1], ic = Fc[3 * f + 2];
+            ok = ia >= 0 && ib >= 0 && ic >= 0 && ia < nv && ib < nv && ic < nv;
+            if (ok) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    tri[threadIdx.x][d] = V[3 * ia + d];
+                    tri[threadIdx.x][3 + d] = V[3 * ib + d];
+                    tri[threadIdx.x][6 + d] = V[3 * ic + d];
+                }
+            }
+        }
+        if (!ok) {  // a padding (or invalid) face: degenerate, far away, no solid angle
+#pragma unroll
+            for (int d = 0; d < 9; ++d) tri[threadIdx.x][d] = 1e18f;
+        }
+        __syncthreads();
+        const int m = min(SDF_T, nf - f0);
+        if (vid < n) {
+            for (int t = 0; t < m; ++t) {
+                const float* T = tri[t];
+                if (T[0] == 1e18f) continue;
+                d2 = fminf(d2, tri_dist2(p, T, T + 3, T + 6));
+                wind += tri_solid_angle(p, T, T + 3, T + 6);
+            }
+        }
+        __syncthreads();
+    }
+    if (vid < n) {
+        const float w = wind * (1.f / (4.f * 3.14159265358979f));
+        out[vid] = (fabsf(w) > 0.5f ? -1.f : 1.f) * sqrtf(d2);
+    }
+}
 
 extern "C" {
 
@@ -2266,6 +2501,16 @@ int mpm_update_render_fields(const mpm_problem* prob, const mpm_particles* par, 
             *prob, *par, n_per_env, render_pos, render_vel, render_active, n_vverts, n_supports, support_idx,
             support_w, vvert_pos, vvert_active);
     }
+    return cuda_ok();
+}
+
+int mpm_sdf_voxelize(const float* vertices, int32_t n_verts, const int32_t* faces, int32_t n_faces, int32_t res,
+                     float radius, float* out, void* stream) {
+    if (!vertices || !faces || !out || n_verts < 3 || n_faces < 1 || res < 2 || res > 1024 || !(radius > 0.f))
+        return MPM_E_INVALID;
+    const int64_t n = (int64_t)res * res * res;
+    k_sdf_voxelize<<<(unsigned)((n + SDF_T - 1) / SDF_T), SDF_T, 0, (cudaStream_t)stream>>>(vertices, n_verts, faces,
+                                                                                          n_faces, res, radius, out);
     return cuda_ok();
 }
 

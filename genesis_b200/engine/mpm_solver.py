@@ -125,15 +125,25 @@ class MPMSolver:
         specs = [InstanceSpec(**spec_kw) for _ in range(self._B)]
         b = self._b200
         rigid = list(getattr(self._scene, "_rigid_entities", []))
-        colliders = [r._collider(env) for r in rigid for env in range(self._B)]
+        tools = list(getattr(self._scene, "_tool_entities", []))
+        # tool rows first (one per tool and environment), each tool's voxel grid once
+        topt = self._scene._other.get("tool_options")
+        floor = topt.floor_height if topt is not None and topt.floor_height is not None else self._scene.sim_options.floor_height
+        grids, colliders, off = [], [], 0
+        for t in tools:
+            g = t._sdf(self._sim.device).reshape(-1)
+            colliders += [t._collider(env, off, floor) for env in range(self._B)]
+            grids.append(g)
+            off += g.numel()
+        colliders += [r._collider(env) for r in rigid for env in range(self._B)]
         grad = self._sim.requires_grad
         if grad:
             from ..materials import MPM
 
             bad = [type(m).__name__ for m in self.unique_materials if not isinstance(m, (MPM.Elastic, MPM.Muscle))]
-            if bad or rigid:
+            if bad or rigid or tools:
                 raise GenesisException("A differentiable scene supports MPM.Elastic and MPM.Muscle entities only "
-                                       f"(got {', '.join(bad) or 'rigid colliders'}).")
+                                       f"(got {', '.join(bad) or 'rigid or tool colliders'}).")
         self.runtime = MPMRuntime(
             specs,
             device=self._sim.device,
@@ -142,11 +152,14 @@ class MPMSolver:
             grid_ctas=b.grid_ctas,
             use_graphs=b.use_cuda_graph and not grad,
             colliders=colliders,
+            sdf_voxels=torch.cat(grids) if grids else None,
             cpic=self._enable_CPIC,  # active only with rigid colliders, as in the reference
             per_particle_lame=grad,
         )
+        for i, t in enumerate(tools):
+            t._bind(self.runtime, [i * self._B + env for env in range(self._B)])
         for i, r in enumerate(rigid):
-            r._bind(self.runtime, [i * self._B + env for env in range(self._B)])
+            r._bind(self.runtime, [(len(tools) + i) * self._B + env for env in range(self._B)])
         pos = np.concatenate([e.init_particles for e in self._entities])
         mat = np.concatenate([np.full(e.n_particles, e.material.idx, dtype=np.uint8) for e in self._entities])
         act = np.concatenate([np.full(e.n_particles, e.active, dtype=bool) for e in self._entities])

@@ -91,6 +91,7 @@ class MPMRuntime:
         grid_ctas: int = 0,
         use_graphs: bool = True,
         colliders: list | None = None,
+        sdf_voxels: torch.Tensor | None = None,
         cpic: bool = False,
     ):
         if not torch.cuda.is_available():
@@ -168,10 +169,21 @@ class MPMRuntime:
         else:
             self.coll_table = None
             self.collider_force = None
+        # the tools' signed-distance voxel grids (mpm_collider.sdf_offset indexes into it)
+        self.sdf_voxels = None
+        if sdf_voxels is not None and sdf_voxels.numel() > 0:
+            self.sdf_voxels = sdf_voxels.to(dev, torch.float32).contiguous()
+        if any(c.kind == nat.COLLIDER_TOOL for c in colliders):
+            n_vox = 0 if self.sdf_voxels is None else self.sdf_voxels.numel()
+            for c in colliders:
+                if c.kind == nat.COLLIDER_TOOL and c.sdf_res != 0 and (
+                        c.sdf_res < 2 or c.sdf_offset < 0 or c.sdf_offset + c.sdf_res ** 3 > n_vox):
+                    raise ValueError("a tool collider's voxel grid lies outside sdf_voxels")
         self.tables = nat.Tables(
             self.inst_table.data_ptr(), self.mat_table.data_ptr(),
             self.coll_table.data_ptr() if colliders else None, len(colliders), 0,
             self.collider_force.data_ptr() if colliders else None,
+            self.sdf_voxels.data_ptr() if self.sdf_voxels is not None else None,
         )
 
         self.state = torch.zeros((nat.MPM_STATE_CH, self.stride), dtype=torch.float32, device=dev)
@@ -296,9 +308,11 @@ class MPMRuntime:
         return self.cpic_normal[:, : self.n].reshape(-1, 3, self.n).permute(0, 2, 1)
 
     def collider_table(self) -> torch.Tensor:
-        """The collider rows as float32 [n_colliders, 24] (pos 0:3, rot 3:12, data 12:15,
-        lin_vel 15:18, ang_vel 18:21, friction, softness, restitution), a view of the
-        device table after each row's two int32 fields; writes go straight to the table."""
+        """The collider rows as float32 [n_colliders, 32] (pos 0:3, rot 3:12, data 12:15,
+        lin_vel 15:18, ang_vel 18:21, friction, softness, restitution 21:24, then the tool
+        fields: sdf_res and its pad 24:26 and sdf_offset 26:28 as integer bits, sdf_scale
+        28:31, floor 31), a view of the device table after each row's two int32 fields;
+        writes go straight to the table."""
         if self.coll_table is None:
             raise RuntimeError("runtime has no colliders")
         stride = C.sizeof(nat.Collider) // 4

@@ -46,6 +46,7 @@ class Scene:
         self._sim = Simulator(self, self.sim_options, self.mpm_options, self.b200_options)
         self._entities = []
         self._rigid_entities = []  # kinematic colliders of the MPM grid op
+        self._tool_entities = []  # tools, coupled before the rigid geoms
         self._emitters = []
         self._is_built = False
         self._B = 1
@@ -67,8 +68,16 @@ class Scene:
             if material.needs_coup:
                 self._rigid_entities.append(ent)
             return ent
+        if isinstance(material, _materials.Tool):
+            from .tool import ToolEntity
+
+            ent = ToolEntity(self, len(self._entities), material, morph, surface)
+            self._entities.append(ent)
+            self._tool_entities.append(ent)
+            return ent
         if material is None or not isinstance(material, _materials.MPM.Base):
-            raise GenesisException("Only gs.materials.MPM.* and gs.materials.Rigid entities are supported by this build.")
+            raise GenesisException("Only gs.materials.MPM.*, gs.materials.Rigid and gs.materials.Tool entities are "
+                                   "supported by this build.")
         ent = self._sim.mpm_solver.add_entity(len(self._entities), material, morph, surface, rng=_globals.rng)
         self._entities.append(ent)
         return ent

@@ -63,6 +63,14 @@ class SimOptions(Options):
             self._steps_local = None
 
 
+class ToolOptions(Options):
+    """Tool solver options (options/solvers.py:265-290): floor_height None takes the
+    SimOptions one; dt is the simulator's."""
+
+    dt: Optional[float] = None
+    floor_height: Optional[float] = None
+
+
 class LegacyCouplerOptions(Options):
     """Accepted for API compatibility; only the MPM grid update of the legacy coupler is on this path."""
 
@@ -133,4 +141,4 @@ class ViewerOptions(Options):
     max_FPS: Optional[int] = 60
 
 
-__all__ = ["SimOptions", "MPMOptions", "LegacyCouplerOptions", "B200Options", "VisOptions", "ViewerOptions"]
+__all__ = ["SimOptions", "MPMOptions", "ToolOptions", "LegacyCouplerOptions", "B200Options", "VisOptions", "ViewerOptions"]

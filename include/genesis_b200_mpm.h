@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 5
+#define MPM_ABI_VERSION 6
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -168,6 +168,14 @@ typedef struct mpm_particles {
 #define MPM_COLLIDER_PLANE 1   /* sd = n . R^T (p - pos), n = data (geom frame, unit) (sdf_decomp.py:94-98) */
 #define MPM_COLLIDER_BOX 2     /* half extents data[0..2]; exact box SDF (the reference samples it on a grid) */
 
+/* Tool entity (engine/entities/tool_entity/mesh.py:80-176, coupled by
+ * legacy_coupler.py:346-350 before the rigid geoms): signed distance sampled trilinearly from
+ * a voxel grid of the mesh (1 outside the grid), normal by central differences of 1e-2
+ * voxel, velocity of the body point from the pose one substep later, friction response
+ * (Tool.friction, coup_softness); no restitution and no reaction force.  Its origin moves at
+ * lin_vel and stays above `floor` (FloorBoundary.impose_pos, boundaries.py:67-70). */
+#define MPM_COLLIDER_TOOL 3
+
 typedef struct mpm_collider {
     int32_t kind;        /* MPM_COLLIDER_* */
     int32_t instance;    /* instance (environment) it acts on */
@@ -176,9 +184,14 @@ typedef struct mpm_collider {
     float data[3];       /* see MPM_COLLIDER_* */
     float lin_vel[3];    /* velocity of the origin */
     float ang_vel[3];    /* angular velocity, world */
-    float friction;      /* coup_friction   (materials/rigid.py:47) */
-    float softness;      /* coup_softness   (materials/rigid.py:48) */
+    float friction;      /* coup_friction   (materials/rigid.py:47); Tool.friction (materials/tool.py:10) */
+    float softness;      /* coup_softness   (materials/rigid.py:48; materials/tool.py:11) */
     float restitution;   /* coup_restitution (materials/rigid.py:49) */
+    int32_t sdf_res;     /* MPM_COLLIDER_TOOL: voxels per axis of its grid */
+    int32_t sdf_pad;
+    int64_t sdf_offset;  /* MPM_COLLIDER_TOOL: index of its first voxel in mpm_tables.sdf_voxels */
+    float sdf_scale[3];  /* voxel coordinate = sdf_scale * (geom-frame point) + (sdf_res - 1) / 2 */
+    float floor;         /* MPM_COLLIDER_TOOL: floor height of the tool solver */
 } mpm_collider;
 
 typedef struct mpm_tables {
@@ -189,6 +202,8 @@ typedef struct mpm_tables {
     int32_t pad0;
     float* collider_force;          /* device, optional [n_colliders][6]: force xyz, torque xyz;
                                        accumulated (the caller zeroes it) */
+    const float* sdf_voxels;        /* device, the voxel grids of the MPM_COLLIDER_TOOL colliders,
+                                       each [sdf_res][sdf_res][sdf_res] (x-major) at its sdf_offset */
 } mpm_tables;
 
 /* ---- sizing ------------------------------------------------------------ */
@@ -366,6 +381,16 @@ int mpm_update_render_fields(const mpm_problem* prob, const mpm_particles* par, 
                              int32_t n_per_env, float* render_pos, float* render_vel, uint8_t* render_active,
                              int32_t n_vverts, int32_t n_supports, const int32_t* support_idx,
                              const float* support_w, float* vvert_pos, uint8_t* vvert_active, void* stream);
+
+/* ---- tool signed-distance grids ------------------------------------------
+ * compute_sdf_data (utils/mesh.py:179-201) for a triangle mesh already normalised as
+ * tool_entity/mesh.py:39-51 does: out[(i * res + j) * res + k] = the signed distance of
+ * the point (-r + 2 r i / (res - 1), same for j, k) (r = radius, 0.6 in the reference) to
+ * the mesh, negative inside.  Distance to the nearest triangle; the sign from the
+ * generalised winding number (inside where it exceeds 1/2).  vertices float [n_verts][3],
+ * faces int32 [n_faces][3]; out float [res^3], all device. */
+int mpm_sdf_voxelize(const float* vertices, int32_t n_verts, const int32_t* faces, int32_t n_faces, int32_t res,
+                     float radius, float* out, void* stream);
 
 /* ---- CUDA graphs --------------------------------------------------------
  * Capture n_substeps of mpm_substeps into an executable graph (the pointers in

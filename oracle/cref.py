@@ -54,6 +54,7 @@ def _structs(dtype):
             ("kind", C.c_int32),
             ("pos", Rt * 3), ("rot", Rt * 9), ("data", Rt * 3), ("lin_vel", Rt * 3), ("ang_vel", Rt * 3),
             ("friction", Rt), ("softness", Rt), ("restitution", Rt),
+            ("sdf", C.c_void_p), ("sdf_res", C.c_int32), ("sdf_scale", Rt * 3), ("floor", Rt),
         ]
 
     return Params, Mat, Coll
@@ -127,9 +128,18 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     if st.get("colliders"):
         cs = st["colliders"]
         carr = (Coll * len(cs))()
-        kinds = {"sphere": 0, "plane": 1, "box": 2}
+        kinds = {"sphere": 0, "plane": 1, "box": 2, "tool": 3}
+        keep = []  # the tools' voxel arrays stay alive for the call
         for i, c in enumerate(cs):
             carr[i].kind = kinds[c.kind]
+            if c.kind == "tool":
+                vox = np.ascontiguousarray(c.sdf, dtype=dt).reshape(-1)
+                keep.append(vox)
+                carr[i].sdf = vox.ctypes.data_as(C.c_void_p)
+                carr[i].sdf_res = int(round(len(vox) ** (1 / 3)))
+                for d in range(3):
+                    carr[i].sdf_scale[d] = float(np.broadcast_to(c.sdf_scale, (3,))[d])
+                carr[i].floor = float(c.floor)
             for d in range(3):
                 carr[i].pos[d] = c.pos[d]
                 carr[i].data[d] = c.data[d]
@@ -154,7 +164,7 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
         for i, c in enumerate(cs):
             moved.append(R.Collider(c.kind, np.array(carr[i].pos[:]), np.array(carr[i].rot[:]).reshape(3, 3),
                                     np.asarray(c.data), np.asarray(c.lin_vel), np.asarray(c.ang_vel), c.friction,
-                                    c.softness, c.restitution))
+                                    c.softness, c.restitution, c.sdf, c.sdf_scale, c.floor))
         out = dict(st)
         out.update(x=x, v=v, C=Cm.reshape(n, 3, 3), F=F.reshape(n, 3, 3), Jp=Jp, colliders=moved, forces=forces)
         if rn is not None:

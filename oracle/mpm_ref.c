@@ -40,6 +40,7 @@
 #define RMAX(a, b) fmaxf(a, b)
 #define RMIN(a, b) fminf(a, b)
 #define R_SIN(x) sinf(x)
+#define R_FLOOR(x) floorf(x)
 #define R_COS(x) cosf(x)
 #else
 #define R_SQRT(x) sqrt(x)
@@ -51,6 +52,7 @@
 #define RMAX(a, b) fmax(a, b)
 #define RMIN(a, b) fmin(a, b)
 #define R_SIN(x) sin(x)
+#define R_FLOOR(x) floor(x)
 #define R_COS(x) cos(x)
 #endif
 
@@ -75,9 +77,13 @@ typedef struct {
 /* kinematic rigid collider of the grid op (legacy_coupler.py:131-343); kind 0 sphere
  * (data[0] radius), 1 plane (data = unit normal, geom frame), 2 box (data = half extents) */
 typedef struct {
-    int32_t kind;
+    int32_t kind; /* 0 sphere, 1 plane, 2 box, 3 tool (voxel signed-distance grid) */
     REAL pos[3], rot[9], data[3], lin_vel[3], ang_vel[3];
     REAL friction, softness, restitution;
+    const REAL* sdf;    /* tool: [sdf_res]^3 voxels, x-major */
+    int32_t sdf_res;
+    REAL sdf_scale[3];  /* tool: voxel = sdf_scale * (geom-frame point) + (sdf_res - 1) / 2 */
+    REAL floor;         /* tool: floor height of the tool solver */
 } ref_collider;
 
 /* ---------------------------------------------------------------- SVD */
@@ -427,9 +433,77 @@ static void collide_rigid(const ref_collider* c, REAL eps, REAL dt, REAL mass, c
     rigid_respond(c, eps, dt, mass, q, n, infl, v, f);
 }
 
+/* ---- tools (engine/entities/tool_entity/mesh.py:80-176) ---- */
+
+/* mesh.py:89-104: trilinear sample at voxel coordinate pv, 1 outside the grid */
+static REAL tool_sdf_at(const ref_collider* c, const REAL* pv) {
+    int res = c->sdf_res;
+    REAL f0 = R_FLOOR(pv[0]), f1 = R_FLOOR(pv[1]), f2 = R_FLOOR(pv[2]);
+    if (!(f0 >= 0 && f1 >= 0 && f2 >= 0 && f0 < res - 1 && f1 < res - 1 && f2 < res - 1)) return 1;
+    int b[3] = {(int)f0, (int)f1, (int)f2};
+    REAL sd = 0;
+    for (int o = 0; o < 8; ++o) {
+        int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+        REAL w = (1 - RABS(pv[0] - (b[0] + i))) * (1 - RABS(pv[1] - (b[1] + j))) * (1 - RABS(pv[2] - (b[2] + k)));
+        sd += w * c->sdf[((int64_t)(b[0] + i) * res + (b[1] + j)) * res + (b[2] + k)];
+    }
+    return sd;
+}
+
+/* Tool.collide (mesh.py:147-176) for a grid node at pos: influence min(exp(-sd / softness), 1);
+ * the body point's velocity from the pose one substep later (mesh.py:139-145), the normal by
+ * central differences of 1e-2 voxel (mesh.py:107-137), friction on the tangential part */
+static void collide_tool(const ref_collider* c, REAL eps, REAL dt, const REAL* pos, REAL* v) {
+    if (!c->sdf || c->sdf_res < 2) return;
+    REAL q[3] = {pos[0] - c->pos[0], pos[1] - c->pos[1], pos[2] - c->pos[2]};
+    REAL pv[3], half = (REAL)0.5 * (c->sdf_res - 1);
+    for (int i = 0; i < 3; ++i)
+        pv[i] = c->sdf_scale[i] * (c->rot[0 * 3 + i] * q[0] + c->rot[1 * 3 + i] * q[1] + c->rot[2 * 3 + i] * q[2]) + half;
+    REAL sd = tool_sdf_at(c, pv);
+    REAL soft = c->softness > eps ? c->softness : eps;
+    REAL infl = RMIN(REXP(-sd / soft), (REAL)1);
+    if (!(sd <= 0 || infl > (REAL)0.1)) return;
+    /* ((E - I) q + dpos) / dt, E the rotation by ang dt */
+    REAL d[3] = {0, 0, 0};
+    REAL wx = c->ang_vel[0] * dt, wy = c->ang_vel[1] * dt, wz = c->ang_vel[2] * dt;
+    REAL th = R_SQRT(wx * wx + wy * wy + wz * wz);
+    if (th > 0) {
+        REAL k[3] = {wx / th, wy / th, wz / th};
+        REAL kq[3] = {k[1] * q[2] - k[2] * q[1], k[2] * q[0] - k[0] * q[2], k[0] * q[1] - k[1] * q[0]};
+        REAL kkq[3] = {k[1] * kq[2] - k[2] * kq[1], k[2] * kq[0] - k[0] * kq[2], k[0] * kq[1] - k[1] * kq[0]};
+        REAL sh = R_SIN(th / 2), s = R_SIN(th), t = 2 * sh * sh;
+        for (int i = 0; i < 3; ++i) d[i] = s * kq[i] + t * kkq[i];
+    }
+    REAL dz = c->lin_vel[2] * dt;
+    if (c->pos[2] + dz < c->floor) dz = c->floor - c->pos[2];
+    REAL vc[3] = {(d[0] + c->lin_vel[0] * dt) / dt, (d[1] + c->lin_vel[1] * dt) / dt, (d[2] + dz) / dt};
+    REAL rv[3] = {v[0] - vc[0], v[1] - vc[1], v[2] - vc[2]};
+    REAL nv[3];
+    for (int i = 0; i < 3; ++i) {
+        REAL a[3] = {pv[0], pv[1], pv[2]}, b[3] = {pv[0], pv[1], pv[2]};
+        a[i] += (REAL)1e-2;
+        b[i] -= (REAL)1e-2;
+        nv[i] = (tool_sdf_at(c, a) - tool_sdf_at(c, b)) / (REAL)2e-2;
+    }
+    REAL nn = R_SQRT(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2] + eps);
+    REAL nm[3] = {nv[0] / nn / c->sdf_scale[0], nv[1] / nn / c->sdf_scale[1], nv[2] / nn / c->sdf_scale[2]};
+    REAL n[3];
+    for (int i = 0; i < 3; ++i) n[i] = c->rot[i * 3 + 0] * nm[0] + c->rot[i * 3 + 1] * nm[1] + c->rot[i * 3 + 2] * nm[2];
+    nn = R_SQRT(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] + eps);
+    for (int i = 0; i < 3; ++i) n[i] /= nn;
+    REAL rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    if (!(rn < 0)) return;
+    REAL rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
+    REAL rtn = R_SQRT(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
+    REAL sc = rtn + rn * c->friction;
+    sc = (sc > 0 ? sc : 0) / rtn;
+    for (int i = 0; i < 3; ++i) v[i] = vc[i] + rt[i] * sc * infl + rv[i] * (1 - infl);
+}
+
 /* constant-velocity kinematic motion over one substep */
 static void advance_collider(ref_collider* c, REAL dt) {
     for (int d = 0; d < 3; ++d) c->pos[d] += c->lin_vel[d] * dt;
+    if (c->kind == 3 && c->pos[2] < c->floor) c->pos[2] = c->floor; /* FloorBoundary.impose_pos */
     REAL wx = c->ang_vel[0] * dt, wy = c->ang_vel[1] * dt, wz = c->ang_vel[2] * dt;
     REAL th = R_SQRT(wx * wx + wy * wy + wz * wz);
     if (th > 0) {
@@ -492,6 +566,7 @@ int ref_substeps_cpic(const ref_params* p, const ref_material* mats, int n, REAL
             for (int i = 0; i < n; ++i) {
                 if (!active[i]) continue;
                 for (int k = 0; k < n_colliders; ++k) {
+                    if (colliders[k].kind == 3) continue; /* CPIC: rigid geoms only */
                     REAL nn[3];
                     REAL* o = rnormal + 3 * ((int64_t)k * n + i);
                     sdf_normal(&colliders[k], p->eps, x + 3 * i, nn);
@@ -566,6 +641,7 @@ int ref_substeps_cpic(const ref_params* p, const ref_material* mats, int n, REAL
                                                 (REAL)(gk + p->lower_cell[2]) * p->dx};
                             int sg = -1;
                             for (int k = 0; k < n_colliders && sg < 0; ++k) {
+                                if (colliders[k].kind == 3) continue;
                                 REAL nc[3];
                                 const REAL* np_ = rnormal + 3 * ((int64_t)k * n + i);
                                 sdf_normal(&colliders[k], p->eps, cp, nc);
@@ -604,9 +680,13 @@ int ref_substeps_cpic(const ref_params* p, const ref_material* mats, int n, REAL
                     pos[d] = (REAL)(I[d] + p->lower_cell[d]) * p->dx;
                 }
                 /* MPM <-> rigid (legacy_coupler.py:385-397), node mass without the 1e3 volume scale */
+                /* MPM <-> Tool first (legacy_coupler.py:381-383) */
                 for (int k = 0; k < n_colliders; ++k)
-                    collide_rigid(&colliders[k], p->eps, p->dt, cell[3] / (REAL)1e3, pos, vel,
-                                  forces ? forces + 6 * k : NULL);
+                    if (colliders[k].kind == 3) collide_tool(&colliders[k], p->eps, p->dt, pos, vel);
+                for (int k = 0; k < n_colliders; ++k)
+                    if (colliders[k].kind != 3)
+                        collide_rigid(&colliders[k], p->eps, p->dt, cell[3] / (REAL)1e3, pos, vel,
+                                      forces ? forces + 6 * k : NULL);
                 for (int d = 0; d < 3; ++d) out[d] = bc_vel(pos[d], vel[d], p->bnd_lo[d], p->bnd_hi[d]);
             }
         }

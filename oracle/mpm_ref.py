@@ -407,7 +407,9 @@ class Collider:
     """A kinematic rigid geom coupled in the grid op (legacy_coupler.py:131-343): kind
     'sphere' (data[0] = radius), 'plane' (data = unit normal, geom frame) or 'box' (data =
     half extents); pose (pos, rot world-from-geom), velocity (lin_vel of pos, ang_vel) and
-    the Rigid material's coupling parameters (materials/rigid.py:46-49)."""
+    the Rigid material's coupling parameters (materials/rigid.py:46-49).  Kind 'tool' is a
+    Tool entity (tool_entity/mesh.py:80-176) with its voxel grid; the C restatement
+    (mpm_ref.c) couples it, this numpy one does not."""
 
     kind: str
     pos: np.ndarray
@@ -418,12 +420,17 @@ class Collider:
     friction: float = 0.1
     softness: float = 0.002
     restitution: float = 0.0
+    sdf: np.ndarray | None = None  # kind 'tool': [res, res, res] voxel signed distances
+    sdf_scale: tuple = (1.0, 1.0, 1.0)  # kind 'tool': voxel = sdf_scale * geom-frame point + (res - 1) / 2
+    floor: float = 0.0  # kind 'tool': the tool solver's floor height
 
 
 def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
     """_func_collide_with_rigid_geom + _func_collide_in_rigid_geom for grid nodes at pos
     (legacy_coupler.py:166-343); sphere and plane SDFs as utils/sdf_decomp.py:91-98, the
     box's exact.  Returns (new velocity, force, torque about c.pos)."""
+    if c.kind == "tool":
+        raise NotImplementedError("tool colliders are coupled by the C restatement (cref)")
     dt = vel.dtype.type
     q = pos - np.asarray(c.pos, dtype=dt)
     R = np.asarray(c.rot, dtype=dt)
