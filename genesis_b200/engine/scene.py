@@ -156,6 +156,10 @@ class Scene:
                 self._sim.mpm_solver.runtime.reset_colliders()
                 if self._sim.mpm_solver.tape is not None:
                     self._sim.mpm_solver.tape.reset()  # a new differentiable rollout
+                tool_state = state.solvers_state[0] if isinstance(state, SimState) else None
+                if tool_state is not None:  # the tool solver's set_state (tool_solver.py:70-74)
+                    for t, ts in zip(self._tool_entities, tool_state.entities):
+                        t.set_state(0, ts)
 
     def save_checkpoint(self, path):
         st = self.get_state()[MPM_INDEX]

@@ -8,7 +8,7 @@ from .. import _globals
 from .. import _native as nat
 from ..exceptions import GenesisException
 from .mpm_solver import NAN_MESSAGE, LegacyCoupler, MPMSolver
-from .states import MPM_INDEX, SOLVER_NAMES, SimState
+from .states import MPM_INDEX, SOLVER_NAMES, SimState, ToolSolverState
 
 
 class Simulator:
@@ -91,6 +91,11 @@ class Simulator:
         self.poll_status()
         slots = [None] * len(SOLVER_NAMES)
         slots[MPM_INDEX] = self.mpm_solver.get_state(self.cur_substep_local)
+        tools = getattr(self._scene, "_tool_entities", [])
+        if tools and self.mpm_solver.is_active:
+            ts = ToolSolverState(self._scene)
+            ts.entities = [t.get_state() for t in tools]
+            slots[SOLVER_NAMES.index("tool")] = ts
         state = SimState(self._scene, self.cur_step_global, slots)
         self._queried_states.append(state)
         return state

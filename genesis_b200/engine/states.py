@@ -61,6 +61,25 @@ class MPMEntityState(MPMSolverState):
         return self._s_global
 
 
+class ToolSolverState:
+    """The tools' states, one ToolEntityState per tool entity (states/solvers.py:114-133)."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self.entities = []
+
+    def serializable(self):
+        self.scene = None
+        for st in self.entities:
+            st.serializable()
+
+    def __len__(self):
+        return len(self.entities)
+
+    def __getitem__(self, index):
+        return self.entities[index]
+
+
 # the reference's solver order (simulator.py:129-140): a scene's state has one entry per solver,
 # None for the solvers that are not active; only the MPM solver exists here
 SOLVER_NAMES = ("tool", "rigid", "avatar", "mpm", "sph", "pbd", "fem", "sf")

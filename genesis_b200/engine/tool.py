@@ -42,6 +42,10 @@ class ToolEntityState:
     def s_global(self):
         return self._s_global
 
+    def serializable(self):
+        self._entity = None
+        self.pos, self.quat, self.vel, self.ang = (t.detach() for t in (self.pos, self.quat, self.vel, self.ang))
+
 
 def normalized_mesh(morph):
     """tool_entity/mesh.py:39-51: the file's vertices centred on their bounding box and divided
@@ -176,6 +180,13 @@ class ToolEntity:
             self._set_cols(_LIN, vel)
         if ang is not None:
             self._set_cols(_ANG, ang)
+
+    def set_state(self, f, state):
+        """Pose and velocities of every environment from a ToolEntityState (tool_entity.py:291-293)."""
+        self._set_cols(_POS, state.pos.reshape(-1, 3))
+        self.set_quaternion(state.quat)
+        self._set_cols(_LIN, state.vel.reshape(-1, 3))
+        self._set_cols(_ANG, state.ang.reshape(-1, 3))
 
     def get_state(self, f=None):
         self._check_built()

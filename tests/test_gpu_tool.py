@@ -139,3 +139,28 @@ def test_differentiable_scene_rejects_tools(tmp_path):
     scene.add_entity(gs.morphs.Mesh(file=path, scale=0.1, pos=(0.5, 0.5, 0.2)), material=gs.materials.Tool())
     with pytest.raises(gs.GenesisException):
         scene.build()
+
+
+def test_scene_state_holds_tools_and_reset_restores_them(tmp_path):
+    """The scene's state carries the tool solver's state at solvers_state[0] (one
+    ToolEntityState per tool, states/solvers.py:114-133); scene.reset(state) puts the tools
+    back where that state had them."""
+    scene, block, tool = _scene(tmp_path, n_envs=2)
+    tool.set_velocity(vel=(0.1, 0.0, 0.2), ang=(0.0, 1.0, 0.0))
+    scene.step()
+    s1 = scene.get_state()
+    ts = s1.solvers_state[0]
+    assert len(ts) == 1 and s1.solvers_state[3] is not None
+    assert torch.allclose(ts[0].pos, tool.get_state().pos)
+    pos1, quat1 = ts[0].pos.clone(), ts[0].quat.clone()
+    x1 = block.get_particles_pos().clone()
+    for _ in range(3):
+        scene.step()
+    assert not torch.allclose(tool.get_state().pos, pos1)
+    scene.reset(s1)
+    st = tool.get_state()
+    assert torch.allclose(st.pos, pos1, atol=1e-7)
+    assert torch.allclose(st.quat, quat1, atol=1e-6)
+    assert torch.allclose(block.get_particles_pos(), x1)
+    scene.reset()  # the built poses
+    assert np.allclose(tool.get_state().pos.cpu().numpy(), [[0.5, 0.5, 0.3]] * 2, atol=1e-7)
