@@ -130,3 +130,18 @@ def test_sim_state_solver_order():
     assert bool((s.solvers_state[3].active == 1).all())
     s.serializable()
     assert s.scene is None
+
+
+def test_tool_solver_state_container():
+    """ToolSolverState holds one entity state per tool (states/solvers.py:114-133)."""
+    import torch
+
+    from genesis_b200.engine.states import ToolSolverState
+    from genesis_b200.engine.tool import ToolEntityState
+
+    z = torch.zeros
+    ts = ToolSolverState("scene")
+    ts.entities = [ToolEntityState("tool", 4, z(2, 3, requires_grad=True), z(2, 4), z(2, 3), z(2, 3))]
+    assert len(ts) == 1 and ts[0].s_global == 4 and ts[0].entity == "tool"
+    ts.serializable()
+    assert ts.scene is None and ts[0].entity is None and not ts[0].pos.requires_grad
