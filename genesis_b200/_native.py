@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -184,6 +184,7 @@ SIGNATURES = {
     "mpm_g2p2g": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp]),
     "mpm_substeps": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp]),
     "mpm_substeps_noalloc": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, i64, vp]),
+    "mpm_noalloc_status": (C.c_int, [_P(Problem), i32, _P(C.c_uint32), vp, vp]),
     "mpm_adjoint_workspace_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
     "mpm_substep_adjoint": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),

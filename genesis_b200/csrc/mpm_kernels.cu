@@ -2229,12 +2229,21 @@ static void* g_noalloc_ptr[64];
 
 // Device address of the scratch array on the current device.  In host code the array's
 // name is only a host-side stand-in, so the address must come from cudaGetSymbolAddress,
-// asked once per device with that device current.
-static int noalloc_scratch(void** out) {
+// asked with that device current.  Outside stream capture the address is asked again on
+// every call, so a context torn down and rebuilt (cudaDeviceReset) is followed to the
+// module's new address; while `s` is capturing, the address cached by an earlier call
+// is used (the first call on a device must therefore come before any capture).
+static int noalloc_scratch(cudaStream_t s, void** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MPM_E_CUDA;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return MPM_E_CUDA;
+    }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || cap == cudaStreamCaptureStatusNone) {
+        if (cap != cudaStreamCaptureStatusNone) return MPM_E_INVALID;  // no set-up inside a capture
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
             cudaGetLastError();
@@ -2254,9 +2263,9 @@ int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_par
     if (!tab || !tab->instances || !tab->materials || n_substeps < 0) return MPM_E_INVALID;
     const uint64_t need = layout_of(*prob).total;
     if (need > (uint64_t)MPM_NOALLOC_SCRATCH_BYTES) return MPM_E_CAPACITY;
-    void* ws = nullptr;
-    if ((rc = noalloc_scratch(&ws))) return rc;
     cudaStream_t s = (cudaStream_t)stream;
+    void* ws = nullptr;
+    if ((rc = noalloc_scratch(s, &ws))) return rc;
     // the array keeps the previous call's contents (possibly another problem's layout):
     // start from the zeroed state mpm_workspace_init gives, then bin the particles
     if (cudaMemsetAsync(ws, 0, need, s) != cudaSuccess) return MPM_E_CUDA;
@@ -2264,6 +2273,30 @@ int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_par
     const bool sorts_first = sort_interval > 0 && (first_substep % sort_interval) == 0;
     if (!sorts_first && (rc = launch_sort(prob, tab, par, ws, s))) return rc;
     return substeps_impl(prob, tab, par, ws, n_substeps, sort_interval, first_substep, s);
+}
+
+int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, uint32_t* inst_out, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!out) return MPM_E_INVALID;
+    if (layout_of(*prob).total > (uint64_t)MPM_NOALLOC_SCRATCH_BYTES) return MPM_E_CAPACITY;
+    cudaStream_t s = (cudaStream_t)stream;
+    void* ws = nullptr;
+    if ((rc = noalloc_scratch(s, &ws))) return rc;
+    Ws w = ws_of(*prob, ws);
+    const size_t ibytes = (size_t)prob->n_instances * 4;
+    uint32_t v = 0;
+    if (cudaMemcpyAsync(&v, &w.counters[CNT_STATUS], 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPM_E_CUDA;
+    if (inst_out && ibytes &&
+        cudaMemcpyAsync(inst_out, w.inst_status, ibytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return MPM_E_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return MPM_E_CUDA;
+    if (clear) {
+        if (cudaMemsetAsync(&w.counters[CNT_STATUS], 0, 4, s) != cudaSuccess) return MPM_E_CUDA;
+        if (ibytes && cudaMemsetAsync(w.inst_status, 0, ibytes, s) != cudaSuccess) return MPM_E_CUDA;
+    }
+    *out = v;
+    return MPM_OK;
 }
 
 // ---------------------------------------------------------------- adjoint

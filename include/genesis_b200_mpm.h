@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 6
+#define MPM_ABI_VERSION 7
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -291,10 +291,25 @@ int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* 
  * any stream capture.  Each call clears the bytes it uses and re-bins the particles, so
  * its results match mpm_substeps; all calls share the one array, so calls that overlap
  * on the GPU (other streams, other threads) race and must be serialised by the caller.
+ * Outside stream capture every call looks the address up again, so a device reset
+ * (cudaDeviceReset) between calls is followed; a call made while `stream` is capturing
+ * uses the address an earlier call found, and returns MPM_E_INVALID if there was none.
+ * The status word of the run (NaN positions, stencils outside the grid, non-finite
+ * velocities) stays in the array until the next call clears it: read it with
+ * mpm_noalloc_status.
  * No counterpart in the reference. */
 #define MPM_NOALLOC_SCRATCH_BYTES (32u << 20)
 int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par,
                          int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
+
+/* The NaN check (mpm_solver.py:505-509, bits of _is_state_valid :451-457) for callers of
+ * mpm_substeps_noalloc, who hold no workspace to pass to mpm_status: reads, from the
+ * library's static array, the status word that the last mpm_substeps_noalloc call with
+ * the same `prob` left, into *out, and, when inst_out is not NULL, the n_instances
+ * per-instance words into inst_out (host memory).  With clear != 0 both are reset
+ * afterwards.  Synchronises the stream; allocates nothing.  Must be called before the
+ * next mpm_substeps_noalloc, which clears them. */
+int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, uint32_t* inst_out, void* stream);
 
 /* ---- differentiation (Elastic corotated / neo-Hookean, Muscle) --------------
  * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with elastic.py:62-83 and

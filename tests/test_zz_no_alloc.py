@@ -3,8 +3,9 @@
 Some callers can't allocate device memory: host applications whose allocator reserves
 the GPU up front, and plugin hosts that forbid cudaMalloc.  For them the library keeps
 its workspace in a static device array.  This file checks that two calls in a row give
-the same state as the ordinary entry point with a caller-allocated workspace, and that
-oversized problems are refused before any work is queued.  It is named so that pytest
+the same state as the ordinary entry point with a caller-allocated workspace and as the
+float64 oracle, that the NaN check reaches such a caller through mpm_noalloc_status, and
+that oversized problems are refused before any work is queued.  It is named so that pytest
 collects it last.
 """
 
@@ -54,6 +55,42 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
         assert np.abs(a["F"] - b["F"]).max() <= 1e-5, call
         assert np.abs(a["Jp"] - b["Jp"]).max() <= 1e-6, call
     assert ref.status() == 0
+    word, inst = C.c_uint32(7), (C.c_uint32 * 1)(7)
+    assert lib.mpm_noalloc_status(C.byref(noa.prob), 0, C.byref(word), inst, _stream()) == 0
+    assert word.value == 0 and inst[0] == 0
+    # the allocation-free run against the float64 oracle, 2 x 20 substeps from the same start
+    from oracle import bridge, cref
+
+    want, rc = cref.substeps(*bridge.from_desc(d, np.float64), 2 * n)
+    assert rc == 0
+    assert np.abs(b["pos"] - want["x"]).max() <= 1e-5
+
+
+@pytest.mark.gpu
+def test_noalloc_status_reports_a_nan_position():
+    """A NaN position planted on the host sets MPM_STATUS_NAN in the word the caller reads back
+    through mpm_noalloc_status; clearing resets it, and the next call starts from zero."""
+    from genesis_b200.engine.runtime import runtime_from_descs
+
+    d = W.elastic_cube(n_side=8)
+    noa = runtime_from_descs([d], use_graphs=False)
+    pos = d.pos.copy()
+    pos[3] = np.nan
+    noa.set_state(pos=pos)
+    lib = nat.load()
+    assert lib.mpm_substeps_noalloc(C.byref(noa.prob), C.byref(noa.tables), C.byref(noa.par), 2, 8, 0,
+                                    _stream()) == 0
+    word, inst = C.c_uint32(0), (C.c_uint32 * 1)(0)
+    assert lib.mpm_noalloc_status(C.byref(noa.prob), 1, C.byref(word), inst, _stream()) == 0
+    assert word.value & nat.MPM_STATUS_NAN and inst[0] & nat.MPM_STATUS_NAN
+    assert lib.mpm_noalloc_status(C.byref(noa.prob), 0, C.byref(word), inst, _stream()) == 0
+    assert word.value == 0 and inst[0] == 0
+    # a clean problem after it: the next call clears the array, so its word reads 0
+    clean = runtime_from_descs([W.elastic_cube(n_side=8)], use_graphs=False)
+    assert lib.mpm_substeps_noalloc(C.byref(clean.prob), C.byref(clean.tables), C.byref(clean.par), 2, 8, 0,
+                                    _stream()) == 0
+    assert lib.mpm_noalloc_status(C.byref(clean.prob), 0, C.byref(word), None, _stream()) == 0
+    assert word.value == 0
 
 
 def test_noalloc_refuses_problems_larger_than_its_scratch():
@@ -70,3 +107,5 @@ def test_noalloc_refuses_problems_larger_than_its_scratch():
     tab = nat.Tables(1, 1)  # never dereferenced: the size check comes first
     rc = lib.mpm_substeps_noalloc(C.byref(prob), C.byref(tab), C.byref(par), 1, 8, 0, None)
     assert rc == nat.MPM_E_CAPACITY
+    word = C.c_uint32()
+    assert lib.mpm_noalloc_status(C.byref(prob), 0, C.byref(word), None, None) == nat.MPM_E_CAPACITY
