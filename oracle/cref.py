@@ -84,9 +84,20 @@ def max_threads() -> int:
 
 
 def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_threads: int = 0,
-             mu_p=None, lam_p=None) -> tuple[dict, int]:
+             mu_p=None, lam_p=None, branch_margin=None) -> tuple[dict, int]:
     """Run n_substeps in C on a copy of the state; returns (new_state, status).  mu_p/lam_p:
-    optional per-particle Lame parameters."""
+    optional per-particle Lame parameters.  branch_margin: optional float array [n] of the
+    state's dtype, lowered in place to each particle's smallest distance (over the run) to
+    its return mapping's branch switch (Sand |tr|, von Mises |delta_gamma|, clamp distance);
+    initialise it to +inf."""
+    if branch_margin is not None:
+        L = lib(p.dtype)
+        assert branch_margin.dtype == np.dtype(p.dtype) and branch_margin.flags.c_contiguous
+        L.ref_set_branch_margin(branch_margin.ctypes.data_as(C.c_void_p))
+        try:
+            return substeps(p, mats, st, n_substeps, n_threads, mu_p, lam_p)
+        finally:
+            L.ref_set_branch_margin(None)
     dt = np.dtype(p.dtype)
     L = lib(dt)
     Params, Mat, Coll = _structs(dt)

@@ -32,6 +32,26 @@ def _mT(A):
     return np.swapaxes(A, -1, -2)
 
 
+def backward_svd(gU, gS, gV, U, S, V):
+    """Restatement of the reference's backward_svd (mpm_solver.py:1106-1129, the PyTorch
+    SVD adjoint), batched over the leading axis: given the adjoints of U, S (a 3x3 matrix,
+    diagonal in the forward) and V of F = U S V^T, the adjoint of F is
+      U [(F o (U^T gU - gU^T U)) S] V^T + U [S ((F o (V^T gV - gV^T V)) V^T)] + U gS V^T,
+    with F_ij = 1 / signmax(s_j^2 - s_i^2, 1e-6) off the diagonal and 0 on it, s_i = S_ii,
+    signmax(a, e) = sign(a) max(|a|, e) (sign(0) = +1)."""
+    vt, ut = _mT(V), _mT(U)
+    s2 = np.diagonal(S, axis1=-2, axis2=-1) ** 2
+    diff = s2[..., None, :] - s2[..., :, None]  # [i, j] = s_j^2 - s_i^2
+    sm = np.where(diff >= 0, 1.0, -1.0) * np.maximum(np.abs(diff), 1e-6)
+    Fm = 1.0 / sm
+    idx = np.arange(3)
+    Fm[..., idx, idx] = 0.0
+    s_term = U @ gS @ vt
+    u_term = U @ ((Fm * (ut @ gU - _mT(gU) @ U)) @ S) @ vt
+    v_term = U @ (S @ ((Fm * (vt @ gV - _mT(gV) @ V)) @ vt))
+    return u_term + v_term + s_term
+
+
 def _weights_and_grads(fx):
     w = [0.5 * (1.5 - fx) ** 2, 0.75 - (fx - 1.0) ** 2, 0.5 * (fx - 0.5) ** 2]
     dw = [-(1.5 - fx), -2.0 * (fx - 1.0), fx - 0.5]

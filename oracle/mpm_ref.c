@@ -290,6 +290,35 @@ static void constitutive(const ref_material* m, REAL eps, REAL J, const REAL* Ft
     }
 }
 
+/* Branch margins (test instrumentation, off unless ref_set_branch_margin gave a buffer):
+ * for each particle, the smallest distance seen so far to the switch of its return
+ * mapping's branch -- Sand |tr| (sand.py:60-62), von Mises |delta_gamma|
+ * (elasto_plastic.py:76-78), clamp / Snow min over d of |S_d - (1 - yield_lower)| and
+ * |S_d - (1 + yield_higher)| (elasto_plastic.py:89, snow.py:67).  A float32 run can take the
+ * other branch where this is within its rounding.  One buffer for the whole library: not
+ * for concurrent calls. */
+static REAL* g_branch_margin = NULL;
+
+void ref_set_branch_margin(REAL* buf) { g_branch_margin = buf; }
+
+static void record_branch_margin(const ref_material* m, REAL eps, const REAL* S, REAL Jp, REAL* out) {
+    REAL d = *out;
+    if (m->kind == 3) {
+        REAL tr = Jp;
+        for (int k = 0; k < 3; ++k) tr += RLOG(RMAX(RABS(S[k]), (REAL)1e-4));
+        d = RMIN(d, RABS(tr));
+    } else if (m->kind == 1 && (m->flags & 2)) {
+        REAL e[3];
+        for (int k = 0; k < 3; ++k) e[k] = RLOG(RMAX(S[k], (REAL)0.05));
+        REAL mean = (e[0] + e[1] + e[2]) / 3, q = eps;
+        for (int k = 0; k < 3; ++k) q += (e[k] - mean) * (e[k] - mean);
+        d = RMIN(d, RABS(R_SQRT(q) - m->vm_threshold));
+    } else if (m->kind == 1 || m->kind == 4) {
+        for (int k = 0; k < 3; ++k) d = RMIN(d, RMIN(RABS(S[k] - m->clamp_lo), RABS(S[k] - m->clamp_hi)));
+    }
+    *out = d;
+}
+
 static REAL bc_vel(REAL pos, REAL vel, REAL lo, REAL hi) {
     if (pos >= hi && vel >= 0) return vel * (REAL)-0.0;
     if (pos <= lo && vel <= 0) return vel * (REAL)-0.0;
@@ -601,6 +630,7 @@ int ref_substeps_cpic(const ref_params* p, const ref_material* mats, int n, REAL
                 mp.lam = lam_p[i];
                 m = &mp;
             }
+            if (g_branch_margin) record_branch_margin(m, p->eps, S, Jp[i], &g_branch_margin[i]);
             constitutive(m, p->eps, J, Ft, U, S, V, Jp[i], Fn, &Jpn, st);
             if ((m->flags & 4) && actu) {
                 /* muscle.py:57-65: stress += stiffness * actu * F_tmp (d d^T) F_tmp^T */

@@ -4,7 +4,7 @@ Tolerances (float32 kernels, float32/float64 oracle):
   * grid mass and momentum sums after p2g: 1e-6 relative;
   * per-node grid values: 1e-5 of the largest node value;
   * particle positions after 100 substeps: 1e-5 of the domain size (1 m); velocities
-    within 1e-5 m/s per m of domain per ms of simulated time scale (reported);
+    1e-5 m/s (the elastic cube);
   * single-substep state per material: the CUDA error against the float64 oracle must be
     within 20x the float32 oracle's own error (+ a small absolute floor), because
     atomics sum in a different order than the oracle.
@@ -49,10 +49,12 @@ def _dense_grid(rt, inst=0):
     return (block_major_to_dense(mm.cpu().numpy(), sp, base), block_major_to_dense(gv.cpu().numpy(), sp, base))
 
 
-def test_p2g_grid_matches_oracle():
+@pytest.mark.parametrize("n_side", [16, 32])
+def test_p2g_grid_matches_oracle(n_side):
+    """Grid mass/momentum after the first p2g; n_side 32 is the full 32,768-particle cube."""
     from oracle import mpm_ref as R
 
-    d = W.elastic_cube(n_side=16)
+    d = W.elastic_cube(n_side=n_side)
     d.vel = np.random.default_rng(5).normal(0, 0.5, size=d.vel.shape)
     rt = _rt([d])
     rt.sort()
@@ -129,31 +131,28 @@ def test_100_substeps_elastic_cube_full_size():
     ex = np.abs(g["pos"] - o["x"]).max()
     ev = np.abs(g["vel"] - o["v"]).max()
     assert ex <= 1e-5, ex
-    assert ev <= 1e-3 * max(1.0, np.abs(o["v"]).max()), ev
+    assert ev <= 1e-5, ev  # m/s (measured ~2e-7)
     assert rt.status() == 0
 
 
 def test_100_substeps_mixed_materials_reduced():
     """Four boxes (Liquid, Sand, Snow, ElastoPlastic) at 12^3 particles each on the 129^3 grid.
 
-    Per material, positions after 100 substeps must be within 1e-5 of the float64 oracle,
-    or within 2x the float32 oracle's own deviation where float32 itself cannot reach 1e-5
-    (Sand: particles near the tr = 0 branch of the Drucker-Prager projection switch
-    branch under float32 rounding; the float32 CPU restatement deviates ~3e-5 there)."""
-    from oracle import cref
+    Per material, positions after 100 substeps within 1e-5 m of the reference's precision-32
+    model computed in float64 (float64 arithmetic with the float32 gs.EPS, which the plastic
+    return mappings use in Matrix.norm(EPS): sand.py:61, elasto_plastic.py:74)."""
+    from oracle import bridge, cref
 
     d = W.mixed_500k(n_side=12)
     rt = _rt([d])
     rt.substeps(100)
     g = _state_np(rt)
-    o, rc = cref.substeps(*_oracle(d, np.float64), 100)
-    o32, _ = cref.substeps(*_oracle(d, np.float32), 100)
+    o, rc = cref.substeps(*bridge.from_desc(d, np.float64, model_dtype=np.float32), 100)
     assert rc == 0
     for m in range(4):
         sel = d.mat_idx == m
         ex = np.abs(g["pos"][sel] - o["x"][sel]).max()
-        e32 = np.abs(o32["x"][sel] - o["x"][sel]).max()
-        assert ex <= max(1e-5, 2 * e32), (m, ex, e32)
+        assert ex <= 1e-5, (m, ex)
 
 
 def test_state_roundtrip_and_sort_permutation():
@@ -259,10 +258,10 @@ def test_full_size_mixed_500k_conservation():
     mm, _ = _dense_grid(rt)
     mats = rt._mats
     masses = np.array([mats[int(k)].mass for k in d.mat_idx])
-    assert np.isclose(mm[..., 3].sum(dtype=np.float64), masses.sum(), rtol=1e-5)
+    assert np.isclose(mm[..., 3].sum(dtype=np.float64), masses.sum(), rtol=1e-6)
     mom = (masses[:, None] * d.vel).sum(0)
     scale = (masses[:, None] * np.abs(d.vel)).sum()
-    assert np.allclose(mm[..., :3].sum(axis=(0, 1, 2), dtype=np.float64), mom, atol=1e-5 * scale)
+    assert np.allclose(mm[..., :3].sum(axis=(0, 1, 2), dtype=np.float64), mom, atol=1e-6 * scale)
     rt.grid_op()
     rt.g2p()
     rt._count += 1
