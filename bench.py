@@ -42,7 +42,7 @@ WORKLOAD = (
     "mixed_500k: 4 x 125,000 particles (Liquid, Sand, Snow, ElastoPlastic), grid_density 128 (129^3 nodes), "
     "dt 5e-5, 100 substeps per step"
 )
-# algorithmic bytes per particle / per active grid node, per kernel
+# algorithmic bytes per particle / per active grid node, per kernel kind
 BYTES = {
     "p2g": (148, 16),  # read x,v,C,F,Jp (100) + material idx & mass (8); write F,Jp (40); grid m+mom (16)
     "grid_op": (0, 28),  # read m+mom (16), write v (12)
@@ -51,6 +51,12 @@ BYTES = {
     # (12) and m+mom write (16).  v and C never leave registers, so the DRAM bytes it must
     # move are lower (x, F, Jp read + written: ~106 B/particle); 'traffic' reports ncu's count.
     "g2p2g": (208, 28),
+    # the same with the grid op folded in: one whole substep, 208 B/particle + 56 B/node
+    # (the node velocity never reaches memory, so the DRAM bytes are lower still)
+    "g2p2g_fold": (208, 56),
+    "g2p_fold": (60, 40),  # grid op (28) + g2p (60 + 12)
+    "grid_clear": (0, 16),  # zero m+mom
+    "sort": (220, 0),  # read + write the 25 state channels, material, flags, ids (~2 x 110)
 }
 SUBSTEP_BYTES = (208, 56)
 
@@ -250,47 +256,56 @@ def reduce_max(world, x: float) -> float:
 
 
 # ------------------------------------------------------------------ CPU (reference arm)
-def cpu_port_rate(desc, target_s=12.0, max_substeps=40):
-    """Time the C/OpenMP restatement on all host threads; returns (rate, threads, sample)."""
+CPU_SUB = 2  # substeps per timed CPU step: a bounded sample of the 100-substep step
+
+
+def cpu_sample(desc, threads, steps, sub=CPU_SUB):
+    """The CPU sample both CPU legs time: the C/OpenMP restatement in float32 from the
+    workload's initial state, one untimed warm-up substep, then `steps` timed steps of `sub`
+    substeps each.  Returns (per-step seconds, final state)."""
     import numpy as np
 
     from oracle import bridge, cref
 
-    threads = os.cpu_count() or 1
     p, mats, st = bridge.from_desc(desc, np.float32)
-    t0 = time.perf_counter()
-    st1, _ = cref.substeps(p, mats, st, 1, n_threads=threads)
-    one = time.perf_counter() - t0
-    n = int(max(1, min(max_substeps, target_s / max(one, 1e-3))))
-    t0 = time.perf_counter()
-    cref.substeps(p, mats, st1, n, n_threads=threads)
-    el = time.perf_counter() - t0
-    rate = desc.n_particles * n / el
-    return rate, threads, f"{desc.n_particles:,} particles x {n} substeps (after 1 warm-up substep), float32"
+    st, _ = cref.substeps(p, mats, st, 1, n_threads=threads)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        st, _ = cref.substeps(p, mats, st, sub, n_threads=threads)
+        times.append(time.perf_counter() - t0)
+    return times, st
+
+
+def cpu_port_rate(desc, steps, single_thread_steps=5):
+    """cpu_baseline leg: the same sample as the reference arm on all host threads, and a
+    shorter prefix of it on one thread."""
+    threads = os.cpu_count() or 1
+    times, _ = cpu_sample(desc, threads, steps)
+    rate = desc.n_particles * CPU_SUB * steps / sum(times)
+    t1, _ = cpu_sample(desc, 1, single_thread_steps)
+    rate1 = desc.n_particles * CPU_SUB * single_thread_steps / sum(t1)
+    sample = (f"{desc.n_particles:,} particles, float32: 1 warm-up substep, then {steps} steps x {CPU_SUB} substeps "
+              "(the reference arm's sample)")
+    single = {"value": rate1, "unit": UNIT, "cores": 1,
+              "sample": f"{desc.n_particles:,} particles, float32: 1 warm-up substep, then "
+                        f"{single_thread_steps} steps x {CPU_SUB} substeps"}
+    return rate, threads, sample, single
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return None
-    import numpy as np
-
     from genesis_b200 import workloads as W
-    from oracle import bridge, cref
 
     d = W.mixed_500k(n_side=args.n_side, grid_density=args.grid_density)
     threads = os.cpu_count() or 1
-    p, mats, st = bridge.from_desc(d, np.float32)
-    sub = 2  # substeps per reference step: a bounded sample of the 100-substep step
-    for _ in range(max(0, min(args.warmup, 1))):
-        st, _ = cref.substeps(p, mats, st, 1, n_threads=threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        st, _ = cref.substeps(p, mats, st, sub, n_threads=threads)
-        times.append(time.perf_counter() - t0)
+    sub = CPU_SUB
+    times, _ = cpu_sample(d, threads, args.steps)
     el = sum(times)
     value = d.n_particles * sub * args.steps / el
-    sample = f"{d.n_particles:,} particles x {sub} substeps per step, float32, {threads} threads"
+    sample = (f"{d.n_particles:,} particles, float32, {threads} threads: 1 warm-up substep, then {args.steps} steps x "
+              f"{sub} substeps")
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -315,42 +330,36 @@ def run_reference(args, world, rank):
 
 
 # ------------------------------------------------------------------ GPU (our arm)
-def kernel_breakdown(rt, n_substeps=20):
-    """Per-kernel CUDA-event durations (ms) over the same launch sequence mpm_substeps uses:
-    p2g + grid_op for the first substep, then fused g2p2g + grid_op, with g2p / sort / p2g
-    where a re-sort falls; the GPU is kept busy so events bracket kernels back to back."""
+def kernel_breakdown(rt, n_substeps):
+    """Per-kernel-kind device time over n_substeps of the mpm_substeps schedule, from CUDA
+    events recorded between consecutive launch groups (mpm_substeps_profile): returns
+    {kind: (ms per launch group, launch groups, kernel launches)} and the total ms.  The GPU
+    is kept busy while the launches are enqueued, so the events bracket kernels back to back."""
     import torch
 
-    ev = lambda: torch.cuda.Event(enable_timing=True)
-    acc = {"sort": [], "p2g": [], "grid_op": [], "g2p": [], "g2p2g": []}
-    K = max(rt.sort_interval, 1)
     torch.cuda.synchronize()
     torch.cuda._sleep(int(2e8))
+    prof = rt.profile_substeps(n_substeps)
+    total = sum(ms for ms, _ in prof.values())
+    out = {}
+    for k, (ms, launches) in prof.items():
+        groups = launches // (SORT_KERNELS if k == "sort" else 1)
+        if groups:
+            out[k] = (ms / groups, groups, launches)
+    return out, total
 
-    def timed(name, fn):
-        a, b = ev(), ev()
-        a.record()
-        fn()
-        b.record()
-        acc[name].append((a, b))
 
-    for i in range(n_substeps):
-        due = rt._count % K == 0
-        if i == 0:
-            if due:
-                timed("sort", rt.sort)
-            timed("p2g", rt.p2g)
-        elif due:
-            timed("g2p", rt.g2p)
-            timed("sort", rt.sort)
-            timed("p2g", rt.p2g)
-        else:
-            timed("g2p2g", rt.g2p2g)
-        timed("grid_op", rt.grid_op)
-        rt._count += 1
-    timed("g2p", rt.g2p)
-    torch.cuda.synchronize()
-    return {k: (statistics.mean(a.elapsed_time(b) for a, b in v) if v else 0.0, len(v)) for k, v in acc.items()}
+SORT_KERNELS = 7  # keys, 3 scan passes, chunk table, scatter, lane deal
+
+
+def launches_per_step(S, K):
+    """Kernel launches of one timed step (S substeps from a sort boundary) on the collider-free
+    scene: the runtime replays one CUDA graph per sort interval of K substeps, each the
+    mpm_substeps schedule: the sort, p2g, K - 1 fused substeps with the grid op folded into
+    them, the last g2p and the clear of the last momentum buffer."""
+    graphs, rest = divmod(S, K)
+    per = lambda k: SORT_KERNELS + 1 + (k - 1) + 2
+    return graphs * per(K) + (per(rest) if rest else 0)
 
 
 def active_nodes(rt):
@@ -483,23 +492,20 @@ def run_ours(args, world, rank, local):
 
     # per-kernel breakdown + roofline of the dominant kernel
     n_act = active_nodes(rt)
-    kb = kernel_breakdown(rt, 3 * args.sort_interval)
+    nsub = 2 * S
+    kb, prof_ms = kernel_breakdown(rt, nsub)
     hbm, src = peaks()
-    dom = max(("p2g", "grid_op", "g2p", "g2p2g"), key=lambda k: kb[k][0] * kb[k][1])
+    dom = max(kb, key=lambda k: kb[k][0] * kb[k][1])
     bp, bc = BYTES[dom]
     alg = bp * d.n_particles + bc * n_act
+    step_sub_ms = dev_ms / (args.steps * S)
     t_dom = kb[dom][0] * 1e-3
     achieved = alg / t_dom / 1e9
     tr = ncu_traffic()
     # the committed ncu figure is the default scene's; other sizes report none
     traffic = tr.get(f"{dom}_dram_bytes_per_launch") if workload_name(args, d) == WORKLOAD else None
-    nsub = 3 * args.sort_interval
-    sub_ms = sum(kb[k][0] * kb[k][1] for k in kb) / nsub
     sub_alg = SUBSTEP_BYTES[0] * d.n_particles + SUBSTEP_BYTES[1] * n_act
-    # launches per timed step: 2 per substep (g2p2g + grid_op), +1 (g2p) at the end and
-    # +8 (g2p, 7 sort kernels, p2g replacing g2p2g) at each re-sort
-    sorts = sum(1 for i in range(S) if i % args.sort_interval == 0)
-    gpu_launches = args.steps * (2 * S + 1 + 8 * sorts)
+    gpu_launches = args.steps * launches_per_step(S, args.sort_interval)
 
     res = {
         "metric": METRIC,
@@ -537,8 +543,16 @@ def run_ours(args, world, rank, local):
             "alg_bytes_per_launch": alg,
             "active_nodes": n_act,
             "kernel_ms": {k: round(v[0], 5) for k, v in kb.items()},
-            "substep_alg_GBs": sub_alg / (sub_ms * 1e-3) / 1e9,
-            "substep_frac": sub_alg / (sub_ms * 1e-3) / 1e9 / hbm,
+            "kernel_share": {k: round(v[0] * v[1] / prof_ms, 4) for k, v in kb.items()},
+            "launches_per_substep": {k: round(v[2] / nsub, 4) for k, v in kb.items()},
+            "timing": f"CUDA events between consecutive launch groups over {nsub} substeps of the same "
+                      "schedule (mpm_substeps_profile, no graph); kernel_ms is per launch group (a sort is 7 "
+                      "kernels)",
+            "profile_ms_per_substep": prof_ms / nsub,
+            "substep_ms": step_sub_ms,
+            "profile_vs_step": (prof_ms / nsub) / step_sub_ms,
+            "substep_alg_GBs": sub_alg / (step_sub_ms * 1e-3) / 1e9,
+            "substep_frac": sub_alg / (step_sub_ms * 1e-3) / 1e9 / hbm,
         },
         "gpu_launches": gpu_launches,
         "clocks": clk,
@@ -576,10 +590,11 @@ def run_batched(args, world, rank):
     torch.cuda.synchronize()
     t_b = reduce_max(world, a.elapsed_time(b) * 1e-3)
     status = bs.rt.status()
-    split = kernel_breakdown(bs.rt, n_substeps=2 * K)
+    split, _ = kernel_breakdown(bs.rt, 2 * K)
     del bs
     torch.cuda.empty_cache()
-    t_s = reduce_max(world, run_sequential(descs, S))
+    per_scene = run_sequential(descs, S, per_scene=True)
+    t_s = reduce_max(world, sum(per_scene))
     return {
         "workload": f"{args.batch_scenes} scenes, N log-uniform [2e3, 2e5], grid 33^3/65^3/97^3, 5 materials, "
                     f"E log-uniform [1e4, 1e6], {S} substeps each",
@@ -593,6 +608,33 @@ def run_batched(args, world, rank):
         "tuning": tuning,
         "kernel_ms": {k: round(v[0], 5) for k, v in split.items()},
         "status_word": status,
+        "amdahl": amdahl_ceiling(descs, per_scene, S, t_b),
+    }
+
+
+def amdahl_ceiling(descs, seq_times, S, t_batched, large=50_000):
+    """How far batching alone can go on this scene set.  Batching removes per-scene costs
+    (launches, grid-op passes, sort and graph boundaries, a persistent grid's tail) that
+    weigh on small scenes; a large scene already runs at the fused kernel's per-particle rate.
+    The ceiling assumes every scene ran at the per-particle-substep rate that the plain path
+    reaches on the large scenes (>= `large` particles) -- removing all per-scene overhead and
+    nothing else -- and divides the sequential time by that."""
+    big = [i for i, d in enumerate(descs) if d.n_particles >= large]
+    work = [d.n_particles * S for d in descs]
+    t_seq = sum(seq_times)
+    t_big = sum(seq_times[i] for i in big)
+    w_big = sum(work[i] for i in big)
+    rate_big = w_big / t_big if t_big > 0 else None
+    t_ideal = sum(work) / rate_big if rate_big else None
+    return {
+        "large_scene_particles": large,
+        "large_scenes": len(big),
+        "sequential_time_fraction_in_large": t_big / t_seq if t_seq else None,
+        "work_fraction_in_large": w_big / sum(work) if work else None,
+        "large_scene_rate": rate_big,
+        "max_speedup_if_all_at_large_rate": t_seq / t_ideal if t_ideal else None,
+        "batched_vs_large_rate": (sum(work) / t_batched) / rate_big if rate_big else None,
+        "three_x_reachable_by_batching_alone": (t_seq / t_ideal >= 3.0) if t_ideal else None,
     }
 
 
@@ -638,6 +680,15 @@ def run_served(args, world, rank, capacity):
         del rt
     seq_lat = serve.sequential_timeline(reqs, durs)
     total_work = sum(work)
+    # capacity at saturation: the same requests all queued at t = 0 (offered load >= capacity)
+    srv_sat = serve.MPMServer(budget_bytes=150e9, tick_substeps=50, keep_results=False)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    res_sat = srv_sat.serve(reqs, realtime=False)
+    wall_sat = reduce_max(world, time.perf_counter() - t0)
+    del srv_sat
+    seq_rate = my_work / sum(durs)
     return {
         "workload": f"{args.serve_requests} Poisson requests (rate {rate:.2f}/s = 80% of measured batched capacity), "
                     "N log-uniform [1e3, 5e5], grid density 32-128, substeps U[100, 2000], 150 GB budget",
@@ -649,10 +700,20 @@ def run_served(args, world, rank, capacity):
         "errors": errors,
         "ticks": srv.ticks,
         "repacks": srv.repacks,
-        "sequential_value": my_work / sum(durs),
+        "sequential_value": seq_rate,
         "sequential_p50_latency_s": serve.percentile(seq_lat, 50),
         "sequential_p99_latency_s": serve.percentile(seq_lat, 99),
         "wall_s": wall,
+        "note": "at 80% offered load the served throughput is the offered load by construction; "
+                "saturation.value is the server's capacity",
+        "saturation": {
+            "value": total_work / wall_sat,
+            "unit": UNIT,
+            "wall_s": wall_sat,
+            "errors": sum(1 for r in res_sat if r.error is not None),
+            "speedup_vs_sequential": (total_work / wall_sat) / (seq_rate * world),
+            "offered": "all requests queued at t = 0",
+        },
     }
 
 
@@ -730,8 +791,9 @@ def main():
         res["served"] = run_served(args, world, rank, cap)
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, threads, sample = cpu_port_rate(d)
-        res["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        rate, threads, sample, single = cpu_port_rate(d, args.steps)
+        res["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                               "single_thread": single}
     if rank == 0:
         print(json.dumps(res))
     if world > 1:

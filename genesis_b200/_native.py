@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -45,6 +45,9 @@ PROBF_NONFREE = 1
 PROBF_CPIC = 2
 
 MAT_ELASTIC, MAT_ELASTOPLASTIC, MAT_LIQUID, MAT_SAND, MAT_SNOW = 0, 1, 2, 3, 4
+
+# kernel kinds of mpm_substeps_profile
+KIND_NAMES = ("sort", "p2g", "grid_op", "g2p", "g2p2g", "g2p2g_fold", "g2p_fold", "grid_clear")
 MATF_NEOHOOKEAN = 1
 MATF_VON_MISES = 2
 MATF_MUSCLE = 4
@@ -185,6 +188,7 @@ SIGNATURES = {
     "mpm_substeps": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp]),
     "mpm_substeps_noalloc": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, i64, vp]),
     "mpm_noalloc_status": (C.c_int, [_P(Problem), i32, _P(C.c_uint32), vp, vp]),
+    "mpm_substeps_profile": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp, vp, vp]),
     "mpm_adjoint_workspace_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
     "mpm_substep_adjoint": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),

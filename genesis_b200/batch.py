@@ -43,10 +43,12 @@ class BatchedScenes:
         return [{k: v[o : o + d.n_particles] for k, v in st.items()} for o, d in zip(self.offsets, self.descs)]
 
 
-def run_sequential(descs, n_substeps: int, **runtime_kw) -> float:
+def run_sequential(descs, n_substeps: int, per_scene: bool = False, **runtime_kw):
     """The plain one-scene-at-a-time path: each scene gets its own runtime and runs alone.
-    Returns device seconds (CUDA events around each scene's substeps, summed)."""
+    Returns device seconds (CUDA events around each scene's substeps, summed), or with
+    per_scene=True the list of each scene's seconds."""
     total = 0.0
+    times = []
     for d in descs:
         rt = runtime_from_descs([d], **runtime_kw)
         rt.substeps(min(n_substeps, rt.sort_interval))  # warm: first sort + graph capture
@@ -55,6 +57,7 @@ def run_sequential(descs, n_substeps: int, **runtime_kw) -> float:
         rt.substeps(n_substeps)
         b.record()
         torch.cuda.synchronize()
-        total += a.elapsed_time(b) * 1e-3
+        times.append(a.elapsed_time(b) * 1e-3)
+        total += times[-1]
         del rt
-    return total
+    return times if per_scene else total

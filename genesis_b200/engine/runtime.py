@@ -660,6 +660,32 @@ class MPMRuntime:
             out.append(d)
         return out
 
+    def profile_substeps(self, n: int) -> dict:
+        """Advance n substeps as substeps() does, without CUDA graphs, timing every launch
+        group with CUDA events (mpm_substeps_profile).  Returns {kind: (ms, launches)} summed
+        over the run; the kinds' times add up to the run's device time."""
+        n = int(n)
+        stream = _cuda_stream_handle()
+        K = max(self.sort_interval, 0)
+        nk = len(nat.KIND_NAMES)
+        ms, cnt = (C.c_float * nk)(), (C.c_int32 * nk)()
+        tot = {k: [0.0, 0] for k in nat.KIND_NAMES}
+        while n > 0:
+            phase = self._count % K if K else 1
+            if not getattr(self, "_sorted_once", False) or (self._dirty and phase != 0):
+                self.sort()
+                self._sorted_once = True
+            self._dirty = False
+            m = min(n, K - self._count % K) if K else n
+            self._call("mpm_substeps_profile", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                       m, K, self._count, ms, cnt, stream)
+            for i, k in enumerate(nat.KIND_NAMES):
+                tot[k][0] += float(ms[i])
+                tot[k][1] += int(cnt[i])
+            n -= m
+            self._count += m
+        return {k: (v[0], v[1]) for k, v in tot.items()}
+
     def fallback_count(self, clear: bool = False) -> int:
         v = C.c_uint64()
         self._call("mpm_fallback_count", C.byref(self.prob), self._ws, int(clear), C.byref(v), _cuda_stream_handle())

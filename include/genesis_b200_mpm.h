@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 7
+#define MPM_ABI_VERSION 8
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -274,7 +274,10 @@ int mpm_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par
               void* stream);
 
 /* n_substeps x (p2g, grid_op, g2p); re-sorts before substep i when
- * sort_interval > 0 and (first_substep + i) % sort_interval == 0. */
+ * sort_interval > 0 and (first_substep + i) % sort_interval == 0.  Problems without
+ * colliders and without non-free particles run the grid op inside the fused g2p/p2g kernel
+ * (the velocity of each node is computed from the momentum where a chunk loads it; three
+ * momentum buffers rotate in the workspace); the results are those of the separate kernels. */
 int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
                  int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
 
@@ -326,6 +329,26 @@ int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, ui
 int mpm_adjoint_workspace_bytes(const mpm_problem* prob, uint64_t* out);
 int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state, float* adj,
                         float* lame_bar, void* workspace, void* adj_workspace, void* stream);
+
+/* ---- timing ----------------------------------------------------------------
+ * mpm_substeps with a CUDA event recorded on `stream` after every launch group: on return
+ * (the stream is synchronised) ms_by_kind[k] holds the device milliseconds spent in kernels
+ * of kind k and launches_by_kind[k] their number of kernel launches, both arrays of
+ * MPM_N_KINDS entries.  Consecutive events bracket consecutive launches, so the kinds' times
+ * add up to the run's device time.  The simulation advances exactly as with mpm_substeps.
+ * No counterpart in the reference (its Taichi kernels are timed by its own profiler). */
+#define MPM_KIND_SORT 0        /* the 7 kernels of mpm_sort_particles */
+#define MPM_KIND_P2G 1
+#define MPM_KIND_GRID_OP 2
+#define MPM_KIND_G2P 3
+#define MPM_KIND_G2P2G 4
+#define MPM_KIND_G2P2G_FOLD 5  /* g2p fused with the next grid op and p2g (collider-free problems) */
+#define MPM_KIND_G2P_FOLD 6    /* g2p fused with the grid op before it */
+#define MPM_KIND_GRID_CLEAR 7  /* clearing the last momentum buffer of a folded run */
+#define MPM_N_KINDS 8
+int mpm_substeps_profile(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                         int32_t n_substeps, int32_t sort_interval, int64_t first_substep, float* ms_by_kind,
+                         int32_t* launches_by_kind, void* stream);
 
 /* Read (and optionally clear) the device status word; synchronises the stream. */
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream);
