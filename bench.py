@@ -51,11 +51,6 @@ BYTES = {
     # (12) and m+mom write (16).  v and C never leave registers, so the DRAM bytes it must
     # move are lower (x, F, Jp read + written: ~106 B/particle); 'traffic' reports ncu's count.
     "g2p2g": (208, 28),
-    # the same with the grid op folded in: one whole substep, 208 B/particle + 56 B/node
-    # (the node velocity never reaches memory, so the DRAM bytes are lower still)
-    "g2p2g_fold": (208, 56),
-    "g2p_fold": (60, 40),  # grid op (28) + g2p (60 + 12)
-    "grid_clear": (0, 16),  # zero m+mom
     "sort": (220, 0),  # read + write the 25 state channels, material, flags, ids (~2 x 110)
 }
 SUBSTEP_BYTES = (208, 56)
@@ -353,12 +348,11 @@ SORT_KERNELS = 7  # keys, 3 scan passes, chunk table, scatter, lane deal
 
 
 def launches_per_step(S, K):
-    """Kernel launches of one timed step (S substeps from a sort boundary) on the collider-free
-    scene: the runtime replays one CUDA graph per sort interval of K substeps, each the
-    mpm_substeps schedule: the sort, p2g, K - 1 fused substeps with the grid op folded into
-    them, the last g2p and the clear of the last momentum buffer."""
+    """Kernel launches of one timed step (S substeps from a sort boundary): the runtime replays
+    one CUDA graph per sort interval of K substeps, each the mpm_substeps schedule: the sort,
+    p2g and grid op, K - 1 times the fused g2p/p2g and the grid op, and the last g2p."""
     graphs, rest = divmod(S, K)
-    per = lambda k: SORT_KERNELS + 1 + (k - 1) + 2
+    per = lambda k: SORT_KERNELS + 2 + 2 * (k - 1) + 1
     return graphs * per(K) + (per(rest) if rest else 0)
 
 

@@ -47,7 +47,7 @@ PROBF_CPIC = 2
 MAT_ELASTIC, MAT_ELASTOPLASTIC, MAT_LIQUID, MAT_SAND, MAT_SNOW = 0, 1, 2, 3, 4
 
 # kernel kinds of mpm_substeps_profile
-KIND_NAMES = ("sort", "p2g", "grid_op", "g2p", "g2p2g", "g2p2g_fold", "g2p_fold", "grid_clear")
+KIND_NAMES = ("sort", "p2g", "grid_op", "g2p", "g2p2g")
 MATF_NEOHOOKEAN = 1
 MATF_VON_MISES = 2
 MATF_MUSCLE = 4

@@ -57,30 +57,14 @@ constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
 constexpr int MAX_SCAN_TILES = SCAN_T * SCAN_ITEMS;  // single-CTA scan of tile sums
 constexpr int64_t MAX_BLOCKS = (int64_t)SCAN_TILE * MAX_SCAN_TILES;
 
-enum Counter {
-    CNT_ACTIVE = 0, CNT_CHUNKS = 1, CNT_STATUS = 2, CNT_SORTED = 3, CNT_FALLBACK = 4 /* u64 at 4,5 */, CNT_DONE = 6,
-    // active-block counts and done counters of the second and third momentum buffers
-    CNT_ACTIVE1 = 8, CNT_ACTIVE2 = 9, CNT_DONE1 = 10, CNT_DONE2 = 11
-};
+enum Counter { CNT_ACTIVE = 0, CNT_CHUNKS = 1, CNT_STATUS = 2, CNT_SORTED = 3, CNT_FALLBACK = 4 /* u64 at 4,5 */, CNT_DONE = 6 };
 constexpr int N_COUNTERS = 16;
 
-// Grid op folded into the fused kernel (problems without colliders, CPIC or non-free
-// particles): three momentum buffers rotate, so a substep's kernel reads the momentum the
-// previous one scattered, scatters into the next buffer and clears the one read two
-// substeps ago; node velocities are computed in each CTA's tile load.
-#ifndef GBM_FOLD_GRID_OP
-#define GBM_FOLD_GRID_OP 1
-#endif
-
 struct Ws {
-    float4* mm;          // grid momentum.xyz + mass, block-major (the scatter target)
+    float4* mm;          // grid momentum.xyz + mass, block-major
     float4* gv;          // grid velocity (w unused)
     uint32_t* flag;      // per grid block: 1 if active this substep
     int2* active;        // active block list {instance, packed block coords}
-    uint32_t* act_count; // its length (a counter)
-    float4* mm_rot[3];   // the rotating momentum buffers of the folded path (mm_rot[0] == mm)
-    uint32_t* flag_rot[3];
-    int2* active_rot[3];
     int* bin_count;      // sort histogram
     int* bin_start;      // exclusive scan of bin_count
     int* chunk_start;    // exclusive scan of chunks per bin
@@ -101,7 +85,7 @@ struct Ws {
 
 static inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
-constexpr int N_LAYOUT = 25;
+constexpr int N_LAYOUT = 19;
 
 struct Layout {
     uint64_t off[N_LAYOUT];
@@ -134,12 +118,6 @@ static Layout layout_of(const mpm_problem& p) {
         n * 4,                     // lam_tmp
         N_COUNTERS * 4,            // counters
         (uint64_t)p.n_instances * 4,  // per-instance status
-        nb * BLK3 * 16,            // mm_rot[1]
-        nb * BLK3 * 16,            // mm_rot[2]
-        nb * 4,                    // flag_rot[1]
-        nb * 4,                    // flag_rot[2]
-        nb * 8,                    // active_rot[1]
-        nb * 8,                    // active_rot[2]
     };
     uint64_t o = 0;
     for (int i = 0; i < N_LAYOUT; ++i) {
@@ -174,45 +152,7 @@ static Ws ws_of(const mpm_problem& p, void* base) {
     w.counters = (uint32_t*)(b + L.off[17]);
     w.inst_status = (uint32_t*)(b + L.off[18]);
     w.tmp_stride = (int64_t)align_up(p.n_particles > 0 ? p.n_particles : 1, 64);
-    w.act_count = &w.counters[CNT_ACTIVE];
-    w.mm_rot[0] = w.mm;
-    w.mm_rot[1] = (float4*)(b + L.off[19]);
-    w.mm_rot[2] = (float4*)(b + L.off[20]);
-    w.flag_rot[0] = w.flag;
-    w.flag_rot[1] = (uint32_t*)(b + L.off[21]);
-    w.flag_rot[2] = (uint32_t*)(b + L.off[22]);
-    w.active_rot[0] = w.active;
-    w.active_rot[1] = (int2*)(b + L.off[23]);
-    w.active_rot[2] = (int2*)(b + L.off[24]);
     return w;
-}
-
-// counters of rotating buffer b: its active-block count and its done counter
-static inline int rot_count(int b) { return b == 0 ? CNT_ACTIVE : (b == 1 ? CNT_ACTIVE1 : CNT_ACTIVE2); }
-static inline int rot_done(int b) { return b == 0 ? CNT_DONE : (b == 1 ? CNT_DONE1 : CNT_DONE2); }
-
-// w with rotating buffer b as the scatter target
-static Ws ws_target(const Ws& w, int b) {
-    Ws t = w;
-    t.mm = w.mm_rot[b];
-    t.flag = w.flag_rot[b];
-    t.active = w.active_rot[b];
-    t.act_count = &w.counters[rot_count(b)];
-    return t;
-}
-
-// a momentum buffer to clear from its active-block list
-struct GridClear {
-    float4* mm;
-    uint32_t* flag;
-    const int2* active;
-    uint32_t* count;
-    uint32_t* done;
-};
-
-static GridClear grid_clear_of(const Ws& w, int b) {
-    return GridClear{w.mm_rot[b], w.flag_rot[b], w.active_rot[b], &w.counters[rot_count(b)],
-                     &w.counters[rot_done(b)]};
 }
 
 // ---------------------------------------------------------------- helpers
@@ -296,7 +236,7 @@ __device__ __forceinline__ void mark_block(Ws& w, int inst, const mpm_instance& 
     const int lb = (bx * I.nblk[1] + by) * I.nblk[2] + bz;
     uint32_t* f = &w.flag[I.blk_base + lb];
     if (*((volatile uint32_t*)f) == 0u && atomicExch(f, 1u) == 0u) {
-        const int i = (int)atomicAdd(w.act_count, 1u);
+        const int i = (int)atomicAdd(&w.counters[CNT_ACTIVE], 1u);
         w.active[i] = make_int2(inst, pack_bc(bx, by, bz));
     }
 }
@@ -1606,153 +1546,6 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
     }
 }
 
-// ---------------------------------------------------------------- grid op folded into the tile load
-
-// The collider-free grid op of one node (legacy_coupler.py:364-375, 495-496), the same
-// arithmetic as k_grid_op: v = (1 / m) p + dt g where m > eps, then the CubeBoundary at the
-// node position (g + grid_offset) dx; 0 elsewhere.
-__device__ __forceinline__ float4 node_velocity(const mpm_instance& I, const float4 mm, int gx, int gy, int gz) {
-    float vx = 0.f, vy = 0.f, vz = 0.f;
-    if (mm.w > I.eps) {
-        const float inv = 1.f / mm.w;
-        vx = inv * mm.x + I.dt * I.gravity[0];
-        vy = inv * mm.y + I.dt * I.gravity[1];
-        vz = inv * mm.z + I.dt * I.gravity[2];
-        vx = bc_vel((float)(gx + I.lower_cell[0]) * I.dx, vx, I.bnd_lo[0], I.bnd_hi[0]);
-        vy = bc_vel((float)(gy + I.lower_cell[1]) * I.dx, vy, I.bnd_lo[1], I.bnd_hi[1]);
-        vz = bc_vel((float)(gz + I.lower_cell[2]) * I.dx, vz, I.bnd_lo[2], I.bnd_hi[2]);
-    }
-    return make_float4(vx, vy, vz, 0.f);
-}
-
-// the chunk's 8^3 velocity tile computed from the momentum the previous substep scattered
-template <int P>
-__device__ __forceinline__ void vel_tile_fold(VelTile& VT, const float4* __restrict__ cur, const Nbhd& h,
-                                              const uint32_t* nd, const mpm_instance& I, int ox, int oy, int oz) {
-#pragma unroll
-    for (int k = 0; k < TN / P; ++k) {
-        const uint32_t d = nd[threadIdx.x + k * P];
-        const int64_t a = nbhd_addr(h, d);
-        const int tx = (d >> 22) & 7, ty = (d >> 25) & 7, tz = (d >> 28) & 7;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (a >= 0) v = node_velocity(I, __ldg(&cur[a]), ox + tx, oy + ty, oz + tz);
-        VT.v[vidx(tx, ty, tz)] = v;
-    }
-}
-
-// Zero the n listed blocks of a momentum buffer and their flags.  The CTA that finishes last
-// resets the buffer's active count: every CTA read n before its own increment of the done
-// counter, so no CTA reads the count after the reset, and no CTA waits on another.
-template <int NT>
-__device__ __forceinline__ void grid_clear_blocks(const GridClear& c, const mpm_instance* __restrict__ inst, int n) {
-    constexpr int G = NT / BLK3;  // blocks per CTA per pass
-    const int grp = threadIdx.x / BLK3, ln = threadIdx.x % BLK3;
-    for (int i = blockIdx.x * G + grp; i < n; i += gridDim.x * G) {
-        const int2 e = c.active[i];
-        const mpm_instance& I = inst[e.x];
-        const BlockCoord bc = unpack_bc(e.y);
-        const int64_t blk = I.blk_base + local_block(I, bc.bx, bc.by, bc.bz);
-        c.mm[blk * BLK3 + ln] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ln == 0) c.flag[blk] = 0u;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && atomicAdd(c.done, 1u) == gridDim.x - 1) {
-        *c.count = 0u;
-        *c.done = 0u;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_grid_clear(const mpm_instance* __restrict__ inst, GridClear c) {
-    const int n = (int)*c.count;
-    grid_clear_blocks<256>(c, inst, n);
-}
-
-// k_g2p2g with the grid op folded in: the velocity tile comes from `cur` (the momentum the
-// previous substep scattered), the scatter goes to a.w.mm, and `prev` (read by the previous
-// substep) is cleared once the chunks are done.
-template <int P, bool MUSCLE>
-__global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P)
-    k_g2p2g_fold(P2GArgs a, const float4* __restrict__ cur, GridClear prev) {
-    __shared__ VelTile VT;
-    __shared__ Tile T;
-    __shared__ Stash<P> SH;
-    Ws& w = a.w;
-    const int n_chunks = (int)w.counters[CNT_CHUNKS];
-    const int n_prev = (int)*prev.count;
-    const int64_t st = a.par.state_stride;
-    float* __restrict__ S = a.par.state;
-    __shared__ uint32_t nd[TN];  // each thread reads back only the entries it wrote
-#pragma unroll
-    for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
-    tile_zero(T, P);
-    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
-        const int4 ch = w.chunks[ci];
-        const mpm_instance& I = a.inst[ch.x];
-        const BlockCoord bc = unpack_bc(ch.y);
-        const Nbhd h = nbhd_of(I, bc);
-        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        vel_tile_fold<P>(VT, cur, h, nd, I, ox, oy, oz);
-        __syncthreads();
-        Payload o;
-        o.live = o.in_tile = false;
-        o.mass = o.bq = 0.f;
-        o.slot = -1;
-        const int p = ch.z + threadIdx.x;
-        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
-            float x[3], nv[3], nC[9];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
-                particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x, SH);
-            }
-        }
-        scatter_flush<P>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd);
-    }
-    grid_clear_blocks<P>(prev, a.inst, n_prev);
-}
-
-// g2p with the grid op folded in (the last substep of a run, or before a re-sort)
-template <int P>
-__global__ void __launch_bounds__(P, 1024 / P) k_g2p_fold(P2GArgs a, const float4* __restrict__ cur, GridClear prev) {
-    __shared__ VelTile VT;
-    Ws& w = a.w;
-    const int n_chunks = (int)w.counters[CNT_CHUNKS];
-    const int n_prev = (int)*prev.count;
-    const int64_t st = a.par.state_stride;
-    float* __restrict__ S = a.par.state;
-    __shared__ uint32_t nd[TN];  // each thread reads back only the entries it wrote
-#pragma unroll
-    for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
-    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
-        const int4 ch = w.chunks[ci];
-        const mpm_instance& I = a.inst[ch.x];
-        const BlockCoord bc = unpack_bc(ch.y);
-        const Nbhd h = nbhd_of(I, bc);
-        const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        vel_tile_fold<P>(VT, cur, h, nd, I, ox, oy, oz);
-        __syncthreads();
-        const int p = ch.z + threadIdx.x;
-        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
-            float x[3], nv[3], nC[9];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather(VT, w, I, ch.x, x, nv, nC, ox, oy, oz)) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    S[(MPM_CH_X + d) * st + p] = x[d];
-                    S[(MPM_CH_V + d) * st + p] = nv[d];
-                }
-#pragma unroll
-                for (int k = 0; k < 9; ++k) S[(MPM_CH_C + k) * st + p] = nC[k];
-            }
-        }
-        __syncthreads();
-    }
-    grid_clear_blocks<P>(prev, a.inst, n_prev);
-}
-
 // non-free particles zero the momentum of their stencil (mpm_solver.py:388-389)
 __global__ void k_nonfree_zero(mpm_problem prob, const mpm_instance* __restrict__ inst, mpm_particles par, Ws w) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1958,8 +1751,6 @@ struct DevInfo {
     int occ_p2g[3] = {0, 0, 0};
     int occ_g2p[3] = {0, 0, 0};
     int occ_g2p2g[3] = {0, 0, 0};
-    int occ_fold[3] = {0, 0, 0};
-    int occ_g2p_fold[3] = {0, 0, 0};
     int occ_grid = 0;
 };
 
@@ -1990,12 +1781,6 @@ static const DevInfo* dev_info() {
         d.occ_g2p2g[0] = occ_of<128>(k_g2p2g<128, false, false>);
         d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256, false, false>);
         d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512, false, false>);
-        d.occ_fold[0] = occ_of<128>(k_g2p2g_fold<128, false>);
-        d.occ_fold[1] = occ_of<256>(k_g2p2g_fold<256, false>);
-        d.occ_fold[2] = occ_of<512>(k_g2p2g_fold<512, false>);
-        d.occ_g2p_fold[0] = occ_of<128>(k_g2p_fold<128>);
-        d.occ_g2p_fold[1] = occ_of<256>(k_g2p_fold<256>);
-        d.occ_g2p_fold[2] = occ_of<512>(k_g2p_fold<512>);
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op, 256, 0);
         d.occ_grid = n > 0 ? n : 1;
@@ -2173,72 +1958,6 @@ static int launch_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_part
     }
     if ((prob->flags & MPM_PROBF_NONFREE) && prob->n_particles > 0)
         k_nonfree_zero<<<(prob->n_particles + 255) / 256, 256, 0, s>>>(*prob, tab->instances, *par, a.w);
-    return cuda_ok();
-}
-
-// the folded path serves problems whose grid op is the MPM core alone (no colliders) and
-// whose p2g needs no non-free pass
-static bool fold_ok(const mpm_problem* prob, const mpm_tables* tab) {
-#if GBM_FOLD_GRID_OP
-    const int nc = tab->colliders ? tab->n_colliders : 0;
-    return nc == 0 && !(prob->flags & MPM_PROBF_NONFREE);
-#else
-    (void)prob;
-    (void)tab;
-    return false;
-#endif
-}
-
-// g2p2g (g2p_only = false) or g2p reading the momentum of rotating buffer `cur`, scattering
-// into `next` (g2p2g only) and clearing `prev`
-static int launch_fold(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, int cur,
-                       int next, int prev, bool g2p_only, cudaStream_t s) {
-    const DevInfo* d = dev_info();
-    if (!d) return MPM_E_CUDA;
-    P2GArgs a;
-    bool cpic;
-    int rc = p2g_args(prob, tab, par, ws, a, cpic);
-    if (rc) return rc;
-    const Ws base = a.w;
-    a.w = ws_target(base, next);
-    const float4* curp = base.mm_rot[cur];
-    const GridClear pc = grid_clear_of(base, prev);
-    const int pi = p_index(prob->chunk_particles);
-    const bool muscle = par->actu != nullptr;
-    if (g2p_only) {
-        const int ctas = persistent_ctas(prob, d->occ_g2p_fold[pi]);
-        switch (prob->chunk_particles) {
-            case 128: k_g2p_fold<128><<<ctas, 128, 0, s>>>(a, curp, pc); break;
-            case 256: k_g2p_fold<256><<<ctas, 256, 0, s>>>(a, curp, pc); break;
-            case 512: k_g2p_fold<512><<<ctas, 512, 0, s>>>(a, curp, pc); break;
-        }
-    } else {
-        const int ctas = persistent_ctas(prob, d->occ_fold[pi]);
-        switch (prob->chunk_particles) {
-            case 128:
-                muscle ? k_g2p2g_fold<128, true><<<ctas, 128, 0, s>>>(a, curp, pc)
-                       : k_g2p2g_fold<128, false><<<ctas, 128, 0, s>>>(a, curp, pc);
-                break;
-            case 256:
-                muscle ? k_g2p2g_fold<256, true><<<ctas, 256, 0, s>>>(a, curp, pc)
-                       : k_g2p2g_fold<256, false><<<ctas, 256, 0, s>>>(a, curp, pc);
-                break;
-            case 512:
-                muscle ? k_g2p2g_fold<512, true><<<ctas, 512, 0, s>>>(a, curp, pc)
-                       : k_g2p2g_fold<512, false><<<ctas, 512, 0, s>>>(a, curp, pc);
-                break;
-        }
-    }
-    return cuda_ok();
-}
-
-static int launch_grid_clear(const mpm_problem* prob, const mpm_tables* tab, void* ws, int b, cudaStream_t s) {
-    const DevInfo* d = dev_info();
-    if (!d) return MPM_E_CUDA;
-    int ctas = d->sms * d->occ_grid;
-    const int64_t need = (prob->n_blocks + 3) / 4;
-    if (ctas > need) ctas = (int)need;
-    k_grid_clear<<<ctas, 256, 0, s>>>(tab->instances, grid_clear_of(ws_of(*prob, ws), b));
     return cuda_ok();
 }
 
@@ -2491,8 +2210,7 @@ struct Prof {
 // n substeps.  The first substep starts with p2g; between substeps the g2p of substep i
 // and the p2g of substep i+1 run fused unless a re-sort falls between them, in which case
 // g2p, sort and p2g run separately; the last substep ends with g2p, so x, v, C, F, Jp are
-// all materialised when the call returns.  Collider-free problems fold the grid op into the
-// fused kernel (three rotating momentum buffers); the others run k_grid_op between.
+// all materialised when the call returns.
 static int substeps_impl(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* ws, int32_t n,
                          int32_t sort_interval, int64_t first, cudaStream_t s, Prof* pr = nullptr) {
     if (n <= 0) return MPM_OK;
@@ -2507,36 +2225,6 @@ static int substeps_impl(const mpm_problem* prob, const mpm_tables* tab, mpm_par
     }
     if ((rc = launch_p2g(prob, tab, par, ws, s))) return rc;
     mark(MPM_KIND_P2G);
-    if (fold_ok(prob, tab)) {
-        // buffer 0 holds p2g's momentum; `next` is always clean, `prev` is cleared by the
-        // kernel that reads `cur`; every buffer is clean again when the run ends
-        int cur = 0, next = 1, prev = 2;
-        for (int32_t i = 1; i < n; ++i) {
-            if (sort_due(i)) {
-                if ((rc = launch_fold(prob, tab, par, ws, cur, next, prev, true, s))) return rc;
-                mark(MPM_KIND_G2P_FOLD);
-                if ((rc = launch_grid_clear(prob, tab, ws, cur, s))) return rc;
-                mark(MPM_KIND_GRID_CLEAR);
-                if ((rc = launch_sort(prob, tab, par, ws, s))) return rc;
-                mark(MPM_KIND_SORT);
-                if ((rc = launch_p2g(prob, tab, par, ws, s))) return rc;
-                mark(MPM_KIND_P2G);
-                cur = 0, next = 1, prev = 2;
-            } else {
-                if ((rc = launch_fold(prob, tab, par, ws, cur, next, prev, false, s))) return rc;
-                mark(MPM_KIND_G2P2G_FOLD);
-                const int t = prev;
-                prev = cur;
-                cur = next;
-                next = t;
-            }
-        }
-        if ((rc = launch_fold(prob, tab, par, ws, cur, next, prev, true, s))) return rc;
-        mark(MPM_KIND_G2P_FOLD);
-        if ((rc = launch_grid_clear(prob, tab, ws, cur, s))) return rc;
-        mark(MPM_KIND_GRID_CLEAR);
-        return MPM_OK;
-    }
     if ((rc = launch_grid_op(prob, tab, ws, s))) return rc;
     mark(MPM_KIND_GRID_OP);
     for (int32_t i = 1; i < n; ++i) {

@@ -274,10 +274,7 @@ int mpm_g2p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par
               void* stream);
 
 /* n_substeps x (p2g, grid_op, g2p); re-sorts before substep i when
- * sort_interval > 0 and (first_substep + i) % sort_interval == 0.  Problems without
- * colliders and without non-free particles run the grid op inside the fused g2p/p2g kernel
- * (the velocity of each node is computed from the momentum where a chunk loads it; three
- * momentum buffers rotate in the workspace); the results are those of the separate kernels. */
+ * sort_interval > 0 and (first_substep + i) % sort_interval == 0. */
 int mpm_substeps(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
                  int32_t n_substeps, int32_t sort_interval, int64_t first_substep, void* stream);
 
@@ -341,11 +338,8 @@ int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mp
 #define MPM_KIND_P2G 1
 #define MPM_KIND_GRID_OP 2
 #define MPM_KIND_G2P 3
-#define MPM_KIND_G2P2G 4
-#define MPM_KIND_G2P2G_FOLD 5  /* g2p fused with the next grid op and p2g (collider-free problems) */
-#define MPM_KIND_G2P_FOLD 6    /* g2p fused with the grid op before it */
-#define MPM_KIND_GRID_CLEAR 7  /* clearing the last momentum buffer of a folded run */
-#define MPM_N_KINDS 8
+#define MPM_KIND_G2P2G 4       /* g2p of one substep fused with p2g of the next */
+#define MPM_N_KINDS 5
 int mpm_substeps_profile(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
                          int32_t n_substeps, int32_t sort_interval, int64_t first_substep, float* ms_by_kind,
                          int32_t* launches_by_kind, void* stream);

@@ -22,6 +22,11 @@ runs are float64 (the reference's ``precision="64"``).  Written here:
   ref_cube.npz         an Elastic cube (E 1e5, nu 0.3, rho 1000: the 32,768-particle benchmark
                        cube's material) of 216 jittered lattice particles thrown at the floor of
                        a 64-per-metre grid, dt 1e-4: state after 1, 20 and 60 substeps.
+  ref_mixed_m32.npz,   the same two scenes with the reference's precision-32 model in float64
+  ref_cube_m32.npz     arithmetic: gs.EPS = float32 epsilon (genesis/__init__.py:205-206, the
+                       grid-mass threshold and the eps of Matrix.norm in the plastic return
+                       mappings), everything else float64.  A float32 run of the reference
+                       computes this model; the float32 CUDA path is held to it.
 
 Only this script reads the reference checkout; the tests read the committed .npz files.
 """
@@ -236,10 +241,16 @@ def main():
     meta, out = functions_fixture(ref)
     np.savez_compressed(os.path.join(HERE, "ref_functions.npz"), meta=np.array(json.dumps(meta)), **out)
     print("ref_functions")
-    for fn in (mixed_fixture, cube_fixture):
-        meta, inputs, rec = fn(ref)
-        np.savez_compressed(os.path.join(HERE, f"{meta['name']}.npz"), meta=np.array(json.dumps(meta)), **inputs,
-                            **rec)
+    eps64 = ref.gs.EPS
+    for suffix, eps in (("", eps64), ("_m32", float(np.finfo(np.float32).eps))):
+        ref.gs.EPS = eps
+        for fn in (mixed_fixture, cube_fixture):
+            meta, inputs, rec = fn(ref)
+            meta["eps"] = eps
+            meta["name"] += suffix
+            np.savez_compressed(os.path.join(HERE, f"{meta['name']}.npz"), meta=np.array(json.dumps(meta)),
+                                **inputs, **rec)
+    ref.gs.EPS = eps64
 
 
 if __name__ == "__main__":

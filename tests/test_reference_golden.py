@@ -79,6 +79,7 @@ def _scene(name):
     p = R.Params(grid_density=meta["grid_density"], lower_bound=tuple(meta["lower_bound"]),
                  upper_bound=tuple(meta["upper_bound"]), particle_size=meta["particle_size"], dt=meta["dt"],
                  gravity=tuple(meta["gravity"]), dtype=np.float64)
+    p.eps = meta.get("eps", p.eps)  # the *_m32 fixtures: the precision-32 model (float32 gs.EPS)
     mats = [R.make_material(k, **dict(kw)) for k, kw in meta["materials"]]
     st = R.make_state(z["pos"], mats, z["mat_idx"], np.float64, v=z["vel"], active=z["active"])
     st.update(C=z["C"].copy(), F=z["F"].copy(), Jp=z["Jp"].astype(np.float64).copy())
@@ -92,7 +93,10 @@ def _scene(name):
     return z, meta, p, mats, st
 
 
-@pytest.mark.parametrize("name", ["ref_mixed", "ref_cube"])
+SCENES = ["ref_mixed", "ref_cube", "ref_mixed_m32", "ref_cube_m32"]
+
+
+@pytest.mark.parametrize("name", SCENES)
 def test_numpy_oracle_reproduces_reference_substeps(name):
     z, meta, p, mats, st = _scene(name)
     gm, gp, _, _ = R.p2g(p, mats, st)
@@ -109,7 +113,7 @@ def test_numpy_oracle_reproduces_reference_substeps(name):
         assert np.abs(st["Jp"] - z[f"Jp_{n}"]).max() < 1e-10, n
 
 
-@pytest.mark.parametrize("name", ["ref_mixed", "ref_cube"])
+@pytest.mark.parametrize("name", SCENES)
 def test_c_oracle_reproduces_reference_substeps(name):
     z, meta, p, mats, st = _scene(name)
     done = 0
