@@ -1,20 +1,22 @@
-// Reverse-mode adjoint of one MPM substep for Elastic (corotated) particles with
+// Reverse-mode adjoint of one MPM substep for every MPM material (Elastic corotated /
+// neo-Hookean, Muscle, ElastoPlastic von Mises / clamp, Liquid, Sand, Snow) with
 // per-particle Lame parameters.  Included by mpm_kernels.cu (same module, namespace gbm).
 //
-// Forward being differentiated (reference: mpm_solver.py:261-449, elastic.py:70-75,
+// Forward being differentiated (reference: mpm_solver.py:261-449, materials/MPM/*.py,
 // legacy_coupler.py:364-375, 495-496):
-//   F_tmp = (I + dt C) F;  F_tmp = U S V^T;  R = U V^T;  J = det F_tmp
-//   P = 2 mu (F_tmp - R) F_tmp^T + lam J (J - 1) I;   A = s P + m C
-//   m_i = sum w m;  p_i = sum w (m v + A d_i)                     (d_i = x_i - x_p)
+//   F_tmp = (I + dt C) F;  F_tmp = U S V^T;  J = det S
+//   (F_new, Jp_new) = the material's return mapping; P = its stress
+//   A = s P + m C;  m_i = sum w m;  p_i = sum w (m v + A d_i)          (d_i = x_i - x_p)
 //   v_i = bc(p_i / m_i + dt g)
 //   v' = sum w v_i;  C' = c sum w v_i u_i^T;  x' = clamp(x + dt v'), v'' = bc(v')
 //                                                                (u_i = d_i / dx, c = 4 inv_dx)
 // Three kernels run after the forward grid of the substep has been recomputed:
 //   k_adj_g2p   particles: adjoint of the gather; scatters the grid-velocity adjoint
 //   k_adj_grid  nodes:     adjoint of p/m + dt g and the boundary
-//   k_adj_p2g   particles: adjoint of the scatter, the stress (polar rotation via the
-//               closed-form SVD adjoint U [(M_ij - M_ji)/(s_i + s_j)] V^T), J, F_tmp
-// The adjoint arrays use the state's planar layout (channel c of slot s at c*stride + s).
+//   k_adj_p2g   particles: adjoint of the scatter, the material (material_adjoint: the return
+//               mapping, the stress and the SVD together, in the SVD basis), J, F_tmp
+// The adjoint arrays use the state's planar layout (channel c of slot s at c*stride + s),
+// the Jp channel included (Snow and Sand carry Jp from one substep to the next).
 #pragma once
 
 struct AdjWs {
@@ -189,7 +191,344 @@ __device__ __forceinline__ void cofactor(const float* F, float* K) {
     K[8] = F[0] * F[4] - F[1] * F[3];
 }
 
-// ---- adjoint of p2g, the corotated stress and compute_F_tmp (mpm_solver.py:261-389)
+// ---- the materials' adjoint in the SVD basis
+// Every material's F_new is U diag(g(s)) V^T (Liquid: J^(1/3) I) and its stress
+// U diag(p(s)) U^T (plus the Muscle term, handled by the caller), with g and p symmetric
+// functions of the singular values s of F_tmp.  Their adjoint follows from g, p, their
+// Jacobians and divided differences:
+//   X = U^T Fn_bar V,  Z = U^T sym(P_bar) U
+//   s_bar_k = sum_i X_ii dg_i/ds_k + Z_ii dp_i/ds_k + Jpn_bar dJp_new/ds_k
+//   Y_ij = 1/2 [(X_ij + X_ji) (g_i - g_j)/(s_i - s_j) + (X_ij - X_ji) (g_i + g_j)/(s_i + s_j)]
+//          + 2 Z_ij s_j (p_i - p_j) / (s_i^2 - s_j^2)                         (i != j)
+//   F_tmp_bar += U (diag(s_bar) + Y) V^T
+// This is the reference's backward (gstaichi autodiff of update_F_S_Jp / update_stress
+// with U, S, V as inputs, then backward_svd, mpm_solver.py:1112-1129) rearranged: equal to it
+// wherever its signmax(s_j^2 - s_i^2, 1e-6) guard is inactive, and the derivative that guard
+// approximates where it is not.  The divided differences are formed through
+// log(c_i / c_j) = log1p((c_i - c_j) / c_j) and expm1, so they stay exact as s_i -> s_j (the
+// rest state and every small strain).
+
+// (g_i - g_j) / (s_i - s_j) where g_i - g_j = g_j expm1(kappa log(c_i / c_j)) and c is the
+// clamped |s| (c = |s| where unclamped); its limit at s_i = s_j is g_j kappa / s_j (0 if clamped)
+__device__ __forceinline__ float ddiff_log(float si, float sj, float ci, float cj, float kappa, float gj) {
+    const float den = si - sj;
+    if (den != 0.f) return gj * expm1f(kappa * log1pf((ci - cj) / cj)) / den;
+    return ci == fabsf(si) ? gj * kappa / sj : 0.f;
+}
+
+struct Spec {
+    float g[3], p[3];
+    float Dg[3][3], Dp[3][3];    // dg_i/ds_k, dp_i/ds_k
+    float DDg[3][3], DDp[3][3];  // (g_i - g_j)/(s_i - s_j), (p_i - p_j)/(s_i - s_j)
+    float dg_dJp[3], dp_dJp[3], dg_dmu[3], dp_dmu[3], dg_dlam[3], dp_dlam[3];
+    float dJpn_ds[3], dJpn_dJp;
+    bool ident;   // F_new = F_tmp
+    bool liquid;  // F_new = J^(1/3) I
+};
+
+// p_i = 2 muc (g_i - 1) g_i + lamc J (J - 1) (the corotated stress's eigenvalues, base.py:86-88)
+__device__ __forceinline__ void spec_corot(Spec& o, float muc, float lamc, float J, const float* Jk) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        o.p[i] = 2.f * muc * (o.g[i] - 1.f) * o.g[i] + lamc * J * (J - 1.f);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            o.Dp[i][k] = 2.f * muc * (2.f * o.g[i] - 1.f) * o.Dg[i][k] + lamc * (2.f * J - 1.f) * Jk[k];
+            o.DDp[i][k] = 2.f * muc * (o.g[i] + o.g[k] - 1.f) * o.DDg[i][k];
+        }
+        o.dp_dmu[i] = 2.f * (o.g[i] - 1.f) * o.g[i] + 2.f * muc * (2.f * o.g[i] - 1.f) * o.dg_dmu[i];
+        o.dp_dlam[i] = J * (J - 1.f);
+    }
+}
+
+__device__ __forceinline__ void spec_ident(Spec& o, const float* s) {
+    o.ident = true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        o.g[i] = s[i];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            o.Dg[i][k] = i == k ? 1.f : 0.f;
+            o.DDg[i][k] = 1.f;
+        }
+    }
+}
+
+// g, p and their derivatives for one material (materials/MPM/*.py, as p2g calls them)
+__device__ void material_spectral(const mpm_material& m, float mu, float lam, float eps, const float* s, float Jp,
+                                  Spec& o) {
+    const float Jk[3] = {s[1] * s[2], s[0] * s[2], s[0] * s[1]};
+    const float J = s[0] * Jk[0];
+    o.ident = o.liquid = false;
+    o.dJpn_dJp = 1.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        o.dg_dJp[i] = o.dp_dJp[i] = o.dg_dmu[i] = o.dg_dlam[i] = o.dJpn_ds[i] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) o.Dg[i][k] = o.DDg[i][k] = 0.f;
+    }
+    switch (m.kind) {
+        case MPM_MAT_ELASTIC:
+            spec_ident(o, s);
+            if (m.flags & MPM_MATF_NEOHOOKEAN) {  // p_i = mu s_i^2 + lam log J - mu (elastic.py:78-81)
+                const float lj = logf(J);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    o.p[i] = mu * s[i] * s[i] + lam * lj - mu;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        o.Dp[i][k] = (i == k ? 2.f * mu * s[i] : 0.f) + lam * Jk[k] / J;
+                        o.DDp[i][k] = mu * (s[i] + s[k]);
+                    }
+                    o.dp_dmu[i] = s[i] * s[i] - 1.f;
+                    o.dp_dlam[i] = lj;
+                }
+            } else {
+                spec_corot(o, mu, lam, J, Jk);
+            }
+            break;
+        case MPM_MAT_LIQUID:  // F_new = J^(1/3) I; stress corotated on F_tmp (liquid.py:50-64)
+            spec_ident(o, s);
+            o.ident = false;
+            o.liquid = true;
+            spec_corot(o, mu, lam, J, Jk);
+            break;
+        case MPM_MAT_ELASTOPLASTIC:
+        case MPM_MAT_SNOW:
+            if (m.kind == MPM_MAT_ELASTOPLASTIC && (m.flags & MPM_MATF_VON_MISES)) {
+                // elasto_plastic.py:70-84
+                float Sc[3], de[3], e[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    Sc[k] = fmaxf(s[k], 0.05f);
+                    de[k] = s[k] > 0.05f ? 1.f / s[k] : 0.f;
+                    e[k] = logf(Sc[k]);
+                }
+                const float mean = (e[0] + e[1] + e[2]) * (1.f / 3.f);
+                const float eh[3] = {e[0] - mean, e[1] - mean, e[2] - mean};
+                const float nn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
+                const float tau = m.vm_threshold * (m.mu / mu);
+                if (nn - tau > 0.f) {
+                    const float r = tau / nn;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) o.g[i] = expf(mean + r * eh[i]);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const float dedk = (1.f / 3.f) + r * ((i == k ? 1.f : 0.f) - (1.f / 3.f)) -
+                                               (r / (nn * nn)) * eh[i] * eh[k];
+                            o.Dg[i][k] = o.g[i] * dedk * de[k];
+                            o.DDg[i][k] = ddiff_log(s[i], s[k], Sc[i], Sc[k], r, o.g[k]);
+                        }
+                        o.dg_dmu[i] = -o.g[i] * eh[i] * tau / (nn * mu);
+                    }
+                } else {
+                    spec_ident(o, s);
+                }
+                spec_corot(o, mu, lam, J, Jk);
+            } else {
+                // clamp (elasto_plastic.py:86-90, snow.py:62-70)
+                bool fr[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    o.g[i] = fminf(fmaxf(s[i], m.clamp_lo), m.clamp_hi);
+                    fr[i] = s[i] > m.clamp_lo && s[i] < m.clamp_hi;
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        o.Dg[i][k] = (i == k && fr[i]) ? 1.f : 0.f;
+                        const float den = s[i] - s[k];
+                        o.DDg[i][k] = den != 0.f ? (o.g[i] - o.g[k]) / den : (fr[i] ? 1.f : 0.f);
+                    }
+                if (m.kind == MPM_MAT_SNOW) {
+                    // Jp_new = Jp prod s / g; stress hardened by h = exp(10 (1 - Jp)) (snow.py:75-79)
+                    const float h = expf(10.f * (1.f - Jp));
+                    const float ratio = (s[0] / o.g[0]) * (s[1] / o.g[1]) * (s[2] / o.g[2]);
+                    const float Jpn = Jp * ratio;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) o.dJpn_ds[i] = fr[i] ? 0.f : Jpn / s[i];
+                    o.dJpn_dJp = ratio;
+                    spec_corot(o, mu * h, lam * h, J, Jk);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        o.dp_dJp[i] = -10.f * o.p[i];
+                        o.dp_dmu[i] *= h;
+                        o.dp_dlam[i] *= h;
+                    }
+                } else {
+                    spec_corot(o, mu, lam, J, Jk);
+                }
+            }
+            break;
+        case MPM_MAT_SAND:
+        default: {
+            // sand.py:51-89: ls = log S_new; p_i = 2 mu ls_i + lam sum(ls) (the stress
+            // U diag(center) V^T F_new^T is U diag(center * S_new) U^T)
+            float Sc[3], de[3], e[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                Sc[k] = fmaxf(fabsf(s[k]), 1e-4f);
+                de[k] = fabsf(s[k]) > 1e-4f ? 1.f / s[k] : 0.f;
+                e[k] = logf(Sc[k]);
+            }
+            const float tr = e[0] + e[1] + e[2] + Jp;
+            const float eh[3] = {e[0] - tr / 3.f, e[1] - tr / 3.f, e[2] - tr / 3.f};
+            const float nn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2] + eps);
+            const float q = (3.f * lam + 2.f * mu) / (2.f * mu) * m.sand_alpha;
+            const float dq_dmu = m.sand_alpha * (-3.f * lam / (2.f * mu * mu));
+            const float dq_dlam = m.sand_alpha * 3.f / (2.f * mu);
+            if (tr >= 0.f) {  // expansion: S_new = I, Jp_new = tr
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    o.g[i] = 1.f;
+                    o.p[i] = 0.f;
+                    o.dp_dmu[i] = o.dp_dlam[i] = 0.f;
+                    o.dJpn_ds[i] = de[i];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) o.Dp[i][k] = o.DDp[i][k] = 0.f;
+                }
+                o.dJpn_dJp = 1.f;
+                break;
+            }
+            o.dJpn_dJp = 0.f;  // Jp_new = 0
+            const bool y = nn + q * tr > 0.f;
+            const float kap = y ? -q * tr / nn : 1.f;
+            float ls[3], dls[3][3], dls_dJp[3], dls_dq[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                ls[i] = y ? tr / 3.f + kap * eh[i] : e[i];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    dls[i][k] = y ? (1.f / 3.f) - q * (eh[i] / nn + (tr / nn) * ((i == k ? 1.f : 0.f) - (1.f / 3.f)) -
+                                                       (tr / (nn * nn * nn)) * eh[i] * (eh[k] + Jp / 3.f))
+                                  : (i == k ? 1.f : 0.f);
+                dls_dJp[i] = y ? (1.f / 3.f) - q * (eh[i] / nn - tr / (3.f * nn) - tr * Jp / (3.f * nn * nn * nn) * eh[i])
+                               : 0.f;
+                dls_dq[i] = y ? -(tr / nn) * eh[i] : 0.f;
+            }
+            const float lsum = ls[0] + ls[1] + ls[2];
+            const float dqs = dls_dq[0] + dls_dq[1] + dls_dq[2];
+            const float djs = dls_dJp[0] + dls_dJp[1] + dls_dJp[2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                o.g[i] = expf(ls[i]);
+                o.p[i] = 2.f * mu * ls[i] + lam * lsum;
+                o.dg_dJp[i] = o.g[i] * dls_dJp[i];
+                o.dg_dmu[i] = o.g[i] * dls_dq[i] * dq_dmu;
+                o.dg_dlam[i] = o.g[i] * dls_dq[i] * dq_dlam;
+                o.dp_dJp[i] = 2.f * mu * dls_dJp[i] + lam * djs;
+                const float dpq = 2.f * mu * dls_dq[i] + lam * dqs;
+                o.dp_dmu[i] = 2.f * ls[i] + dpq * dq_dmu;
+                o.dp_dlam[i] = lsum + dpq * dq_dlam;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float colsum = (dls[0][k] + dls[1][k] + dls[2][k]) * de[k];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    o.Dg[i][k] = o.g[i] * dls[i][k] * de[k];
+                    o.Dp[i][k] = 2.f * mu * dls[i][k] * de[k] + lam * colsum;
+                    o.DDg[i][k] = ddiff_log(s[i], s[k], Sc[i], Sc[k], kap, o.g[k]);
+                    const float den = s[i] - s[k];
+                    o.DDp[i][k] = den != 0.f ? 2.f * mu * kap * log1pf((Sc[i] - Sc[k]) / Sc[k]) / den
+                                             : 2.f * mu * kap / s[k];
+                }
+            }
+            break;
+        }
+    }
+}
+
+// Adds the adjoint of F_tmp for the adjoints Gb of F_new, Jpnb of Jp_new and Pb of the
+// material's stress; sets Jpb (adjoint of the previous Jp) and adds to mub, lamb.
+__device__ void material_adjoint(const mpm_material& m, float mu, float lam, float eps, const float* U, const float* s,
+                                 const float* V, float Jp, const float* Gb, float Jpnb, const float* Pb, float* Ftb,
+                                 float& Jpb, float& mub, float& lamb) {
+    Spec o;
+    material_spectral(m, mu, lam, eps, s, Jp, o);
+    float X[3][3], Z[3][3], T[3][3];
+    // X = U^T Gb V
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[i][j] = Gb[i * 3 + 0] * V[0 * 3 + j] + Gb[i * 3 + 1] * V[1 * 3 + j] + Gb[i * 3 + 2] * V[2 * 3 + j];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) X[i][j] = U[0 * 3 + i] * T[0][j] + U[1 * 3 + i] * T[1][j] + U[2 * 3 + i] * T[2][j];
+    // Z = U^T sym(Pb) U
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc += 0.5f * (Pb[i * 3 + k] + Pb[k * 3 + i]) * U[k * 3 + j];
+            T[i][j] = acc;
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Z[i][j] = U[0 * 3 + i] * T[0][j] + U[1 * 3 + i] * T[1][j] + U[2 * 3 + i] * T[2][j];
+    const bool use_x = !(o.ident || o.liquid);
+    float sbar[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float acc = Jpnb * o.dJpn_ds[k];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) acc += Z[i][i] * o.Dp[i][k] + (use_x ? X[i][i] * o.Dg[i][k] : 0.f);
+        sbar[k] = acc;
+    }
+    Jpb = Jpnb * o.dJpn_dJp;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Jpb += Z[i][i] * o.dp_dJp[i] + (use_x ? X[i][i] * o.dg_dJp[i] : 0.f);
+        mub += Z[i][i] * o.dp_dmu[i] + (use_x ? X[i][i] * o.dg_dmu[i] : 0.f);
+        lamb += Z[i][i] * o.dp_dlam[i] + (use_x ? X[i][i] * o.dg_dlam[i] : 0.f);
+    }
+    if (o.liquid) {
+        // F_new = c I, c = J^(1/3): J_bar = tr(Gb) c / (3 J)
+        const float J = s[0] * (s[1] * s[2]);
+        const float Jb = (Gb[0] + Gb[4] + Gb[8]) * cbrtf(J) / (3.f * J);
+        sbar[0] += Jb * s[1] * s[2];
+        sbar[1] += Jb * s[0] * s[2];
+        sbar[2] += Jb * s[0] * s[1];
+    }
+    float Y[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (i == j) {
+                Y[i][j] = sbar[i];
+                continue;
+            }
+            const float ss = s[i] + s[j];
+            const bool ok = fabsf(ss) > 1e-12f;
+            const float G = ok ? (o.g[i] + o.g[j]) / ss : 0.f;
+            const float Gam = ok ? o.DDp[i][j] / ss : 0.f;
+            float y = 2.f * Z[i][j] * s[j] * Gam;
+            if (use_x) y += 0.5f * ((X[i][j] + X[j][i]) * o.DDg[i][j] + (X[i][j] - X[j][i]) * G);
+            Y[i][j] = y;
+        }
+    // F_tmp_bar += U Y V^T (+ Gb where F_new = F_tmp)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) T[i][j] = Y[i][0] * V[j * 3 + 0] + Y[i][1] * V[j * 3 + 1] + Y[i][2] * V[j * 3 + 2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            Ftb[i * 3 + j] += U[i * 3 + 0] * T[0][j] + U[i * 3 + 1] * T[1][j] + U[i * 3 + 2] * T[2][j] +
+                              (o.ident ? Gb[i * 3 + j] : 0.f);
+}
+
+// ---- adjoint of p2g, the materials and compute_F_tmp (mpm_solver.py:261-389)
 __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ inst,
                           const mpm_material* __restrict__ mats, mpm_particles par, float* adj, float* lame_bar,
                           AdjWs aw) {
@@ -211,7 +550,7 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
         F[k] = S[(MPM_CH_F + k) * st + s];
     }
     if (!finite3(x[0], x[1], x[2])) return;
-    const float mu = par.mu_p ? par.mu_p[s] : m.mu;
+    const float mu = par.mu_p ? ((m.kind == MPM_MAT_LIQUID && m.mu == 0.f) ? 0.f : par.mu_p[s]) : m.mu;
     const float lam = par.lam_p ? par.lam_p[s] : m.lam;
     // forward recompute
     float Ft[9];
@@ -224,11 +563,10 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
             for (int k = 0; k < 3; ++k) acc += I.dt * C[i * 3 + k] * F[k * 3 + j];
             Ft[i * 3 + j] = acc;
         }
-    float U[9], Sg[3], V[9], Rm[9];
+    float U[9], Sg[3], V[9];
     svd3(Ft, U, Sg, V);
-    uvt(U, V, Rm);
     const float J = Sg[0] * (Sg[1] * Sg[2]);
-    const bool neo = (m.flags & MPM_MATF_NEOHOOKEAN) != 0;
+    const float Jp = S[MPM_CH_JP * st + s];
     // muscle actuation (muscle.py:57-65): + ka g g^T with g = F_tmp d, ka = stiffness * actu
     const bool musc = (m.flags & MPM_MATF_MUSCLE) && par.actu;
     float dd[3] = {0.f, 0.f, 0.f}, g[3] = {0.f, 0.f, 0.f}, ka = 0.f;
@@ -240,19 +578,9 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
 #pragma unroll
         for (int a = 0; a < 3; ++a) g[a] = Ft[a * 3 + 0] * dd[0] + Ft[a * 3 + 1] * dd[1] + Ft[a * 3 + 2] * dd[2];
     }
-    float P[9];
-    if (neo) {
-        // mu F_tmp F_tmp^T + (lam log J - mu) I   (elastic.py:78-81)
-        const float dg = lam * logf(J) - mu;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-                P[i * 3 + j] = mu * (Ft[i * 3 + 0] * Ft[j * 3 + 0] + Ft[i * 3 + 1] * Ft[j * 3 + 1] +
-                                     Ft[i * 3 + 2] * Ft[j * 3 + 2]) + (i == j ? dg : 0.f);
-    } else {
-        corotated(mu, lam, J, Ft, Rm, P);
-    }
+    // the forward's stress (the same return mapping and stress code as p2g)
+    float P[9], Fn[9], Jpn;
+    constitutive(m, mu, lam, I.eps, J, Ft, U, Sg, V, Jp, Fn, Jpn, P);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -325,101 +653,17 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
 #pragma unroll
         for (int k = 0; k < 9; ++k) Ftb[k] = 0.f;
     }
-    if (neo) {
-        // P = mu F F^T + (lam log J - mu) I: Ftb += mu (Pb + Pb^T) F + lam tr(Pb) / J dJ/dF
-        const float trP = Pb[0] + Pb[4] + Pb[8];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                float acc = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) acc += (Pb[i * 3 + k] + Pb[k * 3 + i]) * Ft[k * 3 + j];
-                Ftb[i * 3 + j] += mu * acc;
-                mub += Pb[i * 3 + j] * (Ft[i * 3 + 0] * Ft[j * 3 + 0] + Ft[i * 3 + 1] * Ft[j * 3 + 1] +
-                                        Ft[i * 3 + 2] * Ft[j * 3 + 2]);
-            }
-        mub -= trP;
-        lamb = trP * logf(J);
-        float K[9];
-        cofactor(Ft, K);
-        const float Jb = lam * trP / J;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Ftb[k] += Jb * K[k];
-    } else {
-    // P = 2 mu (Ft - R) Ft^T + lam J (J - 1) I
-    float D[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) D[k] = Ft[k] - Rm[k];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const float dft = D[i * 3 + 0] * Ft[j * 3 + 0] + D[i * 3 + 1] * Ft[j * 3 + 1] + D[i * 3 + 2] * Ft[j * 3 + 2];
-            mub += Pb[i * 3 + j] * dft;
-        }
-    mub *= 2.f;
-    const float trP = Pb[0] + Pb[4] + Pb[8];
-    lamb = trP * J * (J - 1.f);
-    float Rb[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            float a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                a1 += Pb[i * 3 + k] * Ft[k * 3 + j];  // (Pb Ft)_ij
-                a2 += Pb[k * 3 + i] * D[k * 3 + j];   // (Pb^T D)_ij
-            }
-            a3 = a1;
-            Ftb[i * 3 + j] += 2.f * mu * (a1 + a2);
-            Rb[i * 3 + j] = -2.f * mu * a3;
-        }
-    const float Jb = lam * (2.f * J - 1.f) * trP;
-    float K[9];
-    cofactor(Ft, K);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) Ftb[k] += Jb * K[k];
-    // polar rotation: Ftb += U X V^T, X_ij = (M_ij - M_ji) / (s_i + s_j), M = U^T Rb V
-    float T[9], M[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            T[i * 3 + j] = Rb[i * 3 + 0] * V[0 * 3 + j] + Rb[i * 3 + 1] * V[1 * 3 + j] + Rb[i * 3 + 2] * V[2 * 3 + j];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            M[i * 3 + j] = U[0 * 3 + i] * T[0 * 3 + j] + U[1 * 3 + i] * T[1 * 3 + j] + U[2 * 3 + i] * T[2 * 3 + j];
-    float X[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const float den = Sg[i] + Sg[j];
-            X[i * 3 + j] = (i == j || fabsf(den) < 1e-12f) ? 0.f : (M[i * 3 + j] - M[j * 3 + i]) / den;
-        }
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            float acc = 0.f;
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b) acc += U[i * 3 + a] * X[a * 3 + b] * V[j * 3 + b];
-            Ftb[i * 3 + j] += acc;
-        }
-    }
-    // F_new = F_tmp (Elastic): the incoming F adjoint adds to F_tmp's
+    // the return mapping, the stress and the SVD (adjoints of F_new and Jp_new come in with adj)
     float* xo = adj + (int64_t)MPM_CH_X * st;
     float* vo = adj + (int64_t)MPM_CH_V * st;
     float* co = adj + (int64_t)MPM_CH_C * st;
     float* fo = adj + (int64_t)MPM_CH_F * st;
+    float* jo = adj + (int64_t)MPM_CH_JP * st;
+    float Gb[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Ftb[k] += fo[k * st + s];
+    for (int k = 0; k < 9; ++k) Gb[k] = fo[k * st + s];
+    float Jpb = 0.f;
+    material_adjoint(m, mu, lam, I.eps, U, Sg, V, Jp, Gb, jo[s], Pb, Ftb, Jpb, mub, lamb);
     // F_tmp = (I + dt C) F
     float Fbn[9];
 #pragma unroll
@@ -446,6 +690,7 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
         co[k * st + s] = Cbn[k];
         fo[k * st + s] = Fbn[k];
     }
+    jo[s] = Jpb;
     lame_bar[s] += mub;
     lame_bar[st + s] += lamb;
 }

@@ -874,7 +874,8 @@ __device__ __forceinline__ void particle_update(const mpm_instance& I, const mpm
     const mpm_material m = mats[I.mat_base + par.mat[p]];
     float mu = m.mu, lam = m.lam;
     if (par.mu_p) {
-        mu = par.mu_p[p];
+        // an inviscid Liquid keeps mu = 0 whatever its per-particle E (liquid.py:47-48)
+        mu = (m.kind == MPM_MAT_LIQUID && m.mu == 0.f) ? 0.f : par.mu_p[p];
         lam = par.lam_p[p];
     }
     // compute_F_tmp: (I + dt C) F   (mpm_solver.py:264-266)

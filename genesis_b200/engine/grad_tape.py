@@ -21,8 +21,8 @@ input overwrote get a zero adjoint) and leaves dL/d(state before step s) for the
 Actuation persists until it is set again, so its gradient accumulates across steps and is
 consumed by the step that set it.
 
-Scope (the adjoint's): Elastic (corotated / neo-Hookean) and Muscle materials, no rigid
-colliders, no emitters; positions may be set only before the first step (setting them later
+Scope (the adjoint's): every MPM material (Elastic, Muscle, ElastoPlastic, Liquid, Sand,
+Snow), no rigid colliders, no emitters; positions may be set only before the first step (setting them later
 re-bins the particles, which would change the slot order the adjoint walks in).
 """
 

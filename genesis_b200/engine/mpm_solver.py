@@ -140,9 +140,9 @@ class MPMSolver:
         if grad:
             from ..materials import MPM
 
-            bad = [type(m).__name__ for m in self.unique_materials if not isinstance(m, (MPM.Elastic, MPM.Muscle))]
+            bad = [type(m).__name__ for m in self.unique_materials if not isinstance(m, MPM.Base)]
             if bad or rigid or tools:
-                raise GenesisException("A differentiable scene supports MPM.Elastic and MPM.Muscle entities only "
+                raise GenesisException("A differentiable scene supports MPM entities only "
                                        f"(got {', '.join(bad) or 'rigid or tool colliders'}).")
         self.runtime = MPMRuntime(
             specs,

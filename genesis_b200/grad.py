@@ -7,14 +7,17 @@ reverse: it restores a segment's checkpoint, recomputes the states inside it, an
 the adjoint of each substep (mpm_substep_adjoint) from the last to the first.  Memory is
 one state per checkpoint plus one segment of states, instead of every substep.
 
-Supported: Elastic scenes (corotated or neo-Hookean) and Muscle scenes, with per-particle
-Young's modulus; gradients with respect to the initial velocity (a uniform v0 (3,), as
-entity.set_velocity sets it, or per particle (N, 3)), the initial positions (an offset (3,) of
-the scene's positions, as entity.set_position moves an entity, or absolute positions (N, 3)),
-per-particle E (N,) and, for Muscle, per-particle actuation (N,) (mpm_solver.py:922-949: the
-reference's actuation gradients; particle_entity.py:415-481: its state-input gradients).  This replaces the reference's requires_grad path
-(simulator.py:294-303, mpm_solver.py:485-517, with the gstaichi autodiff kernels and
-backward_svd at mpm_solver.py:1112-1129) for these cases.
+Supported: scenes of any mix of MPM materials (Elastic corotated or neo-Hookean, Muscle,
+ElastoPlastic von Mises or clamp, Liquid, Sand, Snow) with per-particle Young's modulus (each
+particle's Poisson ratio is its material's); gradients with respect to the initial velocity
+(a uniform v0 (3,), as entity.set_velocity sets it, or per particle (N, 3)), the initial
+positions (an offset (3,) of the scene's positions, as entity.set_position moves an entity, or
+absolute positions (N, 3)), per-particle E (N,) and, for Muscle, per-particle actuation (N,)
+(mpm_solver.py:922-949: the reference's actuation gradients; particle_entity.py:415-481: its
+state-input gradients).  The plastic materials' state (F and Jp) is carried through the
+adjoint.  This replaces the reference's requires_grad path (simulator.py:294-303,
+mpm_solver.py:485-517, with the gstaichi autodiff kernels and backward_svd at
+mpm_solver.py:1112-1129).
 """
 
 from __future__ import annotations
@@ -31,15 +34,22 @@ from .exceptions import GenesisException
 class DifferentiableRollout:
     def __init__(self, desc, checkpoint_every: int = 20, nu: float | None = None):
         kinds = {k for k, _ in desc.materials}
-        if not kinds <= {"elastic", "muscle"} or len(desc.materials) != 1:
-            raise GenesisException("the adjoint supports one Elastic or Muscle material per scene")
-        self.muscle = kinds == {"muscle"}
+        if not kinds <= {"elastic", "muscle", "elastoplastic", "liquid", "sand", "snow"}:
+            raise GenesisException(f"no adjoint for materials {sorted(kinds)}")
+        self.muscle = "muscle" in kinds
         self.desc = desc
         self.k = int(checkpoint_every)
         self.T = int(desc.n_substeps)
-        self.nu = float(nu if nu is not None else desc.materials[0][1].get("nu", 0.2))
         # one sort before the rollout, none after: the adjoint walks the same slot order
         self.rt: MPMRuntime = runtime_from_descs([desc], sort_interval=0, use_graphs=False)
+        mats = self.rt.specs[0].materials
+        mi = torch.as_tensor(desc.mat_idx, dtype=torch.long, device=self.rt.device)
+        nus = torch.tensor([m.nu for m in mats], dtype=torch.float32, device=self.rt.device)
+        # each particle's Poisson ratio (the nu argument overrides every material's) and default Jp
+        self.nu_p = torch.full_like(mi, float(nu), dtype=torch.float32) if nu is not None else nus[mi]
+        self.nu = float(nu if nu is not None else mats[0].nu)
+        self.mat_idx = mi.to(torch.uint8)
+        self.jp0 = torch.tensor([m.default_Jp for m in mats], dtype=torch.float32, device=self.rt.device)[mi]
         if self.rt.mu_p is None:
             raise GenesisException("the differentiable scene needs per-particle E")
         lib = self.rt.lib
@@ -57,7 +67,7 @@ class DifferentiableRollout:
         self.generation = 0  # forwards so far: a backward must follow its own forward
 
     def _lame(self, E):
-        nu = self.nu
+        nu = self.nu_p
         return E / (2.0 * (1.0 + nu)), E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
 
     def forward(self, v0: torch.Tensor, E: torch.Tensor, actu: torch.Tensor | None = None,
@@ -82,15 +92,14 @@ class DifferentiableRollout:
         if self.muscle:
             a = torch.zeros(n, device=dev) if actu is None else actu.detach().to(dev, torch.float32).reshape(n)
             rt.actu[:n] = a
-        mats = torch.zeros(n, dtype=torch.uint8, device=dev)
         rt.load_state(
             pos.contiguous(),
             v0.contiguous(),
             torch.zeros((n, 9), device=dev),
             torch.eye(3, device=dev).reshape(1, 9).repeat(n, 1),
-            torch.ones(n, device=dev),
+            self.jp0,
             torch.ones(n, dtype=torch.bool, device=dev),
-            mats,
+            self.mat_idx,
         )
         mu, lam = self._lame(E)
         rt.set_lame(mu, lam)
@@ -174,7 +183,7 @@ class DifferentiableRollout:
         self.v0_grad = torch.empty((n, 3), dtype=torch.float32, device=rt.device)
         self.v0_grad[gid] = self.adj[3:6, :n].t()
         vbar = self.adj[3:6, :n].sum(dim=1)
-        nu = self.nu
+        nu = self.nu_p[gid]  # the slot order's Poisson ratios
         Ebar_slot = self.lame_bar[0, :n] / (2.0 * (1.0 + nu)) + self.lame_bar[1, :n] * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
         Ebar = torch.empty(n, dtype=torch.float32, device=rt.device)
         Ebar[gid] = Ebar_slot

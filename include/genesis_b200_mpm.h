@@ -311,15 +311,16 @@ int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_par
  * next mpm_substeps_noalloc, which clears them. */
 int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, uint32_t* inst_out, void* stream);
 
-/* ---- differentiation (Elastic corotated / neo-Hookean, Muscle) --------------
- * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with elastic.py:62-83 and
- * muscle.py:57-65; every material of the problem must be an Elastic or a Muscle;
+/* ---- differentiation (every MPM material) -----------------------------------
+ * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with materials/MPM/*.py: Elastic
+ * corotated / neo-Hookean, Muscle, ElastoPlastic von Mises / clamp, Liquid, Sand, Snow;
  * replaces the gstaichi autodiff of substep_post_coupling_grad / couple_grad /
- * substep_pre_coupling_grad, mpm_solver.py:485-517, legacy_coupler.py:996-1017).
+ * substep_pre_coupling_grad, mpm_solver.py:485-517, legacy_coupler.py:996-1017, and its SVD
+ * adjoint backward_svd, :1112-1129).  No colliders (MPM_E_INVALID).
  * `state` is the particle state at the START of the substep (unchanged by the call; the
  * particles must still be in the slot order the last mpm_sort_particles produced).
  * `adj` (float[25][state_stride], same planar layout as the state) holds on entry the
- * adjoint of the substep's output x, v, C, F and on return the adjoint of its input;
+ * adjoint of the substep's output x, v, C, F, Jp and on return the adjoint of its input;
  * `lame_bar` (float[3][state_stride]) accumulates per slot dL/dmu, dL/dlam and, when
  * `state->actu` is set (Muscle), dL/dactu (row 2 is untouched otherwise).
  * The caller allocates adj_workspace (mpm_adjoint_workspace_bytes). */

@@ -130,7 +130,8 @@ def test_differentiable_scene_limits():
     s2 = gs.Scene(sim_options=gs.options.SimOptions(dt=DT, substeps=SUB, requires_grad=True),
                   mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1)))
     s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.3), size=(0.1, 0.1, 0.1)), material=gs.materials.MPM.Sand())
-    with pytest.raises(gs.GenesisException):
+    s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.1), size=(0.3, 0.3, 0.05)), material=gs.materials.Rigid())
+    with pytest.raises(gs.GenesisException):  # no adjoint through rigid colliders
         s2.build()
 
 
