@@ -312,7 +312,7 @@ int mpm_substeps_noalloc(const mpm_problem* prob, const mpm_tables* tab, mpm_par
 int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, uint32_t* inst_out, void* stream);
 
 /* ---- differentiation (every MPM material) -----------------------------------
- * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with materials/MPM/*.py: Elastic
+ * Reverse-mode adjoint of one substep (mpm_solver.py:261-449 with the materials/MPM files: Elastic
  * corotated / neo-Hookean, Muscle, ElastoPlastic von Mises / clamp, Liquid, Sand, Snow;
  * replaces the gstaichi autodiff of substep_post_coupling_grad / couple_grad /
  * substep_pre_coupling_grad, mpm_solver.py:485-517, legacy_coupler.py:996-1017, and its SVD
