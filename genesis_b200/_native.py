@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -144,7 +144,7 @@ class Tables(C.Structure):
     ]
 
 
-COLLIDER_SPHERE, COLLIDER_PLANE, COLLIDER_BOX, COLLIDER_TOOL = 0, 1, 2, 3
+COLLIDER_SPHERE, COLLIDER_PLANE, COLLIDER_BOX, COLLIDER_TOOL, COLLIDER_SDF = 0, 1, 2, 3, 4
 
 
 class Collider(C.Structure):
@@ -164,6 +164,10 @@ class Collider(C.Structure):
         ("sdf_offset", C.c_int64),
         ("sdf_scale", C.c_float * 3),
         ("floor", C.c_float),
+        ("sdf_res3", C.c_int32 * 3),
+        ("sdf_cell", C.c_float),
+        ("sdf_max", C.c_float),
+        ("sdf_pad2", C.c_float),
     ]
 
 

@@ -538,9 +538,54 @@ __global__ void k_build_chunks(mpm_problem prob, const mpm_instance* __restrict_
 
 // ---------------------------------------------------------------- rigid colliders
 
+// MPM_COLLIDER_SDF: distance and geom-frame gradient at geom-frame point l from the sampled
+// grid (sdf_func_sdf / sdf_func_grad, utils/sdf_decomp.py:102-276): trilinear inside the grid,
+// the distance-to-centre proxy outside it
+__device__ __forceinline__ void sdf_sampled(const mpm_collider& c, const float* __restrict__ sdf, float eps,
+                                            const float* l, float& sd, float* gl) {
+    const int r[3] = {c.sdf_res3[0], c.sdf_res3[1], c.sdf_res3[2]};
+    float ps[3], dc[3];
+    bool outside = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float half = 0.5f * (float)(r[d] - 1);
+        ps[d] = c.sdf_scale[d] * l[d] + half;
+        dc[d] = ps[d] - half;
+        outside = outside || ps[d] >= (float)(r[d] - 1) || ps[d] <= 0.f;
+    }
+    if (outside) {
+        // sdf_func_proxy_sdf / _grad: |p - centre| / cell_size + sdf_max, normalize(p - centre)
+        const float d2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
+        sd = sqrtf(d2) / c.sdf_cell + c.sdf_max;
+        const float inv = rsqrtf(d2 + eps);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gl[d] = dc[d] * inv;
+        return;
+    }
+    int b[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) b[d] = min((int)floorf(ps[d]), r[d] - 2);
+    const int64_t N = (int64_t)r[0] * r[1] * r[2];
+    const float* val = sdf + c.sdf_offset;
+    const float* grd = val + N;
+    sd = 0.f;
+    gl[0] = gl[1] = gl[2] = 0.f;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int cx = b[0] + (o >> 2), cy = b[1] + ((o >> 1) & 1), cz = b[2] + (o & 1);
+        const float w = (1.f - fabsf(ps[0] - (float)cx)) * (1.f - fabsf(ps[1] - (float)cy)) * (1.f - fabsf(ps[2] - (float)cz));
+        const int64_t idx = ((int64_t)cx * r[1] + cy) * r[2] + cz;
+        sd += w * val[idx];
+        gl[0] += w * grd[3 * idx + 0];
+        gl[1] += w * grd[3 * idx + 1];
+        gl[2] += w * grd[3 * idx + 2];
+    }
+}
+
 // signed distance sd of the geom at p (utils/sdf_decomp.py:75-300), its world gradient g
 // (unnormalised for the sphere) and q = p - the geom's origin
-__device__ __forceinline__ void sdf_grad(const mpm_collider& c, const float* p, float& sd, float* g, float* q) {
+__device__ __forceinline__ void sdf_grad(const mpm_collider& c, const float* __restrict__ sdf, float eps,
+                                         const float* p, float& sd, float* g, float* q) {
     q[0] = p[0] - c.pos[0];
     q[1] = p[1] - c.pos[1];
     q[2] = p[2] - c.pos[2];
@@ -558,6 +603,8 @@ __device__ __forceinline__ void sdf_grad(const mpm_collider& c, const float* p, 
             gl[0] = c.data[0];
             gl[1] = c.data[1];
             gl[2] = c.data[2];
+        } else if (c.kind == MPM_COLLIDER_SDF) {
+            sdf_sampled(c, sdf, eps, l, sd, gl);
         } else {
             float d[3], o[3];
 #pragma unroll
@@ -597,9 +644,10 @@ __device__ __forceinline__ void unit_normal(const mpm_collider& c, float eps, fl
     n[2] = g[2] * ninv;
 }
 
-__device__ __forceinline__ void collider_normal(const mpm_collider& c, float eps, const float* p, float* n) {
+__device__ __forceinline__ void collider_normal(const mpm_collider& c, const float* __restrict__ sdf, float eps,
+                                                const float* p, float* n) {
     float sd, g[3], q[3];
-    sdf_grad(c, p, sd, g, q);
+    sdf_grad(c, sdf, eps, p, sd, g, q);
     unit_normal(c, eps, g, n);
 }
 
@@ -640,10 +688,10 @@ __device__ __forceinline__ void rigid_respond(const mpm_collider& c, float eps, 
 
 // the grid op's coupling of one node (legacy_coupler.py:166-343): influence
 // min(exp(-sd / softness), 1), acting above 0.1
-__device__ __forceinline__ void collide_rigid(const mpm_collider& c, float eps, float dt, float mass, const float* p,
-                                              float* v, float* fout) {
+__device__ __forceinline__ void collide_rigid(const mpm_collider& c, const float* __restrict__ sdf, float eps, float dt,
+                                              float mass, const float* p, float* v, float* fout) {
     float sd, g[3], q[3], n[3];
-    sdf_grad(c, p, sd, g, q);
+    sdf_grad(c, sdf, eps, p, sd, g, q);
     const float influence = fminf(expf(-sd / fmaxf(1e-10f, c.softness)), 1.f);
     if (!(influence > 0.1f)) return;
     unit_normal(c, eps, g, n);
@@ -771,6 +819,7 @@ struct P2GArgs {
     const mpm_collider* cols;  // CPIC variants only
     int n_cols;
     float* cforce;
+    const float* sdf_voxels;   // sampled grids of MPM_COLLIDER_TOOL / _SDF colliders
 };
 
 // Shared tile in int32 fixed point.  On sm_100 shared-memory float atomicAdd is not a
@@ -988,7 +1037,7 @@ __device__ __forceinline__ void cpic_update_normals(const P2GArgs& a, int inst, 
         const mpm_collider& c = a.cols[k];
         if (c.instance != inst || c.kind == MPM_COLLIDER_TOOL) continue;  // CPIC: rigid geoms only
         float n[3];
-        collider_normal(c, I.eps, x, n);
+        collider_normal(c, a.sdf_voxels, I.eps, x, n);
         float* o = a.par.cpic_normal + (int64_t)(3 * k) * st + g;
         if (n[0] * o[0] + n[1] * o[st] + n[2] * o[2 * st] >= 0.f) {
             o[0] = n[0];
@@ -1009,7 +1058,7 @@ __device__ __forceinline__ uint32_t cpic_separating(const P2GArgs& a, int inst, 
         const mpm_collider& c = a.cols[k];
         if (c.instance != inst || c.kind == MPM_COLLIDER_TOOL) continue;  // CPIC: rigid geoms only
         float n[3];
-        collider_normal(c, I.eps, pos, n);
+        collider_normal(c, a.sdf_voxels, I.eps, pos, n);
         const float* o = a.par.cpic_normal + (int64_t)(3 * k) * st + g;
         if (n[0] * o[0] + n[1] * o[st] + n[2] * o[2 * st] < 0.f) return (uint32_t)(k + 1);
     }
@@ -1639,7 +1688,7 @@ __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_
                 }
                 for (int k = 0; k < n_colliders; ++k) {
                     if (colliders[k].instance != e.x || colliders[k].kind == MPM_COLLIDER_TOOL) continue;
-                    collide_rigid(colliders[k], I.eps, I.dt, mreal, p, v,
+                    collide_rigid(colliders[k], sdf_voxels, I.eps, I.dt, mreal, p, v,
                                   collider_force ? collider_force + 6 * k : nullptr);
                 }
                 vx = v[0];
@@ -1885,7 +1934,8 @@ static int p2g_args(const mpm_problem* prob, const mpm_tables* tab, const mpm_pa
     const int nc = tab->colliders ? tab->n_colliders : 0;
     cpic = (prob->flags & MPM_PROBF_CPIC) && nc > 0;
     if (cpic && (!par->cpic_normal || !par->cpic_sep || nc > 254)) return MPM_E_INVALID;
-    a = P2GArgs{*prob, tab->instances, tab->materials, *par, ws_of(*prob, ws), tab->colliders, nc, tab->collider_force};
+    a = P2GArgs{*prob,           tab->instances, tab->materials,     *par,           ws_of(*prob, ws),
+                tab->colliders, nc,             tab->collider_force, tab->sdf_voxels};
     return MPM_OK;
 }
 

@@ -135,7 +135,12 @@ class MPMSolver:
             colliders += [t._collider(env, off, floor) for env in range(self._B)]
             grids.append(g)
             off += g.numel()
-        colliders += [r._collider(env) for r in rigid for env in range(self._B)]
+        for r in rigid:  # then the rigid geoms, each sampled grid once
+            g = r._sdf(self._sim.device)
+            colliders += [r._collider(env, off) for env in range(self._B)]
+            if g is not None:
+                grids.append(g)
+                off += g.numel()
         grad = self._sim.requires_grad
         if grad:
             from ..materials import MPM

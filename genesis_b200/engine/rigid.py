@@ -6,8 +6,10 @@ removes to its rigid-body solver.  This build has no rigid-body solver: a rigid 
 pose and velocity are set by the caller (set_pos / set_quat / set_dofs_velocity), the
 collider moves at that velocity over the substeps, and the reaction force and torque on
 it are reported by get_coupling_force().  Sphere and Plane use the reference's analytic
-signed distance; a Box uses the exact box distance (the reference samples its SDF on a
-grid of sdf_cell_size).
+signed distance.  A Box is coupled as the reference couples every other geom, through a
+signed-distance grid sampled once at build (box_sdf_grid: the grid of rigid_geom.py:147-193,
+trilinear lookups of distance and gradient in the grid op); B200Options(exact_box_sdf=True)
+uses the exact box distance instead.
 """
 
 from __future__ import annotations
@@ -21,6 +23,37 @@ from ..exceptions import GenesisException
 
 # float32 columns of one mpm_collider row after its two int32 fields
 _POS, _ROT, _DATA, _LIN, _ANG = slice(0, 3), slice(3, 12), slice(12, 15), slice(15, 18), slice(18, 21)
+
+
+def box_sd(p, half):
+    """Exact signed distance of points p [n, 3] to the box [-half, half] (negative inside)."""
+    d = np.abs(p) - half
+    return np.linalg.norm(np.maximum(d, 0.0), axis=1) + np.minimum(d.max(axis=1), 0.0)
+
+
+def box_sdf_grid(half, sdf_cell_size=0.005, sdf_min_res=32, sdf_max_res=128, eps=float(np.finfo(np.float32).eps)):
+    """The signed-distance grid the reference builds for a geom (rigid_geom.py:147-193), for a
+    box mesh centred at its origin: the box's extent padded by 0.2 of its largest side, cell
+    size sdf_cell_size clipped to [grid.max() / (sdf_max_res - 1), grid.min() / max(sdf_min_res
+    - 1, 2)] plus gs.EPS, ceil(grid / cell) + 1 nodes per axis, the distance at every node (the
+    box mesh's signed distance, which is the box's) and its central-difference gradient with
+    a step of 1e-2 cell.  Returns (values [rx, ry, rz], gradients [rx, ry, rz, 3], voxel scale
+    (res - 1) / grid size per axis, cell size, largest value), all float32."""
+    half = np.asarray(half, dtype=np.float64)
+    ext = 2 * half
+    grid = ext.max() * 0.2 + ext
+    cell = eps + np.clip(sdf_cell_size, grid.max() / (sdf_max_res - 1), grid.min() / max(sdf_min_res - 1, 2))
+    res = np.ceil(grid / cell).astype(np.int64) + 1
+    grid = (res - 1) * cell
+    axes = [np.linspace(-grid[d] / 2, grid[d] / 2, res[d]) for d in range(3)]
+    pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+    val = box_sd(pts, half)
+    delta = cell * 1e-2
+    grad = np.stack([(box_sd(pts + delta * e, half) - box_sd(pts - delta * e, half)) / (2 * delta) for e in np.eye(3)],
+                    -1)
+    shape = tuple(int(r) for r in res)
+    return (val.reshape(shape).astype(np.float32), grad.reshape(shape + (3,)).astype(np.float32),
+            ((res - 1) / grid).astype(np.float32), np.float32(cell), np.float32(val.max()))
 
 
 def quat_to_R(q):
@@ -50,13 +83,17 @@ def R_to_quat(R):
 class KinematicRigidEntity:
     """A gs.materials.Rigid entity with a Box, Sphere or Plane morph."""
 
-    def __init__(self, scene, idx, material, morph):
+    def __init__(self, scene, idx, material, morph, exact_box_sdf=False):
+        self._grid = None
         if isinstance(morph, _morphs.Sphere):
             kind, data = nat.COLLIDER_SPHERE, (morph.radius, 0.0, 0.0)
         elif isinstance(morph, _morphs.Plane):
             kind, data = nat.COLLIDER_PLANE, morph.normal
         elif isinstance(morph, _morphs.Box):
-            kind, data = nat.COLLIDER_BOX, tuple(np.asarray(morph.size) / 2)
+            data = tuple(np.asarray(morph.size) / 2)
+            kind = nat.COLLIDER_BOX if exact_box_sdf else nat.COLLIDER_SDF
+            if not exact_box_sdf:
+                self._grid = box_sdf_grid(data, material.sdf_cell_size, material.sdf_min_res, material.sdf_max_res)
         else:
             raise GenesisException("Rigid entities on this path take a Box, Sphere or Plane morph.")
         self._scene = scene
@@ -69,10 +106,25 @@ class KinematicRigidEntity:
         self._rt = None
 
     # ------------------------------------------------------------- build
-    def _collider(self, env):
+    def _sdf(self, device):
+        """The sampled grid's values then gradients, flattened (None for analytic geoms)."""
+        if self._grid is None:
+            return None
+        val, grad = self._grid[0], self._grid[1]
+        return torch.as_tensor(np.concatenate([val.reshape(-1), grad.reshape(-1)]), device=device)
+
+    def _collider(self, env, sdf_offset=0):
         c = nat.Collider()
         c.kind = self._kind
         c.instance = int(env)
+        if self._grid is not None:
+            val, _, scale, cell, vmax = self._grid
+            for d in range(3):
+                c.sdf_res3[d] = int(val.shape[d])
+                c.sdf_scale[d] = float(scale[d])
+            c.sdf_offset = int(sdf_offset)
+            c.sdf_cell = float(cell)
+            c.sdf_max = float(vmax)
         R = quat_to_R(self._morph.quat)
         for d in range(3):
             c.pos[d] = float(self._morph.pos[d])

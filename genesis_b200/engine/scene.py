@@ -63,7 +63,8 @@ class Scene:
         if isinstance(material, _materials.Rigid):
             from .rigid import KinematicRigidEntity
 
-            ent = KinematicRigidEntity(self, len(self._entities), material, morph)
+            ent = KinematicRigidEntity(self, len(self._entities), material, morph,
+                                       exact_box_sdf=self.b200_options.exact_box_sdf)
             self._entities.append(ent)
             if material.needs_coup:
                 self._rigid_entities.append(ent)

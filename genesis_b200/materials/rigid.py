@@ -66,3 +66,15 @@ class Rigid:
     @property
     def gravity_compensation(self):
         return self._gravity_compensation
+
+    @property
+    def sdf_cell_size(self):
+        return self._sdf_cell_size
+
+    @property
+    def sdf_min_res(self):
+        return self._sdf_min_res
+
+    @property
+    def sdf_max_res(self):
+        return self._sdf_max_res

@@ -110,6 +110,8 @@ class B200Options(Options):
                      the first scene call after it has arrived raises; scene.check_state()
                      waits for it),
                      'never' (call scene.check_state() yourself)
+    exact_box_sdf    couple Box rigid entities through the exact box distance instead of the
+                     sampled signed-distance grid the reference uses for every non-analytic geom
     """
 
     sort_interval: int = 50
@@ -117,6 +119,7 @@ class B200Options(Options):
     use_cuda_graph: bool = True
     check_nan: str = "step"
     grid_ctas: int = 0
+    exact_box_sdf: bool = False
 
     def __init__(self, **data):
         super().__init__(**data)

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 8
+#define MPM_ABI_VERSION 9
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -166,7 +166,8 @@ typedef struct mpm_particles {
  * kinematic motion between host updates). */
 #define MPM_COLLIDER_SPHERE 0  /* sd = |p - pos| - data[0]  (utils/sdf_decomp.py:91-92) */
 #define MPM_COLLIDER_PLANE 1   /* sd = n . R^T (p - pos), n = data (geom frame, unit) (sdf_decomp.py:94-98) */
-#define MPM_COLLIDER_BOX 2     /* half extents data[0..2]; exact box SDF (the reference samples it on a grid) */
+#define MPM_COLLIDER_BOX 2     /* half extents data[0..2]; exact box SDF (the reference samples it on a grid:
+                                  MPM_COLLIDER_SDF restates that) */
 
 /* Tool entity (engine/entities/tool_entity/mesh.py:80-176, coupled by
  * legacy_coupler.py:346-350 before the rigid geoms): signed distance sampled trilinearly from
@@ -175,6 +176,17 @@ typedef struct mpm_particles {
  * (Tool.friction, coup_softness); no restitution and no reaction force.  Its origin moves at
  * lin_vel and stays above `floor` (FloorBoundary.impose_pos, boundaries.py:67-70). */
 #define MPM_COLLIDER_TOOL 3
+
+/* Rigid geom through a sampled signed-distance grid, as the reference couples every geom that
+ * is not a sphere or a plane (boxes and meshes: utils/sdf_decomp.py:75-276, grids built by
+ * rigid_geom.py:147-225): sdf_res3[0] x sdf_res3[1] x sdf_res3[2] values (x-major) at
+ * sdf_offset in mpm_tables.sdf_voxels, followed by the same number of gradient triples
+ * [n][3] (central differences of 1e-2 cell of the true distance, as _compute_sd_grad takes
+ * them).  Voxel coordinate = sdf_scale * (geom-frame point) + (sdf_res3 - 1) / 2; inside the
+ * grid the distance and the gradient are trilinear; outside it (any coordinate <= 0 or >=
+ * res - 1) the proxy |voxel - centre| / sdf_cell + sdf_max and the direction to the centre.
+ * Then the same coupling as MPM_COLLIDER_BOX. */
+#define MPM_COLLIDER_SDF 4
 
 typedef struct mpm_collider {
     int32_t kind;        /* MPM_COLLIDER_* */
@@ -192,6 +204,10 @@ typedef struct mpm_collider {
     int64_t sdf_offset;  /* MPM_COLLIDER_TOOL: index of its first voxel in mpm_tables.sdf_voxels */
     float sdf_scale[3];  /* voxel coordinate = sdf_scale * (geom-frame point) + (sdf_res - 1) / 2 */
     float floor;         /* MPM_COLLIDER_TOOL: floor height of the tool solver */
+    int32_t sdf_res3[3]; /* MPM_COLLIDER_SDF: voxels per axis */
+    float sdf_cell;      /* MPM_COLLIDER_SDF: cell size (sdf_cell_size of rigid_geom.py:155-158) */
+    float sdf_max;       /* MPM_COLLIDER_SDF: largest sampled distance */
+    float sdf_pad2;
 } mpm_collider;
 
 typedef struct mpm_tables {

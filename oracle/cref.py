@@ -55,6 +55,7 @@ def _structs(dtype):
             ("pos", Rt * 3), ("rot", Rt * 9), ("data", Rt * 3), ("lin_vel", Rt * 3), ("ang_vel", Rt * 3),
             ("friction", Rt), ("softness", Rt), ("restitution", Rt),
             ("sdf", C.c_void_p), ("sdf_res", C.c_int32), ("sdf_scale", Rt * 3), ("floor", Rt),
+            ("sdf_res3", C.c_int32 * 3), ("sdf_cell", Rt), ("sdf_max", Rt),
         ]
 
     return Params, Mat, Coll
@@ -139,10 +140,20 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
     if st.get("colliders"):
         cs = st["colliders"]
         carr = (Coll * len(cs))()
-        kinds = {"sphere": 0, "plane": 1, "box": 2, "tool": 3}
+        kinds = {"sphere": 0, "plane": 1, "box": 2, "tool": 3, "sdf": 4}
         keep = []  # the tools' voxel arrays stay alive for the call
         for i, c in enumerate(cs):
             carr[i].kind = kinds[c.kind]
+            if c.kind == "sdf":
+                vox = np.ascontiguousarray(np.concatenate([np.asarray(c.sdf, dtype=dt).reshape(-1),
+                                                           np.asarray(c.sdf_grad, dtype=dt).reshape(-1)]))
+                keep.append(vox)
+                carr[i].sdf = vox.ctypes.data_as(C.c_void_p)
+                for d in range(3):
+                    carr[i].sdf_res3[d] = int(np.shape(c.sdf)[d])
+                    carr[i].sdf_scale[d] = float(c.sdf_scale[d])
+                carr[i].sdf_cell = float(c.sdf_cell)
+                carr[i].sdf_max = float(c.sdf_max)
             if c.kind == "tool":
                 vox = np.ascontiguousarray(c.sdf, dtype=dt).reshape(-1)
                 keep.append(vox)
@@ -175,7 +186,8 @@ def substeps(p: R.Params, mats: list[R.Material], st: dict, n_substeps: int, n_t
         for i, c in enumerate(cs):
             moved.append(R.Collider(c.kind, np.array(carr[i].pos[:]), np.array(carr[i].rot[:]).reshape(3, 3),
                                     np.asarray(c.data), np.asarray(c.lin_vel), np.asarray(c.ang_vel), c.friction,
-                                    c.softness, c.restitution, c.sdf, c.sdf_scale, c.floor))
+                                    c.softness, c.restitution, c.sdf, c.sdf_scale, c.floor, c.sdf_grad, c.sdf_cell,
+                                    c.sdf_max))
         out = dict(st)
         out.update(x=x, v=v, C=Cm.reshape(n, 3, 3), F=F.reshape(n, 3, 3), Jp=Jp, colliders=moved, forces=forces)
         if rn is not None:

@@ -82,8 +82,11 @@ typedef struct {
     REAL friction, softness, restitution;
     const REAL* sdf;    /* tool: [sdf_res]^3 voxels, x-major */
     int32_t sdf_res;
-    REAL sdf_scale[3];  /* tool: voxel = sdf_scale * (geom-frame point) + (sdf_res - 1) / 2 */
+    REAL sdf_scale[3];  /* tool, sampled geom: voxel = sdf_scale * (geom-frame point) + (res - 1) / 2 */
     REAL floor;         /* tool: floor height of the tool solver */
+    int32_t sdf_res3[3];/* sampled geom (kind 4): voxels per axis; sdf holds the values, then [n][3] gradients */
+    REAL sdf_cell;      /* sampled geom: cell size */
+    REAL sdf_max;       /* sampled geom: largest sampled distance */
 } ref_collider;
 
 /* ---------------------------------------------------------------- SVD */
@@ -386,6 +389,39 @@ static void sdf_grad(const ref_collider* c, REAL eps, const REAL* pos, REAL* sd_
         if (c->kind == 1) {
             sd = l[0] * c->data[0] + l[1] * c->data[1] + l[2] * c->data[2];
             for (int i = 0; i < 3; ++i) gl[i] = c->data[i];
+        } else if (c->kind == 4) {
+            /* sampled geom: sdf_func_sdf / sdf_func_grad (utils/sdf_decomp.py:102-276) */
+            const int32_t* r = c->sdf_res3;
+            REAL ps[3], dc[3];
+            int outside = 0;
+            for (int i = 0; i < 3; ++i) {
+                REAL half = (REAL)0.5 * (REAL)(r[i] - 1);
+                ps[i] = c->sdf_scale[i] * l[i] + half;
+                dc[i] = ps[i] - half;
+                if (ps[i] >= (REAL)(r[i] - 1) || ps[i] <= 0) outside = 1;
+            }
+            if (outside) {
+                REAL d2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
+                sd = R_SQRT(d2) / c->sdf_cell + c->sdf_max;
+                REAL nn = R_SQRT(d2 + eps);
+                for (int i = 0; i < 3; ++i) gl[i] = dc[i] / nn;
+            } else {
+                int b[3];
+                for (int i = 0; i < 3; ++i) {
+                    b[i] = (int)RFLOOR(ps[i]);
+                    if (b[i] > r[i] - 2) b[i] = r[i] - 2;
+                }
+                const int64_t N = (int64_t)r[0] * r[1] * r[2];
+                sd = 0;
+                gl[0] = gl[1] = gl[2] = 0;
+                for (int o = 0; o < 8; ++o) {
+                    int cx = b[0] + (o >> 2), cy = b[1] + ((o >> 1) & 1), cz = b[2] + (o & 1);
+                    REAL w = (1 - RABS(ps[0] - cx)) * (1 - RABS(ps[1] - cy)) * (1 - RABS(ps[2] - cz));
+                    int64_t idx = ((int64_t)cx * r[1] + cy) * r[2] + cz;
+                    sd += w * c->sdf[idx];
+                    for (int i = 0; i < 3; ++i) gl[i] += w * c->sdf[N + 3 * idx + i];
+                }
+            }
         } else {
             REAL d[3], o[3];
             for (int i = 0; i < 3; ++i) {

@@ -34,6 +34,7 @@ sign of the last singular value.
 
 from __future__ import annotations
 
+import dataclasses
 import math
 from dataclasses import dataclass, field
 
@@ -420,15 +421,46 @@ class Collider:
     friction: float = 0.1
     softness: float = 0.002
     restitution: float = 0.0
-    sdf: np.ndarray | None = None  # kind 'tool': [res, res, res] voxel signed distances
-    sdf_scale: tuple = (1.0, 1.0, 1.0)  # kind 'tool': voxel = sdf_scale * geom-frame point + (res - 1) / 2
+    sdf: np.ndarray | None = None  # kind 'tool' / 'sdf': [rx, ry, rz] voxel signed distances
+    sdf_scale: tuple = (1.0, 1.0, 1.0)  # kind 'tool' / 'sdf': voxel = sdf_scale * geom-frame point + (res - 1) / 2
     floor: float = 0.0  # kind 'tool': the tool solver's floor height
+    sdf_grad: np.ndarray | None = None  # kind 'sdf': [rx, ry, rz, 3] sampled gradient
+    sdf_cell: float = 1.0  # kind 'sdf': cell size
+    sdf_max: float = 0.0  # kind 'sdf': largest sampled distance
+
+
+def sdf_sampled(c: Collider, l, eps):
+    """A geom's sampled signed distance and gradient at geom-frame points l (sdf_func_sdf /
+    sdf_func_grad, utils/sdf_decomp.py:102-276): trilinear in the grid; outside it the proxy
+    |voxel - centre| / cell + sdf_max and the unit direction to the centre."""
+    dt = l.dtype.type
+    r = np.asarray(np.shape(c.sdf))
+    half = (r - 1) * dt(0.5)
+    ps = l * np.asarray(c.sdf_scale, dtype=dt) + half
+    dc = ps - half
+    out = ((ps >= r - 1) | (ps <= 0)).any(1)
+    d2 = (dc * dc).sum(1)
+    sd_out = np.sqrt(d2) / dt(c.sdf_cell) + dt(c.sdf_max)
+    g_out = dc / np.sqrt(d2 + dt(eps))[:, None]
+    b = np.minimum(np.floor(ps).astype(np.int64), r - 2)
+    b = np.clip(b, 0, r - 2)
+    val = np.asarray(c.sdf, dtype=dt)
+    grd = np.asarray(c.sdf_grad, dtype=dt)
+    sd_in = np.zeros(len(l), dtype=dt)
+    g_in = np.zeros_like(l)
+    for o in range(8):
+        cell = b + np.array([o >> 2, (o >> 1) & 1, o & 1])
+        w = np.prod(1 - np.abs(ps - cell), axis=1)
+        sd_in += w * val[cell[:, 0], cell[:, 1], cell[:, 2]]
+        g_in += w[:, None] * grd[cell[:, 0], cell[:, 1], cell[:, 2]]
+    return np.where(out, sd_out, sd_in), np.where(out[:, None], g_out, g_in)
 
 
 def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
     """_func_collide_with_rigid_geom + _func_collide_in_rigid_geom for grid nodes at pos
-    (legacy_coupler.py:166-343); sphere and plane SDFs as utils/sdf_decomp.py:91-98, the
-    box's exact.  Returns (new velocity, force, torque about c.pos)."""
+    (legacy_coupler.py:166-343); sphere and plane SDFs as utils/sdf_decomp.py:91-98, kind
+    'sdf' through its sampled grid (sdf_sampled), kind 'box' the exact box distance.  Returns
+    (new velocity, force, torque about c.pos)."""
     if c.kind == "tool":
         raise NotImplementedError("tool colliders are coupled by the C restatement (cref)")
     dt = vel.dtype.type
@@ -443,6 +475,8 @@ def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
         if c.kind == "plane":
             sd = l @ data
             gl = np.broadcast_to(data, l.shape)
+        elif c.kind == "sdf":
+            sd, gl = sdf_sampled(c, l, eps)
         else:
             d = np.abs(l) - data
             o = np.maximum(d, 0)
@@ -483,8 +517,7 @@ def advance_colliders(p: Params, colliders):
             k = w / th
             K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
             R = (np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K) @ R
-        out.append(Collider(c.kind, np.asarray(c.pos) + np.asarray(c.lin_vel) * p.dt, R, c.data, c.lin_vel, c.ang_vel,
-                            c.friction, c.softness, c.restitution))
+        out.append(dataclasses.replace(c, pos=np.asarray(c.pos) + np.asarray(c.lin_vel) * p.dt, rot=R))
     return out
 
 

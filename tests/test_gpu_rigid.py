@@ -11,12 +11,13 @@ import genesis_b200 as gs
 pytestmark = pytest.mark.gpu
 
 
-def _scene(morph, substeps=10, n_envs=0, **rigid_kw):
+def _scene(morph, substeps=10, n_envs=0, exact_box=False, **rigid_kw):
     gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
     scene = gs.Scene(
         sim_options=gs.options.SimOptions(dt=1e-4 * substeps, substeps=substeps, gravity=(0, 0, -9.8)),
         mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
                                           particle_size=0.01),
+        b200_options=gs.options.B200Options(exact_box_sdf=exact_box),
     )
     block = scene.add_entity(gs.morphs.Box(lower=(0.45, 0.45, 0.33), upper=(0.55, 0.55, 0.43)),
                              material=gs.materials.MPM.Elastic(E=2e4))
@@ -40,26 +41,36 @@ def _oracle(block, collider, v0, n_substeps):
     return out
 
 
-@pytest.mark.parametrize("kind", ["sphere", "box", "plane"])
+@pytest.mark.parametrize("kind", ["sphere", "box", "box_exact", "plane"])
 def test_block_on_rigid_collider_matches_oracle(kind):
+    """box: the reference's sampled signed-distance grid (rigid_geom.py:147-193, trilinear
+    lookups utils/sdf_decomp.py:102-276); box_exact: B200Options(exact_box_sdf=True)."""
+    from genesis_b200.engine.rigid import box_sdf_grid
     from oracle import mpm_ref as R
 
     if kind == "sphere":
         morph = gs.morphs.Sphere(pos=(0.5, 0.5, 0.25), radius=0.06)
         col = R.Collider("sphere", np.array([0.5, 0.5, 0.25]), np.eye(3), np.array([0.06, 0, 0]), friction=0.3)
-    elif kind == "box":
+    elif kind in ("box", "box_exact"):
         morph = gs.morphs.Box(pos=(0.52, 0.5, 0.2), size=(0.3, 0.3, 0.2), euler=(0, 10, 0))
         Rm = gs.morphs._quat_to_R(np.asarray(morph.quat))
-        col = R.Collider("box", np.array([0.52, 0.5, 0.2]), Rm, np.array([0.15, 0.15, 0.1]), friction=0.3)
+        half = np.array([0.15, 0.15, 0.1])
+        if kind == "box_exact":
+            col = R.Collider("box", np.array([0.52, 0.5, 0.2]), Rm, half, friction=0.3)
+        else:
+            val, grad, scale, cell, vmax = box_sdf_grid(half)
+            col = R.Collider("sdf", np.array([0.52, 0.5, 0.2]), Rm, half, friction=0.3, sdf=val, sdf_scale=scale,
+                             sdf_grad=grad, sdf_cell=cell, sdf_max=vmax)
     else:
         morph = gs.morphs.Plane(pos=(0.5, 0.5, 0.3), normal=(0.2, 0.0, 1.0))
         nrm = np.array([0.2, 0.0, 1.0]) / np.linalg.norm([0.2, 0.0, 1.0])
         col = R.Collider("plane", np.array([0.5, 0.5, 0.3]), np.eye(3), nrm, friction=0.3)
-    scene, block, rigid = _scene(morph, coup_friction=0.3)
+    scene, block, rigid = _scene(morph, exact_box=kind == "box_exact", coup_friction=0.3)
     v0 = (0.0, 0.0, -2.0)
     block.set_particles_vel(torch.tensor(v0).expand(block.n_particles, 3))
     o = _oracle(block, col, v0, 40)
-    away = R.Collider(col.kind, np.array([0.5, 0.5, -5.0]), col.rot, col.data)
+    away = R.Collider(col.kind, np.array([0.5, 0.5, -5.0]), col.rot, col.data, sdf=col.sdf, sdf_scale=col.sdf_scale,
+                      sdf_grad=col.sdf_grad, sdf_cell=col.sdf_cell, sdf_max=col.sdf_max)
     free = _oracle(block, away, v0, 40)
     assert np.abs(o["x"] - free["x"]).max() > 1e-4  # the collider changed the trajectory (10x the tolerance)
     for _ in range(4):
