@@ -1,8 +1,11 @@
 """Launch-configuration autotuner for an MPMRuntime.
 
 Picks, by timing short runs on the problem itself, the particles per work item
-(chunk_particles: 128/256/512, i.e. threads per CTA of p2g/g2p/g2p2g), the re-sort
-interval and the persistent CTA count.  The grid block edge is fixed at 4 nodes (it sets
+(chunk_particles: 128/256, i.e. threads per CTA of p2g/g2p/g2p2g), the re-sort
+interval and the persistent CTA count (grid_ctas; the candidates are given per SM:
+0 is the library default of one CTA per resident slot, i.e. SMs x occupancy, 4 per SM
+leaves slots free for a concurrent stream, 14 per SM is two waves of the 128-particle
+kernels, which evens out the tail when the work items are few and uneven).  The grid block edge is fixed at 4 nodes (it sets
 the block-major grid layout and the 8^3 shared tile).  Results are cached per problem
 signature (particle and grid-block counts rounded to powers of two) in a JSON file so a
 served or batched workload tunes once.
@@ -20,7 +23,7 @@ import torch
 DEFAULT_CANDIDATES = {
     "chunk_particles": (128, 256),
     "sort_interval": (25, 50, 100),
-    "grid_ctas": (0,),
+    "grid_ctas_per_sm": (0, 4, 14),
 }
 
 _lock = threading.Lock()
@@ -74,6 +77,9 @@ def tune(rt, candidates=None, trial_substeps: int = 100, use_cache: bool = True,
     tuning does not change the simulation.  Returns (best_config, {config: ms/substep})."""
     cand = dict(DEFAULT_CANDIDATES)
     cand.update(candidates or {})
+    if "grid_ctas" not in cand:
+        sms = torch.cuda.get_device_properties(rt.device).multi_processor_count
+        cand["grid_ctas"] = tuple(int(k) * sms for k in cand["grid_ctas_per_sm"])
     sig = signature(rt)
     if use_cache:
         with _lock:

@@ -26,6 +26,11 @@ namespace gbm {
 #endif
 constexpr int kSvdUnroll = GBM_SVD_UNROLL;
 
+// QR of the column-sorted B = A V: 0 Givens rotations, 1 Gram-Schmidt with a cross product
+#ifndef GBM_SVD_TAIL
+#define GBM_SVD_TAIL 0
+#endif
+
 // One Jacobi rotation in plane (P, Q) of the symmetric matrix a, accumulated into v.
 template <int P, int Q>
 __device__ __forceinline__ void jacobi_pq(float (&a)[3][3], float (&v)[3][3]) {
@@ -187,6 +192,47 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* 
     if (n0 < n1) swap_cols_neg<0, 1>(b, v, n0, n1);
     if (n0 < n2) swap_cols_neg<0, 2>(b, v, n0, n2);
     if (n1 < n2) swap_cols_neg<1, 2>(b, v, n1, n2);
+#if GBM_SVD_TAIL == 1
+    // QR of B by Gram-Schmidt: u0 = b0 / |b0|, u1 = the part of b1 orthogonal to u0,
+    // normalised, u2 = u0 x u1 (so det U = +1), R's diagonal (|b0|, |b1 - (u0.b1) u0|, u2.b2).
+    // This is the QR with r00, r11 >= 0 that the Givens rotations below compute (unique for
+    // rank >= 2).  A (near) zero b0 selects u0 = e_x; a b1 parallel to u0 selects for u1 the
+    // unit vector orthogonal to u0 in the plane of u0 and the axis u0 is least aligned with.
+    {
+        const bool ok0 = n0 > 1e-30f;
+        const float r0 = rsqrtf(ok0 ? n0 : 1.f);
+        const float u0[3] = {ok0 ? b[0][0] * r0 : 1.f, ok0 ? b[1][0] * r0 : 0.f, ok0 ? b[2][0] * r0 : 0.f};
+        const float d01 = u0[0] * b[0][1] + u0[1] * b[1][1] + u0[2] * b[2][1];
+        float w1[3] = {b[0][1] - d01 * u0[0], b[1][1] - d01 * u0[1], b[2][1] - d01 * u0[2]};
+        float m1 = w1[0] * w1[0] + w1[1] * w1[1] + w1[2] * w1[2];
+        if (!(m1 > 1e-30f)) {
+            // rank <= 1: e_k - (u0.e_k) u0 for the k of the smallest |u0_k|
+            const float a0 = fabsf(u0[0]), a1 = fabsf(u0[1]), a2 = fabsf(u0[2]);
+            const int k = (a0 <= a1 && a0 <= a2) ? 0 : (a1 <= a2 ? 1 : 2);
+            const float uk = k == 0 ? u0[0] : (k == 1 ? u0[1] : u0[2]);
+            w1[0] = (k == 0 ? 1.f : 0.f) - uk * u0[0];
+            w1[1] = (k == 1 ? 1.f : 0.f) - uk * u0[1];
+            w1[2] = (k == 2 ? 1.f : 0.f) - uk * u0[2];
+            m1 = w1[0] * w1[0] + w1[1] * w1[1] + w1[2] * w1[2];
+        }
+        const float r1 = rsqrtf(m1);
+        const float u1[3] = {w1[0] * r1, w1[1] * r1, w1[2] * r1};
+        const float u2[3] = {u0[1] * u1[2] - u0[2] * u1[1], u0[2] * u1[0] - u0[0] * u1[2],
+                             u0[0] * u1[1] - u0[1] * u1[0]};
+        S[0] = ok0 ? n0 * r0 : 0.f;
+        S[1] = u1[0] * b[0][1] + u1[1] * b[1][1] + u1[2] * b[2][1];
+        S[2] = u2[0] * b[0][2] + u2[1] * b[1][2] + u2[2] * b[2][2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            U[i * 3 + 0] = u0[i];
+            U[i * 3 + 1] = u1[i];
+            U[i * 3 + 2] = u2[i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) V[i * 3 + j] = v[i][j];
+        }
+        return;
+    }
+#endif
     // Givens QR: B = U R
     float u[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
     float c, s;

@@ -377,9 +377,10 @@ def material_vjp(mat, eps, U, S, V, Ft, Jp, mu, lam, actu, mdir, Fn_bar, Jpn_bar
             out["Jp"][:, 0], out["mu"][:, 0], out["lam"][:, 0], out["actu"][:, 0])
 
 
-def forward_materials(p, mats, st, mu, lam):
+def forward_materials(p, mats, st, mu, lam, colliders=None):
     """One substep of mpm_ref.substep for any mix of MPM materials (all particles active), with
-    per-particle mu / lam; returns the new state and the intermediates of backward_materials."""
+    per-particle mu / lam and the grid op's kinematic colliders (tools, rigid geoms) at this
+    substep's poses; returns the new state and the intermediates of backward_materials."""
     x, v, C, F, Jp = st["x"], st["v"], st["C"], st["F"], st["Jp"]
     n = x.shape[0]
     mi = np.asarray(st["mat"])
@@ -400,14 +401,15 @@ def forward_materials(p, mats, st, mu, lam):
         mass[sel] = R.particle_mass(p, m)
     s = -p.dt * p.p_vol * 4 * p.inv_dx * p.inv_dx
     A = s * P + mass[:, None, None] * C
-    out, inter = _grid_and_g2p(p, st, A, mass)
+    out, inter = _grid_and_g2p(p, st, A, mass, colliders)
     out.update(F=Fn, Jp=Jpn)
     inter.update(Ft=Ft, U=U, S=S, V=V, P=P, A=A, s=s, mass=mass)
     return out, inter
 
 
-def _grid_and_g2p(p, st, A, mass):
-    """p2g scatter of (m v + A d), grid op and g2p of mpm_ref.substep (no colliders)."""
+def _grid_and_g2p(p, st, A, mass, colliders=None):
+    """p2g scatter of (m v + A d), grid op (with the colliders' responses, tools first, as
+    legacy_coupler.py:381-397 orders them) and g2p of mpm_ref.substep."""
     x, v = st["x"], st["v"]
     n = x.shape[0]
     base, fx, w, dw, node0 = _stencil(p, x)
@@ -431,6 +433,20 @@ def _grid_and_g2p(p, st, A, mass):
     vg[act] = gp[act] / gm[act][:, None] + p.dt * np.asarray(p.gravity)[None, :]
     idx = np.array(np.unravel_index(np.arange(G), res)).T
     gpos = (idx + p.lower_cell[None, :]) * p.dx
+    chain = []  # (collider index, collider, its input velocity on the active nodes)
+    if colliders:
+        va = vg[act]
+        ma = gm[act] / 1e3
+        order = [k for k, c in enumerate(colliders) if c.kind == "tool"] + \
+                [k for k, c in enumerate(colliders) if c.kind != "tool"]
+        for k in order:
+            c = colliders[k]
+            chain.append((k, c, va))
+            if c.kind == "tool":
+                va = R.collide_tool(c, p.eps, p.dt, gpos[act], va)
+            else:
+                va = R.collide_rigid(c, p.eps, p.dt, gpos[act], va, ma)[0]
+        vg[act] = va
     gmask = np.ones((G, 3))
     for c in range(3):
         up = (gpos[:, c] >= p.bnd_hi[c]) & (vg[:, c] >= 0)
@@ -458,8 +474,40 @@ def _grid_and_g2p(p, st, A, mass):
     out = dict(st)
     out.update(x=np.clip(xs, p.bnd_lo, p.bnd_hi), v=nv * vmask, C=nC)
     inter = dict(fx=fx, w=w, dw=dw, lin=lin_all, gm=gm, gp=gp, vh=vh, gmask=gmask, act=act, nv=nv, pmask=pmask,
-                 vmask=vmask)
+                 vmask=vmask, chain=chain, gpos=gpos, n_colliders=len(colliders or []))
     return out, inter
+
+
+def collider_vjp(p, c, pos, vin, vbar, mass=None, h=1e-30):
+    """Adjoint of one collider's response at grid nodes pos [G, 3] (input velocity vin [G, 3],
+    output adjoint vbar [G, 3]), by complex-step derivatives (exact to round-off, every branch
+    taken on real parts): returns (vin_bar [G, 3], pos_bar [3], lin_vel_bar [3]).  For a tool,
+    pos_bar / lin_vel_bar are the derivatives with respect to its position and linear
+    velocity at this substep (its normal, influence and vel_collider all depend on them); a
+    rigid geom's pose is taken as given (zero)."""
+    G = len(vin)
+    vin_bar = np.zeros((G, 3))
+    pos_bar = np.zeros(3)
+    lin_bar = np.zeros(3)
+
+    def resp(vv, tp=None, tl=None):
+        if c.kind == "tool":
+            return R.collide_tool(c, p.eps, p.dt, pos, vv, tool_pos=tp, tool_lin_vel=tl)
+        return R.collide_rigid(c, p.eps, p.dt, pos, vv, mass)[0]
+
+    for k in range(3):
+        vv = vin.astype(np.complex128)
+        vv[:, k] += 1j * h
+        vin_bar[:, k] = (np.imag(resp(vv)) / h * vbar).sum(1)
+    if c.kind == "tool":
+        for k in range(3):
+            tp = np.asarray(c.pos, dtype=np.complex128).copy()
+            tp[k] += 1j * h
+            pos_bar[k] = (np.imag(resp(vin.astype(np.complex128), tp=tp)) / h * vbar).sum()
+            tl = np.asarray(c.lin_vel, dtype=np.complex128).copy()
+            tl[k] += 1j * h
+            lin_bar[k] = (np.imag(resp(vin.astype(np.complex128), tl=tl)) / h * vbar).sum()
+    return vin_bar, pos_bar, lin_bar
 
 
 def backward_materials(p, mats, st, mu, lam, inter, adj):
@@ -491,9 +539,20 @@ def backward_materials(p, mats, st, mu, lam, inter, adj):
         wbar = (vbar * vh).sum(1) + c4 * (vh * Cu).sum(1)
         ubar = (c4 * wt)[:, None] * np.einsum("nji,nj->ni", Cbar, vh)
         xbar += wbar[:, None] * gw - p.inv_dx * ubar
-    # grid op
+    # grid op: the boundary, then the colliders in reverse order
     vg_bar = vh_bar * inter["gmask"]
     act = inter["act"]
+    cbar = np.zeros((inter["n_colliders"], 2, 3))  # per collider: (pos_bar, lin_vel_bar)
+    if inter["chain"]:
+        va_bar = vg_bar[act]
+        gpa = inter["gpos"][act]
+        ma = inter["gm"][act] / 1e3
+        for k, c, vin in reversed(inter["chain"]):
+            va_bar, pb, lb = collider_vjp(p, c, gpa, vin, va_bar, mass=ma)
+            cbar[k, 0] += pb
+            cbar[k, 1] += lb
+        vg_bar = np.zeros_like(vg_bar)
+        vg_bar[act] = va_bar
     pbar = np.zeros((G, 3))
     mbar = np.zeros(G)
     pbar[act] = vg_bar[act] / inter["gm"][act][:, None]
@@ -542,7 +601,10 @@ def backward_materials(p, mats, st, mu, lam, inter, adj):
         Jp_bar[sel], mu_bar[sel], lam_bar[sel], actu_bar[sel] = jb, mb_, lb, ab
     F_bar_n = _mT(np.eye(3) + p.dt * C) @ Ft_bar
     Cbar_n += p.dt * Ft_bar @ _mT(F)
-    return dict(x=xbar, v=vbar_n, C=Cbar_n, F=F_bar_n, Jp=Jp_bar), mu_bar, lam_bar, actu_bar
+    out = dict(x=xbar, v=vbar_n, C=Cbar_n, F=F_bar_n, Jp=Jp_bar)
+    if inter["n_colliders"]:
+        out["colliders"] = cbar
+    return out, mu_bar, lam_bar, actu_bar
 
 
 def rollout_materials(p, mats, st0, mu, lam, n_substeps, target, grad=True, weights=None):
@@ -573,6 +635,50 @@ def rollout_materials(p, mats, st0, mu, lam, n_substeps, target, grad=True, weig
         mu_bar += mb
         lam_bar += lb
     return loss, adj["v"].sum(0), mu_bar, lam_bar, adj
+
+
+def rollout_colliders(p, mats, st0, mu, lam, colliders, lin_vel, weights, grad=True):
+    """loss = sum(weights * x_T) over T = len(lin_vel) substeps of any material mix with
+    kinematic colliders (tool_entity.py:178-191: pos_{t+1} = pos_t + lin_vel_t dt, a tool's
+    origin kept above its floor, rot_{t+1} = exp(ang dt) rot_t), lin_vel [T, n_colliders, 3]
+    the colliders' linear velocity at each substep (what set_velocity gives them), and
+    (grad=True) its gradients with respect to every particle's initial velocity [n, 3], the
+    colliders' initial positions [n_colliders, 3] and lin_vel [T, n_colliders, 3].  Rotations
+    and angular velocities are not differentiated."""
+    import dataclasses
+
+    lin_vel = np.asarray(lin_vel, dtype=np.float64)
+    T = lin_vel.shape[0]
+    cols = list(colliders)
+    states, inters, hist = [st0], [], []
+    st = st0
+    for t in range(T):
+        cols = [dataclasses.replace(c, lin_vel=lin_vel[t, k].copy()) for k, c in enumerate(cols)]
+        hist.append(cols)
+        st, it = forward_materials(p, mats, st, mu, lam, colliders=cols)
+        states.append(st)
+        inters.append(it)
+        cols = R.advance_colliders(p, cols)
+    loss = float((weights * states[-1]["x"]).sum())
+    if not grad:
+        return loss
+    n = st0["x"].shape[0]
+    adj = dict(x=np.asarray(weights, dtype=np.float64).copy(), v=np.zeros((n, 3)), C=np.zeros((n, 3, 3)),
+               F=np.zeros((n, 3, 3)), Jp=np.zeros(n))
+    pos_bar = np.zeros((len(colliders), 3))  # dL/d(collider position after substep t)
+    lin_bar = np.zeros_like(lin_vel)
+    for t in range(T - 1, -1, -1):
+        for k, c in enumerate(hist[t]):
+            pb = pos_bar[k].copy()
+            if c.kind == "tool" and c.pos[2] + c.lin_vel[2] * p.dt < c.floor:
+                pb[2] = 0.0  # clamped to the floor: the new z depends on neither
+            lin_bar[t, k] += p.dt * pb
+            pos_bar[k] = pb
+        adj, _, _, _ = backward_materials(p, mats, states[t], mu, lam, inters[t], adj)
+        cb = adj.pop("colliders")
+        pos_bar += cb[:, 0]
+        lin_bar[t] += cb[:, 1]
+    return loss, adj["v"], pos_bar, lin_bar
 
 
 # ---------------------------------------------------------------- the kernel's formulation

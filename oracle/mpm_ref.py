@@ -409,8 +409,7 @@ class Collider:
     'sphere' (data[0] = radius), 'plane' (data = unit normal, geom frame) or 'box' (data =
     half extents); pose (pos, rot world-from-geom), velocity (lin_vel of pos, ang_vel) and
     the Rigid material's coupling parameters (materials/rigid.py:46-49).  Kind 'tool' is a
-    Tool entity (tool_entity/mesh.py:80-176) with its voxel grid; the C restatement
-    (mpm_ref.c) couples it, this numpy one does not."""
+    Tool entity (tool_entity/mesh.py:80-176) with its voxel grid (collide_tool)."""
 
     kind: str
     pos: np.ndarray
@@ -456,13 +455,85 @@ def sdf_sampled(c: Collider, l, eps):
     return np.where(out, sd_out, sd_in), np.where(out[:, None], g_out, g_in)
 
 
+def _where_pos(x):
+    """max(x, 0) deciding on the real part (complex-step safe)."""
+    return np.where(np.real(x) > 0, x, 0)
+
+
+def tool_sdf_at(vox, pv):
+    """mesh.py:89-104 (Mesh.sdf_): trilinear sample of the voxel grid vox [r, r, r] at voxel
+    coordinates pv [G, 3]; 1 where floor(pv) leaves [0, r - 2].  Complex pv (the complex
+    step of the adjoint oracle) is sampled with the cell and |.| decided on the real part."""
+    r = vox.shape[0]
+    base = np.floor(np.real(pv)).astype(np.int64)
+    out = ((base >= r - 1) | (base < 0)).any(1)
+    b = np.clip(base, 0, r - 2)
+    sd = np.zeros(len(pv), dtype=np.result_type(pv.dtype, vox.dtype))
+    for o in range(8):
+        cell = b + np.array([o >> 2, (o >> 1) & 1, o & 1])
+        d = pv - cell
+        w = np.prod(1 - np.where(np.real(d) >= 0, d, -d), axis=1)
+        sd = sd + w * vox[cell[:, 0], cell[:, 1], cell[:, 2]]
+    return np.where(out, 1.0, sd)
+
+
+def collide_tool(c: Collider, eps, sdt, pos, vel, tool_pos=None, tool_lin_vel=None):
+    """Tool.collide (tool_entity/mesh.py:147-176) for grid nodes at pos [G, 3] with velocity
+    vel [G, 3]: influence min(exp(-sd / max(EPS, softness)), 1), acting where sd <= 0 or the
+    influence is above 0.1; the body point's velocity from the pose one substep later
+    (vel_collider, mesh.py:139-145, the origin kept above the tool solver's floor); the
+    normal from central differences of 1e-2 voxel, normalised in the voxel frame, mapped to
+    the world and normalised again (mesh.py:107-137); friction on the tangential part.
+    tool_pos / tool_lin_vel replace c.pos / c.lin_vel (the adjoint oracle passes complex
+    values for its complex-step derivatives; every branch is decided on real parts)."""
+    tp = np.asarray(c.pos if tool_pos is None else tool_pos)
+    tl = np.asarray(c.lin_vel if tool_lin_vel is None else tool_lin_vel)
+    Rm = np.asarray(c.rot, dtype=np.float64)
+    sc = np.asarray(c.sdf_scale, dtype=np.float64)
+    vox = np.asarray(c.sdf, dtype=np.float64)
+    half = 0.5 * (vox.shape[0] - 1)
+    q = pos - tp[None, :]
+    pv = (q @ Rm) * sc[None, :] + half
+    sd = tool_sdf_at(vox, pv)
+    e = np.exp(-sd / max(eps, c.softness))
+    infl = np.where(np.real(e) < 1, e, 1.0)
+    near = (np.real(sd) <= 0) | (np.real(infl) > 0.1)
+    w = np.asarray(c.ang_vel, dtype=np.float64) * sdt
+    th = float(np.linalg.norm(w))
+    d = np.zeros_like(q)
+    if th > 0:
+        k = np.broadcast_to(w / th, q.shape)
+        kq = np.cross(k, q)
+        d = np.sin(th) * kq + 2 * np.sin(th / 2) ** 2 * np.cross(k, kq)
+    dpos = tl * sdt
+    if np.real(tp[2] + dpos[2]) < c.floor:
+        dpos = np.array([dpos[0], dpos[1], c.floor - tp[2]])
+    vc = (d + dpos[None, :]) / sdt
+    rv = vel - vc
+    cols = []
+    for i in range(3):
+        a, b = pv.copy(), pv.copy()
+        a[:, i] += 1e-2
+        b[:, i] -= 1e-2
+        cols.append((tool_sdf_at(vox, a) - tool_sdf_at(vox, b)) / 2e-2)
+    nv = np.stack(cols, 1)
+    nv = nv / np.sqrt((nv * nv).sum(1) + eps)[:, None]
+    n = (nv / sc[None, :]) @ Rm.T
+    n = n / np.sqrt((n * n).sum(1) + eps)[:, None]
+    rn = (rv * n).sum(1)
+    rt = rv - rn[:, None] * n
+    rtn = np.sqrt((rt * rt).sum(1) + eps)
+    s_ = _where_pos(rtn + rn * c.friction) / rtn
+    nvel = vc + rt * (s_ * infl)[:, None] + rv * (1 - infl)[:, None]
+    hit = near & (np.real(rn) < 0)
+    return np.where(hit[:, None], nvel, vel)
+
+
 def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
     """_func_collide_with_rigid_geom + _func_collide_in_rigid_geom for grid nodes at pos
     (legacy_coupler.py:166-343); sphere and plane SDFs as utils/sdf_decomp.py:91-98, kind
     'sdf' through its sampled grid (sdf_sampled), kind 'box' the exact box distance.  Returns
     (new velocity, force, torque about c.pos)."""
-    if c.kind == "tool":
-        raise NotImplementedError("tool colliders are coupled by the C restatement (cref)")
     dt = vel.dtype.type
     q = pos - np.asarray(c.pos, dtype=dt)
     R = np.asarray(c.rot, dtype=dt)
@@ -495,10 +566,10 @@ def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
     vr = np.asarray(c.lin_vel, dtype=dt)[None, :] + np.cross(np.asarray(c.ang_vel, dtype=dt)[None, :], q)
     rv = vel - vr
     rn = (rv * n).sum(1)
-    hit = (infl > 0.1) & (rn < 0)
+    hit = (infl > 0.1) & (np.real(rn) < 0)
     rt = rv - rn[:, None] * n
     rtn = np.sqrt((rt * rt).sum(1) + dt(eps))
-    sc = np.maximum(dt(0), rtn + rn * dt(c.friction)) / rtn
+    sc = _where_pos(rtn + rn * dt(c.friction)) / rtn
     rnew = rt * sc[:, None] - n * (rn * dt(c.restitution))[:, None]
     nv = vr + rnew * infl[:, None] + rv * (dt(1) - infl)[:, None]
     out_v = np.where(hit[:, None], nv, vel)
@@ -517,7 +588,10 @@ def advance_colliders(p: Params, colliders):
             k = w / th
             K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
             R = (np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K) @ R
-        out.append(dataclasses.replace(c, pos=np.asarray(c.pos) + np.asarray(c.lin_vel) * p.dt, rot=R))
+        pos = np.asarray(c.pos) + np.asarray(c.lin_vel) * p.dt
+        if c.kind == "tool":  # the tool solver's FloorBoundary.impose_pos (tool_entity.py:180-182)
+            pos[2] = max(pos[2], c.floor)
+        out.append(dataclasses.replace(c, pos=pos, rot=R))
     return out
 
 
@@ -534,7 +608,14 @@ def grid_op(p: Params, gm, gp, colliders=None, forces=None):
     v = v + dt(p.dt) * np.asarray(p.gravity, dtype=dt)[None, :]
     idx = np.argwhere(act)
     pos = (idx + p.lower_cell[None, :]).astype(dt) * dt(p.dx)
+    for c in colliders or []:  # MPM <-> Tool first (legacy_coupler.py:381-383)
+        if c.kind == "tool":
+            v = collide_tool(c, p.eps, p.dt, pos, v).astype(dt)
     for c in colliders or []:
+        if c.kind == "tool":
+            if forces is not None:
+                forces.append((np.zeros(3), np.zeros(3)))
+            continue
         v, f, t = collide_rigid(c, p.eps, p.dt, pos, v, (m / dt(1e3)).astype(dt))
         if forces is not None:
             forces.append((f, t))

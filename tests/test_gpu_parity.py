@@ -279,9 +279,9 @@ def test_retune_and_autotune_preserve_the_simulation():
     d = W.mixed_500k(n_side=10)
     a = _rt([d], use_graphs=False)
     b = _rt([d], use_graphs=False)
-    best, times = autotune.tune(b, candidates={"chunk_particles": (128, 256), "sort_interval": (10, 20)},
-                                trial_substeps=20, use_cache=False)
-    assert set(best) == {"chunk_particles", "sort_interval", "grid_ctas"} and len(times) == 4
+    best, times = autotune.tune(b, candidates={"chunk_particles": (128, 256), "sort_interval": (10, 20),
+                                               "grid_ctas_per_sm": (0, 14)}, trial_substeps=20, use_cache=False)
+    assert set(best) == {"chunk_particles", "sort_interval", "grid_ctas"} and len(times) == 8
     assert np.array_equal(_state_np(a)["pos"], _state_np(b)["pos"])  # trials were rolled back
     a.substeps(30)
     b.substeps(30)
