@@ -545,6 +545,9 @@ def run_ours(args, world, rank, local):
             "profile_ms_per_substep": prof_ms / nsub,
             "substep_ms": step_sub_ms,
             "profile_vs_step": (prof_ms / nsub) / step_sub_ms,
+            # the profiled shares applied to the graph-replayed step (the events' own gaps,
+            # ~13% of the profiled run, spread in proportion): these sum to substep_ms
+            "kernel_ms_in_step": {k: round(v[0] * step_sub_ms * nsub / prof_ms, 5) for k, v in kb.items()},
             "substep_alg_GBs": sub_alg / (step_sub_ms * 1e-3) / 1e9,
             "substep_frac": sub_alg / (step_sub_ms * 1e-3) / 1e9 / hbm,
         },

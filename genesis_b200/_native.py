@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 9
+ABI_VERSION = 10
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -195,6 +195,7 @@ SIGNATURES = {
     "mpm_substeps_profile": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp, vp, vp]),
     "mpm_adjoint_workspace_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
     "mpm_substep_adjoint": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp]),
+    "mpm_substep_adjoint_colliders": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp, vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),
     "mpm_status_enqueue": (C.c_int, [_P(Problem), vp, vp, vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),

@@ -148,34 +148,296 @@ __global__ void k_adj_g2p(mpm_problem prob, const mpm_instance* __restrict__ ins
 }
 
 // ---- adjoint of the grid update (legacy_coupler.py:364-375, 495-496)
-__global__ void k_adj_grid(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w, AdjWs aw) {
+// ---- adjoint of the colliders' responses (legacy_coupler.py:297-350, tool_entity/mesh.py:147-176)
+
+// Adjoint of the shared response v' = vc + (rt sc - n rn e) infl + rv (1 - infl) with rv = v - vc,
+// rn = rv.n (acting only where rn < 0), rt = rv - rn n, sc = max(0, |rt|_eps + rn mu) / |rt|_eps
+// (|x|_eps = sqrt(|x|^2 + eps), e the restitution): given ob = dL/dv', returns dL/drv, dL/dn and
+// dL/dinfl (dL/dvc = ob - dL/drv).
+__device__ __forceinline__ void respond_vjp(const float* rv, const float* n, float infl, float mu, float e, float eps,
+                                            const float* ob, float* rvb, float* nb, float& inflb) {
+    const float rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    const float rt[3] = {rv[0] - rn * n[0], rv[1] - rn * n[1], rv[2] - rn * n[2]};
+    const float rtn = sqrtf(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2] + eps);
+    const float m = rtn + rn * mu;
+    const float mp = fmaxf(0.f, m);
+    const float sc = mp / rtn;
+    float rtb[3], scb = 0.f, rnb = 0.f;
+    inflb = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float rnew = rt[i] * sc - n[i] * rn * e;
+        inflb += ob[i] * (rnew - rv[i]);
+        const float rnewb = ob[i] * infl;
+        rvb[i] = ob[i] * (1.f - infl);
+        rtb[i] = rnewb * sc;
+        scb += rnewb * rt[i];
+        rnb -= e * rnewb * n[i];
+        nb[i] = -e * rnewb * rn;
+    }
+    float rtnb = -scb * mp / (rtn * rtn);
+    if (m > 0.f) {
+        const float mb = scb / rtn;
+        rtnb += mb;
+        rnb += mb * mu;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        rtb[i] += rtnb * rt[i] / rtn;
+        rvb[i] += rtb[i];
+    }
+    rnb -= rtb[0] * n[0] + rtb[1] * n[1] + rtb[2] * n[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        nb[i] -= rn * rtb[i];
+        rvb[i] += rnb * n[i];
+        nb[i] += rnb * rv[i];
+    }
+}
+
+// The trilinear voxel sample of tool_sdf_at and its gradient with respect to the voxel
+// coordinate (d(1 - |d|)/dpv = -1 for d >= 0, +1 below); zero gradient outside the grid,
+// where the sample is the constant 1.
+__device__ __forceinline__ float tool_sdf_grad_at(const float* __restrict__ vox, int res, const float* pv, float* g) {
+    g[0] = g[1] = g[2] = 0.f;
+    const float f0 = floorf(pv[0]), f1 = floorf(pv[1]), f2 = floorf(pv[2]);
+    if (!(f0 >= 0.f && f1 >= 0.f && f2 >= 0.f && f0 < (float)(res - 1) && f1 < (float)(res - 1) &&
+          f2 < (float)(res - 1)))
+        return 1.f;
+    const int b0 = (int)f0, b1 = (int)f1, b2 = (int)f2;
+    float sd = 0.f;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+        const float d0 = pv[0] - (float)(b0 + i), d1 = pv[1] - (float)(b1 + j), d2 = pv[2] - (float)(b2 + k);
+        const float a0 = 1.f - fabsf(d0), a1 = 1.f - fabsf(d1), a2 = 1.f - fabsf(d2);
+        const float val = vox[((int64_t)(b0 + i) * res + (b1 + j)) * res + (b2 + k)];
+        sd += a0 * a1 * a2 * val;
+        g[0] += (d0 >= 0.f ? -1.f : 1.f) * a1 * a2 * val;
+        g[1] += (d1 >= 0.f ? -1.f : 1.f) * a0 * a2 * val;
+        g[2] += (d2 >= 0.f ? -1.f : 1.f) * a0 * a1 * val;
+    }
+    return sd;
+}
+
+// Adjoint of collide_tool at grid node p with input velocity v: vb holds dL/d(output velocity)
+// on entry and dL/dv on return; dL/d(tool position) and dL/d(tool linear velocity) are added
+// to pb and lb.  The influence, the normal (central differences of the trilinear sample, so
+// its derivative is the difference of the sample's gradients) and the body point's velocity
+// all depend on the tool's position; the rotation is taken as given.
+__device__ void collide_tool_vjp(const mpm_collider& c, const float* __restrict__ sdf_voxels, float eps, float dt,
+                                 const float* p, const float* v, float* vb, float* pb, float* lb) {
+    if (!sdf_voxels || c.sdf_res < 2) return;
+    const float* vox = sdf_voxels + c.sdf_offset;
+    const int res = c.sdf_res;
+    const float q[3] = {p[0] - c.pos[0], p[1] - c.pos[1], p[2] - c.pos[2]};
+    const float half = 0.5f * (float)(res - 1);
+    float pv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        pv[i] = c.sdf_scale[i] * (c.rot[0 * 3 + i] * q[0] + c.rot[1 * 3 + i] * q[1] + c.rot[2 * 3 + i] * q[2]) + half;
+    float gsd[3];
+    const float sd = tool_sdf_grad_at(vox, res, pv, gsd);
+    const float soft = fmaxf(eps, c.softness);
+    const float ex = expf(-sd / soft);
+    const float infl = fminf(ex, 1.f);
+    if (!(sd <= 0.f || infl > 0.1f)) return;
+    // vel_collider: ((E - I) q + dpos) / dt, (E - I) q = M q with M = sin(th) K + 2 sin^2(th / 2) K^2
+    float M[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    {
+        const float wx = c.ang_vel[0] * dt, wy = c.ang_vel[1] * dt, wz = c.ang_vel[2] * dt;
+        const float th = sqrtf(wx * wx + wy * wy + wz * wz);
+        if (th > 0.f) {
+            const float k[3] = {wx / th, wy / th, wz / th};
+            const float K[9] = {0.f, -k[2], k[1], k[2], 0.f, -k[0], -k[1], k[0], 0.f};
+            const float sh = sinf(0.5f * th), s = sinf(th), t = 2.f * sh * sh;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+                    M[a * 3 + b] = s * K[a * 3 + b] + t * (K[a * 3 + 0] * K[0 * 3 + b] + K[a * 3 + 1] * K[1 * 3 + b] +
+                                                           K[a * 3 + 2] * K[2 * 3 + b]);
+        }
+    }
+    float dz = c.lin_vel[2] * dt;
+    const bool clamped = c.pos[2] + dz < c.floor;
+    if (clamped) dz = c.floor - c.pos[2];
+    float vc[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) vc[i] = (M[i * 3 + 0] * q[0] + M[i * 3 + 1] * q[1] + M[i * 3 + 2] * q[2]) / dt;
+    vc[0] += c.lin_vel[0];
+    vc[1] += c.lin_vel[1];
+    vc[2] += dz / dt;
+    const float rv[3] = {v[0] - vc[0], v[1] - vc[1], v[2] - vc[2]};
+    // the normal and the Jacobian H of its central differences: H_ij = d nv_i / d pv_j
+    float nv[3], H[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float a[3] = {pv[0], pv[1], pv[2]}, b[3] = {pv[0], pv[1], pv[2]};
+        a[i] += 1e-2f;
+        b[i] -= 1e-2f;
+        float ga[3], gb[3];
+        nv[i] = (tool_sdf_grad_at(vox, res, a, ga) - tool_sdf_grad_at(vox, res, b, gb)) / 2e-2f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) H[i * 3 + j] = (ga[j] - gb[j]) / 2e-2f;
+    }
+    const float s1 = rsqrtf(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2] + eps);
+    const float nm[3] = {nv[0] * s1 / c.sdf_scale[0], nv[1] * s1 / c.sdf_scale[1], nv[2] * s1 / c.sdf_scale[2]};
+    float nr[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) nr[i] = c.rot[i * 3 + 0] * nm[0] + c.rot[i * 3 + 1] * nm[1] + c.rot[i * 3 + 2] * nm[2];
+    const float s2 = rsqrtf(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2] + eps);
+    const float n[3] = {nr[0] * s2, nr[1] * s2, nr[2] * s2};
+    const float rn = rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2];
+    if (!(rn < 0.f)) return;
+    const float ob[3] = {vb[0], vb[1], vb[2]};
+    float rvb[3], nb[3], inflb;
+    respond_vjp(rv, n, infl, c.friction, 0.f, eps, ob, rvb, nb, inflb);
+    const float vcb[3] = {ob[0] - rvb[0], ob[1] - rvb[1], ob[2] - rvb[2]};
+    // n = nr s2 -> nr; nr = R nm -> nm; nm = nv s1 / scale -> nv
+    const float dn = nr[0] * nb[0] + nr[1] * nb[1] + nr[2] * nb[2];
+    float nrb[3], nmb[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) nrb[i] = s2 * nb[i] - s2 * s2 * s2 * nr[i] * dn;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        nmb[i] = (c.rot[0 * 3 + i] * nrb[0] + c.rot[1 * 3 + i] * nrb[1] + c.rot[2 * 3 + i] * nrb[2]) / c.sdf_scale[i];
+    const float dv = nv[0] * nmb[0] + nv[1] * nmb[1] + nv[2] * nmb[2];
+    float nvb[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) nvb[i] = s1 * nmb[i] - s1 * s1 * s1 * nv[i] * dv;
+    // pv: the normal's differences and the influence
+    const float sdb = (ex < 1.f) ? -inflb * infl / soft : 0.f;
+    float pvb[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) pvb[j] = H[0 * 3 + j] * nvb[0] + H[1 * 3 + j] * nvb[1] + H[2 * 3 + j] * nvb[2] + sdb * gsd[j];
+    // pv = scale (R^T q) + half, and vc's rotation part M q / dt
+    float qb[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        qb[i] = c.rot[i * 3 + 0] * c.sdf_scale[0] * pvb[0] + c.rot[i * 3 + 1] * c.sdf_scale[1] * pvb[1] +
+                c.rot[i * 3 + 2] * c.sdf_scale[2] * pvb[2] +
+                (M[0 * 3 + i] * vcb[0] + M[1 * 3 + i] * vcb[1] + M[2 * 3 + i] * vcb[2]) / dt;
+    // q = p - pos; vc's translation: lin_vel, or (floor - pos_z) / dt once clamped
+    pb[0] -= qb[0];
+    pb[1] -= qb[1];
+    pb[2] -= qb[2];
+    lb[0] += vcb[0];
+    lb[1] += vcb[1];
+    if (clamped)
+        pb[2] -= vcb[2] / dt;
+    else
+        lb[2] += vcb[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) vb[i] = rvb[i];
+}
+
+// Adjoint of collide_rigid with respect to the node velocity only (the geom's pose and
+// velocity are taken as given): vb holds dL/d(output velocity) on entry, dL/dv on return.
+__device__ void collide_rigid_vjp(const mpm_collider& c, const float* __restrict__ sdf, float eps, const float* p,
+                                  const float* v, float* vb) {
+    float sd, g[3], q[3], n[3];
+    sdf_grad(c, sdf, eps, p, sd, g, q);
+    const float infl = fminf(expf(-sd / fmaxf(1e-10f, c.softness)), 1.f);
+    if (!(infl > 0.1f)) return;
+    unit_normal(c, eps, g, n);
+    const float vr[3] = {c.lin_vel[0] + c.ang_vel[1] * q[2] - c.ang_vel[2] * q[1],
+                         c.lin_vel[1] + c.ang_vel[2] * q[0] - c.ang_vel[0] * q[2],
+                         c.lin_vel[2] + c.ang_vel[0] * q[1] - c.ang_vel[1] * q[0]};
+    const float rv[3] = {v[0] - vr[0], v[1] - vr[1], v[2] - vr[2]};
+    if (!(rv[0] * n[0] + rv[1] * n[1] + rv[2] * n[2] < 0.f)) return;
+    const float ob[3] = {vb[0], vb[1], vb[2]};
+    float nb[3], inflb;
+    respond_vjp(rv, n, infl, c.friction, c.restitution, eps, ob, vb, nb, inflb);
+}
+
+// The grid op's collider chain on one node, stopped before collider `stop` of the given kind
+// (tools first in index order, then the rigid geoms): the velocity that collider receives.
+__device__ void collider_chain(const mpm_collider* __restrict__ cs, int nc, int inst, const float* __restrict__ sdf,
+                               float eps, float dt, const float* p, float* v, bool stop_tool, int stop) {
+    for (int k = 0; k < nc; ++k) {
+        if (cs[k].instance != inst || cs[k].kind != MPM_COLLIDER_TOOL) continue;
+        if (stop_tool && k == stop) return;
+        collide_tool(cs[k], sdf, eps, dt, p, v);
+    }
+    for (int k = 0; k < nc; ++k) {
+        if (cs[k].instance != inst || cs[k].kind == MPM_COLLIDER_TOOL) continue;
+        if (!stop_tool && k == stop) return;
+        collide_rigid(cs[k], sdf, eps, dt, 0.f, p, v, nullptr);
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Adjoint of the grid op per node: the boundary, the colliders' responses in reverse order
+// (tools' position / linear-velocity adjoints summed per warp into cbar[6 k ..]), then
+// v = p / m + dt g.  Every thread runs the collider loops, so the warp sums see full warps.
+__global__ void k_adj_grid(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w, AdjWs aw,
+                           const mpm_collider* __restrict__ cs, int nc, const float* __restrict__ sdf, float* cbar) {
     const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= prob.n_blocks * BLK3) return;
-    const int64_t blk = node / BLK3;
+    const bool in = node < prob.n_blocks * BLK3;
+    const int64_t blk = in ? node / BLK3 : 0;
     const int ln = (int)(node % BLK3);
-    const mpm_instance& I = inst[find_instance_by_block(inst, prob.n_instances, blk)];
-    const float4 mm = aw.saved_mm[node];
+    const int ii = in ? find_instance_by_block(inst, prob.n_instances, blk) : 0;
+    const mpm_instance& I = inst[ii];
+    const float4 mm = in ? aw.saved_mm[node] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool act = in && mm.w > I.eps;
     float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (mm.w > I.eps) {
+    float p[3] = {0.f, 0.f, 0.f}, vin[3] = {0.f, 0.f, 0.f}, vb[3] = {0.f, 0.f, 0.f}, pm[3] = {mm.x, mm.y, mm.z};
+    const float inv = act ? 1.f / mm.w : 0.f;
+    if (act) {
         const BlockCoord bc = block_coord((int)(blk - I.blk_base), I);
         const int lxyz[3] = {ln / (BLK * BLK), (ln / BLK) % BLK, ln % BLK};
         const int bxyz[3] = {bc.bx, bc.by, bc.bz};
-        const float inv = 1.f / mm.w;
-        const float pm[3] = {mm.x, mm.y, mm.z};
-        const float4 vb4 = aw.vbar[node];
-        const float vbin[3] = {vb4.x, vb4.y, vb4.z};
-        float vb[3], dotp = 0.f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const float v = inv * pm[d] + I.dt * I.gravity[d];
-            const float pos = (float)(bxyz[d] * BLK + lxyz[d] + I.lower_cell[d]) * I.dx;
-            const bool zero = (pos >= I.bnd_hi[d] && v >= 0.f) || (pos <= I.bnd_lo[d] && v <= 0.f);
-            vb[d] = zero ? 0.f : vbin[d];
-            dotp += vb[d] * pm[d];
+            vin[d] = inv * pm[d] + I.dt * I.gravity[d];
+            p[d] = (float)(bxyz[d] * BLK + lxyz[d] + I.lower_cell[d]) * I.dx;
         }
+        float v[3] = {vin[0], vin[1], vin[2]};
+        if (nc > 0) collider_chain(cs, nc, ii, sdf, I.eps, I.dt, p, v, false, nc);
+        const float4 vb4 = aw.vbar[node];
+        const float vbin[3] = {vb4.x, vb4.y, vb4.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const bool zero = (p[d] >= I.bnd_hi[d] && v[d] >= 0.f) || (p[d] <= I.bnd_lo[d] && v[d] <= 0.f);
+            vb[d] = zero ? 0.f : vbin[d];
+        }
+    }
+    // the colliders in reverse order: the rigid geoms, then the tools
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool tools = pass == 1;
+        for (int k = nc - 1; k >= 0; --k) {
+            const bool is_tool = cs[k].kind == MPM_COLLIDER_TOOL;
+            if (is_tool != tools) continue;
+            float pb[3] = {0.f, 0.f, 0.f}, lb[3] = {0.f, 0.f, 0.f};
+            if (act && cs[k].instance == ii) {
+                float vk[3] = {vin[0], vin[1], vin[2]};
+                collider_chain(cs, nc, ii, sdf, I.eps, I.dt, p, vk, tools, k);
+                if (tools)
+                    collide_tool_vjp(cs[k], sdf, I.eps, I.dt, p, vk, vb, pb, lb);
+                else
+                    collide_rigid_vjp(cs[k], sdf, I.eps, p, vk, vb);
+            }
+            if (tools && cbar) {
+                float r[6] = {pb[0], pb[1], pb[2], lb[0], lb[1], lb[2]};
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    r[j] = warp_sum(r[j]);
+                    if ((threadIdx.x & 31) == 0 && r[j] != 0.f) atomicAdd(&cbar[6 * k + j], r[j]);
+                }
+            }
+        }
+    }
+    if (act) {
+        const float dotp = vb[0] * pm[0] + vb[1] * pm[1] + vb[2] * pm[2];
         out = make_float4(vb[0] * inv, vb[1] * inv, vb[2] * inv, -dotp * inv * inv);
     }
-    aw.pmbar[node] = out;
+    if (in) aw.pmbar[node] = out;
 }
 
 // cofactor matrix of F (= det(F) F^-T)
@@ -691,6 +953,7 @@ __global__ void k_adj_p2g(mpm_problem prob, const mpm_instance* __restrict__ ins
         fo[k * st + s] = Fbn[k];
     }
     jo[s] = Jpb;
-    lame_bar[s] += mub;
+    // inviscid Liquid never reads its mu (liquid.py:47-48): no gradient flows to it
+    lame_bar[s] += (m.kind == MPM_MAT_LIQUID && m.mu == 0.f) ? 0.f : mub;
     lame_bar[st + s] += lamb;
 }

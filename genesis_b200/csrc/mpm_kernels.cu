@@ -1959,7 +1959,9 @@ static int launch_p2g(const mpm_problem* prob, const mpm_tables* tab, mpm_partic
     return cuda_ok();
 }
 
-static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* ws, cudaStream_t s) {
+// advance = false (the adjoint's recompute): the colliders keep their pose and accumulate no force
+static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* ws, cudaStream_t s,
+                          bool advance = true) {
     const DevInfo* d = dev_info();
     if (!d) return MPM_E_CUDA;
     int ctas = prob->grid_ctas > 0 ? prob->grid_ctas : d->sms * d->occ_grid;
@@ -1967,9 +1969,9 @@ static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* 
     if (ctas > need) ctas = (int)need;
     if (tab->n_colliders < 0) return MPM_E_INVALID;
     const int nc = tab->colliders ? tab->n_colliders : 0;
-    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc, tab->collider_force,
-                                    tab->sdf_voxels);
-    if (nc > 0)
+    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc,
+                                    advance ? tab->collider_force : nullptr, tab->sdf_voxels);
+    if (nc > 0 && advance)
         k_advance_colliders<<<(nc + 63) / 64, 64, 0, s>>>(tab->instances, prob->n_instances, tab->colliders, nc);
     return cuda_ok();
 }
@@ -2437,14 +2439,17 @@ int mpm_adjoint_workspace_bytes(const mpm_problem* prob, uint64_t* out) {
     return MPM_OK;
 }
 
-int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state, float* adj,
-                        float* lame_bar, void* workspace, void* adj_workspace, void* stream) {
+int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state,
+                                  float* adj, float* lame_bar, float* collider_bar, void* workspace,
+                                  void* adj_workspace, void* stream) {
     int rc = check_problem(prob);
     if (rc) return rc;
     if ((rc = check_par(prob, state))) return rc;
     if (!tab || !tab->instances || !tab->materials || !adj || !lame_bar || !workspace || !adj_workspace)
         return MPM_E_INVALID;
-    if (tab->colliders && tab->n_colliders > 0) return MPM_E_INVALID;  // the adjoint has no rigid coupling
+    const int nc = (tab->colliders && tab->n_colliders > 0) ? tab->n_colliders : 0;
+    if (tab->n_colliders < 0) return MPM_E_INVALID;
+    if (nc > 0 && (prob->flags & MPM_PROBF_CPIC)) return MPM_E_INVALID;  // no adjoint of the particle-level coupling
     cudaStream_t s = (cudaStream_t)stream;
     const int n = prob->n_particles;
     AdjWs aw = adj_ws_of(*prob, adj_workspace);
@@ -2459,14 +2464,20 @@ int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mp
     if ((rc = launch_p2g(prob, tab, &sp, workspace, s))) return rc;
     const size_t nodes = (size_t)prob->n_blocks * BLK3;
     if (cudaMemcpyAsync(aw.saved_mm, w.mm, nodes * 16, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return MPM_E_CUDA;
-    if ((rc = launch_grid_op(prob, tab, workspace, s))) return rc;
+    if ((rc = launch_grid_op(prob, tab, workspace, s, false))) return rc;
     if (cudaMemsetAsync(aw.vbar, 0, nodes * 16, s) != cudaSuccess) return MPM_E_CUDA;
     if (n > 0) {
         k_adj_g2p<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, *state, adj, w, aw);
-        k_adj_grid<<<(int)((nodes + 255) / 256), 256, 0, s>>>(*prob, tab->instances, w, aw);
+        k_adj_grid<<<(int)((nodes + 255) / 256), 256, 0, s>>>(*prob, tab->instances, w, aw, tab->colliders, nc,
+                                                               tab->sdf_voxels, collider_bar);
         k_adj_p2g<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, tab->materials, *state, adj, lame_bar, aw);
     }
     return cuda_ok();
+}
+
+int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state, float* adj,
+                        float* lame_bar, void* workspace, void* adj_workspace, void* stream) {
+    return mpm_substep_adjoint_colliders(prob, tab, state, adj, lame_bar, nullptr, workspace, adj_workspace, stream);
 }
 
 int mpm_status(const mpm_problem* prob, void* workspace, int32_t clear, uint32_t* out, void* stream) {

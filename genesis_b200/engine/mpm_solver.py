@@ -146,9 +146,9 @@ class MPMSolver:
             from ..materials import MPM
 
             bad = [type(m).__name__ for m in self.unique_materials if not isinstance(m, MPM.Base)]
-            if bad or rigid or tools:
-                raise GenesisException("A differentiable scene supports MPM entities only "
-                                       f"(got {', '.join(bad) or 'rigid or tool colliders'}).")
+            if bad:
+                raise GenesisException("A differentiable scene supports MPM entities, tools and rigid colliders "
+                                       f"only (got {', '.join(bad)}).")
         self.runtime = MPMRuntime(
             specs,
             device=self._sim.device,

@@ -168,18 +168,44 @@ class ToolEntity:
     def faces(self):
         return self._faces
 
+    def _tape(self):
+        solver = getattr(self._scene._sim, "mpm_solver", None)
+        return getattr(solver, "tape", None)
+
     def set_position(self, pos):
+        if self._tape() is not None:  # a differentiable scene: an input of the next step
+            self._tape().record_input(self, "tool_pos", pos, None)
+            return
         self._set_cols(_POS, pos)
+
+    def _apply_input(self, kind, value):
+        self._set_cols({"tool_pos": _POS, "tool_vel": _LIN, "tool_ang": _ANG}[kind], value)
+
+    def _input_grad(self, shape, g):
+        """dL/d(value) of a set_position / set_velocity input from dL/d(the rows it wrote) g
+        [n_envs, 3] (a value given once for every environment gets their sum)."""
+        with torch.enable_grad():
+            a = torch.zeros(shape, dtype=torch.float32, device=g.device, requires_grad=True)
+            out = a.reshape(-1, 3).expand(g.shape[0], 3)
+            (ga,) = torch.autograd.grad(out, a, grad_outputs=g)
+        return ga
 
     def set_quaternion(self, quat):
         q = np.asarray(torch.as_tensor(quat).detach().cpu(), dtype=np.float64).reshape(-1, 4)
         self._set_cols(_ROT, np.stack([quat_to_R(qq).reshape(9) for qq in q]))
 
     def set_velocity(self, vel=None, ang=None):
+        tape = self._tape()
         if vel is not None:
-            self._set_cols(_LIN, vel)
+            if tape is not None:
+                tape.record_input(self, "tool_vel", vel, None)
+            else:
+                self._set_cols(_LIN, vel)
         if ang is not None:
-            self._set_cols(_ANG, ang)
+            if tape is not None:
+                tape.record_input(self, "tool_ang", ang, None)
+            else:
+                self._set_cols(_ANG, ang)
 
     def set_state(self, f, state):
         """Pose and velocities of every environment from a ToolEntityState (tool_entity.py:291-293)."""

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 9
+#define MPM_ABI_VERSION 10
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -332,7 +332,13 @@ int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, ui
  * corotated / neo-Hookean, Muscle, ElastoPlastic von Mises / clamp, Liquid, Sand, Snow;
  * replaces the gstaichi autodiff of substep_post_coupling_grad / couple_grad /
  * substep_pre_coupling_grad, mpm_solver.py:485-517, legacy_coupler.py:996-1017, and its SVD
- * adjoint backward_svd, :1112-1129).  No colliders (MPM_E_INVALID).
+ * adjoint backward_svd, :1112-1129).  The grid op's colliders are differentiated as the
+ * table holds them for this substep (their pose at its start): the tools' responses
+ * (tool_entity/mesh.py:147-176) with respect to the node velocity and the tool's position and
+ * linear velocity, the rigid geoms' (legacy_coupler.py:297-341) with respect to the node
+ * velocity, their pose taken as given; the particle-level coupling (MPM_PROBF_CPIC) with
+ * colliders is not differentiated (MPM_E_INVALID).  The colliders are neither moved nor
+ * given forces by the call.
  * `state` is the particle state at the START of the substep (unchanged by the call; the
  * particles must still be in the slot order the last mpm_sort_particles produced).
  * `adj` (float[25][state_stride], same planar layout as the state) holds on entry the
@@ -343,6 +349,14 @@ int mpm_noalloc_status(const mpm_problem* prob, int32_t clear, uint32_t* out, ui
 int mpm_adjoint_workspace_bytes(const mpm_problem* prob, uint64_t* out);
 int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state, float* adj,
                         float* lame_bar, void* workspace, void* adj_workspace, void* stream);
+/* mpm_substep_adjoint that also accumulates, into collider_bar (device float[n_colliders][6],
+ * zeroed by the caller; may be NULL), dL/d(position) and dL/d(linear velocity) of every tool
+ * collider at this substep through this substep's grid op (rows of rigid geoms stay zero).  The
+ * chain between substeps (pos' = pos + lin_vel dt, the tool's origin kept above its floor:
+ * tool_entity.py:178-191) is the caller's. */
+int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state,
+                                  float* adj, float* lame_bar, float* collider_bar, void* workspace,
+                                  void* adj_workspace, void* stream);
 
 /* ---- timing ----------------------------------------------------------------
  * mpm_substeps with a CUDA event recorded on `stream` after every launch group: on return

@@ -533,8 +533,9 @@ def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
     """_func_collide_with_rigid_geom + _func_collide_in_rigid_geom for grid nodes at pos
     (legacy_coupler.py:166-343); sphere and plane SDFs as utils/sdf_decomp.py:91-98, kind
     'sdf' through its sampled grid (sdf_sampled), kind 'box' the exact box distance.  Returns
-    (new velocity, force, torque about c.pos)."""
-    dt = vel.dtype.type
+    (new velocity, force, torque about c.pos).  A complex vel (the adjoint oracle's complex
+    step) leaves the geometry real."""
+    dt = np.float64 if np.iscomplexobj(vel) else vel.dtype.type
     q = pos - np.asarray(c.pos, dtype=dt)
     R = np.asarray(c.rot, dtype=dt)
     data = np.asarray(c.data, dtype=dt)
@@ -564,6 +565,7 @@ def collide_rigid(c: Collider, eps, sdt, pos, vel, mass):
         infl = np.minimum(np.exp(-sd / max(1e-10, c.softness)), dt(1)).astype(dt)
     n = g / np.sqrt((g * g).sum(1) + dt(eps))[:, None]
     vr = np.asarray(c.lin_vel, dtype=dt)[None, :] + np.cross(np.asarray(c.ang_vel, dtype=dt)[None, :], q)
+    dt = vel.dtype.type  # the response in vel's type
     rv = vel - vr
     rn = (rv * n).sum(1)
     hit = (infl > 0.1) & (np.real(rn) < 0)

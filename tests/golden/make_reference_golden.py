@@ -22,8 +22,9 @@ runs are float64 (the reference's ``precision="64"``).  Written here:
   ref_cube.npz         an Elastic cube (E 1e5, nu 0.3, rho 1000: the 32,768-particle benchmark
                        cube's material) of 216 jittered lattice particles thrown at the floor of
                        a 64-per-metre grid, dt 1e-4: state after 1, 20 and 60 substeps.
-  ref_mixed_m32.npz,   the same two scenes with the reference's precision-32 model in float64
-  ref_cube_m32.npz     arithmetic: gs.EPS = float32 epsilon (genesis/__init__.py:205-206, the
+  ref_functions_m32.npz, ref_mixed_m32.npz, ref_cube_m32.npz
+                       the same with the reference's precision-32 model in float64
+                       arithmetic: gs.EPS = float32 epsilon (genesis/__init__.py:205-206, the
                        grid-mass threshold and the eps of Matrix.norm in the plastic return
                        mappings), everything else float64.  A float32 run of the reference
                        computes this model; the float32 CUDA path is held to it.
@@ -238,12 +239,12 @@ def cube_fixture(ref, seed=22):
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GENESIS_REFERENCE", "/root/reference")
     ref = T.Reference(root, precision="64")
-    meta, out = functions_fixture(ref)
-    np.savez_compressed(os.path.join(HERE, "ref_functions.npz"), meta=np.array(json.dumps(meta)), **out)
-    print("ref_functions")
     eps64 = ref.gs.EPS
     for suffix, eps in (("", eps64), ("_m32", float(np.finfo(np.float32).eps))):
         ref.gs.EPS = eps
+        meta, out = functions_fixture(ref)
+        np.savez_compressed(os.path.join(HERE, f"ref_functions{suffix}.npz"), meta=np.array(json.dumps(meta)), **out)
+        print(f"ref_functions{suffix}")
         for fn in (mixed_fixture, cube_fixture):
             meta, inputs, rec = fn(ref)
             meta["eps"] = eps

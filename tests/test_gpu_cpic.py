@@ -1,7 +1,8 @@
 """CPIC against rigid colliders (mpm_solver.py:357-379, 412-427; legacy_coupler.py:498-525) on
 the GPU through gs.Scene: a block falling onto a fixed slab far thinner than a grid cell
 matches the float64 oracle, stays on its side of the slab (it leaks through without CPIC), and
-every particle remembers the side it came from."""
+every particle remembers the side it came from.  The slab is the exact box
+(B200Options(exact_box_sdf=True)), the oracle's kind 'box'."""
 
 import numpy as np
 import pytest
@@ -20,6 +21,10 @@ def _scene(cpic, substeps=10, z0=0.33):
         sim_options=gs.options.SimOptions(dt=1e-4 * substeps, substeps=substeps, gravity=(0, 0, -9.8)),
         mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1), grid_density=64,
                                           particle_size=0.01, enable_CPIC=cpic),
+        # the exact box: a 2 mm slab is below the resolution of the reference's sampled grid
+        # (sdf_cell_size 5 mm), whose blended gradients near the slab's faces would stand in
+        # for the side each particle remembers
+        b200_options=gs.options.B200Options(exact_box_sdf=True),
     )
     block = scene.add_entity(gs.morphs.Box(lower=(0.45, 0.45, z0), upper=(0.55, 0.55, z0 + 0.1)),
                              material=gs.materials.MPM.Elastic(E=2e4))

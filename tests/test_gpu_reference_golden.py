@@ -3,9 +3,9 @@
 legacy_coupler.py, boundaries.py and materials/MPM/*.py executed unchanged on a numpy
 stand-in for gstaichi, float64).
 
-* every material variant's return mapping (F_new, Jp_new) and stress, read back after one
-  p2g from particles whose stencils do not overlap (so each grid node's momentum is one
-  particle's stress contribution);
+* every material variant's return mapping (F_new, Jp_new) and stress (the precision-32
+  model's fixture, ref_functions_m32), read back after one p2g from particles whose stencils
+  do not overlap (so each grid node's momentum is one particle's stress contribution);
 * whole substeps over 9 material variants (random F, C, Jp, velocity; inactive particles;
   muscle actuation) and a cube thrown at the floor: grid mass/momentum after the first p2g
   and the full state after each snapshot.
@@ -15,8 +15,10 @@ precision-32 model computed in float64 (float32 gs.EPS, "_m32").  The float32 CU
 held to the precision-32 model; its distance from the precision-64 run is printed (-s).
 
 Tolerances (float32 kernels against the float64 fixtures): positions 1e-5 of the 1 m domain
-after every snapshot; F and Jp 1e-5; velocities no more than 4x the float32 C restatement's
-own deviation from the same fixture, plus 1e-6 m/s (velocities reach 1.7 m/s with |C| up to
+after every snapshot; F and Jp 1e-5, or 4x the float32 C restatement's own deviation from the
+same fixture plus 1e-6 where that is larger (after 20 substeps of the random mixed scene's
+plastic flow, float32 itself deviates by ~5e-6 in F and Jp); velocities no more than 4x the
+float32 C restatement's own deviation, plus 1e-6 m/s (velocities reach 1.7 m/s with |C| up to
 70 /s in the random mixed scene, where float32 itself deviates by ~1e-5 m/s); grid mass and
 momentum totals 1e-6 relative, per node 1e-5 of the largest node; F_new 2e-6 and Jp_new 2e-6
 relative to the largest entry of each variant; stress (through the momentum it scatters) 1e-5
@@ -53,7 +55,7 @@ def _weights(fx):
 def test_material_functions_and_stress_match_reference():
     from genesis_b200.engine.runtime import runtime_from_descs
 
-    z = np.load(os.path.join(HERE, "ref_functions.npz"))
+    z = np.load(os.path.join(HERE, "ref_functions_m32.npz"))  # the precision-32 model, as the kernels
     meta = json.loads(str(z["meta"]))
     variants = meta["variants"]
     nv, n = len(variants), len(z["m0_F_tmp"])
@@ -194,11 +196,15 @@ def test_substeps_match_reference(name):
         eJ = np.abs(got["Jp"] - z[f"Jp_{n}"]).max()
         o32 = _f32_oracle(z, meta, n)
         e32v = np.abs(o32["v"] - z[f"v_{n}"]).max()
+        e32F = np.abs(o32["F"] - z[f"F_{n}"]).max()
+        e32J = np.abs(o32["Jp"] - z[f"Jp_{n}"]).max()
         ex64 = np.abs(got["pos"] - z64[f"x_{n}"]).max()
         ev64 = np.abs(got["vel"] - z64[f"v_{n}"]).max()
         print(f"\n[reference] {name} after {n}: precision-32 model |dx| {ex:.2e} |dv| {ev:.2e} (float32 C "
-              f"restatement {e32v:.2e}) |dF| {eF:.2e} |dJp| {eJ:.2e}; precision 64 |dx| {ex64:.2e} |dv| {ev64:.2e}")
-        assert ex < 1e-5 and eF < 1e-5 and eJ < 1e-5, (n, ex, eF, eJ)
+              f"restatement {e32v:.2e}) |dF| {eF:.2e} ({e32F:.2e}) |dJp| {eJ:.2e} ({e32J:.2e}); precision 64 "
+              f"|dx| {ex64:.2e} |dv| {ev64:.2e}")
+        assert ex < 1e-5, (n, ex)
+        assert eF <= max(1e-5, 4 * e32F + 1e-6) and eJ <= max(1e-5, 4 * e32J + 1e-6), (n, eF, e32F, eJ, e32J)
         assert ev <= 4 * e32v + 1e-6, (n, ev, e32v)
         assert np.array_equal(got["pos"][~act], z["pos"][~act].astype(np.float32).astype(np.float64))
     assert rt.status() == 0

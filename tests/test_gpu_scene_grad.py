@@ -126,13 +126,19 @@ def test_differentiable_scene_limits():
     scene.step()
     with pytest.raises(gs.GenesisException):
         ent.set_position(torch.zeros(3, device="cuda"))
-    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
-    s2 = gs.Scene(sim_options=gs.options.SimOptions(dt=DT, substeps=SUB, requires_grad=True),
-                  mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1)))
-    s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.3), size=(0.1, 0.1, 0.1)), material=gs.materials.MPM.Sand())
-    s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.1), size=(0.3, 0.3, 0.05)), material=gs.materials.Rigid())
-    with pytest.raises(gs.GenesisException):  # no adjoint through rigid colliders
-        s2.build()
+    for cpic in (False, True):
+        gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+        s2 = gs.Scene(sim_options=gs.options.SimOptions(dt=DT, substeps=SUB, requires_grad=True),
+                      mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(1, 1, 1),
+                                                        enable_CPIC=cpic))
+        s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.3), size=(0.1, 0.1, 0.1)), material=gs.materials.MPM.Sand())
+        s2.add_entity(gs.morphs.Box(pos=(0.5, 0.5, 0.1), size=(0.3, 0.3, 0.05)), material=gs.materials.Rigid())
+        if cpic:
+            with pytest.raises(gs.GenesisException):  # no adjoint of the particle-level coupling
+                s2.build()
+        else:  # a rigid collider is differentiated with respect to the node velocities
+            s2.build()
+            s2.step()
 
 
 def test_gradients_with_environments():

@@ -1,7 +1,7 @@
 """Tool entities on the GPU (tool_entity/mesh.py:80-176, legacy_coupler.py:346-350): the
 voxel signed-distance grid of mpm_sdf_voxelize against the float64 oracle, an MPM block
 pushed by a moving, spinning tool against the C restatement, the tool's kinematics and its
-floor, and the refusal of tools in differentiable scenes."""
+floor, and tools in differentiable scenes."""
 
 import os
 
@@ -130,15 +130,19 @@ def test_tool_floor_height_from_options(tmp_path):
     assert np.isclose(tool.get_state().pos.cpu().numpy()[0, 2], 0.15)
 
 
-def test_differentiable_scene_rejects_tools(tmp_path):
+def test_differentiable_scene_takes_tools(tmp_path):
+    """A differentiable scene with a tool builds and steps; the tool's inputs become step inputs
+    (their gradients are checked in tests/test_gpu_tool_grad.py)."""
     gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
     scene = gs.Scene(sim_options=gs.options.SimOptions(dt=1e-3, substeps=10, requires_grad=True))
     scene.add_entity(gs.morphs.Box(lower=(0.4, 0.4, 0.4), upper=(0.5, 0.5, 0.5)), material=gs.materials.MPM.Elastic())
     v, f = mesh.cylinder_mesh()
     path = _write_obj(os.path.join(tmp_path, "t.obj"), v, f)
-    scene.add_entity(gs.morphs.Mesh(file=path, scale=0.1, pos=(0.5, 0.5, 0.2)), material=gs.materials.Tool())
-    with pytest.raises(gs.GenesisException):
-        scene.build()
+    tool = scene.add_entity(gs.morphs.Mesh(file=path, scale=0.1, pos=(0.5, 0.5, 0.2)), material=gs.materials.Tool())
+    scene.build()
+    tool.set_velocity(vel=(0.0, 0.0, 0.5))
+    scene.step()
+    assert np.allclose(tool.get_state().pos.cpu().numpy()[0], [0.5, 0.5, 0.2 + 0.5e-3], atol=1e-6)
 
 
 def test_scene_state_holds_tools_and_reset_restores_them(tmp_path):

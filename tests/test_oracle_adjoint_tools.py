@@ -127,3 +127,31 @@ def test_tool_rollout_gradient_matches_central_differences(case):
     noise = 8 * np.finfo(np.float64).eps * abs(loss) / h  # the differences' round-off
     for name, c, got, fd in checks:
         assert abs(got - fd) <= 1e-5 * max(abs(fd), 1e-3 * scale) + noise, (name, c, got, fd)
+
+
+def test_rigid_response_adjoint_matches_central_differences():
+    """collider_vjp of a tilted, moving, spinning box with restitution (legacy_coupler.py:297-341;
+    its pose taken as given) against central differences of collide_rigid in the node velocity."""
+    rng = np.random.default_rng(7)
+    p = R.Params(grid_density=64, particle_size=0.01, dt=1e-3, dtype=np.float64)
+    th = 0.4
+    rot = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+    c = R.Collider("box", np.array([0.5, 0.5, 0.5]), rot, np.array([0.05, 0.03, 0.04]), np.array([0.2, 0.0, -0.1]),
+                   np.array([0.0, 0.0, 1.0]), friction=0.3, softness=0.01, restitution=0.4)
+    nodes = c.pos + rng.uniform(-0.07, 0.07, size=(300, 3))
+    v = rng.normal(size=(300, 3))
+    vbar = rng.normal(size=(300, 3))
+    mass = np.full(300, 1e-3)
+    got, pb, lb = A.collider_vjp(p, c, nodes, v, vbar, mass=mass)
+    assert np.all(pb == 0) and np.all(lb == 0)
+    h = 1e-7
+    fd = np.zeros_like(v)
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = h
+        up = R.collide_rigid(c, p.eps, p.dt, nodes, v + e, mass)[0]
+        dn = R.collide_rigid(c, p.eps, p.dt, nodes, v - e, mass)[0]
+        fd[:, k] = ((up - dn) / (2 * h) * vbar).sum(1)
+    hit = np.abs(got - vbar).max(1) > 1e-12  # nodes the response acted on
+    assert hit.sum() > 20
+    assert np.abs(got - fd).max() <= 1e-6 * np.abs(fd).max()

@@ -18,8 +18,8 @@ from oracle import mpm_ref as R
 HERE = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def _fx():
-    z = np.load(os.path.join(HERE, "ref_functions.npz"))
+def _fx(suffix=""):
+    z = np.load(os.path.join(HERE, f"ref_functions{suffix}.npz"))
     return z, json.loads(str(z["meta"]))
 
 
@@ -27,12 +27,14 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / max(1.0, np.abs(b).max()))
 
 
+@pytest.mark.parametrize("suffix", ["", "_m32"])
 @pytest.mark.parametrize("vi", range(9))
-def test_material_functions_match_reference(vi):
+def test_material_functions_match_reference(vi, suffix):
     """update_F_S_Jp and update_stress of oracle/mpm_ref.py against the reference's own methods
     (elastic.py, elasto_plastic.py, liquid.py, sand.py, snow.py, muscle.py) on F_tmp with
-    singular values 0.3-1.6, some nearly repeated."""
-    z, meta = _fx()
+    singular values 0.3-1.6, some nearly repeated; at float64 gs.EPS and at the precision-32
+    model's float32 gs.EPS (_m32)."""
+    z, meta = _fx(suffix)
     kind, kw = meta["variants"][vi]
     m = R.make_material(kind, **dict(kw))
     F = z[f"m{vi}_F_tmp"]
