@@ -684,6 +684,8 @@ def run_served(args, world, rank, capacity):
     t0 = time.perf_counter()
     res_sat = srv_sat.serve(reqs, realtime=False)
     wall_sat = reduce_max(world, time.perf_counter() - t0)
+    sat_stats = {"ticks": srv_sat.ticks, "repacks": srv_sat.repacks, "repack_host_s": srv_sat.repack_s,
+                 "substeps_per_tick": srv_sat.substeps_run / max(1, srv_sat.ticks)}
     del srv_sat
     seq_rate = my_work / sum(durs)
     return {
@@ -697,6 +699,7 @@ def run_served(args, world, rank, capacity):
         "errors": errors,
         "ticks": srv.ticks,
         "repacks": srv.repacks,
+        "repack_host_s": srv.repack_s,
         "sequential_value": seq_rate,
         "sequential_p50_latency_s": serve.percentile(seq_lat, 50),
         "sequential_p99_latency_s": serve.percentile(seq_lat, 99),
@@ -710,6 +713,7 @@ def run_served(args, world, rank, capacity):
             "errors": sum(1 for r in res_sat if r.error is not None),
             "speedup_vs_sequential": (total_work / wall_sat) / (seq_rate * world),
             "offered": "all requests queued at t = 0",
+            **sat_stats,
         },
     }
 

@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from . import _globals
-from . import materials, morphs, options, surfaces, textures
+from . import force_fields, materials, morphs, options, surfaces, textures
 from .engine.emitter import Emitter
 from .engine.scene import Scene
 from .exceptions import GenesisException

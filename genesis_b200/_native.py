@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 10
+ABI_VERSION = 11
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -141,7 +141,37 @@ class Tables(C.Structure):
         ("pad0", C.c_int32),
         ("collider_force", C.c_void_p),
         ("sdf_voxels", C.c_void_p),
+        ("force_fields", C.c_void_p),
+        ("n_force_fields", C.c_int32),
+        ("pad1", C.c_int32),
+        ("ff_perm", C.c_void_p),
     ]
+
+
+class ForceField(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("active", C.c_int32),
+        ("vec", C.c_float * 3),
+        ("dir", C.c_float * 3),
+        ("center", C.c_float * 3),
+        ("strength", C.c_float),
+        ("strength2", C.c_float),
+        ("radius", C.c_float),
+        ("falloff_pow", C.c_float),
+        ("falloff_min", C.c_float),
+        ("falloff_max", C.c_float),
+        ("flow", C.c_float),
+        ("damping", C.c_float),
+        ("linear", C.c_float),
+        ("quadratic", C.c_float),
+        ("frequency", C.c_float),
+        ("perm_offset", C.c_int32),
+        ("seed", C.c_uint32),
+    ]
+
+
+FF_CONSTANT, FF_WIND, FF_POINT, FF_DRAG, FF_NOISE, FF_VORTEX, FF_TURBULENCE = range(7)
 
 
 COLLIDER_SPHERE, COLLIDER_PLANE, COLLIDER_BOX, COLLIDER_TOOL, COLLIDER_SDF = 0, 1, 2, 3, 4
@@ -237,10 +267,10 @@ def load(path: str | None = None):
             fn.argtypes = args
         if lib.mpm_abi_version() != ABI_VERSION:
             raise NativeLibraryError("ABI version mismatch between genesis_b200 and " + LIB_NAME)
-        sizes = (C.c_int32 * 6)()
+        sizes = (C.c_int32 * 7)()
         lib.mpm_struct_sizes(sizes)
         mine = (C.sizeof(Instance), C.sizeof(Material), C.sizeof(Problem), C.sizeof(Particles), C.sizeof(Tables),
-                C.sizeof(Collider))
+                C.sizeof(Collider), C.sizeof(ForceField))
         if tuple(sizes) != mine:
             raise NativeLibraryError(f"struct layout mismatch: library {tuple(sizes)} vs binding {mine}")
         _lib = lib

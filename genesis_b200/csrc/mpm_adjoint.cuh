@@ -55,10 +55,6 @@ static inline AdjWs adj_ws_of(const mpm_problem& p, void* base) {
     return a;
 }
 
-__device__ __forceinline__ float& w_vbar_x(const AdjWs& a, int64_t n) { return a.vbar[n].x; }
-__device__ __forceinline__ float& w_vbar_y(const AdjWs& a, int64_t n) { return a.vbar[n].y; }
-__device__ __forceinline__ float& w_vbar_z(const AdjWs& a, int64_t n) { return a.vbar[n].z; }
-
 __device__ __forceinline__ void bspline_d(float fx, float* w, float* dw) {
     const float a = 1.5f - fx, b = fx - 1.f, c = fx - 0.5f;
     w[0] = 0.5f * a * a;
@@ -132,9 +128,9 @@ __global__ void k_adj_g2p(mpm_problem prob, const mpm_instance* __restrict__ ins
                 float Cu[3];
 #pragma unroll
                 for (int a = 0; a < 3; ++a) Cu[a] = Cb[a * 3 + 0] * u[0] + Cb[a * 3 + 1] * u[1] + Cb[a * 3 + 2] * u[2];
-                atomicAdd(&w_vbar_x(aw, na), wt * vb[0] + c * wt * Cu[0]);
-                atomicAdd(&w_vbar_y(aw, na), wt * vb[1] + c * wt * Cu[1]);
-                atomicAdd(&w_vbar_z(aw, na), wt * vb[2] + c * wt * Cu[2]);
+                // one 16-byte vector reduction per node (sm_90+) instead of three scalar ones
+                atomicAdd(&aw.vbar[na], make_float4(wt * vb[0] + c * wt * Cu[0], wt * vb[1] + c * wt * Cu[1],
+                                                    wt * vb[2] + c * wt * Cu[2], 0.f));
                 const float wbar = vb[0] * vh[0] + vb[1] * vh[1] + vb[2] * vh[2] +
                                    c * (vh[0] * Cu[0] + vh[1] * Cu[1] + vh[2] * Cu[2]);
 #pragma unroll
@@ -373,11 +369,54 @@ __device__ __forceinline__ float warp_sum(float x) {
     return x;
 }
 
+// Adjoint of one force field's v += acc(p, v) dt with respect to v (its Jacobian is symmetric):
+// vb holds dL/d(v after) on entry and dL/d(v before) on return.  CONSTANT, WIND and
+// TURBULENCE's noise do not depend on v; NOISE is refused by differentiable scenes.
+__device__ void force_field_vjp(const mpm_force_field& f, float eps, float dt, const float* p, const float* v,
+                                float* vb) {
+    switch (f.kind) {
+        case MPM_FF_POINT: {
+            const float c = 1.f - dt * f.flow * point_falloff(f, eps, p);
+            vb[0] *= c;
+            vb[1] *= c;
+            vb[2] *= c;
+            break;
+        }
+        case MPM_FF_DRAG: {
+            const float vn = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            const float dot = v[0] * vb[0] + v[1] * vb[1] + v[2] * vb[2];
+            const float q = vn > 0.f ? dt * f.quadratic * dot / vn : 0.f;
+            const float c = 1.f - dt * (f.linear + f.quadratic * vn);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vb[d] = c * vb[d] - q * v[d];
+            break;
+        }
+        case MPM_FF_VORTEX: {
+            const float c = 1.f - dt * f.damping;
+            vb[0] *= c;
+            vb[1] *= c;
+            vb[2] *= c;
+            break;
+        }
+        case MPM_FF_TURBULENCE: {
+            const float c = 1.f - dt * f.flow;
+            vb[0] *= c;
+            vb[1] *= c;
+            vb[2] *= c;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
 // Adjoint of the grid op per node: the boundary, the colliders' responses in reverse order
-// (tools' position / linear-velocity adjoints summed per warp into cbar[6 k ..]), then
-// v = p / m + dt g.  Every thread runs the collider loops, so the warp sums see full warps.
+// (tools' position / linear-velocity adjoints summed per warp into cbar[6 k ..]), the force
+// fields in reverse order, then v = p / m + dt g.  Every thread runs the collider loops, so
+// the warp sums see full warps.
 __global__ void k_adj_grid(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w, AdjWs aw,
-                           const mpm_collider* __restrict__ cs, int nc, const float* __restrict__ sdf, float* cbar) {
+                           const mpm_collider* __restrict__ cs, int nc, const float* __restrict__ sdf, float* cbar,
+                           const mpm_force_field* __restrict__ ffs, int n_ff, const int* __restrict__ ff_perm) {
     const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = node < prob.n_blocks * BLK3;
     const int64_t blk = in ? node / BLK3 : 0;
@@ -398,7 +437,8 @@ __global__ void k_adj_grid(mpm_problem prob, const mpm_instance* __restrict__ in
             vin[d] = inv * pm[d] + I.dt * I.gravity[d];
             p[d] = (float)(bxyz[d] * BLK + lxyz[d] + I.lower_cell[d]) * I.dx;
         }
-        float v[3] = {vin[0], vin[1], vin[2]};
+        if (n_ff > 0) apply_force_fields(ffs, n_ff, ff_perm, I.eps, I.dt, p, vin, node, 0u);
+        float v[3] = {vin[0], vin[1], vin[2]};  // vin: the colliders' input from here on
         if (nc > 0) collider_chain(cs, nc, ii, sdf, I.eps, I.dt, p, v, false, nc);
         const float4 vb4 = aw.vbar[node];
         const float vbin[3] = {vb4.x, vb4.y, vb4.z};
@@ -431,6 +471,17 @@ __global__ void k_adj_grid(mpm_problem prob, const mpm_instance* __restrict__ in
                     if ((threadIdx.x & 31) == 0 && r[j] != 0.f) atomicAdd(&cbar[6 * k + j], r[j]);
                 }
             }
+        }
+    }
+    if (act && n_ff > 0) {
+        // the force fields in reverse order, each from the velocity it received
+        for (int k = n_ff - 1; k >= 0; --k) {
+            if (!ffs[k].active) continue;
+            float vk[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vk[d] = inv * pm[d] + I.dt * I.gravity[d];
+            apply_force_fields(ffs, k, ff_perm, I.eps, I.dt, p, vk, node, 0u);
+            force_field_vjp(ffs[k], I.eps, I.dt, p, vk, vb);
         }
     }
     if (act) {

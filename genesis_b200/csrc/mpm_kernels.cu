@@ -57,7 +57,15 @@ constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
 constexpr int MAX_SCAN_TILES = SCAN_T * SCAN_ITEMS;  // single-CTA scan of tile sums
 constexpr int64_t MAX_BLOCKS = (int64_t)SCAN_TILE * MAX_SCAN_TILES;
 
-enum Counter { CNT_ACTIVE = 0, CNT_CHUNKS = 1, CNT_STATUS = 2, CNT_SORTED = 3, CNT_FALLBACK = 4 /* u64 at 4,5 */, CNT_DONE = 6 };
+enum Counter {
+    CNT_ACTIVE = 0,
+    CNT_CHUNKS = 1,
+    CNT_STATUS = 2,
+    CNT_SORTED = 3,
+    CNT_FALLBACK = 4 /* u64 at 4,5 */,
+    CNT_DONE = 6,
+    CNT_GRID_OPS = 7  // grid ops run on this workspace (the NOISE force field's counter)
+};
 constexpr int N_COUNTERS = 16;
 
 struct Ws {
@@ -1650,11 +1658,152 @@ __global__ void k_advance_colliders(const mpm_instance* __restrict__ inst, int n
     }
 }
 
+// ---------------------------------------------------------------- force fields
+// engine/force_fields.py, applied by the grid op (legacy_coupler.py:377-379)
+
+// splitmix64's output function (Steele, Lea and Flood, OOPSLA 2014): a well-mixed 64-bit
+// value per 64-bit key, the counter-based uniform source of the NOISE field
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// Ken Perlin's improved noise (2002), as PerlinNoiseField._noise (force_fields.py:441-540)
+// states it over a 512-entry permutation table P (a 256-permutation written twice)
+__device__ __forceinline__ float perlin_fade(float t) { return t * t * t * (t * (t * 6.f - 15.f) + 10.f); }
+__device__ __forceinline__ float perlin_lerp(float t, float a, float b) { return a + t * (b - a); }
+__device__ __forceinline__ float perlin_grad(int h, float x, float y, float z) {
+    h &= 15;
+    const float u = h < 8 ? x : y;
+    const float v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
+    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
+__device__ float perlin(const int* __restrict__ P, float freq, float x, float y, float z) {
+    x *= freq;
+    y *= freq;
+    z *= freq;
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    const int X = (int)fx & 255, Y = (int)fy & 255, Z = (int)fz & 255;
+    x -= fx;
+    y -= fy;
+    z -= fz;
+    const float u = perlin_fade(x), v = perlin_fade(y), w = perlin_fade(z);
+    const int A = P[X] + Y, AA = P[A] + Z, AB = P[A + 1] + Z;
+    const int B = P[X + 1] + Y, BA = P[B] + Z, BB = P[B + 1] + Z;
+    return perlin_lerp(
+        w,
+        perlin_lerp(v, perlin_lerp(u, perlin_grad(P[AA], x, y, z), perlin_grad(P[BA], x - 1.f, y, z)),
+                    perlin_lerp(u, perlin_grad(P[AB], x, y - 1.f, z), perlin_grad(P[BB], x - 1.f, y - 1.f, z))),
+        perlin_lerp(v,
+                    perlin_lerp(u, perlin_grad(P[AA + 1], x, y, z - 1.f), perlin_grad(P[BA + 1], x - 1.f, y, z - 1.f)),
+                    perlin_lerp(u, perlin_grad(P[AB + 1], x, y - 1.f, z - 1.f),
+                                perlin_grad(P[BB + 1], x - 1.f, y - 1.f, z - 1.f))));
+}
+
+// POINT's falloff 1 / (sqrt(|r|^2 + eps) + 1)^falloff_pow and VORTEX's, shared by the adjoint
+__device__ __forceinline__ float point_falloff(const mpm_force_field& f, float eps, const float* p) {
+    const float r[3] = {p[0] - f.vec[0], p[1] - f.vec[1], p[2] - f.vec[2]};
+    return 1.f / powf(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + eps) + 1.f, f.falloff_pow);
+}
+__device__ __forceinline__ float vortex_falloff(const mpm_force_field& f, float rho) {
+    if (rho < f.falloff_min) return 1.f;
+    if (rho < f.falloff_max) return 1.f / powf(rho - f.falloff_min + 1.f, f.falloff_pow);
+    return 0.f;
+}
+
+// acceleration of one (active) field at node p with velocity v; node / ops key the NOISE draw
+__device__ void force_field_acc(const mpm_force_field& f, const int* __restrict__ perm, float eps, const float* p,
+                                const float* v, int64_t node, uint32_t ops, float* acc) {
+    acc[0] = acc[1] = acc[2] = 0.f;
+    switch (f.kind) {
+        case MPM_FF_CONSTANT:
+            acc[0] = f.vec[0];
+            acc[1] = f.vec[1];
+            acc[2] = f.vec[2];
+            break;
+        case MPM_FF_WIND: {
+            const float q[3] = {p[0] - f.center[0], p[1] - f.center[1], p[2] - f.center[2]};
+            const float c[3] = {q[1] * f.dir[2] - q[2] * f.dir[1], q[2] * f.dir[0] - q[0] * f.dir[2],
+                                q[0] * f.dir[1] - q[1] * f.dir[0]};
+            if (!(sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) > f.radius)) {
+                acc[0] = f.vec[0];
+                acc[1] = f.vec[1];
+                acc[2] = f.vec[2];
+            }
+            break;
+        }
+        case MPM_FF_POINT: {
+            const float r[3] = {p[0] - f.vec[0], p[1] - f.vec[1], p[2] - f.vec[2]};
+            const float rad = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + eps);
+            const float fo = 1.f / powf(rad + 1.f, f.falloff_pow);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float a = f.strength * r[d] / rad;
+                acc[d] = (a + (a - v[d]) * f.flow) * fo;
+            }
+            break;
+        }
+        case MPM_FF_DRAG: {
+            const float vn = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[d] = -f.linear * v[d] - f.quadratic * vn * v[d];
+            break;
+        }
+        case MPM_FF_NOISE: {
+            const uint64_t h = mix64(mix64(((uint64_t)f.seed << 32) | ops) ^ (uint64_t)node);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float u = (float)(mix64(h + (uint64_t)d) >> 40) * (1.f / 16777216.f);
+                acc[d] = (u * 2.f - 1.f) * f.strength;
+            }
+            break;
+        }
+        case MPM_FF_VORTEX: {
+            const float rx = p[0] - f.center[0], ry = p[1] - f.center[1];
+            const float fo = vortex_falloff(f, sqrtf(rx * rx + ry * ry));
+            acc[0] = fo * (f.strength * -ry + f.strength2 * -rx) - f.damping * v[0];
+            acc[1] = fo * (f.strength * rx + f.strength2 * -ry) - f.damping * v[1];
+            acc[2] = -f.damping * v[2];
+            break;
+        }
+        case MPM_FF_TURBULENCE: {
+            if (!perm) break;
+            const int* P = perm + f.perm_offset;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float a = perlin(P + 512 * d, f.frequency, p[0], p[1], p[2]) * f.strength;
+                acc[d] = a + (a - v[d]) * f.flow;
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// v += acc dt for every active field in order (each sees the velocity the previous ones left)
+__device__ __forceinline__ void apply_force_fields(const mpm_force_field* __restrict__ ffs, int n, const int* perm,
+                                                   float eps, float dt, const float* p, float* v, int64_t node,
+                                                   uint32_t ops) {
+    for (int k = 0; k < n; ++k) {
+        if (!ffs[k].active) continue;
+        float a[3];
+        force_field_acc(ffs[k], perm, eps, p, v, node, ops, a);
+        v[0] += a[0] * dt;
+        v[1] += a[1] * dt;
+        v[2] += a[2] * dt;
+    }
+}
+
 // at most 64 registers (4 CTAs per SM): the collider responses, rare, may spill instead
 __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w,
                                                  const mpm_collider* __restrict__ colliders, int n_colliders,
-                                                 float* collider_force, const float* __restrict__ sdf_voxels) {
+                                                 float* collider_force, const float* __restrict__ sdf_voxels,
+                                                 const mpm_force_field* __restrict__ ffs, int n_ff,
+                                                 const int* __restrict__ ff_perm, int count_op) {
     const int n_active = (int)w.counters[CNT_ACTIVE];
+    const uint32_t ops = w.counters[CNT_GRID_OPS];
     const int gpc = blockDim.x / BLK3;
     const int grp = threadIdx.x / BLK3;
     const int ln = threadIdx.x % BLK3;
@@ -1676,6 +1825,14 @@ __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_
             const float px = (float)(bc.bx * BLK + lx + I.lower_cell[0]) * I.dx;
             const float py = (float)(bc.by * BLK + ly + I.lower_cell[1]) * I.dx;
             const float pz = (float)(bc.bz * BLK + lz + I.lower_cell[2]) * I.dx;
+            if (n_ff > 0) {  // external force fields (legacy_coupler.py:377-379)
+                const float p[3] = {px, py, pz};
+                float v[3] = {vx, vy, vz};
+                apply_force_fields(ffs, n_ff, ff_perm, I.eps, I.dt, p, v, g, ops);
+                vx = v[0];
+                vy = v[1];
+                vz = v[2];
+            }
             if (n_colliders > 0) {
                 // MPM <-> rigid (legacy_coupler.py:385-397), before the boundary; the node
                 // mass without the 1e3 particle-volume scale (legacy_coupler.py:375)
@@ -1711,6 +1868,7 @@ __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_
         if (atomicAdd(&w.counters[CNT_DONE], 1u) == gridDim.x - 1) {
             w.counters[CNT_ACTIVE] = 0u;
             w.counters[CNT_DONE] = 0u;
+            if (count_op) w.counters[CNT_GRID_OPS] = ops + 1u;
         }
     }
 }
@@ -1969,8 +2127,11 @@ static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* 
     if (ctas > need) ctas = (int)need;
     if (tab->n_colliders < 0) return MPM_E_INVALID;
     const int nc = tab->colliders ? tab->n_colliders : 0;
+    if (tab->n_force_fields < 0 || (tab->n_force_fields > 0 && !tab->force_fields)) return MPM_E_INVALID;
+    const int nff = tab->force_fields ? tab->n_force_fields : 0;
     k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc,
-                                    advance ? tab->collider_force : nullptr, tab->sdf_voxels);
+                                    advance ? tab->collider_force : nullptr, tab->sdf_voxels, tab->force_fields, nff,
+                                    tab->ff_perm, advance ? 1 : 0);
     if (nc > 0 && advance)
         k_advance_colliders<<<(nc + 63) / 64, 64, 0, s>>>(tab->instances, prob->n_instances, tab->colliders, nc);
     return cuda_ok();
@@ -2145,14 +2306,15 @@ extern "C" {
 
 int mpm_abi_version(void) { return MPM_ABI_VERSION; }
 
-int mpm_struct_sizes(int32_t* out6) {
-    if (!out6) return MPM_E_INVALID;
-    out6[0] = (int32_t)sizeof(mpm_instance);
-    out6[1] = (int32_t)sizeof(mpm_material);
-    out6[2] = (int32_t)sizeof(mpm_problem);
-    out6[3] = (int32_t)sizeof(mpm_particles);
-    out6[4] = (int32_t)sizeof(mpm_tables);
-    out6[5] = (int32_t)sizeof(mpm_collider);
+int mpm_struct_sizes(int32_t* out7) {
+    if (!out7) return MPM_E_INVALID;
+    out7[0] = (int32_t)sizeof(mpm_instance);
+    out7[1] = (int32_t)sizeof(mpm_material);
+    out7[2] = (int32_t)sizeof(mpm_problem);
+    out7[3] = (int32_t)sizeof(mpm_particles);
+    out7[4] = (int32_t)sizeof(mpm_tables);
+    out7[5] = (int32_t)sizeof(mpm_collider);
+    out7[6] = (int32_t)sizeof(mpm_force_field);
     return MPM_OK;
 }
 
@@ -2469,7 +2631,9 @@ int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab
     if (n > 0) {
         k_adj_g2p<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, *state, adj, w, aw);
         k_adj_grid<<<(int)((nodes + 255) / 256), 256, 0, s>>>(*prob, tab->instances, w, aw, tab->colliders, nc,
-                                                               tab->sdf_voxels, collider_bar);
+                                                               tab->sdf_voxels, collider_bar, tab->force_fields,
+                                                               tab->force_fields ? tab->n_force_fields : 0,
+                                                               tab->ff_perm);
         k_adj_p2g<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, tab->materials, *state, adj, lame_bar, aw);
     }
     return cuda_ok();

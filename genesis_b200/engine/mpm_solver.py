@@ -149,6 +149,10 @@ class MPMSolver:
             if bad:
                 raise GenesisException("A differentiable scene supports MPM entities, tools and rigid colliders "
                                        f"only (got {', '.join(bad)}).")
+        from .. import force_fields as _ff
+
+        ffs = list(getattr(self._scene, "_force_fields", []))
+        ff_rows, ff_perm = _ff.pack(ffs)
         self.runtime = MPMRuntime(
             specs,
             device=self._sim.device,
@@ -160,7 +164,11 @@ class MPMSolver:
             sdf_voxels=torch.cat(grids) if grids else None,
             cpic=self._enable_CPIC,  # active only with rigid colliders, as in the reference
             per_particle_lame=grad,
+            force_fields=ff_rows,
+            ff_perm=ff_perm,
         )
+        for k, f in enumerate(ffs):  # activate() / deactivate() now write the device row
+            f._solver, f._row = self, k
         for i, t in enumerate(tools):
             t._bind(self.runtime, [i * self._B + env for env in range(self._B)])
         for i, r in enumerate(rigid):

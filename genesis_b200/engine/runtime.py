@@ -93,6 +93,8 @@ class MPMRuntime:
         colliders: list | None = None,
         sdf_voxels: torch.Tensor | None = None,
         cpic: bool = False,
+        force_fields: list | None = None,
+        ff_perm: np.ndarray | None = None,
     ):
         if not torch.cuda.is_available():
             raise RuntimeError("genesis_b200 needs a CUDA device (sm_100a); there is no CPU path")
@@ -179,11 +181,27 @@ class MPMRuntime:
                 if c.kind == nat.COLLIDER_TOOL and c.sdf_res != 0 and (
                         c.sdf_res < 2 or c.sdf_offset < 0 or c.sdf_offset + c.sdf_res ** 3 > n_vox):
                     raise ValueError("a tool collider's voxel grid lies outside sdf_voxels")
+        # external force fields of the grid op (mpm_force_field rows) and the turbulence fields'
+        # permutation tables (mpm_force_field.perm_offset indexes into them)
+        force_fields = list(force_fields or [])
+        self.n_force_fields = len(force_fields)
+        self.ff_table = self.ff_perm = None
+        if force_fields:
+            perm_n = 0 if ff_perm is None else int(np.asarray(ff_perm).size)
+            for f in force_fields:
+                if f.kind == nat.FF_TURBULENCE and (f.perm_offset < 0 or f.perm_offset + 3 * 512 > perm_n):
+                    raise ValueError("a turbulence field's permutation tables lie outside ff_perm")
+            arr = (nat.ForceField * len(force_fields))(*force_fields)
+            self.ff_table = torch.from_numpy(np.frombuffer(bytes(arr), dtype=np.uint8).copy()).to(dev)
+            if perm_n:
+                self.ff_perm = torch.as_tensor(np.asarray(ff_perm, dtype=np.int32).reshape(-1), device=dev)
         self.tables = nat.Tables(
             self.inst_table.data_ptr(), self.mat_table.data_ptr(),
             self.coll_table.data_ptr() if colliders else None, len(colliders), 0,
             self.collider_force.data_ptr() if colliders else None,
             self.sdf_voxels.data_ptr() if self.sdf_voxels is not None else None,
+            self.ff_table.data_ptr() if force_fields else None, len(force_fields), 0,
+            self.ff_perm.data_ptr() if self.ff_perm is not None else None,
         )
 
         self.state = torch.zeros((nat.MPM_STATE_CH, self.stride), dtype=torch.float32, device=dev)
@@ -306,6 +324,13 @@ class MPMRuntime:
         if self.cpic_normal is None:
             raise RuntimeError("runtime has no CPIC state")
         return self.cpic_normal[:, : self.n].reshape(-1, 3, self.n).permute(0, 2, 1)
+
+    def set_force_field_active(self, k: int, active: bool):
+        """ForceField.activate / deactivate (force_fields.py:21-32) of row k, stream-ordered."""
+        if self.ff_table is None or not 0 <= k < self.n_force_fields:
+            raise IndexError("no such force field")
+        off = k * C.sizeof(nat.ForceField) + nat.ForceField.active.offset
+        self.ff_table.view(torch.int32)[off // 4] = 1 if active else 0
 
     def collider_table(self) -> torch.Tensor:
         """The collider rows as float32 [n_colliders, 32] (pos 0:3, rot 3:12, data 12:15,

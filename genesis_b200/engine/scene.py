@@ -48,6 +48,7 @@ class Scene:
         self._rigid_entities = []  # kinematic colliders of the MPM grid op
         self._tool_entities = []  # tools, coupled before the rigid geoms
         self._emitters = []
+        self._force_fields = []
         self._is_built = False
         self._B = 1
         self._n_envs = 0
@@ -102,6 +103,28 @@ class Scene:
     @property
     def emitters(self):
         return self._emitters
+
+    def add_force_field(self, force_field):
+        """Register an external acceleration field of the MPM grid op (scene.py:720-736); it acts
+        once activated."""
+        from .. import force_fields as _ff
+
+        if self._is_built:
+            raise GenesisException("Scene is already built.")
+        if not isinstance(force_field, _ff.ForceField):
+            raise GenesisException("`force_field` must be a gs.force_fields.ForceField.")
+        if isinstance(force_field, _ff.Custom):
+            raise GenesisException("Custom force fields (a gstaichi function) are not supported.")
+        if self.sim_options.requires_grad and isinstance(force_field, _ff.Noise):
+            raise GenesisException("The Noise force field is not supported in differentiable mode (its draws are "
+                                   "not replayed by the backward pass).")
+        force_field.scene = self
+        self._force_fields.append(force_field)
+        return force_field
+
+    @property
+    def force_fields(self):
+        return self._force_fields
 
     def build(self, n_envs=0, env_spacing=(0.0, 0.0), n_envs_per_row=None, center_envs_at_origin=True,
               compile_kernels=None):

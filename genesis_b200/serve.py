@@ -98,6 +98,17 @@ class AdmissionQueue:
         self.pending.append((req, need))
         return None
 
+    def admissible_particles(self, n_active: int) -> int:
+        """Particles of the requests pop_admissible would admit now (nothing is popped)."""
+        total, used, k = 0, self.in_use, 0
+        for req, need in self.pending:
+            if n_active + k >= self.max_active or used + need > self.budget:
+                break
+            used += need
+            k += 1
+            total += req.scene.n_particles
+        return total
+
     def pop_admissible(self, n_active: int) -> list:
         out = []
         while self.pending and n_active + len(out) < self.max_active and self.in_use + self.pending[0][1] <= self.budget:
@@ -118,8 +129,11 @@ class MPMServer:
                  min_live_particles: int = 2_000_000):
         """admit_wait > 0 batches admissions: while at least min_live_particles are being
         advanced, queued requests join (which costs a repack of every live rollout) only
-        once their particles reach admit_ratio of the live ones or the oldest has waited
-        admit_wait seconds.  admit_wait = 0 admits at every tick."""
+        once the particles that fit now reach admit_ratio of the live ones, or once the
+        oldest has waited admit_wait seconds and the last repack is admit_wait seconds old.
+        admit_wait = 0 admits at every tick.  A tick advances up to tick_substeps substeps,
+        split where live rollouts finish (each is read back and retired, stream-ordered, at
+        its own last substep), with one wait for the GPU per tick."""
         self.tick = int(tick_substeps)
         self.admit_wait = float(admit_wait)
         self.admit_ratio = float(admit_ratio)
@@ -133,12 +147,21 @@ class MPMServer:
         self.active: list[_Slot] = []
         self.ticks = 0
         self.repacks = 0
+        self.repack_s = 0.0  # host seconds spent building layouts
         self.particle_substeps = 0
+        self.substeps_run = 0  # substeps enqueued, over every tick
 
     # ------------------------------------------------------------------ packing
     def _repack(self, new_slots):
         """Build a runtime for the live rollouts plus new_slots: continuing rollouts keep
         their device state; retired ones (holes) are dropped."""
+        t_start = time.perf_counter()
+        try:
+            self._repack_layout(new_slots)
+        finally:
+            self.repack_s += time.perf_counter() - t_start
+
+    def _repack_layout(self, new_slots):
         live = [s for s in self.active if not s.retired]
         if self.rt is not None and live:
             exported = self.rt.export_instances()
@@ -212,6 +235,7 @@ class MPMServer:
         bad = nat.MPM_STATUS_NAN | nat.MPM_STATUS_NONFINITE_VEL
         i = 0
         n_live = lambda: sum(1 for s in self.active if not s.retired)
+        last_repack = -math.inf
 
         def push_arrivals():
             nonlocal i
@@ -224,19 +248,24 @@ class MPMServer:
                 i += 1
 
         def admit():
+            nonlocal last_repack
             if not self.queue.pending:
                 return False
             if self.admit_wait > 0.0 and n_live():
                 live_p = sum(s.req.scene.n_particles for s in self.active if not s.retired)
                 if live_p >= self.min_live_particles:
-                    pend_p = sum(r.scene.n_particles for r, _ in self.queue.pending)
+                    fit_p = self.queue.admissible_particles(n_live())
+                    if fit_p == 0:
+                        return False
                     oldest = self.queue.pending[0][0]
                     waited = clock() - (oldest.arrival if realtime else 0.0)
-                    if pend_p < self.admit_ratio * live_p and waited < self.admit_wait:
+                    stale = waited >= self.admit_wait and clock() - last_repack >= self.admit_wait
+                    if fit_p < self.admit_ratio * live_p and not stale:
                         return False
             admitted = self.queue.pop_admissible(n_live())
             if not admitted:
                 return False
+            last_repack = clock()
             now = clock()
             new_slots = []
             for req, need in admitted:
@@ -253,28 +282,38 @@ class MPMServer:
                 if i < len(reqs) and realtime:
                     time.sleep(max(0.0, min(0.05, reqs[i].arrival - clock())))
                 continue
-            # ---- enqueue one tick, the read of its statuses and of its finished results
+            # ---- enqueue one tick (segments ending where live rollouts finish, each finished
+            # rollout read back and retired right after its last substep), then the read of
+            # the instances' statuses
             tick_slots = [s for s in self.active if not s.retired]
-            T = min(self.tick, min(s.remaining for s in tick_slots))
-            self.rt.substeps(T)
-            self.ticks += 1
-            self.particle_substeps += T * sum(s.req.scene.n_particles for s in tick_slots)
             tick_index = {id(s): k for k, s in enumerate(self.active)}
-            for s in tick_slots:
-                s.remaining -= T
-            finishing = [s for s in tick_slots if s.remaining == 0]
+            T = min(self.tick, max(s.remaining for s in tick_slots))
             fin_host = {}
-            if finishing and self.keep_results:
-                st = self.rt.get_state(("pos", "vel"))
-                offs = self.rt.instance_offsets
+            done = 0
+            while True:
+                finishing = [s for s in tick_slots if s.remaining == 0 and not s.retired]
+                if finishing and self.keep_results:
+                    st = self.rt.get_state(("pos", "vel"))
+                    offs = self.rt.instance_offsets
+                    for s in finishing:
+                        k = tick_index[id(s)]
+                        sl = slice(offs[k], offs[k] + s.req.scene.n_particles)
+                        fin_host[id(s)] = tuple(_download(st[key][sl]) for key in ("pos", "vel"))
                 for s in finishing:
-                    k = tick_index[id(s)]
-                    sl = slice(offs[k], offs[k] + s.req.scene.n_particles)
-                    fin_host[id(s)] = tuple(_download(st[key][sl]) for key in ("pos", "vel"))
+                    self._retire(tick_index[id(s)])
+                running = [s for s in tick_slots if s.remaining > 0]
+                if not running or done >= T:
+                    break
+                seg = min(T - done, min(s.remaining for s in running))
+                self.rt.substeps(seg)
+                self.particle_substeps += seg * sum(s.req.scene.n_particles for s in running)
+                self.substeps_run += seg
+                done += seg
+                for s in running:
+                    s.remaining -= seg
+            self.ticks += 1
             status_host, status_ev = self.rt.instance_status_enqueue(clear=True)
             # ---- host work while the tick runs (all GPU work it issues is stream-ordered)
-            for s in finishing:
-                self._retire(tick_index[id(s)])
             push_arrivals()
             admit()
             # ---- wait for the tick

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 10
+#define MPM_ABI_VERSION 11
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -210,6 +210,54 @@ typedef struct mpm_collider {
     float sdf_pad2;
 } mpm_collider;
 
+/* External force (acceleration) fields of the grid op (engine/force_fields.py; applied per
+ * active node after gravity and before the tools, legacy_coupler.py:377-379:
+ * v += acc(pos, v) dt for each field in order, each seeing the velocity the previous ones
+ * left).  Every field acts on every instance of the problem.  Kinds and the fields they read:
+ *   CONSTANT    acc = vec                                             (force_fields.py:49-82)
+ *   WIND        acc = vec where |(pos - center) x dir| <= radius, else 0          (:85-144)
+ *   POINT       r = pos - vec, d = r / sqrt(|r|^2 + eps); acc = strength d;
+ *               acc += (acc - v) flow; acc /= (sqrt(|r|^2 + eps) + 1)^falloff_pow (:147-198)
+ *   DRAG        acc = -linear v - quadratic |v| v                                (:201-229)
+ *   NOISE       acc = strength (2 u - 1), u uniform in [0, 1)^3 from a counter-based hash of
+ *               (seed, node, the problem's grid-op count): the reference draws ti.random, a
+ *               stream this does not reproduce                                   (:232-260)
+ *   VORTEX      about the z axis through center: r2 = (pos - center).xy, rho = |r2|;
+ *               falloff 1 below falloff_min, 1 / (rho - falloff_min + 1)^falloff_pow below
+ *               falloff_max, else 0; acc = falloff (strength (-r2.y, r2.x, 0) +
+ *               strength2 (-r2.x, -r2.y, 0)) - damping v                         (:263-369)
+ *   TURBULENCE  acc = strength (N_x, N_y, N_z)(pos) with N the improved Perlin noise over
+ *               three 512-entry permutation tables at perm[perm_offset ...] (x, y, z) at
+ *               spatial frequency `frequency`; acc += (acc - v) flow            (:372-540) */
+#define MPM_FF_CONSTANT 0
+#define MPM_FF_WIND 1
+#define MPM_FF_POINT 2
+#define MPM_FF_DRAG 3
+#define MPM_FF_NOISE 4
+#define MPM_FF_VORTEX 5
+#define MPM_FF_TURBULENCE 6
+
+typedef struct mpm_force_field {
+    int32_t kind;        /* MPM_FF_* */
+    int32_t active;      /* ForceField.activate / deactivate: 0 = no effect */
+    float vec[3];        /* CONSTANT, WIND: direction * strength; POINT: position */
+    float dir[3];        /* WIND: unit direction */
+    float center[3];     /* WIND, VORTEX: center */
+    float strength;      /* POINT, NOISE, TURBULENCE; VORTEX: strength_perpendicular */
+    float strength2;     /* VORTEX: strength_radial */
+    float radius;        /* WIND */
+    float falloff_pow;   /* POINT, VORTEX */
+    float falloff_min;   /* VORTEX */
+    float falloff_max;   /* VORTEX (may be +inf) */
+    float flow;          /* POINT, TURBULENCE */
+    float damping;       /* VORTEX */
+    float linear;        /* DRAG */
+    float quadratic;     /* DRAG */
+    float frequency;     /* TURBULENCE */
+    int32_t perm_offset; /* TURBULENCE: first entry of its 3 x 512 permutation tables in perm */
+    uint32_t seed;       /* NOISE */
+} mpm_force_field;
+
 typedef struct mpm_tables {
     const mpm_instance* instances;  /* device, n_instances entries */
     const mpm_material* materials;  /* device, n_materials entries */
@@ -220,6 +268,10 @@ typedef struct mpm_tables {
                                        accumulated (the caller zeroes it) */
     const float* sdf_voxels;        /* device, the voxel grids of the MPM_COLLIDER_TOOL colliders,
                                        each [sdf_res][sdf_res][sdf_res] (x-major) at its sdf_offset */
+    const mpm_force_field* force_fields; /* device, n_force_fields entries (may be NULL if none) */
+    int32_t n_force_fields;
+    int32_t pad1;
+    const int32_t* ff_perm;         /* device, the TURBULENCE fields' permutation tables */
 } mpm_tables;
 
 /* ---- sizing ------------------------------------------------------------ */
@@ -228,9 +280,9 @@ typedef struct mpm_tables {
 int mpm_abi_version(void);
 
 /* sizeof(mpm_instance), sizeof(mpm_material), sizeof(mpm_problem), sizeof(mpm_particles),
- * sizeof(mpm_tables), sizeof(mpm_collider) as compiled into the library, so a binding can
- * verify its mirror of these structs. */
-int mpm_struct_sizes(int32_t* out6);
+ * sizeof(mpm_tables), sizeof(mpm_collider), sizeof(mpm_force_field) as compiled into the
+ * library, so a binding can verify its mirror of these structs. */
+int mpm_struct_sizes(int32_t* out7);
 
 /* Upper bound on the number of p2g/g2p work items for a problem. */
 int mpm_max_chunks(int32_t n_particles, int64_t n_blocks, int32_t chunk_particles, int32_t* out);

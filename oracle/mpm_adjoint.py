@@ -401,15 +401,15 @@ def forward_materials(p, mats, st, mu, lam, colliders=None):
         mass[sel] = R.particle_mass(p, m)
     s = -p.dt * p.p_vol * 4 * p.inv_dx * p.inv_dx
     A = s * P + mass[:, None, None] * C
-    out, inter = _grid_and_g2p(p, st, A, mass, colliders)
+    out, inter = _grid_and_g2p(p, st, A, mass, colliders, st.get("force_fields"))
     out.update(F=Fn, Jp=Jpn)
     inter.update(Ft=Ft, U=U, S=S, V=V, P=P, A=A, s=s, mass=mass)
     return out, inter
 
 
-def _grid_and_g2p(p, st, A, mass, colliders=None):
-    """p2g scatter of (m v + A d), grid op (with the colliders' responses, tools first, as
-    legacy_coupler.py:381-397 orders them) and g2p of mpm_ref.substep."""
+def _grid_and_g2p(p, st, A, mass, colliders=None, force_fields=None):
+    """p2g scatter of (m v + A d), grid op (the force fields, then the colliders' responses,
+    tools first, as legacy_coupler.py:377-397 orders them) and g2p of mpm_ref.substep."""
     x, v = st["x"], st["v"]
     n = x.shape[0]
     base, fx, w, dw, node0 = _stencil(p, x)
@@ -433,6 +433,13 @@ def _grid_and_g2p(p, st, A, mass, colliders=None):
     vg[act] = gp[act] / gm[act][:, None] + p.dt * np.asarray(p.gravity)[None, :]
     idx = np.array(np.unravel_index(np.arange(G), res)).T
     gpos = (idx + p.lower_cell[None, :]) * p.dx
+    ff_chain = []  # (field, its input velocity on the active nodes)
+    if force_fields:
+        va = vg[act]
+        for f in force_fields:
+            ff_chain.append((f, va))
+            va = va + R.force_field_acc(f, gpos[act], va, p.eps) * p.dt
+        vg[act] = va
     chain = []  # (collider index, collider, its input velocity on the active nodes)
     if colliders:
         va = vg[act]
@@ -474,8 +481,19 @@ def _grid_and_g2p(p, st, A, mass, colliders=None):
     out = dict(st)
     out.update(x=np.clip(xs, p.bnd_lo, p.bnd_hi), v=nv * vmask, C=nC)
     inter = dict(fx=fx, w=w, dw=dw, lin=lin_all, gm=gm, gp=gp, vh=vh, gmask=gmask, act=act, nv=nv, pmask=pmask,
-                 vmask=vmask, chain=chain, gpos=gpos, n_colliders=len(colliders or []))
+                 vmask=vmask, chain=chain, gpos=gpos, n_colliders=len(colliders or []), ff_chain=ff_chain)
     return out, inter
+
+
+def force_field_vjp(p, f, pos, vin, vbar, h=1e-30):
+    """Adjoint of v + acc(pos, v) dt with respect to v at nodes pos, by complex steps."""
+    out = np.zeros_like(vin)
+    for k in range(3):
+        vv = vin.astype(np.complex128)
+        vv[:, k] += 1j * h
+        dv = vv + R.force_field_acc(f, pos, vv, p.eps) * p.dt
+        out[:, k] = (np.imag(dv) / h * vbar).sum(1)
+    return out
 
 
 def collider_vjp(p, c, pos, vin, vbar, mass=None, h=1e-30):
@@ -551,6 +569,13 @@ def backward_materials(p, mats, st, mu, lam, inter, adj):
             va_bar, pb, lb = collider_vjp(p, c, gpa, vin, va_bar, mass=ma)
             cbar[k, 0] += pb
             cbar[k, 1] += lb
+        vg_bar = np.zeros_like(vg_bar)
+        vg_bar[act] = va_bar
+    if inter["ff_chain"]:
+        va_bar = vg_bar[act]
+        gpa = inter["gpos"][act]
+        for f, vin in reversed(inter["ff_chain"]):
+            va_bar = force_field_vjp(p, f, gpa, vin, va_bar)
         vg_bar = np.zeros_like(vg_bar)
         vg_bar[act] = va_bar
     pbar = np.zeros((G, 3))
@@ -675,9 +700,10 @@ def rollout_colliders(p, mats, st0, mu, lam, colliders, lin_vel, weights, grad=T
             lin_bar[t, k] += p.dt * pb
             pos_bar[k] = pb
         adj, _, _, _ = backward_materials(p, mats, states[t], mu, lam, inters[t], adj)
-        cb = adj.pop("colliders")
-        pos_bar += cb[:, 0]
-        lin_bar[t] += cb[:, 1]
+        cb = adj.pop("colliders", None)
+        if cb is not None:
+            pos_bar += cb[:, 0]
+            lin_bar[t] += cb[:, 1]
     return loss, adj["v"], pos_bar, lin_bar
 
 

@@ -597,7 +597,104 @@ def advance_colliders(p: Params, colliders):
     return out
 
 
-def grid_op(p: Params, gm, gp, colliders=None, forces=None):
+# ---------------------------------------------------------------- external force fields
+# engine/force_fields.py: what each class's __init__ derives from its arguments, and _get_acc.
+
+
+def _perlin_perm(seed, seed_offset, wrap_size=256):
+    """PerlinNoiseField's table (force_fields.py:447-460)."""
+    perm = np.arange(wrap_size, dtype=np.int64)
+    if seed is not None:
+        np.random.RandomState(seed + seed_offset).shuffle(perm)
+    return np.concatenate([perm, perm])
+
+
+def make_force_field(name: str, **kw) -> dict:
+    """An active field with the reference constructor's arguments (force_fields.py:49-421)."""
+    f = dict(name=name)
+    if name in ("Constant", "Wind"):
+        d = np.asarray(kw.get("direction", (1, 0, 0)), dtype=np.float64)
+        f.update(direction=d / np.linalg.norm(d), strength=kw.get("strength", 1.0))
+        if name == "Wind":
+            f.update(radius=kw.get("radius", 1), center=np.asarray(kw.get("center", (0, 0, 0)), dtype=np.float64))
+    elif name == "Point":
+        f.update(strength=kw.get("strength", 1.0), position=np.asarray(kw.get("position", (0, 0, 0)), float),
+                 falloff_pow=kw.get("falloff_pow", 0.0), flow=kw.get("flow", 1.0))
+    elif name == "Drag":
+        f.update(linear=kw.get("linear", 0.0), quadratic=kw.get("quadratic", 0.0))
+    elif name == "Vortex":
+        f.update(center=np.asarray(kw.get("center", (0.0, 0.0, 0.0)), float),
+                 sp=kw.get("strength_perpendicular", 20.0), sr=kw.get("strength_radial", 0.0),
+                 falloff_pow=kw.get("falloff_pow", 2.0), falloff_min=kw.get("falloff_min", 0.01),
+                 falloff_max=kw.get("falloff_max", np.inf), damping=kw.get("damping", 0.0))
+    elif name == "Turbulence":
+        seed = kw.get("seed")
+        f.update(strength=kw.get("strength", 1.0), frequency=kw.get("frequency", 3), flow=kw.get("flow", 0.0),
+                 perms=[_perlin_perm(seed, k) for k in range(3)])
+    else:
+        raise ValueError(f"no oracle for force field {name}")
+    return f
+
+
+def _perlin(P, freq, x, y, z):
+    """PerlinNoiseField._noise (force_fields.py:495-540) at arrays of points."""
+    x, y, z = x * freq, y * freq, z * freq
+    fx, fy, fz = np.floor(x), np.floor(y), np.floor(z)
+    X, Y, Z = fx.astype(np.int64) & 255, fy.astype(np.int64) & 255, fz.astype(np.int64) & 255
+    x, y, z = x - fx, y - fy, z - fz
+    fade = lambda t: t * t * t * (t * (t * 6 - 15) + 10)
+    lerp = lambda t, a, b: a + t * (b - a)
+
+    def grad(h, x, y, z):
+        h = h & 15
+        u = np.where(h < 8, x, y)
+        v = np.where(h < 4, y, np.where((h == 12) | (h == 14), x, z))
+        return np.where(h & 1, -u, u) + np.where(h & 2, -v, v)
+
+    u, v, w = fade(x), fade(y), fade(z)
+    A = P[X] + Y
+    AA, AB = P[A] + Z, P[A + 1] + Z
+    B = P[X + 1] + Y
+    BA, BB = P[B] + Z, P[B + 1] + Z
+    return lerp(w, lerp(v, lerp(u, grad(P[AA], x, y, z), grad(P[BA], x - 1, y, z)),
+                        lerp(u, grad(P[AB], x, y - 1, z), grad(P[BB], x - 1, y - 1, z))),
+                lerp(v, lerp(u, grad(P[AA + 1], x, y, z - 1), grad(P[BA + 1], x - 1, y, z - 1)),
+                        lerp(u, grad(P[AB + 1], x, y - 1, z - 1), grad(P[BB + 1], x - 1, y - 1, z - 1))))
+
+
+def force_field_acc(f: dict, pos, vel, eps):
+    """_get_acc of an active field at points pos [G, 3] with velocities vel [G, 3]."""
+    n = f["name"]
+    if n == "Constant":
+        return np.broadcast_to(f["direction"] * f["strength"], pos.shape).copy()
+    if n == "Wind":
+        dist = np.linalg.norm(np.cross(pos - f["center"], f["direction"]), axis=1)
+        return np.where((dist > f["radius"])[:, None], 0.0, f["direction"] * f["strength"])
+    if n == "Point":
+        r = pos - f["position"]
+        rad = np.sqrt((r * r).sum(1) + eps)
+        acc = f["strength"] * r / rad[:, None]
+        acc = acc + (acc - vel) * f["flow"]
+        return acc * (1.0 / (rad + 1.0) ** f["falloff_pow"])[:, None]
+    if n == "Drag":  # |v| as sqrt(v.v), analytic for the adjoint oracle's complex steps
+        return -f["linear"] * vel - f["quadratic"] * np.sqrt((vel * vel).sum(1))[:, None] * vel
+    if n == "Vortex":
+        rx, ry = pos[:, 0] - f["center"][0], pos[:, 1] - f["center"][1]
+        rho = np.sqrt(rx * rx + ry * ry)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            fo = np.where(rho < f["falloff_min"], 1.0,
+                          np.where(rho < f["falloff_max"], 1.0 / (rho - f["falloff_min"] + 1.0) ** f["falloff_pow"], 0.0))
+        perp = np.stack([-ry, rx, np.zeros_like(rx)], 1)
+        radial = -np.stack([rx, ry, np.zeros_like(rx)], 1)
+        return fo[:, None] * (f["sp"] * perp + f["sr"] * radial) - f["damping"] * vel
+    if n == "Turbulence":
+        acc = np.stack([_perlin(P, f["frequency"], pos[:, 0], pos[:, 1], pos[:, 2]) for P in f["perms"]], 1)
+        acc = acc * f["strength"]
+        return acc + (acc - vel) * f["flow"]
+    raise ValueError(n)
+
+
+def grid_op(p: Params, gm, gp, colliders=None, forces=None, force_fields=None):
     """MPM core of LegacyCoupler.mpm_grid_op (legacy_coupler.py:364-375, 495-496), with the
     rigid coupling of :385-397 for kinematic colliders (forces, if a list, receives one
     (force, torque) pair per collider)."""
@@ -610,6 +707,8 @@ def grid_op(p: Params, gm, gp, colliders=None, forces=None):
     v = v + dt(p.dt) * np.asarray(p.gravity, dtype=dt)[None, :]
     idx = np.argwhere(act)
     pos = (idx + p.lower_cell[None, :]).astype(dt) * dt(p.dx)
+    for f in force_fields or []:  # external force fields (legacy_coupler.py:377-379)
+        v = (v + force_field_acc(f, pos.astype(np.float64), v.astype(np.float64), p.eps) * p.dt).astype(dt)
     for c in colliders or []:  # MPM <-> Tool first (legacy_coupler.py:381-383)
         if c.kind == "tool":
             v = collide_tool(c, p.eps, p.dt, pos, v).astype(dt)
@@ -669,7 +768,7 @@ def substep(p: Params, mats: list[Material], st: dict, return_grid: bool = False
     """One full substep: p2g, grid op, g2p.  ``st`` is not modified."""
     gm, gp, F_new, Jp_new = p2g(p, mats, st)
     colliders = st.get("colliders")
-    vel = grid_op(p, gm, gp, colliders)
+    vel = grid_op(p, gm, gp, colliders, force_fields=st.get("force_fields"))
     xn, vn, Cn = g2p(p, st, vel)
     out = dict(st)
     out.update(x=xn, v=vn, C=Cn, F=F_new, Jp=Jp_new)

@@ -14,12 +14,13 @@
     } while (0)
 
 int main(void) {
-    int32_t sizes[6];
+    int32_t sizes[7];
     CHECK(mpm_abi_version() == MPM_ABI_VERSION, "abi version");
     CHECK(mpm_struct_sizes(sizes) == MPM_OK, "struct sizes call");
     CHECK(sizes[0] == (int32_t)sizeof(mpm_instance) && sizes[1] == (int32_t)sizeof(mpm_material) &&
               sizes[2] == (int32_t)sizeof(mpm_problem) && sizes[3] == (int32_t)sizeof(mpm_particles) &&
-              sizes[4] == (int32_t)sizeof(mpm_tables) && sizes[5] == (int32_t)sizeof(mpm_collider),
+              sizes[4] == (int32_t)sizeof(mpm_tables) && sizes[5] == (int32_t)sizeof(mpm_collider) &&
+              sizes[6] == (int32_t)sizeof(mpm_force_field),
           "struct layout seen from C");
     int32_t max_chunks = 0;
     CHECK(mpm_max_chunks(100000, 4913, 128, &max_chunks) == MPM_OK && max_chunks >= 100000 / 128, "max chunks");

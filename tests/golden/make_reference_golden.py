@@ -22,6 +22,13 @@ runs are float64 (the reference's ``precision="64"``).  Written here:
   ref_cube.npz         an Elastic cube (E 1e5, nu 0.3, rho 1000: the 32,768-particle benchmark
                        cube's material) of 216 jittered lattice particles thrown at the floor of
                        a 64-per-metre grid, dt 1e-4: state after 1, 20 and 60 substeps.
+  ref_force_fields.npz the reference's force fields (engine/force_fields.py: Constant, Wind,
+                       Point, Drag, Vortex, Turbulence seeded and unseeded) through their own
+                       get_acc at 96 random positions and velocities each, and a scene of two
+                       blocks (Elastic, Liquid) under Constant + Vortex + Turbulence + Drag +
+                       Point + Wind stepped by MPMSolver + LegacyCoupler (the fields enter
+                       mpm_grid_op, legacy_coupler.py:377-379): state after 1, 5 and 15
+                       substeps, precision-32 model.
   ref_functions_m32.npz, ref_mixed_m32.npz, ref_cube_m32.npz
                        the same with the reference's precision-32 model in float64
                        arithmetic: gs.EPS = float32 epsilon (genesis/__init__.py:205-206, the
@@ -236,6 +243,74 @@ def cube_fixture(ref, seed=22):
     return meta, inputs, rec
 
 
+# (class name, kwargs) of the force-field fixtures; every field is activated
+FORCE_FIELDS = [
+    ("Constant", dict(direction=(1.0, -2.0, 0.5), strength=2.5)),
+    ("Wind", dict(direction=(0.0, 1.0, 0.2), strength=3.0, radius=0.35, center=(0.45, 0.0, 0.5))),
+    ("Point", dict(strength=-2.0, position=(0.5, 0.45, 0.55), falloff_pow=1.5, flow=0.3)),
+    ("Drag", dict(linear=0.4, quadratic=0.25)),
+    ("Vortex", dict(center=(0.42, 0.5, 0.0), strength_perpendicular=5.0, strength_radial=1.0, falloff_pow=2.0,
+                    falloff_min=0.05, falloff_max=0.8, damping=0.1)),
+    ("Vortex", dict(center=(0.5, 0.5, 0.0))),
+    ("Turbulence", dict(strength=2.0, frequency=3, flow=0.1, seed=7)),
+    ("Turbulence", dict(strength=1.0, frequency=5)),
+]
+FIELDS_IN_SCENE = [
+    ("Constant", dict(direction=(0.0, 0.0, 1.0), strength=3.0)),
+    ("Vortex", dict(center=(0.25, 0.25, 0.0), strength_perpendicular=8.0, strength_radial=2.0, falloff_pow=2.0,
+                    falloff_min=0.02, falloff_max=0.4, damping=0.2)),
+    ("Turbulence", dict(strength=4.0, frequency=6, flow=0.2, seed=3)),
+    ("Drag", dict(linear=0.5, quadratic=0.3)),
+    ("Point", dict(strength=1.5, position=(0.3, 0.2, 0.3), falloff_pow=1.0, flow=0.1)),
+    ("Wind", dict(direction=(1.0, 0.0, 0.0), strength=2.0, radius=0.05, center=(0.25, 0.25, 0.25))),
+]
+
+
+def force_field_fixture(ref, seed=23):
+    ff = T._load("genesis.engine.force_fields", os.path.join(ref.root, "genesis", "engine", "force_fields.py"))
+    rng = np.random.default_rng(seed)
+    n = 96
+    out = {}
+    for k, (name, kw) in enumerate(FORCE_FIELDS):
+        f = getattr(ff, name)(**kw)
+        f.activate()
+        pos = rng.uniform(-0.2, 1.2, size=(n, 3))
+        vel = rng.normal(0.0, 1.0, size=(n, 3))
+        acc = np.stack([np.asarray(f.get_acc(np.asarray(pos[i]).view(T.TiArr), np.asarray(vel[i]).view(T.TiArr),
+                                                 0.0, -1)) for i in range(n)])
+        out.update({f"f{k}_pos": pos, f"f{k}_vel": vel, f"f{k}_acc": acc})
+    # a scene under several fields at once, stepped by the reference's solver and coupler
+    specs = [(("elastic", dict(E=2e4, nu=0.3)), rng.uniform(0.18, 0.3, size=(60, 3))),
+             (("liquid", dict(E=1e5, nu=0.2)), rng.uniform(0.2, 0.32, size=(60, 3)))]
+    blocks = [(ref_material(ref, k, kw), pos) for (k, kw), pos in specs]
+    density, upper, psize, dt, grav = 32, (0.5, 0.5, 0.5), 0.01, 5e-4, (0.0, 0.0, -9.8)
+    sc = T.Scene(ref, density, (0.0, 0.0, 0.0), upper, psize, dt, grav, blocks)
+    N = sum(p.shape[0] for _, p in specs)
+    vel = rng.normal(0.0, 0.3, size=(N, 3))
+    sc.set_state(vel=vel)
+    for name, kw in FIELDS_IN_SCENE:
+        f = getattr(ff, name)(**kw)
+        f.activate()
+        sc.solver._ffs.append(f)
+    snaps = [1, 5, 15]
+    done = 0
+    for s_ in snaps:
+        while done < s_:
+            sc.substep()
+            done += 1
+        st = sc.state()
+        for a, b in (("x", "pos"), ("v", "vel"), ("F", "F")):
+            out[f"scene_{a}_{s_}"] = st[b]
+    out["scene_pos"] = np.concatenate([p for _, p in specs])
+    out["scene_vel"] = vel
+    out["scene_mat_idx"] = np.repeat(np.arange(len(specs)), [p.shape[0] for _, p in specs])
+    meta = dict(eps=ref.gs.EPS, fields=[[nm, kw] for nm, kw in FORCE_FIELDS],
+                scene=dict(fields=[[nm, kw] for nm, kw in FIELDS_IN_SCENE],
+                           materials=[[k, kw] for (k, kw), _ in specs], grid_density=density, upper_bound=list(upper),
+                           particle_size=psize, dt=dt, gravity=list(grav), snapshots=snaps))
+    return meta, out
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GENESIS_REFERENCE", "/root/reference")
     ref = T.Reference(root, precision="64")
@@ -251,6 +326,10 @@ def main():
             meta["name"] += suffix
             np.savez_compressed(os.path.join(HERE, f"{meta['name']}.npz"), meta=np.array(json.dumps(meta)),
                                 **inputs, **rec)
+    ref.gs.EPS = float(np.finfo(np.float32).eps)
+    meta, out = force_field_fixture(ref)
+    np.savez_compressed(os.path.join(HERE, "ref_force_fields.npz"), meta=np.array(json.dumps(meta)), **out)
+    print("ref_force_fields")
     ref.gs.EPS = eps64
 
 

@@ -78,6 +78,9 @@ class TiArr(np.ndarray):
     def dot(self, other):
         return np.sum(np.asarray(self) * np.asarray(other))
 
+    def cross(self, other):
+        return np.cross(np.asarray(self), np.asarray(other)).view(TiArr)
+
     def outer_product(self, other):
         return np.multiply.outer(np.asarray(self), np.asarray(other)).view(TiArr)
 
@@ -166,6 +169,8 @@ def template(*a, **k):
 
 # ----------------------------------------------------------------------------- fields
 def _flat_index(key):
+    if key is None:  # field[None]: the element of a 0-d field
+        return ()
     if not isinstance(key, tuple):
         key = (key,)
     out = []
@@ -510,6 +515,7 @@ class Reference:
     """The reference's MPM classes, imported unchanged from a Genesis checkout at `root`."""
 
     def __init__(self, root: str, precision: str = "64"):
+        self.root = root
         self.gs = install(precision)
         g = os.path.join(root, "genesis", "engine")
         bnd = _load("genesis.engine.boundaries.boundaries", os.path.join(g, "boundaries", "boundaries.py"))

@@ -39,10 +39,11 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
 
 def test_abi_and_struct_layout(lib):
     assert lib.mpm_abi_version() == nat.ABI_VERSION
-    sizes = (C.c_int32 * 6)()
+    sizes = (C.c_int32 * 7)()
     assert lib.mpm_struct_sizes(sizes) == 0
     assert tuple(sizes) == (C.sizeof(nat.Instance), C.sizeof(nat.Material), C.sizeof(nat.Problem),
-                            C.sizeof(nat.Particles), C.sizeof(nat.Tables), C.sizeof(nat.Collider))
+                            C.sizeof(nat.Particles), C.sizeof(nat.Tables), C.sizeof(nat.Collider),
+                            C.sizeof(nat.ForceField))
 
 
 def _prob(n=1000, nb=512, P=256):

@@ -1,0 +1,164 @@
+"""External force fields in the grid op on the GPU (engine/force_fields.py,
+legacy_coupler.py:377-379): a scene under six fields at once against the fixture made by the
+reference's own code, activation through gs.Scene, the Noise field's counter-based draws, and
+the adjoint through the fields' velocity terms against the float64 oracle."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import genesis_b200 as gs
+from genesis_b200 import force_fields as gff
+from genesis_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_scene_under_force_fields_matches_reference():
+    """Constant, Vortex, Turbulence, Drag, Point and Wind together on an Elastic and a Liquid
+    block (tests/golden/ref_force_fields.npz, the reference's precision-32 model).  Tolerances:
+    positions 1e-5 m, F 1e-5, velocities 1e-4 m/s (float32 kernels against float64)."""
+    from genesis_b200.engine.runtime import MPMRuntime, spec_from_desc
+    from genesis_b200.materials import MPM
+
+    z = np.load(os.path.join(HERE, "ref_force_fields.npz"))
+    meta = json.loads(str(z["meta"]))
+    sc = meta["scene"]
+    d = W.SceneDesc(name="ref_force_fields", grid_density=sc["grid_density"], particle_size=sc["particle_size"],
+                    dt=sc["dt"], n_substeps=sc["snapshots"][-1], pos=z["scene_pos"], vel=z["scene_vel"],
+                    mat_idx=z["scene_mat_idx"], materials=[(k, dict(kw)) for k, kw in sc["materials"]],
+                    upper_bound=tuple(sc["upper_bound"]), gravity=tuple(sc["gravity"]))
+    spec = spec_from_desc(d, W.make_materials(d, MPM))
+    objs = [getattr(gff, n)(**kw) for n, kw in sc["fields"]]
+    for o in objs:
+        o.activate()
+    rows, perm = gff.pack(objs)
+    rt = MPMRuntime([spec], use_graphs=False, force_fields=rows, ff_perm=perm)
+    rt.init_particles(d.pos, d.mat_idx, vel=d.vel)
+    done = 0
+    for n in sc["snapshots"]:
+        rt.substeps(n - done)
+        done = n
+        st = rt.get_state(("pos", "vel", "F"))
+        torch.cuda.synchronize()
+        g = {k: v.cpu().numpy().astype(np.float64) for k, v in st.items()}
+        ex = np.abs(g["pos"] - z[f"scene_x_{n}"]).max()
+        ev = np.abs(g["vel"] - z[f"scene_v_{n}"]).max()
+        eF = np.abs(g["F"] - z[f"scene_F_{n}"]).max()
+        print(f"\n[reference] force fields after {n}: |dx| {ex:.2e} |dv| {ev:.2e} |dF| {eF:.2e}")
+        assert ex < 1e-5 and eF < 1e-5 and ev < 1e-4, (n, ex, ev, eF)
+    assert rt.status() == 0
+
+
+def _scene(fields, requires_grad=False, substeps=5):
+    gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+    scene = gs.Scene(
+        sim_options=gs.options.SimOptions(dt=2.5e-3, substeps=substeps, gravity=(0, 0, -9.8),
+                                          requires_grad=requires_grad),
+        mpm_options=gs.options.MPMOptions(lower_bound=(0, 0, 0), upper_bound=(0.5, 0.5, 0.5), grid_density=32,
+                                          particle_size=0.01),
+    )
+    block = scene.add_entity(gs.morphs.Box(lower=(0.18, 0.18, 0.2), upper=(0.3, 0.3, 0.3)),
+                             material=gs.materials.MPM.Elastic(E=2e4, nu=0.3))
+    for f in fields:
+        scene.add_force_field(f)
+    scene.build()
+    return scene, block
+
+
+def test_activation_through_the_scene():
+    """A Constant field of 9.8 m/s^2 upwards cancels gravity while active (fields start
+    inactive, force_fields.py:18-32); add_force_field after build and Custom are refused."""
+    up = gff.Constant(direction=(0, 0, 1), strength=9.8)
+    scene, block = _scene([up])
+    assert not up.active
+    scene.step()
+    v1 = block.get_particles_vel().mean(0).cpu().numpy()
+    assert v1[2] < -0.1  # falling: the field is off
+    up.activate()
+    for _ in range(3):
+        scene.step()
+    v2 = block.get_particles_vel().mean(0).cpu().numpy()
+    assert abs(v2[2] - v1[2]) < 2e-3  # no net acceleration while active
+    up.deactivate()
+    scene.step()
+    v3 = block.get_particles_vel().mean(0).cpu().numpy()
+    assert v3[2] < v2[2] - 0.1
+    with pytest.raises(gs.GenesisException):
+        scene.add_force_field(gff.Drag(linear=1.0))
+    with pytest.raises(gs.GenesisException):
+        gs.init(backend=gs.gpu, precision="32", seed=0, logging_level="warning")
+        gs.Scene().add_force_field(gff.Custom(lambda pos, vel, t, i: pos))
+
+
+def test_noise_is_reproducible_and_centred():
+    def run(seed):
+        nz = gff.Noise(strength=40.0, seed=seed)
+        nz.activate()
+        scene, block = _scene([nz])
+        x0 = block.get_particles_pos().clone()
+        for _ in range(4):
+            scene.step()
+        return block.get_particles_pos(), block.get_particles_vel(), x0
+
+    a, va, x0 = run(1)
+    b, vb, _ = run(1)
+    c, _, _ = run(2)
+    assert torch.equal(a, b)  # the same draws for the same seed
+    assert (a - c).abs().max() > 1e-5  # other draws for another seed
+    scene, block = _scene([])
+    for _ in range(4):
+        scene.step()
+    free_v = block.get_particles_vel()
+    dv = (va - free_v).cpu().numpy()
+    # 20 substeps of uniform kicks of +-40 * 2.5e-3 / 5 m/s per node: the block's mean velocity
+    # moves far less than one kick, the particles' spread shows them
+    assert np.abs(dv.mean(0)).max() < 0.3 * 40 * 5e-4 * 20 ** 0.5
+    assert dv.std() > 1e-3
+
+
+def test_gradient_through_force_fields_matches_oracle():
+    """dL/dv0 of L = sum W . x after 3 steps (15 substeps) of a block under Drag, Vortex damping,
+    Point and Turbulence flow, against the float64 adjoint oracle (the fields' v-terms by
+    complex steps; tests/test_force_fields_host.py checks it against central differences)."""
+    from oracle import mpm_adjoint as A
+    from oracle import mpm_ref as R
+
+    spec = [("Drag", dict(linear=0.8, quadratic=0.5)),
+            ("Vortex", dict(center=(0.25, 0.25, 0.0), strength_perpendicular=8.0, strength_radial=2.0,
+                            falloff_min=0.02, falloff_max=0.4, damping=0.6)),
+            ("Point", dict(strength=1.5, position=(0.3, 0.2, 0.3), falloff_pow=1.0, flow=0.7)),
+            ("Turbulence", dict(strength=4.0, frequency=6, flow=0.9, seed=3))]
+    objs = [getattr(gff, n)(**kw) for n, kw in spec]
+    for o in objs:
+        o.activate()
+    scene, block = _scene(objs, requires_grad=True)
+    n = block.n_particles
+    W_ = np.random.default_rng(4).normal(size=(n, 3))
+    v0 = torch.tensor([0.3, -0.2, -0.5], device="cuda", requires_grad=True)
+    block.set_velocity(v0)
+    for _ in range(3):
+        scene.step()
+    pos = scene.get_state().solvers_state[3].pos
+    loss = (pos * torch.as_tensor(W_, dtype=torch.float32, device="cuda")).sum()
+    loss.backward()
+    g = v0.grad.cpu().numpy()
+
+    p = R.Params(grid_density=32, upper_bound=(0.5, 0.5, 0.5), particle_size=0.01, dt=5e-4, dtype=np.float64)
+    p.eps = float(np.finfo(np.float32).eps)
+    mats = [R.make_material("elastic", E=2e4, nu=0.3)]
+    x0 = np.asarray(block.init_particles, dtype=np.float64)
+    st = R.make_state(x0, mats, np.zeros(n, np.int64), np.float64, v=np.tile([0.3, -0.2, -0.5], (n, 1)))
+    st["force_fields"] = [R.make_force_field(nm, **kw) for nm, kw in spec]
+    mu, lam = np.full(n, mats[0].mu), np.full(n, mats[0].lam)
+    lo, vbar, _, _ = A.rollout_colliders(p, mats, st, mu, lam, [], np.zeros((15, 0, 3)), W_)
+    go = vbar.sum(0)
+    err = np.abs(g - go).max() / np.abs(go).max()
+    print(f"\n[grad] force fields: loss {float(loss):.6e} (oracle {lo:.6e}); dL/dv0 {g} (oracle {go}), rel. err {err:.1e}")
+    assert abs(float(loss) - lo) <= 1e-4 * abs(lo)
+    assert err <= 2e-3
