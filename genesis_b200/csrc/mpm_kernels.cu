@@ -1796,7 +1796,10 @@ __device__ __forceinline__ void apply_force_fields(const mpm_force_field* __rest
     }
 }
 
-// at most 64 registers (4 CTAs per SM): the collider responses, rare, may spill instead
+// at most 64 registers (4 CTAs per SM): the collider responses, rare, may spill instead.
+// FF: the problem has force fields (a separate instantiation keeps their registers out of
+// the common path)
+template <bool FF>
 __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_instance* __restrict__ inst, Ws w,
                                                  const mpm_collider* __restrict__ colliders, int n_colliders,
                                                  float* collider_force, const float* __restrict__ sdf_voxels,
@@ -1825,7 +1828,7 @@ __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_
             const float px = (float)(bc.bx * BLK + lx + I.lower_cell[0]) * I.dx;
             const float py = (float)(bc.by * BLK + ly + I.lower_cell[1]) * I.dx;
             const float pz = (float)(bc.bz * BLK + lz + I.lower_cell[2]) * I.dx;
-            if (n_ff > 0) {  // external force fields (legacy_coupler.py:377-379)
+            if (FF && n_ff > 0) {  // external force fields (legacy_coupler.py:377-379)
                 const float p[3] = {px, py, pz};
                 float v[3] = {vx, vy, vz};
                 apply_force_fields(ffs, n_ff, ff_perm, I.eps, I.dt, p, v, g, ops);
@@ -1990,7 +1993,7 @@ static const DevInfo* dev_info() {
         d.occ_g2p2g[1] = occ_of<256>(k_g2p2g<256, false, false>);
         d.occ_g2p2g[2] = occ_of<512>(k_g2p2g<512, false, false>);
         int n = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_op<false>, 256, 0);
         d.occ_grid = n > 0 ? n : 1;
         d.sms = sms > 0 ? sms : 1;
     }
@@ -2129,9 +2132,14 @@ static int launch_grid_op(const mpm_problem* prob, const mpm_tables* tab, void* 
     const int nc = tab->colliders ? tab->n_colliders : 0;
     if (tab->n_force_fields < 0 || (tab->n_force_fields > 0 && !tab->force_fields)) return MPM_E_INVALID;
     const int nff = tab->force_fields ? tab->n_force_fields : 0;
-    k_grid_op<<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc,
-                                    advance ? tab->collider_force : nullptr, tab->sdf_voxels, tab->force_fields, nff,
-                                    tab->ff_perm, advance ? 1 : 0);
+    if (nff > 0)
+        k_grid_op<true><<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc,
+                                              advance ? tab->collider_force : nullptr, tab->sdf_voxels,
+                                              tab->force_fields, nff, tab->ff_perm, advance ? 1 : 0);
+    else
+        k_grid_op<false><<<ctas, 256, 0, s>>>(*prob, tab->instances, ws_of(*prob, ws), tab->colliders, nc,
+                                               advance ? tab->collider_force : nullptr, tab->sdf_voxels, nullptr, 0,
+                                               nullptr, advance ? 1 : 0);
     if (nc > 0 && advance)
         k_advance_colliders<<<(nc + 63) / 64, 64, 0, s>>>(tab->instances, prob->n_instances, tab->colliders, nc);
     return cuda_ok();

@@ -1,7 +1,9 @@
 """External force fields in the grid op on the GPU (engine/force_fields.py,
 legacy_coupler.py:377-379): a scene under six fields at once against the fixture made by the
 reference's own code, activation through gs.Scene, the Noise field's counter-based draws, and
-the adjoint through the fields' velocity terms against the float64 oracle."""
+the adjoint through the fields' velocity terms against the float64 oracle.  Runs are not
+bitwise reproducible (the grid flush's float reductions have no fixed order), so reproducibility
+is checked to round-off."""
 
 import json
 import os
@@ -79,7 +81,7 @@ def test_activation_through_the_scene():
     assert not up.active
     scene.step()
     v1 = block.get_particles_vel().mean(0).cpu().numpy()
-    assert v1[2] < -0.1  # falling: the field is off
+    assert v1[2] < -0.9 * 9.8 * 2.5e-3  # falling under gravity for one 2.5 ms step: the field is off
     up.activate()
     for _ in range(3):
         scene.step()
@@ -88,7 +90,7 @@ def test_activation_through_the_scene():
     up.deactivate()
     scene.step()
     v3 = block.get_particles_vel().mean(0).cpu().numpy()
-    assert v3[2] < v2[2] - 0.1
+    assert v3[2] < v2[2] - 0.9 * 9.8 * 2.5e-3
     with pytest.raises(gs.GenesisException):
         scene.add_force_field(gff.Drag(linear=1.0))
     with pytest.raises(gs.GenesisException):
@@ -109,8 +111,11 @@ def test_noise_is_reproducible_and_centred():
     a, va, x0 = run(1)
     b, vb, _ = run(1)
     c, _, _ = run(2)
-    assert torch.equal(a, b)  # the same draws for the same seed
-    assert (a - c).abs().max() > 1e-5  # other draws for another seed
+    # the same draws for the same seed (up to the order of the flush's float reductions,
+    # which is not fixed), other draws for another seed
+    same, other = float((a - b).abs().max()), float((a - c).abs().max())
+    print(f"\n[force fields] noise: same seed max|dx| {same:.2e}, other seed {other:.2e}")
+    assert same < 1e-6 and other > 100 * max(same, 1e-8)
     scene, block = _scene([])
     for _ in range(4):
         scene.step()

@@ -12,7 +12,10 @@ isolated, one per 4^3 block, C = 0, so F_tmp = F exactly):
   to 1e-4 s_j + 2^-20 s_0.
 * Snow with its lower clamp at 0.5 (yield_lower = 0.5) writes Jp_new = Jp prod_i s_i / 0.5
   over the singular values below 0.5 (snow.py:62-70): the small singular values' relative
-  error, in float32 relative precision.  Held to 1e-5 relative per clamped singular value.
+  error, in float32 relative precision.  Held per clamped singular value to 1e-5 relative or
+  2^-22 s_0 / s_i, whichever is larger: a float32 SVD of A cannot resolve s_i better than a few
+  ulps of s_0 (forming A V alone rounds at that level), and that floor is 2.4e-4 relative at
+  s_i = 1e-3 s_0 (measured: 2e-5).
 
 Cases: singular values (1, 1e-2, 1e-3), (1, 1, 1e-3), (1.2, 1e-2, 1e-2 (1 + 1e-4)), nearly
 repeated (1, 1 + 1e-6, 0.5) and the well-conditioned range of the benchmark scenes
@@ -109,4 +112,7 @@ def test_svd_reconstruction_on_ill_conditioned_F():
         assert rec < 3e-6, (name, rec)
         assert ok_s.all(), (name, (dE / s[sel]).max(0))
         assert leak.max() <= 1.0, (name, leak.max())
-        assert (jrel <= 1e-5 * np.maximum(n_low, 1)).all(), (name, jrel.max())
+        # each clamped s_i's relative error: 1e-5, or float32's own floor for it, a few ulps of
+        # s_0 over s_i (forming B = A V in float32 already costs that), whichever is larger
+        bound = np.where(low[sel], np.maximum(1e-5, 2.0**-22 * s0 / s[sel]), 0.0).sum(1)
+        assert (jrel <= np.maximum(bound, 1e-6)).all(), (name, jrel.max(), bound.max())
