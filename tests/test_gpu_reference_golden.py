@@ -22,8 +22,10 @@ float32 C restatement's own deviation, plus 1e-6 m/s (velocities reach 1.7 m/s w
 70 /s in the random mixed scene, where float32 itself deviates by ~1e-5 m/s); grid mass and
 momentum totals 1e-6 relative, per node 1e-5 of the largest node; F_new 2e-6 and Jp_new 2e-6
 relative to the largest entry of each variant; stress (through the momentum it scatters) 1e-5
-of each particle's largest node value plus the shared tile's fixed-point resolution, 2^-22 of
-the chunk's payload bound per contribution (asserted at 2^-21).
+of each particle's largest node value, or 4x the float32 C restatement's own stress error where
+that is larger (a yielding von Mises particle's stress hangs on s_new - 1 ~ 1e-2, which a
+float32 SVD's singular values leave ~1e-5 uncertain), plus the shared tile's fixed-point
+resolution, 2^-22 of the chunk's payload bound per contribution (asserted at 2^-21).
 """
 
 import json
@@ -90,6 +92,30 @@ def test_material_functions_and_stress_match_reference():
     grid = _dense(rt)
     lo = np.round(density * np.asarray(d.lower_bound)).astype(int)
     scale = -dt * (psize**3 * 1e3) * 4 * density * density
+    # the float32 C restatement on the same isolated particles: after one substep an isolated
+    # particle's C is A / m = scale * stress / m (the B-spline's moments), so its stress is
+    # read back as C m / scale; its deviation from the fixture is float32's own, with its own
+    # float32 SVD (near a yield surface the stress depends on s_new - 1 ~ 1e-2, so the SVD's
+    # few-ulp singular values already cost ~1e-5 of it)
+    from oracle import cref
+    from oracle import mpm_ref as R
+
+    p32 = R.Params(grid_density=density, particle_size=psize, dt=dt, gravity=(0.0, 0.0, 0.0), dtype=np.float32)
+    p32.eps = float(np.finfo(np.float32).eps)
+    mats32 = [R.make_material(k, **dict(kw)) for k, kw in variants]
+    st32 = R.make_state(pos, mats32, mat_idx, np.float32)
+    st32.update(F=F0.astype(np.float32), Jp=Jp0.astype(np.float32))
+    if mus:
+        actu32 = np.zeros(nv * n, np.float32)
+        mdir32 = np.tile(np.float32([0, 0, 1]), (nv * n, 1))
+        for v in mus:
+            actu32[v * n:(v + 1) * n] = z[f"m{v}_actu"]
+            mdir32[v * n:(v + 1) * n] = z[f"m{v}_mdir"]
+        st32.update(actu=actu32, mdir=mdir32)
+    out32, rc32 = cref.substeps(p32, mats32, st32, 1)
+    assert rc32 == 0
+    mass = np.array([R.particle_mass(p32, mats32[k]) for k in mat_idx])
+    stress32 = out32["C"].astype(np.float64) * (mass / scale)[:, None, None]
     for v in range(nv):
         sl = slice(v * n, (v + 1) * n)
         want_F, want_Jp, want_s = z[f"m{v}_F_new"], z[f"m{v}_Jp_new"], z[f"m{v}_stress"]
@@ -115,9 +141,12 @@ def test_material_functions_and_stress_match_reference():
         # the tile's payload bound of each particle (v = 0, C = 0): 1.5 dx max_i sum_j |A_ij|
         bound = 1.5 * dx * np.abs(scale * want_s).sum(axis=2).max(axis=1)
         err = np.abs(got - want).max(axis=(0, 2))
-        tol = 1e-5 * np.abs(want).max(axis=(0, 2)) + 2.0**-21 * bound
+        # float32's own deviation, in node-momentum units (w <= 1, |dpos| <= 1.5 dx per axis)
+        e32 = 1.5 * dx * np.abs(scale * (stress32[sl] - want_s)).sum(axis=2).max(axis=1)
+        tol = np.maximum(1e-5 * np.abs(want).max(axis=(0, 2)), 4 * e32) + 2.0**-21 * bound
         print(f"\n[reference] {variants[v][0]} {variants[v][1]}: F_new {eF:.1e}, Jp_new {eJ:.1e}, stress "
-              f"max err / tol {float((err / tol).max()):.2f}")
+              f"max err / tol {float((err / tol).max()):.2f} (float32 C restatement: max rel. stress err "
+              f"{float((np.abs(stress32[sl] - want_s).max(axis=(1, 2)) / np.abs(want_s).max(axis=(1, 2))).max()):.1e})")
         assert (err <= tol).all(), (variants[v], float((err / tol).max()))
 
 
