@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 11
+ABI_VERSION = 12
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -240,6 +240,7 @@ SIGNATURES = {
     "mpm_update_render_fields": (C.c_int, [_P(Problem), _P(Particles), i32, i32, vp, vp, vp, i32, i32, vp, vp, vp,
                                            vp, vp]),
     "mpm_sdf_voxelize": (C.c_int, [vp, i32, vp, i32, i32, C.c_float, vp, vp]),
+    "mpm_sdf_grid": (C.c_int, [vp, i32, vp, i32, _P(C.c_float), _P(C.c_float), _P(C.c_int32), vp, vp]),
     "mpm_graph_create": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, i32, i64, vp, _P(vp)]),
     "mpm_graph_launch": (C.c_int, [vp, vp]),
     "mpm_graph_destroy": (C.c_int, [vp]),

@@ -557,7 +557,7 @@ __device__ __forceinline__ void sdf_sampled(const mpm_collider& c, const float* 
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const float half = 0.5f * (float)(r[d] - 1);
-        ps[d] = c.sdf_scale[d] * l[d] + half;
+        ps[d] = c.sdf_scale[d] * (l[d] - c.data[d]) + half;  // data: the grid's centre, geom frame
         dc[d] = ps[d] - half;
         outside = outside || ps[d] >= (float)(r[d] - 1) || ps[d] <= 0.f;
     }
@@ -2264,14 +2264,24 @@ __device__ __forceinline__ float tri_solid_angle(const float* p, const float* a,
 
 constexpr int SDF_T = 256;
 
-__global__ void __launch_bounds__(SDF_T) k_sdf_voxelize(const float* __restrict__ V, int nv, const int* __restrict__ Fc,
-                                                        int nf, int res, float radius, float* __restrict__ out) {
+// Signed distance of a closed triangle mesh at the nodes of an axis-aligned grid (node (i, j, k)
+// at origin + (i, j, k) * step, x-major): the nearest-triangle distance, negative where the
+// generalised winding number exceeds 1/2.  Faces are staged through shared memory SDF_T at a time.
+struct SdfGrid {
+    float origin[3];
+    float step[3];
+    int res[3];
+};
+
+__global__ void __launch_bounds__(SDF_T) k_sdf_grid(const float* __restrict__ V, int nv, const int* __restrict__ Fc,
+                                                    int nf, SdfGrid G, float* __restrict__ out) {
     __shared__ float tri[SDF_T][9];
-    const int64_t n = (int64_t)res * res * res;
+    const int64_t n = (int64_t)G.res[0] * G.res[1] * G.res[2];
     const int64_t vid = (int64_t)blockIdx.x * SDF_T + threadIdx.x;
-    const int i = (int)(vid / ((int64_t)res * res)), j = (int)((vid / res) % res), k = (int)(vid % res);
-    const float step = 2.f * radius / (float)(res - 1);
-    const float p[3] = {-radius + step * (float)i, -radius + step * (float)j, -radius + step * (float)k};
+    const int i = (int)(vid / ((int64_t)G.res[1] * G.res[2])), j = (int)((vid / G.res[2]) % G.res[1]),
+              k = (int)(vid % G.res[2]);
+    const float p[3] = {G.origin[0] + G.step[0] * (float)i, G.origin[1] + G.step[1] * (float)j,
+                        G.origin[2] + G.step[2] * (float)k};
     float d2 = 3.402823466e38f, wind = 0.f;
     for (int f0 = 0; f0 < nf; f0 += SDF_T) {
         const int f = f0 + threadIdx.x;
@@ -2852,9 +2862,34 @@ int mpm_sdf_voxelize(const float* vertices, int32_t n_verts, const int32_t* face
                      float radius, float* out, void* stream) {
     if (!vertices || !faces || !out || n_verts < 3 || n_faces < 1 || res < 2 || res > 1024 || !(radius > 0.f))
         return MPM_E_INVALID;
+    SdfGrid G;
+    const float step = 2.f * radius / (float)(res - 1);
+    for (int d = 0; d < 3; ++d) {
+        G.origin[d] = -radius;
+        G.step[d] = step;
+        G.res[d] = res;
+    }
     const int64_t n = (int64_t)res * res * res;
-    k_sdf_voxelize<<<(unsigned)((n + SDF_T - 1) / SDF_T), SDF_T, 0, (cudaStream_t)stream>>>(vertices, n_verts, faces,
-                                                                                          n_faces, res, radius, out);
+    k_sdf_grid<<<(unsigned)((n + SDF_T - 1) / SDF_T), SDF_T, 0, (cudaStream_t)stream>>>(vertices, n_verts, faces,
+                                                                                      n_faces, G, out);
+    return cuda_ok();
+}
+
+int mpm_sdf_grid(const float* vertices, int32_t n_verts, const int32_t* faces, int32_t n_faces, const float* origin,
+                 const float* step, const int32_t* res, float* out, void* stream) {
+    if (!vertices || !faces || !out || !origin || !step || !res || n_verts < 3 || n_faces < 1) return MPM_E_INVALID;
+    SdfGrid G;
+    int64_t n = 1;
+    for (int d = 0; d < 3; ++d) {
+        if (res[d] < 1 || res[d] > 4096 || !(step[d] >= 0.f)) return MPM_E_INVALID;
+        G.origin[d] = origin[d];
+        G.step[d] = step[d];
+        G.res[d] = res[d];
+        n *= res[d];
+    }
+    if (n > (int64_t)1 << 30) return MPM_E_CAPACITY;
+    k_sdf_grid<<<(unsigned)((n + SDF_T - 1) / SDF_T), SDF_T, 0, (cudaStream_t)stream>>>(vertices, n_verts, faces,
+                                                                                      n_faces, G, out);
     return cuda_ok();
 }
 

@@ -172,13 +172,21 @@ class Mesh(Morph):
     box lattice over the scaled mesh's bounds, of which the points inside the closed mesh are
     kept; inside is an exact even-odd ray test here (the reference keeps points with a
     negative winding-number signed distance, which is the same set for a closed mesh).
-    Fields of the reference's Mesh that only matter to rigid bodies or to the renderer
-    (decimate, convexify, coacd_options, group_by_material, ...) are accepted and ignored."""
+    `convexify` and `decompose_object_error_threshold` choose a rigid entity's collision geom
+    (engine/rigid.py); the other fields of the reference's Mesh that only matter to rigid
+    bodies or to the renderer (decimate, coacd_options, group_by_material, ...) are accepted
+    and ignored."""
 
-    def __init__(self, file, scale=1.0, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, **kw):
+    def __init__(self, file, scale=1.0, pos=(0.0, 0.0, 0.0), euler=(0.0, 0.0, 0.0), quat=None, convexify=None,
+                 decompose_object_error_threshold=0.15, **kw):
         super().__init__(pos=pos, euler=euler, quat=quat, **kw)
         from . import mesh as _mesh
 
+        # read by rigid entities (options/morphs.py:505-565): a collision geom is the mesh's
+        # convex hull unless that is convexify=False or the hull's volume error is above the
+        # threshold (the reference then decomposes the mesh into convex parts)
+        self.convexify = convexify
+        self.decompose_object_error_threshold = float(decompose_object_error_threshold)
         self.file = str(file)
         if not self.file.lower().endswith(".obj"):
             raise GenesisException(f"Unsupported mesh file (only .obj is read): {self.file}")

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 11
+#define MPM_ABI_VERSION 12
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -182,8 +182,9 @@ typedef struct mpm_particles {
  * rigid_geom.py:147-225): sdf_res3[0] x sdf_res3[1] x sdf_res3[2] values (x-major) at
  * sdf_offset in mpm_tables.sdf_voxels, followed by the same number of gradient triples
  * [n][3] (central differences of 1e-2 cell of the true distance, as _compute_sd_grad takes
- * them).  Voxel coordinate = sdf_scale * (geom-frame point) + (sdf_res3 - 1) / 2; inside the
- * grid the distance and the gradient are trilinear; outside it (any coordinate <= 0 or >=
+ * them).  Voxel coordinate = sdf_scale * (geom-frame point - data) + (sdf_res3 - 1) / 2, data
+ * the grid's centre in the geom frame (the centre of the geom's vertex bounds, 0 for a box);
+ * inside the grid the distance and the gradient are trilinear; outside it (any coordinate <= 0 or >=
  * res - 1) the proxy |voxel - centre| / sdf_cell + sdf_max and the direction to the centre.
  * Then the same coupling as MPM_COLLIDER_BOX. */
 #define MPM_COLLIDER_SDF 4
@@ -506,6 +507,15 @@ int mpm_update_render_fields(const mpm_problem* prob, const mpm_particles* par, 
  * faces int32 [n_faces][3]; out float [res^3], all device. */
 int mpm_sdf_voxelize(const float* vertices, int32_t n_verts, const int32_t* faces, int32_t n_faces, int32_t res,
                      float radius, float* out, void* stream);
+/* Signed distance of a closed triangle mesh (device vertices [n_verts][3], faces [n_faces][3])
+ * at the nodes of an axis-aligned grid: node (i, j, k) at origin + (i, j, k) * step (host
+ * float[3] each), res (host int32[3]) nodes per axis, written x-major into out (device,
+ * res[0] * res[1] * res[2] floats).  The distance to the nearest triangle, negative where the
+ * generalised winding number exceeds 1/2: igl.signed_distance for a closed mesh, as
+ * RigidGeom._compute_sd (engine/entities/rigid_entity/rigid_geom.py:247-249) evaluates it on
+ * the geom's sampling grid. */
+int mpm_sdf_grid(const float* vertices, int32_t n_verts, const int32_t* faces, int32_t n_faces, const float* origin,
+                 const float* step, const int32_t* res, float* out, void* stream);
 
 /* ---- CUDA graphs --------------------------------------------------------
  * Capture n_substeps of mpm_substeps into an executable graph (the pointers in

@@ -396,7 +396,7 @@ static void sdf_grad(const ref_collider* c, REAL eps, const REAL* pos, REAL* sd_
             int outside = 0;
             for (int i = 0; i < 3; ++i) {
                 REAL half = (REAL)0.5 * (REAL)(r[i] - 1);
-                ps[i] = c->sdf_scale[i] * l[i] + half;
+                ps[i] = c->sdf_scale[i] * (l[i] - c->data[i]) + half; /* data: the grid's centre, geom frame */
                 dc[i] = ps[i] - half;
                 if (ps[i] >= (REAL)(r[i] - 1) || ps[i] <= 0) outside = 1;
             }

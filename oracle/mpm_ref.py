@@ -430,12 +430,13 @@ class Collider:
 
 def sdf_sampled(c: Collider, l, eps):
     """A geom's sampled signed distance and gradient at geom-frame points l (sdf_func_sdf /
-    sdf_func_grad, utils/sdf_decomp.py:102-276): trilinear in the grid; outside it the proxy
-    |voxel - centre| / cell + sdf_max and the unit direction to the centre."""
+    sdf_func_grad, utils/sdf_decomp.py:102-276): trilinear in the grid centred at c.data (the
+    centre of the geom's vertex bounds, T_mesh_to_sdf of rigid_geom.py:180-185); outside it
+    the proxy |voxel - centre| / cell + sdf_max and the unit direction to the centre."""
     dt = l.dtype.type
     r = np.asarray(np.shape(c.sdf))
     half = (r - 1) * dt(0.5)
-    ps = l * np.asarray(c.sdf_scale, dtype=dt) + half
+    ps = (l - np.asarray(c.data, dtype=dt)) * np.asarray(c.sdf_scale, dtype=dt) + half
     dc = ps - half
     out = ((ps >= r - 1) | (ps <= 0)).any(1)
     d2 = (dc * dc).sum(1)

@@ -59,7 +59,7 @@ def test_block_on_rigid_collider_matches_oracle(kind):
             col = R.Collider("box", np.array([0.52, 0.5, 0.2]), Rm, half, friction=0.3)
         else:
             val, grad, scale, cell, vmax = box_sdf_grid(half)
-            col = R.Collider("sdf", np.array([0.52, 0.5, 0.2]), Rm, half, friction=0.3, sdf=val, sdf_scale=scale,
+            col = R.Collider("sdf", np.array([0.52, 0.5, 0.2]), Rm, np.zeros(3), friction=0.3, sdf=val, sdf_scale=scale,
                              sdf_grad=grad, sdf_cell=cell, sdf_max=vmax)
     else:
         morph = gs.morphs.Plane(pos=(0.5, 0.5, 0.3), normal=(0.2, 0.0, 1.0))
@@ -104,3 +104,49 @@ def test_colliders_per_environment():
         scene.step()
     z = block.get_particles_pos()[..., 2].min(dim=1).values.cpu()
     assert z[0] > 0.3 - 1.5 / 64 and z[1] < z[0] - 0.01  # env 1's floor is lower
+
+
+def test_block_on_rigid_mesh_matches_oracle(tmp_path):
+    """A rigid Mesh (a tilted, off-origin icosphere, convex: its collision geom is its hull) through
+    the reference's sampled grid (rigid_geom.py:147-193): the grid mpm_sdf_grid samples against
+    the float64 signed-distance oracle at its nodes, then a block landing on it against the C
+    restatement through the same grid."""
+    from genesis_b200 import mesh
+    from oracle import mpm_ref as R
+    from oracle import sdf_ref
+
+    v, f = mesh.icosphere(subdivisions=2, radius=0.5)
+    v = v + np.array([0.1, -0.05, 0.0])  # off the mesh origin: the grid is centred on the bounds
+    path = tmp_path / "ball.obj"
+    with open(path, "w") as fh:
+        for q in v:
+            fh.write(f"v {q[0]:.9f} {q[1]:.9f} {q[2]:.9f}\n")
+        for t in f:
+            fh.write(f"f {t[0] + 1} {t[1] + 1} {t[2] + 1}\n")
+    morph = gs.morphs.Mesh(file=str(path), scale=0.14, pos=(0.49, 0.5, 0.2), euler=(0, 15, 10))
+    scene, block, rigid = _scene(morph, coup_friction=0.3)
+    val, grad, scale, cell, vmax = rigid._grid
+    centre = rigid._data
+    res = np.array(val.shape)
+    # the sampled distances at a random subset of the nodes against the oracle's exact ones
+    rng = np.random.default_rng(0)
+    idx = rng.integers(0, res, size=(400, 3))
+    pts = centre + (idx - (res - 1) / 2) * cell
+    exact = sdf_ref.signed_distance(pts, morph.vertices, morph.faces)
+    assert np.abs(val[idx[:, 0], idx[:, 1], idx[:, 2]] - exact).max() < 2e-6
+    Rm = gs.morphs._quat_to_R(np.asarray(morph.quat))
+    col = R.Collider("sdf", np.array(morph.pos), Rm, centre.astype(np.float64), friction=0.3,
+                     sdf=val.astype(np.float64), sdf_scale=scale, sdf_grad=grad.astype(np.float64), sdf_cell=cell,
+                     sdf_max=vmax)
+    v0 = (0.0, 0.0, -2.0)
+    block.set_particles_vel(torch.tensor(v0).expand(block.n_particles, 3))
+    o = _oracle(block, col, v0, 40)
+    away = R.Collider("sdf", np.array([0.5, 0.5, -5.0]), Rm, col.data, sdf=col.sdf, sdf_scale=scale,
+                      sdf_grad=col.sdf_grad, sdf_cell=cell, sdf_max=vmax)
+    free = _oracle(block, away, v0, 40)
+    assert np.abs(o["x"] - free["x"]).max() > 1e-4  # the mesh changed the trajectory (10x the tolerance)
+    for _ in range(4):
+        scene.step()
+    g = block.get_particles_pos().cpu().numpy()
+    print(f"\n[rigid mesh] grid {tuple(res)}, cell {cell:.4f}: max|dx| vs oracle {np.abs(g - o['x']).max():.2e}")
+    assert np.abs(g - o["x"]).max() < 1e-5

@@ -29,7 +29,7 @@ def test_grid_layout_follows_the_reference_formula():
 def test_lookup_stays_within_interpolation_error():
     half = np.array([0.15, 0.15, 0.1])
     val, grad, scale, cell, vmax = box_sdf_grid(half)
-    col = R.Collider("sdf", np.zeros(3), np.eye(3), half, sdf=val, sdf_scale=scale, sdf_grad=grad, sdf_cell=cell,
+    col = R.Collider("sdf", np.zeros(3), np.eye(3), np.zeros(3), sdf=val, sdf_scale=scale, sdf_grad=grad, sdf_cell=cell,
                      sdf_max=vmax)
     rng = np.random.default_rng(0)
     inner = 0.5 * (np.array(val.shape) - 1) / scale * 0.99  # inside the grid (outside it: the proxy)
@@ -53,7 +53,7 @@ def test_numpy_and_c_restatements_agree_through_the_grid():
     half = np.array([0.15, 0.15, 0.1])
     val, grad, scale, cell, vmax = box_sdf_grid(half)
     Rm = np.array([[np.cos(0.2), 0, np.sin(0.2)], [0, 1, 0], [-np.sin(0.2), 0, np.cos(0.2)]])
-    col = R.Collider("sdf", np.array([0.52, 0.5, 0.2]), Rm, half, friction=0.3, sdf=val, sdf_scale=scale,
+    col = R.Collider("sdf", np.array([0.52, 0.5, 0.2]), Rm, np.zeros(3), friction=0.3, sdf=val, sdf_scale=scale,
                      sdf_grad=grad, sdf_cell=cell, sdf_max=vmax)
     rng = np.random.default_rng(1)
     n = 400
@@ -70,3 +70,36 @@ def test_numpy_and_c_restatements_agree_through_the_grid():
     for _ in range(30):
         s2 = R.substep(p, mats, s2)
     assert np.abs(c_out["x"] - s2["x"]).max() < 1e-10
+
+
+def test_mesh_collision_geom_and_grid_layout():
+    """A rigid Mesh's collision geom (utils/mesh.py:301-400 for an object): the convex hull,
+    faces oriented outwards, for a convex mesh or with convexify on and a small hull error; the
+    mesh itself with convexify=False or a hull error above decompose_object_error_threshold.
+    And the sampling grid's layout (rigid_geom.py:147-170) for a mesh off its origin."""
+    from genesis_b200 import mesh
+    from genesis_b200.engine.rigid import collision_mesh, sdf_grid_layout
+
+    class M:  # the fields collision_mesh reads from a gs.morphs.Mesh
+        def __init__(self, v, f, convexify=None, thr=0.15):
+            self.vertices, self.faces = v, f
+            self.convexify, self.decompose_object_error_threshold = convexify, thr
+
+    v, f = mesh.icosphere(subdivisions=2, radius=0.4)
+    hv, hf = collision_mesh(M(v, f))
+    assert len(hf) == len(f)  # convex: the hull has the same faces
+    tv = hv[hf]
+    assert (np.einsum("ij,ij->i", np.cross(tv[:, 1] - tv[:, 0], tv[:, 2] - tv[:, 0]), tv[:, 0]) > 0).all()
+    # an L-shaped (non-convex) prism: hull volume 4/3 of the mesh's
+    bv, bf = mesh.box_mesh((1.0, 1.0, 1.0))
+    L = np.concatenate([bv, bv + [1.0, 0.0, 0.0], bv + [0.0, 1.0, 0.0]])
+    Lf = np.concatenate([bf, bf + 8, bf + 16])
+    assert collision_mesh(M(L, Lf, convexify=False))[1] is Lf
+    assert collision_mesh(M(L, Lf))[1] is Lf  # hull error ~0.5 > 0.15: not convexified
+    assert len(collision_mesh(M(L, Lf, thr=1.0))[1]) != len(Lf)
+    centre, res, cell, grid = sdf_grid_layout(np.array([0.1, 0.2, 0.3]), np.array([0.5, 0.4, 0.9]))
+    assert np.allclose(centre, [0.3, 0.3, 0.6])
+    ext = np.array([0.4, 0.2, 0.6])
+    g0 = ext.max() * 0.2 + ext
+    c = np.float32(np.finfo(np.float32).eps) + np.clip(0.005, g0.max() / 127, g0.min() / 31)
+    assert np.isclose(cell, c) and np.array_equal(res, np.ceil(g0 / c).astype(int) + 1)
