@@ -123,7 +123,8 @@ def test_block_on_rigid_mesh_matches_oracle(tmp_path):
             fh.write(f"v {q[0]:.9f} {q[1]:.9f} {q[2]:.9f}\n")
         for t in f:
             fh.write(f"f {t[0] + 1} {t[1] + 1} {t[2] + 1}\n")
-    morph = gs.morphs.Mesh(file=str(path), scale=0.14, pos=(0.49, 0.5, 0.2), euler=(0, 15, 10))
+    morph = gs.morphs.Mesh(file=str(path), scale=0.14, pos=(0.49, 0.5, 0.26), euler=(0, 15, 10))
+    # the hull's top (z ~ 0.33) sits just under the falling block (z >= 0.335), inside its grid
     scene, block, rigid = _scene(morph, coup_friction=0.3)
     val, grad, scale, cell, vmax = rigid._grid
     centre = rigid._data
