@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 12
+ABI_VERSION = 13
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -226,6 +226,9 @@ SIGNATURES = {
     "mpm_adjoint_workspace_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
     "mpm_substep_adjoint": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp]),
     "mpm_substep_adjoint_colliders": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp, vp]),
+    "mpm_substeps_record": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, vp, vp, vp]),
+    "mpm_substeps_adjoint_recorded": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, vp, vp, vp, vp, vp,
+                                                vp]),
     "mpm_status": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint32), vp]),
     "mpm_status_enqueue": (C.c_int, [_P(Problem), vp, vp, vp]),
     "mpm_fallback_count": (C.c_int, [_P(Problem), vp, i32, _P(C.c_uint64), vp]),

@@ -45,7 +45,16 @@ namespace gbm {
 #define GBM_OUTER_UNROLL 3
 #endif
 
+// packed float2 arithmetic (sm_100's FFMA2 / FMUL2: two float32 lanes per instruction) in the
+// gather and the scatter; each lane is rounded exactly as the scalar form
+// (bit 0: scatter, bit 1: gather)
+#ifndef GBM_F32X2
+#define GBM_F32X2 3
+#endif
+
 constexpr int kOuterUnroll = GBM_OUTER_UNROLL;
+constexpr bool kF32x2Scatter = (GBM_F32X2 & 1) != 0;
+constexpr bool kF32x2Gather = (GBM_F32X2 & 2) != 0;
 constexpr int BLK = MPM_BLOCK;         // grid block edge
 constexpr int BLK3 = BLK * BLK * BLK;  // nodes per block
 constexpr int MARGIN = 1;              // drift margin of the shared tile (nodes)
@@ -189,6 +198,9 @@ __device__ __forceinline__ void set_status(const Ws& w, int inst, uint32_t bit) 
     atomicOr(&w.counters[CNT_STATUS], bit);
     atomicOr(&w.inst_status[inst], bit);
 }
+
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 // quadratic B-spline weights (mpm_solver.py:350, 397)
 __device__ __forceinline__ void bspline(float fx, float* w) {
@@ -1257,6 +1269,38 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
             float As[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) As[k] = o.A[k] * sq;
+            if constexpr (kF32x2Scatter && !CPIC) {
+                // the same arithmetic on lane pairs: (momentum x, momentum y) and (momentum z,
+                // mass); the mass lane's affine coefficients are 0, so it stays ms exactly
+                constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: round-to-nearest integer
+                const float2 q01 = make_float2(mq0, mq1), q2m = make_float2(mq2, ms);
+                const float2 Ax = make_float2(As[0], As[3]), Ax2 = make_float2(As[6], 0.f);
+                const float2 Ay = make_float2(As[1], As[4]), Ay2 = make_float2(As[7], 0.f);
+                const float2 Az = make_float2(As[2], As[5]), Az2 = make_float2(As[8], 0.f);
+#pragma unroll kOuterUnroll
+                for (int i = 0; i < 3; ++i) {
+                    const float2 fi = dup2((float)i), wxi = dup2(sel3(wx, i));
+                    const float2 b01 = fma2(Ax, fi, q01), b2m = fma2(Ax2, fi, q2m);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const float2 fj = dup2((float)j);
+                        const float2 wij = __fmul2_rn(wxi, dup2(wy[j]));
+                        const float2 c01 = fma2(Ay, fj, b01), c2m = fma2(Ay2, fj, b2m);
+                        const int row = tidx(lx + i, ly + j, lz);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const float2 fk = dup2((float)k);
+                            const float2 wt = __fmul2_rn(wij, dup2(wz[k]));
+                            const float2 r01 = fma2(wt, fma2(Az, fk, c01), dup2(kMagic));
+                            const float2 r2m = fma2(wt, fma2(Az2, fk, c2m), dup2(kMagic));
+                            atomicAdd(&T.t[0][row + k], __float_as_int(r01.x) - 0x4B400000);
+                            atomicAdd(&T.t[1][row + k], __float_as_int(r01.y) - 0x4B400000);
+                            atomicAdd(&T.t[2][row + k], __float_as_int(r2m.x) - 0x4B400000);
+                            atomicAdd(&T.t[3][row + k], __float_as_int(r2m.y) - 0x4B400000);
+                        }
+                    }
+                }
+            } else {
             // factored per axis: the (i, j) partial sums and weights are reused for the 3 k
 #pragma unroll kOuterUnroll
             for (int i = 0; i < 3; ++i) {
@@ -1285,6 +1329,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
                         atomicAdd(&T.t[3][row + k], fix_mul(wt, ms));
                     }
                 }
+            }
             }
         } else {
             // drifted since the last sort (or a non-finite stress): bounds-checked global path
@@ -1387,6 +1432,61 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
             wyd[k] = wy[k] * ((float)k - fx[1]);
             wxd[k] = wx[k] * ((float)k - fx[0]);
         }
+        if constexpr (kF32x2Gather) {
+            // the same sums on lane pairs (x, y) and (z, w); the tile's w is 0
+            const float2 z2 = make_float2(0.f, 0.f);
+            float2 vp[2] = {z2, z2}, c0[2] = {z2, z2}, c1[2] = {z2, z2}, c2[2] = {z2, z2};
+#pragma unroll kOuterUnroll
+            for (int i = 0; i < 3; ++i) {
+                float2 a0[2] = {z2, z2}, ay[2] = {z2, z2}, az[2] = {z2, z2};
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    float2 s0[2] = {z2, z2}, s1[2] = {z2, z2};
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float4 g = VT.v[vidx(lx + i, ly + j, lz + k)];
+                        const float2 gp[2] = {make_float2(g.x, g.y), make_float2(g.z, g.w)};
+                        const float2 wk = dup2(wz[k]), wdk = dup2(wzd[k]);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            s0[h] = fma2(wk, gp[h], s0[h]);
+                            s1[h] = fma2(wdk, gp[h], s1[h]);
+                        }
+                    }
+                    const float2 wj = dup2(wy[j]), wdj = dup2(wyd[j]);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        a0[h] = fma2(wj, s0[h], a0[h]);
+                        ay[h] = fma2(wdj, s0[h], ay[h]);
+                        az[h] = fma2(wj, s1[h], az[h]);
+                    }
+                }
+                const float2 wi = dup2(sel3(wx, i)), wdi = dup2(sel3(wxd, i));
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    vp[h] = fma2(wi, a0[h], vp[h]);
+                    c0[h] = fma2(wdi, a0[h], c0[h]);
+                    c1[h] = fma2(wi, ay[h], c1[h]);
+                    c2[h] = fma2(wi, az[h], c2[h]);
+                }
+            }
+            nv[0] = vp[0].x;
+            nv[1] = vp[0].y;
+            nv[2] = vp[1].x;
+            const float2 cs = dup2(I.c_scale);
+            c0[0] = __fmul2_rn(c0[0], cs);
+            c1[0] = __fmul2_rn(c1[0], cs);
+            c2[0] = __fmul2_rn(c2[0], cs);
+            nC[0] = c0[0].x;
+            nC[1] = c1[0].x;
+            nC[2] = c2[0].x;
+            nC[3] = c0[0].y;
+            nC[4] = c1[0].y;
+            nC[5] = c2[0].y;
+            nC[6] = c0[1].x * I.c_scale;
+            nC[7] = c1[1].x * I.c_scale;
+            nC[8] = c2[1].x * I.c_scale;
+        } else {
 #pragma unroll kOuterUnroll
         for (int i = 0; i < 3; ++i) {
             float a0[3] = {0.f, 0.f, 0.f}, ay[3] = {0.f, 0.f, 0.f}, az[3] = {0.f, 0.f, 0.f};
@@ -1421,6 +1521,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k) nC[k] *= I.c_scale;
+        }
     } else {
 #pragma unroll 1
         for (int i = 0; i < 3; ++i)
@@ -2653,6 +2754,73 @@ int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab
                                                                tab->force_fields ? tab->n_force_fields : 0,
                                                                tab->ff_perm);
         k_adj_p2g<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, tab->materials, *state, adj, lame_bar, aw);
+    }
+    return cuda_ok();
+}
+
+int mpm_substeps_record(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                        int32_t n_substeps, float* state_rec, void* grid_rec, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !workspace || n_substeps < 0) return MPM_E_INVALID;
+    if (tab->colliders && tab->n_colliders > 0) return MPM_E_INVALID;
+    if (n_substeps > 0 && (!state_rec || !grid_rec)) return MPM_E_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t plane = (size_t)MPM_STATE_CH * (size_t)par->state_stride;  // floats per recorded state
+    const size_t nodes = (size_t)prob->n_blocks * BLK3;
+    float4* g = (float4*)grid_rec;
+    Ws w = ws_of(*prob, workspace);
+    for (int32_t j = 0; j < n_substeps; ++j) {
+        if (cudaMemcpyAsync(state_rec + (size_t)j * plane, par->state, plane * 4, cudaMemcpyDeviceToDevice, s) !=
+            cudaSuccess)
+            return MPM_E_CUDA;
+        if ((rc = launch_p2g(prob, tab, par, workspace, s))) return rc;
+        // the grid op clears the momentum behind itself: keep the p2g result first
+        if (cudaMemcpyAsync(g + (2 * (size_t)j) * nodes, w.mm, nodes * 16, cudaMemcpyDeviceToDevice, s) !=
+            cudaSuccess)
+            return MPM_E_CUDA;
+        if ((rc = launch_grid_op(prob, tab, workspace, s))) return rc;
+        if (cudaMemcpyAsync(g + (2 * (size_t)j + 1) * nodes, w.gv, nodes * 16, cudaMemcpyDeviceToDevice, s) !=
+            cudaSuccess)
+            return MPM_E_CUDA;
+        if ((rc = launch_g2p(prob, tab, par, workspace, s))) return rc;
+    }
+    return cuda_ok();
+}
+
+int mpm_substeps_adjoint_recorded(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* par,
+                                  int32_t first, int32_t count, const float* state_rec, const void* grid_rec,
+                                  float* adj, float* lame_bar, void* adj_workspace, void* stream) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if ((rc = check_par(prob, par))) return rc;
+    if (!tab || !tab->instances || !tab->materials || !adj || !lame_bar || !adj_workspace || first < 0 || count < 0)
+        return MPM_E_INVALID;
+    if (tab->colliders && tab->n_colliders > 0) return MPM_E_INVALID;
+    if (count > 0 && (!state_rec || !grid_rec)) return MPM_E_INVALID;
+    if (tab->n_force_fields < 0 || (tab->n_force_fields > 0 && !tab->force_fields)) return MPM_E_INVALID;
+    const int nff = tab->force_fields ? tab->n_force_fields : 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = prob->n_particles;
+    const size_t plane = (size_t)MPM_STATE_CH * (size_t)par->state_stride;
+    const size_t nodes = (size_t)prob->n_blocks * BLK3;
+    const float4* g = (const float4*)grid_rec;
+    AdjWs aw = adj_ws_of(*prob, adj_workspace);
+    Ws w{};  // the adjoint kernels read only the grid velocity from it
+    for (int32_t j = first + count - 1; j >= first; --j) {
+        mpm_particles sp = *par;
+        sp.state = const_cast<float*>(state_rec) + (size_t)j * plane;
+        aw.saved_mm = const_cast<float4*>(g + (2 * (size_t)j) * nodes);
+        w.gv = const_cast<float4*>(g + (2 * (size_t)j + 1) * nodes);
+        if (cudaMemsetAsync(aw.vbar, 0, nodes * 16, s) != cudaSuccess) return MPM_E_CUDA;
+        if (n > 0) {
+            k_adj_g2p<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, sp, adj, w, aw);
+            k_adj_grid<<<(int)((nodes + 255) / 256), 256, 0, s>>>(*prob, tab->instances, w, aw, nullptr, 0,
+                                                                   tab->sdf_voxels, nullptr, tab->force_fields, nff,
+                                                                   tab->ff_perm);
+            k_adj_p2g<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, tab->materials, sp, adj, lame_bar, aw);
+        }
     }
     return cuda_ok();
 }

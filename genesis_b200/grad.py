@@ -3,9 +3,13 @@ torch.autograd.Function.
 
 The forward pass advances the scene with the ordinary kernels and keeps the particle
 state every ``checkpoint_every`` substeps.  The backward pass walks the segments in
-reverse: it restores a segment's checkpoint, recomputes the states inside it, and runs
-the adjoint of each substep (mpm_substep_adjoint) from the last to the first.  Memory is
-one state per checkpoint plus one segment of states, instead of every substep.
+reverse: it restores a segment's checkpoint, recomputes the segment once while recording each
+substep's input state and grid (mpm_substeps_record), and runs the adjoint of each substep
+from the last to the first on those records (mpm_substeps_adjoint_recorded), so no substep's
+forward is evaluated twice in the reverse pass.  The recompute of the segment before runs on a
+second stream beside that adjoint (neither reads what the other writes), which fills a GPU
+that one small scene leaves mostly idle.  Memory is one state per checkpoint plus two
+segments of states and grids, instead of every substep.
 
 Supported: scenes of any mix of MPM materials (Elastic corotated or neo-Hookean, Muscle,
 ElastoPlastic von Mises or clamp, Liquid, Sand, Snow) with per-particle Young's modulus (each
@@ -136,6 +140,28 @@ class DifferentiableRollout:
             C.byref(rt.prob), C.byref(rt.tables), C.byref(par), C.c_void_p(self.adj.data_ptr()),
             C.c_void_p(self.lame_bar.data_ptr()), rt._ws, C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
 
+    def _records(self):
+        """Two buffers of per-substep records of one checkpoint segment (one being written
+        while the adjoint reads the other): input states [k, 25, stride] and grids
+        [k, 2, nodes, 4] (momentum + mass after p2g, velocity after the grid op), kept across
+        backward calls."""
+        rt = self.rt
+        nodes = int(rt.prob.n_blocks) * 64
+        if getattr(self, "_rec", None) is None:
+            self._rec = [(torch.empty((self.k,) + tuple(rt.state.shape), dtype=torch.float32, device=rt.device),
+                          torch.empty((self.k, 2, nodes, 4), dtype=torch.float32, device=rt.device))
+                         for _ in range(2)]
+        return self._rec
+
+    def _adjoint_recorded(self, first: int, count: int, rec_state: torch.Tensor, rec_grid: torch.Tensor):
+        if count <= 0:
+            return
+        rt = self.rt
+        nat.check("mpm_substeps_adjoint_recorded", rt.lib.mpm_substeps_adjoint_recorded(
+            C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), first, count,
+            C.c_void_p(rec_state.data_ptr()), C.c_void_p(rec_grid.data_ptr()), C.c_void_p(self.adj.data_ptr()),
+            C.c_void_p(self.lame_bar.data_ptr()), C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
+
     def backward(self, pos_grad: torch.Tensor):
         """pos_grad: dL/dx_final [N,3] in API order (or, after a forward with record,
         [len(record), N, 3]) -> (dL/dv0 [3], dL/dE [N], dL/dactu [N] or None).  The per-particle
@@ -161,20 +187,52 @@ class DifferentiableRollout:
 
         add(self.T)
         final = rt.state.clone()
-        t_end = self.T
-        for ci in range(len(self.checkpoints) - 1, -1, -1):
-            t0 = ci * self.k
-            m = t_end - t0
-            rt.state.copy_(self.checkpoints[ci])
-            states = []
-            for _ in range(m):  # recompute the segment, one materialised state per substep
-                states.append(rt.state.clone())
-                rt.substeps(1)
+        recs = self._records()
+        main = torch.cuda.current_stream(rt.device)
+        if getattr(self, "_side", None) is None:
+            self._side = torch.cuda.Stream(device=rt.device)
+        side = self._side
+        lib = rt.lib
+        nseg = len(self.checkpoints)
+        rec_done: list = [None] * nseg
+        adj_done: list = [None] * nseg
+
+        def record(c):
+            # recompute segment c once on the side stream, recording each substep's input state
+            # and grid into buffer c % 2, after the adjoint that last read that buffer (c + 2)
+            t0, t1 = c * self.k, min((c + 1) * self.k, self.T)
+            rs, rg = recs[c % 2]
+            with torch.cuda.stream(side):
+                if c + 2 < nseg:
+                    side.wait_event(adj_done[c + 2])
+                rt.state.copy_(self.checkpoints[c])
+                nat.check("mpm_substeps_record", lib.mpm_substeps_record(
+                    C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), rt._ws, t1 - t0,
+                    C.c_void_p(rs.data_ptr()), C.c_void_p(rg.data_ptr()), _cuda_stream_handle()))
+                rec_done[c] = torch.cuda.Event()
+                rec_done[c].record(side)
+
+        side.wait_stream(main)
+        record(nseg - 1)
+        for ci in range(nseg - 1, -1, -1):
+            if ci > 0:
+                record(ci - 1)  # runs beside this segment's adjoint: it reads only the records
+            t0, t1 = ci * self.k, min((ci + 1) * self.k, self.T)
+            m = t1 - t0
+            rs, rg = recs[ci % 2]
+            main.wait_event(rec_done[ci])
+            # the adjoint of substeps m-1 .. 0, split where dL/dx of an interior substep enters
+            hi = m
             for j in range(m - 1, -1, -1):
-                if t0 + j + 1 != self.T:
-                    add(t0 + j + 1)
-                self._adjoint_substep(states[j])
-            t_end = t0
+                r = t0 + j + 1
+                if r != self.T and r in inject:
+                    self._adjoint_recorded(j + 1, hi - j - 1, rs, rg)
+                    add(r)
+                    hi = j + 1
+            self._adjoint_recorded(0, hi, rs, rg)
+            adj_done[ci] = torch.cuda.Event()
+            adj_done[ci].record(main)
+        main.wait_stream(side)
         add(0)
         rt.state.copy_(final)
         gid = rt.gid[:n].long()

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 12
+#define MPM_ABI_VERSION 13
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -410,6 +410,29 @@ int mpm_substep_adjoint(const mpm_problem* prob, const mpm_tables* tab, const mp
 int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* state,
                                   float* adj, float* lame_bar, float* collider_bar, void* workspace,
                                   void* adj_workspace, void* stream);
+
+/* Checkpointed reverse pass without a second forward per substep.  The reference's autodiff
+ * re-runs the forward of every substep inside its backward (substep_pre_coupling_grad /
+ * couple_grad / substep_post_coupling_grad re-evaluate p2g and the grid op before their .grad,
+ * mpm_solver.py:485-517, legacy_coupler.py:996-1017); here the recompute of a checkpoint
+ * segment records what the adjoint reads, and the adjoint reads it back:
+ *   mpm_substeps_record advances the particles by n_substeps substeps (p2g, grid op, g2p per
+ *     substep, no re-sort: the particles must be binned by an earlier mpm_sort_particles) and
+ *     stores, for substep j, its input state in state_rec[j] (float[25][state_stride], the
+ *     state's planar layout) and its grid in grid_rec[j] (two float4[n_blocks * 64] planes: the
+ *     momentum and mass after p2g, then the velocity after the grid op).
+ *   mpm_substeps_adjoint_recorded runs the adjoint of recorded substeps first + count - 1 down
+ *     to first, as mpm_substep_adjoint would for each (adj and lame_bar as there), reading
+ *     state_rec and grid_rec instead of recomputing them.
+ * Both refuse colliders (MPM_E_INVALID: their poses move between substeps); force fields are
+ * allowed.  state_rec holds n_substeps * 25 * state_stride floats, grid_rec n_substeps * 2 *
+ * n_blocks * 64 * 16 bytes.  The particle tables of `par` (mat, pflags, mu_p, lam_p, actu, ...)
+ * must be the ones of the recorded run; its state pointer is not read by the adjoint. */
+int mpm_substeps_record(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
+                        int32_t n_substeps, float* state_rec, void* grid_rec, void* stream);
+int mpm_substeps_adjoint_recorded(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* par,
+                                  int32_t first, int32_t count, const float* state_rec, const void* grid_rec,
+                                  float* adj, float* lame_bar, void* adj_workspace, void* stream);
 
 /* ---- timing ----------------------------------------------------------------
  * mpm_substeps with a CUDA event recorded on `stream` after every launch group: on return
