@@ -15,7 +15,8 @@ nodes over the checkpointed CUDA adjoint (mpm_substep_adjoint):
 `loss.backward()` then needs no scene call: autograd runs every query of a state and the step
 that consumes it before the step that produced it, so when `_Step.backward` of step s runs, the
 adjoint buffer holds dL/d(state after step s) minus the queries of that state, which it adds;
-it recomputes the step's substeps from its checkpoint, runs their adjoints in reverse, reads
+it recomputes the step's substeps from its checkpoint (once, recording each substep's input state
+and grid, mpm_substeps_record, when no collider moves), runs their adjoints in reverse, reads
 the gradients of the step's inputs (undoing them in reverse order: the state components an
 input overwrote get a zero adjoint) and leaves dL/d(state before step s) for the step before.
 Actuation persists until it is set again, so its gradient accumulates across steps and is
@@ -148,6 +149,26 @@ class SceneTape:
         if self.n_colliders:
             self.tool_bar += self.cbar
 
+    def _adjoint_step_recorded(self, m: int):
+        rt = self.rt
+        if getattr(self, "_rec", None) is None or self._rec[0].shape[0] != m:
+            nodes = int(rt.prob.n_blocks) * 64
+            self._rec = (torch.empty((m,) + tuple(rt.state.shape), dtype=torch.float32, device=rt.device),
+                         torch.empty((m, 2, nodes, 4), dtype=torch.float32, device=rt.device))
+        rs, rg = self._rec
+        stream = _cuda_stream_handle()
+        nat.check("mpm_substeps_record", rt.lib.mpm_substeps_record(
+            C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), rt._ws, m, C.c_void_p(rs.data_ptr()),
+            C.c_void_p(rg.data_ptr()), stream))
+        par = nat.Particles.from_buffer_copy(rt.par)
+        if not self.muscle:
+            par.actu = None
+            par.muscle_dir = None
+        nat.check("mpm_substeps_adjoint_recorded", rt.lib.mpm_substeps_adjoint_recorded(
+            C.byref(rt.prob), C.byref(rt.tables), C.byref(par), 0, m, C.c_void_p(rs.data_ptr()),
+            C.c_void_p(rg.data_ptr()), C.c_void_p(self.adj.data_ptr()), C.c_void_p(self.lame_bar.data_ptr()),
+            C.c_void_p(self.adj_ws.data_ptr()), stream))
+
     def _chain_colliders(self, cols):
         """Carry dL/d(pose after a substep) back over its motion pos' = pos + lin_vel dt (a
         tool's z held at its floor where pos_z + v_z dt falls below it), cols the collider
@@ -200,15 +221,19 @@ class _Step(torch.autograd.Function):
             rt.actu.copy_(ctx.actu)
         if tape.n_colliders:
             rt.collider_table().copy_(ctx.cols)
-        states = []
-        for _ in range(tape.solver._sim.substeps):  # recompute the step, one state per substep
-            states.append((rt.state.clone(), rt.collider_table().clone() if tape.n_colliders else None))
-            rt.substeps(1)
-        for st, cols in reversed(states):
-            if tape.n_colliders:
+        if tape.n_colliders:
+            states = []
+            for _ in range(tape.solver._sim.substeps):  # recompute the step, one state per substep
+                states.append((rt.state.clone(), rt.collider_table().clone()))
+                rt.substeps(1)
+            for st, cols in reversed(states):
                 tape._chain_colliders(cols)
                 rt.collider_table().copy_(cols)  # the substep's poses, for its grid op's adjoint
-            tape._adjoint_substep(st)
+                tape._adjoint_substep(st)
+        else:
+            # no collider moves between substeps: recompute the step once, recording each
+            # substep's input state and grid, and run the adjoints on the records
+            tape._adjoint_step_recorded(tape.solver._sim.substeps)
         rt.state.copy_(live)
         if tape.muscle:
             rt.actu.copy_(live_actu)
