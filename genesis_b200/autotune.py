@@ -88,26 +88,21 @@ def tune(rt, candidates=None, trial_substeps: int = 100, use_cache: bool = True,
             best = cache[sig]["best"]
             rt.retune(**best)
             return best, cache[sig].get("times", {})
-    saved = None
-    if restore_state:
-        saved = (rt.state.clone(), rt.mat.clone(), rt.pflags.clone(), rt.gid.clone(), rt.slot.clone(),
-                 None if rt.mu_p is None else rt.mu_p.clone(), None if rt.lam_p is None else rt.lam_p.clone(),
-                 rt._count)
-    times = {}
-    best, best_t = None, float("inf")
-    for P in cand["chunk_particles"]:
-        for K in cand["sort_interval"]:
-            for G in cand["grid_ctas"]:
-                rt.retune(chunk_particles=P, sort_interval=K, grid_ctas=G)
-                rt._count = 0
-                n = max(trial_substeps, K)
-                rt.substeps(K)  # warm-up (graph capture, first sort)
-                t = time_substeps(rt, (n // K) * K)
-                key = f"P{P}_K{K}_G{G}"
-                times[key] = t
-                if t < best_t:
-                    best, best_t = {"chunk_particles": P, "sort_interval": K, "grid_ctas": G}, t
-    if saved is not None:
+    # every candidate starts from the same particle state: timed on a simulation that moves
+    # on between candidates, the ones tried first would see an earlier (and, as a scene
+    # settles into contact and plastic flow, cheaper) stretch of it
+    saved = (rt.state.clone(), rt.mat.clone(), rt.pflags.clone(), rt.gid.clone(), rt.slot.clone(),
+             None if rt.mu_p is None else rt.mu_p.clone(), None if rt.lam_p is None else rt.lam_p.clone(),
+             rt._count)
+    # the colliders move with the substeps and accumulate reaction forces
+    cols = rt.collider_table().clone() if getattr(rt, "coll_table", None) is not None else None
+    cforce = rt.collider_force.clone() if getattr(rt, "collider_force", None) is not None else None
+
+    def restore():
+        if cols is not None:
+            rt.collider_table().copy_(cols)
+        if cforce is not None:
+            rt.collider_force.copy_(cforce)
         st, mat, pf, gid, slot, mu, lam, count = saved
         rt.state.copy_(st)
         rt.mat.copy_(mat)
@@ -118,6 +113,25 @@ def tune(rt, candidates=None, trial_substeps: int = 100, use_cache: bool = True,
             rt.mu_p.copy_(mu)
             rt.lam_p.copy_(lam)
         rt._count = count
+        rt._sorted_once = False  # the binning in the workspace belongs to the advanced state
+
+    times = {}
+    best, best_t = None, float("inf")
+    for P in cand["chunk_particles"]:
+        for K in cand["sort_interval"]:
+            for G in cand["grid_ctas"]:
+                restore()
+                rt.retune(chunk_particles=P, sort_interval=K, grid_ctas=G)
+                rt._count = 0
+                n = max(trial_substeps, K)
+                rt.substeps(K)  # warm-up (graph capture, first sort)
+                t = time_substeps(rt, (n // K) * K)
+                key = f"P{P}_K{K}_G{G}"
+                times[key] = t
+                if t < best_t:
+                    best, best_t = {"chunk_particles": P, "sort_interval": K, "grid_ctas": G}, t
+    if restore_state:
+        restore()
     rt.retune(**best)
     rt._sorted_once = False
     if use_cache:

@@ -46,15 +46,25 @@ namespace gbm {
 #endif
 
 // packed float2 arithmetic (sm_100's FFMA2 / FMUL2: two float32 lanes per instruction) in the
-// gather and the scatter; each lane is rounded exactly as the scalar form
-// (bit 0: scatter, bit 1: gather)
+// gather and the scatter; each lane is rounded exactly as the scalar form.  GBM_F32X2 for the
+// 128-particle work items (bit 0: scatter, bit 1: gather; both measured 2.6% faster on the
+// 500k scene, the scatter alone 1.8%)
 #ifndef GBM_F32X2
 #define GBM_F32X2 3
 #endif
 
 constexpr int kOuterUnroll = GBM_OUTER_UNROLL;
-constexpr bool kF32x2Scatter = (GBM_F32X2 & 1) != 0;
-constexpr bool kF32x2Gather = (GBM_F32X2 & 2) != 0;
+// GBM_F32X2_WIDE: the same bits for the 256- and 512-particle work items, whose register
+// budget differs: there the packed gather costs spills (40 B against 16 B at 256 threads per
+// CTA) and measured slower on the 256-scene batch (7.21e9 against 7.35e9 particle-substeps/s
+// with the packed scatter alone)
+#ifndef GBM_F32X2_WIDE
+#define GBM_F32X2_WIDE 1
+#endif
+template <int P>
+constexpr bool kF32x2Scatter = ((P <= 128 ? GBM_F32X2 : GBM_F32X2_WIDE) & 1) != 0;
+template <int P>
+constexpr bool kF32x2Gather = ((P <= 128 ? GBM_F32X2 : GBM_F32X2_WIDE) & 2) != 0;
 constexpr int BLK = MPM_BLOCK;         // grid block edge
 constexpr int BLK3 = BLK * BLK * BLK;  // nodes per block
 constexpr int MARGIN = 1;              // drift margin of the shared tile (nodes)
@@ -1269,7 +1279,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
             float As[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) As[k] = o.A[k] * sq;
-            if constexpr (kF32x2Scatter && !CPIC) {
+            if constexpr (kF32x2Scatter<P> && !CPIC) {
                 // the same arithmetic on lane pairs: (momentum x, momentum y) and (momentum z,
                 // mass); the mass lane's affine coefficients are 0, so it stays ms exactly
                 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: round-to-nearest integer
@@ -1403,7 +1413,7 @@ __device__ __forceinline__ void vel_tile_load(VelTile& VT, const Ws& w, const Nb
 // g2p gather (mpm_solver.py:396-431): v = sum w v_i, C = 4 inv_dx sum w v_i (off - fx)^T;
 // then x += dt v and the boundary (mpm_solver.py:434-437).  Returns false if nothing
 // could be gathered (non-finite x).
-template <bool CPIC = false>
+template <int P, bool CPIC = false>
 __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm_instance& I, int inst, float* x,
                                        float* nv, float* nC, int ox, int oy, int oz, const P2GArgs* cp = nullptr,
                                        int p = 0) {
@@ -1432,7 +1442,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
             wyd[k] = wy[k] * ((float)k - fx[1]);
             wxd[k] = wx[k] * ((float)k - fx[0]);
         }
-        if constexpr (kF32x2Gather) {
+        if constexpr (kF32x2Gather<P>) {
             // the same sums on lane pairs (x, y) and (z, w); the tile's w is 0
             const float2 z2 = make_float2(0.f, 0.f);
             float2 vp[2] = {z2, z2}, c0[2] = {z2, z2}, c1[2] = {z2, z2}, c2[2] = {z2, z2};
@@ -1638,7 +1648,7 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
             float x[3], nv[3], nC[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
-            if (gather<CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
+            if (gather<P, CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     S[(MPM_CH_X + d) * st + p] = x[d];
@@ -1687,7 +1697,7 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
             if constexpr (CPIC) o.slot = p;  // a particle with a non-finite x leaves no separated nodes
-            if (gather<CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
+            if (gather<P, CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) S[(MPM_CH_X + d) * st + p] = x[d];
                 if constexpr (CPIC) {
