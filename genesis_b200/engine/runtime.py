@@ -66,6 +66,13 @@ class InstanceSpec:
         return int(np.prod(self.nblk))
 
 
+def _h2d(a: np.ndarray, dev) -> torch.Tensor:
+    """Host array -> device tensor through pinned memory, stream-ordered without blocking the
+    host (a copy from pageable memory would wait for the GPU to reach it: a runtime built while
+    another one's substeps run, as the server's repacks are, would stall the host until they end)."""
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(dev, non_blocking=True)
+
+
 def _cuda_stream_handle():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream or None)
 
@@ -156,8 +163,8 @@ class MPMRuntime:
             flags=0,
         )
         dev = self.device
-        self.inst_table = torch.from_numpy(nat.instances_to_bytes(insts)).to(dev)
-        self.mat_table = torch.from_numpy(nat.materials_to_bytes(mats)).to(dev)
+        self.inst_table = _h2d(nat.instances_to_bytes(insts), dev)
+        self.mat_table = _h2d(nat.materials_to_bytes(mats), dev)
         # kinematic rigid colliders of the grid op (mpm_collider rows) and their reaction
         # force / torque accumulators
         colliders = list(colliders or [])
@@ -165,7 +172,7 @@ class MPMRuntime:
         self.last_step_substeps = 0
         if colliders:
             arr = (nat.Collider * len(colliders))(*colliders)
-            self.coll_table = torch.from_numpy(np.frombuffer(bytes(arr), dtype=np.uint8).copy()).to(dev)
+            self.coll_table = _h2d(np.frombuffer(bytes(arr), dtype=np.uint8).copy(), dev)
             self.coll_init = self.coll_table.clone()
             self.collider_force = torch.zeros((len(colliders), 6), dtype=torch.float32, device=dev)
         else:
@@ -192,7 +199,7 @@ class MPMRuntime:
                 if f.kind == nat.FF_TURBULENCE and (f.perm_offset < 0 or f.perm_offset + 3 * 512 > perm_n):
                     raise ValueError("a turbulence field's permutation tables lie outside ff_perm")
             arr = (nat.ForceField * len(force_fields))(*force_fields)
-            self.ff_table = torch.from_numpy(np.frombuffer(bytes(arr), dtype=np.uint8).copy()).to(dev)
+            self.ff_table = _h2d(np.frombuffer(bytes(arr), dtype=np.uint8).copy(), dev)
             if perm_n:
                 self.ff_perm = torch.as_tensor(np.asarray(ff_perm, dtype=np.int32).reshape(-1), device=dev)
         self.tables = nat.Tables(
