@@ -84,19 +84,24 @@ __global__ void k_adj_g2p(mpm_problem prob, const mpm_instance* __restrict__ ins
     locate(I, x, base, fx);
 #pragma unroll
     for (int d = 0; d < 3; ++d) bspline_d(fx[d], wv[d], dwv[d]);
-    // recompute the gathered velocity for the boundary masks
+    // recompute the gathered velocity for the boundary masks.  The 27 node velocities are
+    // loaded once, all issued before the first is used (one CTA per SM at the differentiable
+    // scenes' sizes: the loads' latency, not bandwidth, sets this kernel's time), and kept in
+    // registers for the scatter below.
+    float4 gn[27];
+#pragma unroll
+    for (int n = 0; n < 27; ++n) {
+        const int gx = base[0] + n / 9, gy = base[1] + (n / 3) % 3, gz = base[2] + n % 3;
+        gn[n] = node_ok(I, gx, gy, gz) ? w.gv[node_addr(I, gx, gy, gz)] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     float nv[3] = {0.f, 0.f, 0.f};
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            for (int k = 0; k < 3; ++k) {
-                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
-                if (!node_ok(I, gx, gy, gz)) continue;
-                const float4 g = w.gv[node_addr(I, gx, gy, gz)];
-                const float wt = wv[0][i] * wv[1][j] * wv[2][k];
-                nv[0] += wt * g.x;
-                nv[1] += wt * g.y;
-                nv[2] += wt * g.z;
-            }
+#pragma unroll
+    for (int n = 0; n < 27; ++n) {
+        const float wt = wv[0][n / 9] * wv[1][(n / 3) % 3] * wv[2][n % 3];
+        nv[0] += wt * gn[n].x;
+        nv[1] += wt * gn[n].y;
+        nv[2] += wt * gn[n].z;
+    }
     float gxb[3], vb[3], Cb[9];
     const float* xin = adj + (int64_t)MPM_CH_X * st;
     const float* vin = adj + (int64_t)MPM_CH_V * st;
@@ -113,32 +118,31 @@ __global__ void k_adj_g2p(mpm_problem prob, const mpm_instance* __restrict__ ins
     for (int k = 0; k < 9; ++k) Cb[k] = cin[k * st + s];
     float xb[3] = {gxb[0], gxb[1], gxb[2]};
     const float c = I.c_scale;
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            for (int k = 0; k < 3; ++k) {
-                const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
-                if (!node_ok(I, gx, gy, gz)) continue;
-                const int64_t na = node_addr(I, gx, gy, gz);
-                const float4 g = w.gv[na];
-                const float vh[3] = {g.x, g.y, g.z};
-                const float wt = wv[0][i] * wv[1][j] * wv[2][k];
-                const float gw[3] = {dwv[0][i] * wv[1][j] * wv[2][k] * I.inv_dx, wv[0][i] * dwv[1][j] * wv[2][k] * I.inv_dx,
-                                     wv[0][i] * wv[1][j] * dwv[2][k] * I.inv_dx};
-                const float u[3] = {(float)i - fx[0], (float)j - fx[1], (float)k - fx[2]};
-                float Cu[3];
 #pragma unroll
-                for (int a = 0; a < 3; ++a) Cu[a] = Cb[a * 3 + 0] * u[0] + Cb[a * 3 + 1] * u[1] + Cb[a * 3 + 2] * u[2];
-                // one 16-byte vector reduction per node (sm_90+) instead of three scalar ones
-                atomicAdd(&aw.vbar[na], make_float4(wt * vb[0] + c * wt * Cu[0], wt * vb[1] + c * wt * Cu[1],
-                                                    wt * vb[2] + c * wt * Cu[2], 0.f));
-                const float wbar = vb[0] * vh[0] + vb[1] * vh[1] + vb[2] * vh[2] +
-                                   c * (vh[0] * Cu[0] + vh[1] * Cu[1] + vh[2] * Cu[2]);
+    for (int n = 0; n < 27; ++n) {
+        const int i = n / 9, j = (n / 3) % 3, k = n % 3;
+        const int gx = base[0] + i, gy = base[1] + j, gz = base[2] + k;
+        if (!node_ok(I, gx, gy, gz)) continue;
+        const int64_t na = node_addr(I, gx, gy, gz);
+        const float vh[3] = {gn[n].x, gn[n].y, gn[n].z};
+        const float wt = wv[0][i] * wv[1][j] * wv[2][k];
+        const float gw[3] = {dwv[0][i] * wv[1][j] * wv[2][k] * I.inv_dx, wv[0][i] * dwv[1][j] * wv[2][k] * I.inv_dx,
+                             wv[0][i] * wv[1][j] * dwv[2][k] * I.inv_dx};
+        const float u[3] = {(float)i - fx[0], (float)j - fx[1], (float)k - fx[2]};
+        float Cu[3];
 #pragma unroll
-                for (int e = 0; e < 3; ++e) {
-                    const float ub = c * wt * (Cb[0 * 3 + e] * vh[0] + Cb[1 * 3 + e] * vh[1] + Cb[2 * 3 + e] * vh[2]);
-                    xb[e] += wbar * gw[e] - I.inv_dx * ub;
-                }
-            }
+        for (int a = 0; a < 3; ++a) Cu[a] = Cb[a * 3 + 0] * u[0] + Cb[a * 3 + 1] * u[1] + Cb[a * 3 + 2] * u[2];
+        // one 16-byte vector reduction per node (sm_90+) instead of three scalar ones
+        atomicAdd(&aw.vbar[na], make_float4(wt * vb[0] + c * wt * Cu[0], wt * vb[1] + c * wt * Cu[1],
+                                            wt * vb[2] + c * wt * Cu[2], 0.f));
+        const float wbar = vb[0] * vh[0] + vb[1] * vh[1] + vb[2] * vh[2] +
+                           c * (vh[0] * Cu[0] + vh[1] * Cu[1] + vh[2] * Cu[2]);
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const float ub = c * wt * (Cb[0 * 3 + e] * vh[0] + Cb[1 * 3 + e] * vh[1] + Cb[2 * 3 + e] * vh[2]);
+            xb[e] += wbar * gw[e] - I.inv_dx * ub;
+        }
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d) aw.xbar[d * aw.stride + s] = xb[d];
 }
