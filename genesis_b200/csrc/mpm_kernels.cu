@@ -1679,8 +1679,22 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
 #pragma unroll
     for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
     tile_zero(T, P);
+    // the next work item's descriptor is loaded one item ahead, and each item's particle
+    // position and flags are in flight during its velocity-tile load: the item start's chain of
+    // dependent loads (descriptor -> tile; then position -> gather) loses two L2 round trips
+    int4 next = blockIdx.x < n_chunks ? w.chunks[blockIdx.x] : make_int4(0, 0, 0, 0);
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
-        const int4 ch = w.chunks[ci];
+        const int4 ch = next;
+        if (ci + (int)gridDim.x < n_chunks) next = w.chunks[ci + gridDim.x];
+        const int p = ch.z + threadIdx.x;
+        const bool have = p < ch.w;
+        float x[3] = {0.f, 0.f, 0.f};
+        uint8_t pf = 0;
+        if (have) {
+            pf = a.par.pflags[p];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
+        }
         const mpm_instance& I = a.inst[ch.x];
         const BlockCoord bc = unpack_bc(ch.y);
         const Nbhd h = nbhd_of(I, bc);
@@ -1691,11 +1705,8 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
         o.live = o.in_tile = false;
         o.mass = o.bq = 0.f;
         o.slot = -1;
-        const int p = ch.z + threadIdx.x;
-        if (p < ch.w && (a.par.pflags[p] & MPM_PFLAG_ACTIVE)) {
-            float x[3], nv[3], nC[9];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = S[(MPM_CH_X + d) * st + p];
+        if (have && (pf & MPM_PFLAG_ACTIVE)) {
+            float nv[3], nC[9];
             if constexpr (CPIC) o.slot = p;  // a particle with a non-finite x leaves no separated nodes
             if (gather<P, CPIC>(VT, w, I, ch.x, x, nv, nC, ox, oy, oz, &a, p)) {
 #pragma unroll
