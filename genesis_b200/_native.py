@@ -16,7 +16,7 @@ import numpy as np
 LIB_NAME = "libgenesis_b200_mpm.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
-ABI_VERSION = 13
+ABI_VERSION = 14
 
 MPM_OK = 0
 MPM_E_INVALID = -1
@@ -226,6 +226,7 @@ SIGNATURES = {
     "mpm_adjoint_workspace_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
     "mpm_substep_adjoint": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp]),
     "mpm_substep_adjoint_colliders": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, vp, vp, vp, vp, vp]),
+    "mpm_record_grid_bytes": (C.c_int, [_P(Problem), _P(C.c_uint64)]),
     "mpm_substeps_record": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), vp, i32, vp, vp, vp]),
     "mpm_substeps_adjoint_recorded": (C.c_int, [_P(Problem), _P(Tables), _P(Particles), i32, i32, vp, vp, vp, vp, vp,
                                                 vp]),

@@ -495,6 +495,64 @@ __global__ void k_adj_grid(mpm_problem prob, const mpm_instance* __restrict__ in
     if (in) aw.pmbar[node] = out;
 }
 
+// The grid op's adjoint over the active blocks a recorded substep lists (no colliders: the
+// recorded reverse pass refuses them), with the same per-node arithmetic as k_adj_grid.
+// vbar is cleared behind the read, so it is zero again for the substep before (whose g2p
+// adjoint writes only inside its own active blocks) without a pass over the whole grid.
+__global__ void __launch_bounds__(256) k_adj_grid_active(mpm_problem prob, const mpm_instance* __restrict__ inst,
+                                                         AdjWs aw, const int2* __restrict__ active,
+                                                         const uint32_t* __restrict__ n_active_p,
+                                                         const mpm_force_field* __restrict__ ffs, int n_ff,
+                                                         const int* __restrict__ ff_perm) {
+    const int n_active = (int)*n_active_p;
+    const int gpc = blockDim.x / BLK3;
+    const int grp = threadIdx.x / BLK3;
+    const int ln = threadIdx.x % BLK3;
+    const int lxyz[3] = {ln / (BLK * BLK), (ln / BLK) % BLK, ln % BLK};
+    for (int i = blockIdx.x * gpc + grp; i < n_active; i += gridDim.x * gpc) {
+        const int2 e = active[i];
+        const mpm_instance& I = inst[e.x];
+        const BlockCoord bc = unpack_bc(e.y);
+        const int64_t node = (I.blk_base + local_block(I, bc.bx, bc.by, bc.bz)) * BLK3 + ln;
+        const float4 mm = aw.saved_mm[node];
+        const bool act = mm.w > I.eps;
+        float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (act) {
+            const float inv = 1.f / mm.w;
+            const float pm[3] = {mm.x, mm.y, mm.z};
+            const int bxyz[3] = {bc.bx, bc.by, bc.bz};
+            float p[3], v[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                v[d] = inv * pm[d] + I.dt * I.gravity[d];
+                p[d] = (float)(bxyz[d] * BLK + lxyz[d] + I.lower_cell[d]) * I.dx;
+            }
+            if (n_ff > 0) apply_force_fields(ffs, n_ff, ff_perm, I.eps, I.dt, p, v, node, 0u);
+            const float4 vb4 = aw.vbar[node];
+            const float vbin[3] = {vb4.x, vb4.y, vb4.z};
+            float vb[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const bool zero = (p[d] >= I.bnd_hi[d] && v[d] >= 0.f) || (p[d] <= I.bnd_lo[d] && v[d] <= 0.f);
+                vb[d] = zero ? 0.f : vbin[d];
+            }
+            // the force fields in reverse order, each from the velocity it received
+            for (int k = n_ff - 1; k >= 0; --k) {
+                if (!ffs[k].active) continue;
+                float vk[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) vk[d] = inv * pm[d] + I.dt * I.gravity[d];
+                apply_force_fields(ffs, k, ff_perm, I.eps, I.dt, p, vk, node, 0u);
+                force_field_vjp(ffs[k], I.eps, I.dt, p, vk, vb);
+            }
+            const float dotp = vb[0] * pm[0] + vb[1] * pm[1] + vb[2] * pm[2];
+            out = make_float4(vb[0] * inv, vb[1] * inv, vb[2] * inv, -dotp * inv * inv);
+        }
+        aw.pmbar[node] = out;
+        aw.vbar[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
 // cofactor matrix of F (= det(F) F^-T)
 __device__ __forceinline__ void cofactor(const float* F, float* K) {
     K[0] = F[4] * F[8] - F[5] * F[7];

@@ -2779,6 +2779,71 @@ int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab
     return cuda_ok();
 }
 
+// One recorded substep of grid_rec: the momentum and mass after p2g and the velocity after
+// the grid op (float4 per node each), then the active-block list the grid op walked and its
+// length.
+struct RecGrid {
+    float4* mm;
+    float4* gv;
+    int2* active;
+    uint32_t* n_active;
+};
+
+static uint64_t rec_grid_bytes(const mpm_problem& p) {
+    const uint64_t nodes = (uint64_t)p.n_blocks * BLK3;
+    return align_up(nodes * 32 + (uint64_t)p.n_blocks * 8 + 16, 256);
+}
+
+static RecGrid rec_grid_of(const mpm_problem& p, void* base, int32_t j) {
+    char* b = (char*)base + (uint64_t)j * rec_grid_bytes(p);
+    const uint64_t nodes = (uint64_t)p.n_blocks * BLK3;
+    RecGrid r;
+    r.mm = (float4*)b;
+    r.gv = (float4*)(b + nodes * 16);
+    r.active = (int2*)(b + nodes * 32);
+    r.n_active = (uint32_t*)(b + nodes * 32 + (uint64_t)p.n_blocks * 8);
+    return r;
+}
+
+// Record the p2g result of the active blocks: their list, its length and their momentum and
+// mass (the grid op, which runs next, clears both behind itself).  One 64-thread group per
+// block; the adjoint reads nothing outside the active blocks.
+__device__ __forceinline__ int64_t block_of_entry(const mpm_instance* __restrict__ inst, int2 e) {
+    const mpm_instance& I = inst[e.x];
+    const BlockCoord bc = unpack_bc(e.y);
+    return I.blk_base + local_block(I, bc.bx, bc.by, bc.bz);
+}
+
+__global__ void __launch_bounds__(256) k_record_p2g(const mpm_instance* __restrict__ inst, Ws w, RecGrid r) {
+    const int n_active = (int)w.counters[CNT_ACTIVE];
+    const int gpc = blockDim.x / BLK3, grp = threadIdx.x / BLK3, ln = threadIdx.x % BLK3;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *r.n_active = (uint32_t)n_active;
+    for (int i = blockIdx.x * gpc + grp; i < n_active; i += gridDim.x * gpc) {
+        const int2 e = w.active[i];
+        if (ln == 0) r.active[i] = e;
+        const int64_t blk = block_of_entry(inst, e);
+        r.mm[blk * BLK3 + ln] = w.mm[blk * BLK3 + ln];
+    }
+}
+
+// Record the grid op's velocity of the blocks k_record_p2g listed.
+__global__ void __launch_bounds__(256) k_record_gv(const mpm_instance* __restrict__ inst, Ws w, RecGrid r) {
+    const int n_active = (int)*r.n_active;
+    const int gpc = blockDim.x / BLK3, grp = threadIdx.x / BLK3, ln = threadIdx.x % BLK3;
+    for (int i = blockIdx.x * gpc + grp; i < n_active; i += gridDim.x * gpc) {
+        const int64_t blk = block_of_entry(inst, r.active[i]);
+        r.gv[blk * BLK3 + ln] = w.gv[blk * BLK3 + ln];
+    }
+}
+
+int mpm_record_grid_bytes(const mpm_problem* prob, uint64_t* out) {
+    int rc = check_problem(prob);
+    if (rc) return rc;
+    if (!out) return MPM_E_INVALID;
+    *out = rec_grid_bytes(*prob);
+    return MPM_OK;
+}
+
 int mpm_substeps_record(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
                         int32_t n_substeps, float* state_rec, void* grid_rec, void* stream) {
     int rc = check_problem(prob);
@@ -2789,22 +2854,23 @@ int mpm_substeps_record(const mpm_problem* prob, const mpm_tables* tab, mpm_part
     if (n_substeps > 0 && (!state_rec || !grid_rec)) return MPM_E_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t plane = (size_t)MPM_STATE_CH * (size_t)par->state_stride;  // floats per recorded state
-    const size_t nodes = (size_t)prob->n_blocks * BLK3;
-    float4* g = (float4*)grid_rec;
     Ws w = ws_of(*prob, workspace);
+    const DevInfo* d = dev_info();
+    if (!d) return MPM_E_CUDA;
+    int rctas = d->sms * 4;
+    const int64_t need = (prob->n_blocks + 3) / 4;
+    if (rctas > need) rctas = (int)(need > 0 ? need : 1);
     for (int32_t j = 0; j < n_substeps; ++j) {
+        const RecGrid r = rec_grid_of(*prob, grid_rec, j);
         if (cudaMemcpyAsync(state_rec + (size_t)j * plane, par->state, plane * 4, cudaMemcpyDeviceToDevice, s) !=
             cudaSuccess)
             return MPM_E_CUDA;
         if ((rc = launch_p2g(prob, tab, par, workspace, s))) return rc;
-        // the grid op clears the momentum behind itself: keep the p2g result first
-        if (cudaMemcpyAsync(g + (2 * (size_t)j) * nodes, w.mm, nodes * 16, cudaMemcpyDeviceToDevice, s) !=
-            cudaSuccess)
-            return MPM_E_CUDA;
+        // the grid op clears the momentum behind itself and resets the active count: keep the
+        // p2g result and the list first
+        k_record_p2g<<<rctas, 256, 0, s>>>(tab->instances, w, r);
         if ((rc = launch_grid_op(prob, tab, workspace, s))) return rc;
-        if (cudaMemcpyAsync(g + (2 * (size_t)j + 1) * nodes, w.gv, nodes * 16, cudaMemcpyDeviceToDevice, s) !=
-            cudaSuccess)
-            return MPM_E_CUDA;
+        k_record_gv<<<rctas, 256, 0, s>>>(tab->instances, w, r);
         if ((rc = launch_g2p(prob, tab, par, workspace, s))) return rc;
     }
     return cuda_ok();
@@ -2826,20 +2892,26 @@ int mpm_substeps_adjoint_recorded(const mpm_problem* prob, const mpm_tables* tab
     const int n = prob->n_particles;
     const size_t plane = (size_t)MPM_STATE_CH * (size_t)par->state_stride;
     const size_t nodes = (size_t)prob->n_blocks * BLK3;
-    const float4* g = (const float4*)grid_rec;
     AdjWs aw = adj_ws_of(*prob, adj_workspace);
     Ws w{};  // the adjoint kernels read only the grid velocity from it
+    // the grid adjoint clears vbar behind itself over each substep's active blocks, which hold
+    // every node the g2p adjoint writes: one clear per call
+    if (count > 0 && cudaMemsetAsync(aw.vbar, 0, nodes * 16, s) != cudaSuccess) return MPM_E_CUDA;
+    const DevInfo* d = dev_info();
+    if (!d) return MPM_E_CUDA;
+    int gctas = d->sms * 4;
+    const int64_t need = (prob->n_blocks + 3) / 4;
+    if (gctas > need) gctas = (int)(need > 0 ? need : 1);
     for (int32_t j = first + count - 1; j >= first; --j) {
+        const RecGrid r = rec_grid_of(*prob, const_cast<void*>(grid_rec), j);
         mpm_particles sp = *par;
         sp.state = const_cast<float*>(state_rec) + (size_t)j * plane;
-        aw.saved_mm = const_cast<float4*>(g + (2 * (size_t)j) * nodes);
-        w.gv = const_cast<float4*>(g + (2 * (size_t)j + 1) * nodes);
-        if (cudaMemsetAsync(aw.vbar, 0, nodes * 16, s) != cudaSuccess) return MPM_E_CUDA;
+        aw.saved_mm = r.mm;
+        w.gv = r.gv;
         if (n > 0) {
             k_adj_g2p<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, sp, adj, w, aw);
-            k_adj_grid<<<(int)((nodes + 255) / 256), 256, 0, s>>>(*prob, tab->instances, w, aw, nullptr, 0,
-                                                                   tab->sdf_voxels, nullptr, tab->force_fields, nff,
-                                                                   tab->ff_perm);
+            k_adj_grid_active<<<gctas, 256, 0, s>>>(*prob, tab->instances, aw, r.active, r.n_active, tab->force_fields,
+                                                    nff, tab->ff_perm);
             k_adj_p2g<<<(n + 127) / 128, 128, 0, s>>>(*prob, tab->instances, tab->materials, sp, adj, lame_bar, aw);
         }
     }

@@ -152,9 +152,10 @@ class SceneTape:
     def _adjoint_step_recorded(self, m: int):
         rt = self.rt
         if getattr(self, "_rec", None) is None or self._rec[0].shape[0] != m:
-            nodes = int(rt.prob.n_blocks) * 64
+            gb = C.c_uint64()
+            nat.check("mpm_record_grid_bytes", rt.lib.mpm_record_grid_bytes(C.byref(rt.prob), C.byref(gb)))
             self._rec = (torch.empty((m,) + tuple(rt.state.shape), dtype=torch.float32, device=rt.device),
-                         torch.empty((m, 2, nodes, 4), dtype=torch.float32, device=rt.device))
+                         torch.empty(m * int(gb.value), dtype=torch.uint8, device=rt.device))
         rs, rg = self._rec
         stream = _cuda_stream_handle()
         nat.check("mpm_substeps_record", rt.lib.mpm_substeps_record(

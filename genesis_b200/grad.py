@@ -142,14 +142,15 @@ class DifferentiableRollout:
 
     def _records(self):
         """Two buffers of per-substep records of one checkpoint segment (one being written
-        while the adjoint reads the other): input states [k, 25, stride] and grids
-        [k, 2, nodes, 4] (momentum + mass after p2g, velocity after the grid op), kept across
-        backward calls."""
+        while the adjoint reads the other): input states [k, 25, stride] and grid records
+        (momentum + mass after p2g, velocity after the grid op, the active-block list;
+        mpm_record_grid_bytes each), kept across backward calls."""
         rt = self.rt
-        nodes = int(rt.prob.n_blocks) * 64
         if getattr(self, "_rec", None) is None:
+            gb = C.c_uint64()
+            nat.check("mpm_record_grid_bytes", rt.lib.mpm_record_grid_bytes(C.byref(rt.prob), C.byref(gb)))
             self._rec = [(torch.empty((self.k,) + tuple(rt.state.shape), dtype=torch.float32, device=rt.device),
-                          torch.empty((self.k, 2, nodes, 4), dtype=torch.float32, device=rt.device))
+                          torch.empty(self.k * int(gb.value), dtype=torch.uint8, device=rt.device))
                          for _ in range(2)]
         return self._rec
 

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 13
+#define MPM_ABI_VERSION 14
 
 #define MPM_OK 0
 #define MPM_E_INVALID -1     /* bad argument / inconsistent sizes */
@@ -419,15 +419,20 @@ int mpm_substep_adjoint_colliders(const mpm_problem* prob, const mpm_tables* tab
  *   mpm_substeps_record advances the particles by n_substeps substeps (p2g, grid op, g2p per
  *     substep, no re-sort: the particles must be binned by an earlier mpm_sort_particles) and
  *     stores, for substep j, its input state in state_rec[j] (float[25][state_stride], the
- *     state's planar layout) and its grid in grid_rec[j] (two float4[n_blocks * 64] planes: the
- *     momentum and mass after p2g, then the velocity after the grid op).
+ *     state's planar layout) and its grid in the j-th record of grid_rec, each
+ *     mpm_record_grid_bytes long: the momentum and mass after p2g and the velocity after the
+ *     grid op (float4[n_blocks * 64] planes, written only in the active blocks), then the active
+ *     grid blocks the grid op walked (int32 pairs {instance, packed block coordinates}, room for
+ *     n_blocks of them) and their number.
  *   mpm_substeps_adjoint_recorded runs the adjoint of recorded substeps first + count - 1 down
  *     to first, as mpm_substep_adjoint would for each (adj and lame_bar as there), reading
- *     state_rec and grid_rec instead of recomputing them.
+ *     state_rec and grid_rec instead of recomputing them; its grid adjoint visits only each
+ *     substep's active blocks.
  * Both refuse colliders (MPM_E_INVALID: their poses move between substeps); force fields are
- * allowed.  state_rec holds n_substeps * 25 * state_stride floats, grid_rec n_substeps * 2 *
- * n_blocks * 64 * 16 bytes.  The particle tables of `par` (mat, pflags, mu_p, lam_p, actu, ...)
- * must be the ones of the recorded run; its state pointer is not read by the adjoint. */
+ * allowed.  state_rec holds n_substeps * 25 * state_stride floats, grid_rec n_substeps *
+ * mpm_record_grid_bytes bytes.  The particle tables of `par` (mat, pflags, mu_p, lam_p, actu,
+ * ...) must be the ones of the recorded run; its state pointer is not read by the adjoint. */
+int mpm_record_grid_bytes(const mpm_problem* prob, uint64_t* out);
 int mpm_substeps_record(const mpm_problem* prob, const mpm_tables* tab, mpm_particles* par, void* workspace,
                         int32_t n_substeps, float* state_rec, void* grid_rec, void* stream);
 int mpm_substeps_adjoint_recorded(const mpm_problem* prob, const mpm_tables* tab, const mpm_particles* par,

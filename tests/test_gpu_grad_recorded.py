@@ -68,11 +68,12 @@ def test_record_and_recorded_adjoint_match_the_per_substep_adjoint():
     nb = C.c_uint64()
     nat.check("mpm_adjoint_workspace_bytes", lib.mpm_adjoint_workspace_bytes(C.byref(rt.prob), C.byref(nb)))
     aws = torch.empty(int(nb.value), dtype=torch.uint8, device=rt.device)
-    nodes = int(rt.prob.n_blocks) * 64
+    gb = C.c_uint64()
+    nat.check("mpm_record_grid_bytes", lib.mpm_record_grid_bytes(C.byref(rt.prob), C.byref(gb)))
 
     # recorded forward: the states it stores are the per-substep states of an ordinary run
     rec_state = torch.empty((m,) + tuple(rt.state.shape), dtype=torch.float32, device=rt.device)
-    rec_grid = torch.empty((m, 2, nodes, 4), dtype=torch.float32, device=rt.device)
+    rec_grid = torch.empty(m * int(gb.value), dtype=torch.uint8, device=rt.device)
     nat.check("mpm_substeps_record", lib.mpm_substeps_record(
         C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), rt._ws, m, C.c_void_p(rec_state.data_ptr()),
         C.c_void_p(rec_grid.data_ptr()), _stream()))
