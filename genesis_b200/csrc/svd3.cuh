@@ -28,6 +28,10 @@ namespace gbm {
 #define GBM_SVD_UNROLL 1
 #endif
 constexpr int kSvdUnroll = GBM_SVD_UNROLL;
+// early-exit level of the Jacobi sweeps: off-diagonal mass of A^T A against its trace
+#ifndef GBM_SVD_TOL
+#define GBM_SVD_TOL 1e-7f
+#endif
 
 // One Jacobi rotation in plane (P, Q) of the symmetric matrix a, accumulated into v.
 template <int P, int Q>
@@ -141,7 +145,7 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* S, float* 
     // threshold, or one relative to each pair's own diagonal, changes neither the benchmark
     // scenes' trajectories nor the small-direction accuracy below, measured: the limit there
     // is forming A^T A in float32, which the one-sided sweep after the QR ordering addresses.)
-    const float thr = 1e-7f * (a[0][0] + a[1][1] + a[2][2]);
+    const float thr = GBM_SVD_TOL * (a[0][0] + a[1][1] + a[2][2]);
     auto converged = [&]() {
         return __all_sync(__activemask(), !need_uv || !(fabsf(a[0][1]) + fabsf(a[0][2]) + fabsf(a[1][2]) > thr));
     };
