@@ -594,8 +594,12 @@ class MPMRuntime:
                 self._sorted_once = True
                 self._dirty = False
             if n > 0:
-                self._call("mpm_substeps", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
-                           n, 0, self._count, stream)
+                if self.use_graphs:
+                    # one captured graph per run length (a rollout's checkpoint segments repeat it)
+                    self._call("mpm_graph_launch", self._graph_unsorted(n), stream)
+                else:
+                    self._call("mpm_substeps", C.byref(self.prob), C.byref(self.tables), C.byref(self.par),
+                               self._ws, n, 0, self._count, stream)
                 self._count += n
             return
         K = max(self.sort_interval, 1)
@@ -616,6 +620,22 @@ class MPMRuntime:
                        m, K, self._count, stream)
             n -= m
             self._count += m
+
+    def _graph_unsorted(self, n: int):
+        """A graph of n substeps without a sort (the runtime never re-sorts)."""
+        key = ("unsorted", n, self.prob.flags)
+        g = self._graphs.get(key)
+        if g is None:
+            side = torch.cuda.Stream(device=self.device)
+            side.wait_stream(torch.cuda.current_stream())
+            h = C.c_void_p()
+            with torch.cuda.stream(side):
+                self._call("mpm_graph_create", C.byref(self.prob), C.byref(self.tables), C.byref(self.par), self._ws,
+                           n, 0, 0, C.c_void_p(side.cuda_stream), C.byref(h))
+            torch.cuda.current_stream().wait_stream(side)
+            g = h
+            self._graphs[key] = g
+        return g
 
     def _graph(self, K: int):
         key = (K, self.prob.flags)

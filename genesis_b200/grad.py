@@ -45,7 +45,7 @@ class DifferentiableRollout:
         self.k = int(checkpoint_every)
         self.T = int(desc.n_substeps)
         # one sort before the rollout, none after: the adjoint walks the same slot order
-        self.rt: MPMRuntime = runtime_from_descs([desc], sort_interval=0, use_graphs=False)
+        self.rt: MPMRuntime = runtime_from_descs([desc], sort_interval=0)
         mats = self.rt.specs[0].materials
         mi = torch.as_tensor(desc.mat_idx, dtype=torch.long, device=self.rt.device)
         nus = torch.tensor([m.nu for m in mats], dtype=torch.float32, device=self.rt.device)
