@@ -8,7 +8,8 @@ substep's input state and grid (mpm_substeps_record), and runs the adjoint of ea
 from the last to the first on those records (mpm_substeps_adjoint_recorded), so no substep's
 forward is evaluated twice in the reverse pass.  The recompute of the segment before runs on a
 second stream beside that adjoint (neither reads what the other writes), which fills a GPU
-that one small scene leaves mostly idle.  Memory is one state per checkpoint plus two
+that one small scene leaves mostly idle; both are replayed as CUDA graphs captured on first
+use (per record buffer and run length).  Memory is one state per checkpoint plus two
 segments of states and grids, instead of every substep.
 
 Supported: scenes of any mix of MPM materials (Elastic corotated or neo-Hookean, Muscle,
@@ -154,14 +155,32 @@ class DifferentiableRollout:
                          for _ in range(2)]
         return self._rec
 
-    def _adjoint_recorded(self, first: int, count: int, rec_state: torch.Tensor, rec_grid: torch.Tensor):
+    def _replay(self, key, launch):
+        """Run `launch` (library calls on the current stream, fixed buffers) as a CUDA graph
+        captured on first use and replayed on the current stream after."""
+        if getattr(self, "_graphs", None) is None:
+            self._graphs = {}
+        g = self._graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                launch()
+            self._graphs[key] = g
+        g.replay()
+
+    def _adjoint_recorded(self, first: int, count: int, buf: int):
         if count <= 0:
             return
         rt = self.rt
-        nat.check("mpm_substeps_adjoint_recorded", rt.lib.mpm_substeps_adjoint_recorded(
-            C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), first, count,
-            C.c_void_p(rec_state.data_ptr()), C.c_void_p(rec_grid.data_ptr()), C.c_void_p(self.adj.data_ptr()),
-            C.c_void_p(self.lame_bar.data_ptr()), C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
+        rs, rg = self._rec[buf]
+
+        def launch():
+            nat.check("mpm_substeps_adjoint_recorded", rt.lib.mpm_substeps_adjoint_recorded(
+                C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), first, count,
+                C.c_void_p(rs.data_ptr()), C.c_void_p(rg.data_ptr()), C.c_void_p(self.adj.data_ptr()),
+                C.c_void_p(self.lame_bar.data_ptr()), C.c_void_p(self.adj_ws.data_ptr()), _cuda_stream_handle()))
+
+        self._replay(("adjoint", buf, first, count), launch)
 
     def backward(self, pos_grad: torch.Tensor):
         """pos_grad: dL/dx_final [N,3] in API order (or, after a forward with record,
@@ -203,13 +222,17 @@ class DifferentiableRollout:
             # and grid into buffer c % 2, after the adjoint that last read that buffer (c + 2)
             t0, t1 = c * self.k, min((c + 1) * self.k, self.T)
             rs, rg = recs[c % 2]
+
+            def launch():
+                nat.check("mpm_substeps_record", lib.mpm_substeps_record(
+                    C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), rt._ws, t1 - t0,
+                    C.c_void_p(rs.data_ptr()), C.c_void_p(rg.data_ptr()), _cuda_stream_handle()))
+
             with torch.cuda.stream(side):
                 if c + 2 < nseg:
                     side.wait_event(adj_done[c + 2])
                 rt.state.copy_(self.checkpoints[c])
-                nat.check("mpm_substeps_record", lib.mpm_substeps_record(
-                    C.byref(rt.prob), C.byref(rt.tables), C.byref(rt.par), rt._ws, t1 - t0,
-                    C.c_void_p(rs.data_ptr()), C.c_void_p(rg.data_ptr()), _cuda_stream_handle()))
+                self._replay(("record", c % 2, t1 - t0), launch)
                 rec_done[c] = torch.cuda.Event()
                 rec_done[c].record(side)
 
@@ -220,17 +243,16 @@ class DifferentiableRollout:
                 record(ci - 1)  # runs beside this segment's adjoint: it reads only the records
             t0, t1 = ci * self.k, min((ci + 1) * self.k, self.T)
             m = t1 - t0
-            rs, rg = recs[ci % 2]
             main.wait_event(rec_done[ci])
             # the adjoint of substeps m-1 .. 0, split where dL/dx of an interior substep enters
             hi = m
             for j in range(m - 1, -1, -1):
                 r = t0 + j + 1
                 if r != self.T and r in inject:
-                    self._adjoint_recorded(j + 1, hi - j - 1, rs, rg)
+                    self._adjoint_recorded(j + 1, hi - j - 1, ci % 2)
                     add(r)
                     hi = j + 1
-            self._adjoint_recorded(0, hi, rs, rg)
+            self._adjoint_recorded(0, hi, ci % 2)
             adj_done[ci] = torch.cuda.Event()
             adj_done[ci].record(main)
         main.wait_stream(side)
