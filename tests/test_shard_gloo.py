@@ -1,5 +1,7 @@
 """Multi-process sharding of independent scenes on CPU: two gloo ranks partition a batch
-by work, each 'processes' its shard, and the gathered results cover every scene once."""
+by work, each advances its shard (with the CPU restatement standing in for the CUDA kernels:
+there is no GPU here), and the gathered results cover every scene once and equal a
+single-process run of the same scenes."""
 
 import os
 
@@ -11,6 +13,14 @@ from genesis_b200 import shard
 from genesis_b200 import workloads as W
 
 
+def _advance(d, n_substeps=3):
+    from oracle import bridge, cref
+
+    out, rc = cref.substeps(*bridge.from_desc(d, np.float64), n_substeps)
+    assert rc == 0
+    return out["x"]
+
+
 def _worker(rank, world, port, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -20,8 +30,8 @@ def _worker(rank, world, port, q):
     try:
         descs = W.batch_scenes(n_scenes=24, n_range=(500, 5000), densities=(32,))
         mine = shard.my_shard(descs, rank, world)
-        # stand-in for the batched run: per scene, its name and particle count
-        res = [(d.name, d.n_particles) for d in mine]
+        # each rank advances its own scenes; per scene its name, particle count and final positions
+        res = [(d.name, d.n_particles, _advance(d)) for d in mine]
         allres = shard.gather_objects(res, world)
         if rank == 0:
             q.put(allres)
@@ -41,10 +51,15 @@ def test_two_gloo_ranks_cover_every_scene_once():
         p.join(timeout=60)
         assert p.exitcode == 0
     descs = W.batch_scenes(n_scenes=24, n_range=(500, 5000), densities=(32,))
-    names = sorted(n for part in allres for n, _ in part)
+    names = sorted(n for part in allres for n, _, _ in part)
     assert names == sorted(d.name for d in descs)
-    loads = [sum(n for _, n in part) for part in allres]
+    loads = [sum(n for _, n, _ in part) for part in allres]
     assert max(loads) <= 1.34 * (sum(loads) / 2)  # LPT balance bound with slack
+    # the sharded results are the single-process ones (each scene is independent; the
+    # restatement's threaded grid sums may round in another order, so to float64 round-off)
+    got = {name: x for part in allres for name, _, x in part}
+    for d in descs[:6]:
+        assert np.abs(got[d.name] - _advance(d)).max() <= 1e-12, d.name
 
 
 def test_partition_is_balanced_and_complete():
