@@ -892,6 +892,7 @@ struct Tile {
 // distinct within each 8-lane phase of a 16-byte load.
 constexpr int VYS = TILE;           // y-stride (nodes)
 constexpr int VXS = TXS;            // x-stride (68 nodes)
+static_assert(VXS == TXS && VYS == TILE, "the velocity tile shares the scatter tile's node index");
 __device__ __forceinline__ int vidx(int x, int y, int z) { return x * VXS + y * VYS + z; }
 
 struct VelTile {
@@ -1156,18 +1157,19 @@ __device__ __forceinline__ void cpic_correct(const P2GArgs& a, const VelTile* VT
 // Tile node n of the 8^3 tile whose origin is (4b - 1) per axis lies in grid block b + db
 // (db in {-1, 0, 1}) at in-block offset (t + 3) & 3.  These depend only on n, so each
 // thread packs them once for the nodes it owns:
-//   bits 0-5 in-block node index, 6-7/8-9/10-11 db + 1 per axis, 12-21 shared-tile index,
-//   22-24/25-27/28-30 tile coordinates
+//   bits 0-5 in-block node index, 6-10 neighbour id (dbx + 1) 9 + (dby + 1) 3 + (dbz + 1),
+//   12-21 shared-tile index, 22-24/25-27/28-30 tile coordinates
 __device__ __forceinline__ uint32_t node_desc(int n) {
     const int t[3] = {n >> 6, (n >> 3) & 7, n & 7};
     uint32_t d = 0;
-    int ln = 0;
+    int ln = 0, nid = 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         ln = ln * BLK + ((t[a] + 3) & 3);
-        d |= (uint32_t)((t[a] + 3) >> 2) << (6 + 2 * a);
+        nid = nid * 3 + ((t[a] + 3) >> 2);
         d |= (uint32_t)t[a] << (22 + 3 * a);
     }
+    d |= (uint32_t)nid << 6;
     d |= (uint32_t)ln;
     d |= (uint32_t)tidx(t[0], t[1], t[2]) << 12;
     return d;
@@ -1194,10 +1196,28 @@ __device__ __forceinline__ Nbhd nbhd_of(const mpm_instance& I, const BlockCoord&
 
 // grid address of tile node d, or -1 if its block lies outside the grid
 __device__ __forceinline__ int64_t nbhd_addr(const Nbhd& h, uint32_t d) {
-    const uint32_t ex = (d >> 6) & 3, ey = (d >> 8) & 3, ez = (d >> 10) & 3;
+    const uint32_t nid = (d >> 6) & 31;
+    const uint32_t ex = nid / 9, ey = (nid / 3) % 3, ez = nid % 3;
     if (!((h.vx >> ex) & (h.vy >> ey) & (h.vz >> ez) & 1u)) return -1;
     const int g = h.g0 + ((int)ex - 1) * h.sx + ((int)ey - 1) * h.sy + ((int)ez - 1);
     return ((int64_t)g << 6) + (d & 63);
+}
+
+// The 27 neighbour blocks of a work item's block as global block indices (-1 outside the
+// grid), by neighbour id; threads 0..26 write one entry each.  With it a tile node's grid
+// address is one shared load and a shift from its descriptor.
+__device__ __forceinline__ void nb_table(const mpm_instance& I, const BlockCoord& bc, int* tab) {
+    if (threadIdx.x < 27) {
+        const int t = (int)threadIdx.x;
+        const int bx = bc.bx + t / 9 - 1, by = bc.by + (t / 3) % 3 - 1, bz = bc.bz + t % 3 - 1;
+        const bool in = bx >= 0 && by >= 0 && bz >= 0 && bx < I.nblk[0] && by < I.nblk[1] && bz < I.nblk[2];
+        tab[t] = in ? (int)(I.blk_base + (bx * I.nblk[1] + by) * I.nblk[2] + bz) : -1;
+    }
+}
+
+__device__ __forceinline__ int64_t tab_addr(const int* tab, uint32_t d) {
+    const int blk = tab[(d >> 6) & 31];
+    return blk < 0 ? -1 : ((int64_t)blk << 6) + (d & 63);
 }
 
 // zero the whole tile (once per kernel; the flush re-zeroes what it touched)
@@ -1217,7 +1237,7 @@ __device__ __forceinline__ void tile_zero(Tile& T, int P) {
 // thread owns (nd), and the next chunk writes the tile only after two more barriers.
 template <int P, bool CPIC = false>
 __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const mpm_instance& I, int inst,
-                                              const BlockCoord& bc, int ox, int oy, int oz, Ws& w, const Nbhd& h,
+                                              const BlockCoord& bc, int ox, int oy, int oz, Ws& w, const int* tab,
                                               const uint32_t* nd, const P2GArgs* cp = nullptr) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const float wbq = warp_max(o.in_tile ? o.bq : 0.f);
@@ -1255,7 +1275,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
     if (threadIdx.x < 27 && cnt > 0) {
         const int t = (int)threadIdx.x;
         const int e[3] = {t / 9, (t / 3) % 3, t % 3};  // db + 1 per axis
-        bool on = ((h.vx >> e[0]) & (h.vy >> e[1]) & (h.vz >> e[2]) & 1u) != 0u;
+        bool on = tab[t] >= 0;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             if (e[a] == 0) on = on && ((rch >> (2 * a)) & 1u);
@@ -1386,7 +1406,7 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
         if ((mi | m0 | m1 | m2) != 0) {
             const int tx = (d >> 22) & 7, ty = (d >> 25) & 7, tz = (d >> 28) & 7;
             const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
-            const int64_t a = nbhd_addr(h, d);
+            const int64_t a = tab_addr(tab, d);
             if (a < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
                 set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
             } else {
@@ -1397,6 +1417,17 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
             T.t[2][t] = 0;
             T.t[3][t] = 0;
         }
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void vel_tile_load_tab(VelTile& VT, const Ws& w, const int* tab, const uint32_t* nd) {
+#pragma unroll
+    for (int k = 0; k < TN / P; ++k) {
+        const uint32_t d = nd[threadIdx.x + k * P];
+        const int64_t a = tab_addr(tab, d);
+        // the velocity tile has the scatter tile's layout, so the descriptor's tile index serves
+        VT.v[(d >> 12) & 1023] = a >= 0 ? w.gv[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
@@ -1592,11 +1623,15 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
 #pragma unroll
     for (int k = 0; k < TN / P; ++k) nd[threadIdx.x + k * P] = node_desc(threadIdx.x + k * P);
     tile_zero(T, P);
+    // the item's neighbour-block table, first read behind the scatter's first barrier; two
+    // buffers, as the previous item's flush may still read its own
+    __shared__ int nbt[2][27];
+    int tb = 0;
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = w.chunks[ci];
         const mpm_instance& I = a.inst[ch.x];
         const BlockCoord bc = unpack_bc(ch.y);
-        const Nbhd h = nbhd_of(I, bc);
+        nb_table(I, bc, nbt[tb]);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
         Payload o;
         o.live = o.in_tile = false;
@@ -1619,7 +1654,8 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a
             }
             particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, v, C, ox, oy, oz, o, w, ch.x, SH);
         }
-        scatter_flush<P, CPIC>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd, &a);
+        scatter_flush<P, CPIC>(T, o, I, ch.x, bc, ox, oy, oz, w, nbt[tb], nd, &a);
+        tb ^= 1;
     }
 }
 
@@ -1683,6 +1719,12 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
     // position and flags are in flight during its velocity-tile load: the item start's chain of
     // dependent loads (descriptor -> tile; then position -> gather) loses two L2 round trips
     int4 next = blockIdx.x < n_chunks ? w.chunks[blockIdx.x] : make_int4(0, 0, 0, 0);
+    // neighbour-block tables (global block index per neighbour id): each item's is built during
+    // the item before (behind that item's tile barrier; read at this item's tile load and flush)
+    __shared__ int nbt[2][27];
+    int tb = 0;
+    if ((int)blockIdx.x < n_chunks) nb_table(a.inst[next.x], unpack_bc(next.y), nbt[0]);
+    __syncthreads();
     for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
         const int4 ch = next;
         if (ci + (int)gridDim.x < n_chunks) next = w.chunks[ci + gridDim.x];
@@ -1697,10 +1739,11 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
         }
         const mpm_instance& I = a.inst[ch.x];
         const BlockCoord bc = unpack_bc(ch.y);
-        const Nbhd h = nbhd_of(I, bc);
         const int ox = bc.bx * BLK - MARGIN, oy = bc.by * BLK - MARGIN, oz = bc.bz * BLK - MARGIN;
-        vel_tile_load<P>(VT, w, h, nd);
+        vel_tile_load_tab<P>(VT, w, nbt[tb], nd);
         __syncthreads();
+        // the other table was last read by the previous item's flush, before this barrier
+        if (ci + (int)gridDim.x < n_chunks) nb_table(a.inst[next.x], unpack_bc(next.y), nbt[tb ^ 1]);
         Payload o;
         o.live = o.in_tile = false;
         o.mass = o.bq = 0.f;
@@ -1722,7 +1765,8 @@ __global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs
                 particle_update<P, MUSCLE>(I, a.mats, a.par, p, x, nv, nC, ox, oy, oz, o, w, ch.x, SH);
             }
         }
-        scatter_flush<P, CPIC>(T, o, I, ch.x, bc, ox, oy, oz, w, h, nd, &a);
+        scatter_flush<P, CPIC>(T, o, I, ch.x, bc, ox, oy, oz, w, nbt[tb], nd, &a);
+        tb ^= 1;
     }
 }
 
