@@ -40,6 +40,13 @@ namespace gbm {
 #ifndef GBM_P2G_THREADS_PER_SM
 #define GBM_P2G_THREADS_PER_SM 896
 #endif
+// the same for 256- and 512-particle work items: 4 CTAs of 256 threads (64 registers) ran the
+// 256-scene batch 1.2% faster than 3 (80 registers); 128-particle items keep 7 CTAs of 128
+#ifndef GBM_P2G_THREADS_PER_SM_WIDE
+#define GBM_P2G_THREADS_PER_SM_WIDE 1024
+#endif
+template <int P>
+constexpr int kP2GCtasPerSM = (P <= 128 ? GBM_P2G_THREADS_PER_SM : GBM_P2G_THREADS_PER_SM_WIDE) / P;
 // unroll factor of the outermost stencil loops (3: fully unrolled, 1: rolled, smaller code)
 #ifndef GBM_OUTER_UNROLL
 #define GBM_OUTER_UNROLL 3
@@ -1204,20 +1211,25 @@ __device__ __forceinline__ int64_t nbhd_addr(const Nbhd& h, uint32_t d) {
 }
 
 // The 27 neighbour blocks of a work item's block as global block indices (-1 outside the
-// grid), by neighbour id; threads 0..26 write one entry each.  With it a tile node's grid
-// address is one shared load and a shift from its descriptor.
+// grid), by neighbour id, NB_PARTIAL set on blocks that reach past the grid's last node (the
+// grid's last block layer, whose padding nodes the flush must not write); threads 0..26
+// write one entry each.  With it a tile node's grid address is one shared load and a shift
+// from its descriptor.
+constexpr int NB_PARTIAL = 1 << 30;
+
 __device__ __forceinline__ void nb_table(const mpm_instance& I, const BlockCoord& bc, int* tab) {
     if (threadIdx.x < 27) {
         const int t = (int)threadIdx.x;
         const int bx = bc.bx + t / 9 - 1, by = bc.by + (t / 3) % 3 - 1, bz = bc.bz + t % 3 - 1;
         const bool in = bx >= 0 && by >= 0 && bz >= 0 && bx < I.nblk[0] && by < I.nblk[1] && bz < I.nblk[2];
-        tab[t] = in ? (int)(I.blk_base + (bx * I.nblk[1] + by) * I.nblk[2] + bz) : -1;
+        const bool partial = (bx + 1) * BLK > I.res[0] || (by + 1) * BLK > I.res[1] || (bz + 1) * BLK > I.res[2];
+        tab[t] = in ? (int)(I.blk_base + (bx * I.nblk[1] + by) * I.nblk[2] + bz) | (partial ? NB_PARTIAL : 0) : -1;
     }
 }
 
 __device__ __forceinline__ int64_t tab_addr(const int* tab, uint32_t d) {
     const int blk = tab[(d >> 6) & 31];
-    return blk < 0 ? -1 : ((int64_t)blk << 6) + (d & 63);
+    return blk < 0 ? -1 : ((int64_t)(blk & ~NB_PARTIAL) << 6) + (d & 63);
 }
 
 // zero the whole tile (once per kernel; the flush re-zeroes what it touched)
@@ -1404,12 +1416,17 @@ __device__ __forceinline__ void scatter_flush(Tile& T, const Payload& o, const m
         const int t = (d >> 12) & 1023;
         const int mi = T.t[3][t], m0 = T.t[0][t], m1 = T.t[1][t], m2 = T.t[2][t];
         if ((mi | m0 | m1 | m2) != 0) {
-            const int tx = (d >> 22) & 7, ty = (d >> 25) & 7, tz = (d >> 28) & 7;
-            const int gx = ox + tx, gy = oy + ty, gz = oz + tz;
-            const int64_t a = tab_addr(tab, d);
-            if (a < 0 || gx >= I.res[0] || gy >= I.res[1] || gz >= I.res[2]) {
+            const int e = tab[(d >> 6) & 31];
+            bool ok = e >= 0;
+            if (ok && (e & NB_PARTIAL)) {
+                // a block of the grid's last layer: its padding nodes lie outside the grid
+                const int tx = (d >> 22) & 7, ty = (d >> 25) & 7, tz = (d >> 28) & 7;
+                ok = ox + tx < I.res[0] && oy + ty < I.res[1] && oz + tz < I.res[2];
+            }
+            if (!ok) {
                 set_status(w, inst, MPM_STATUS_OUT_OF_GRID);
             } else {
+                const int64_t a = ((int64_t)(e & ~NB_PARTIAL) << 6) + (d & 63);
                 atomicAdd(&w.mm[a], make_float4((float)m0 * iq, (float)m1 * iq, (float)m2 * iq, (float)mi * im));
             }
             T.t[0][t] = 0;
@@ -1612,7 +1629,7 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
 // ---------------------------------------------------------------- p2g
 
 template <int P, bool MUSCLE, bool CPIC>
-__global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_p2g(P2GArgs a) {
+__global__ void __launch_bounds__(P, kP2GCtasPerSM<P>) k_p2g(P2GArgs a) {
     __shared__ Tile T;
     __shared__ Stash<P> SH;
     Ws& w = a.w;
@@ -1703,7 +1720,7 @@ __global__ void __launch_bounds__(P, 1024 / P) k_g2p(P2GArgs a) {
 // g2p of substep n fused with p2g of substep n+1: the new v and C never leave registers
 // (they are recomputed from the grid by the next gather), only x, F and Jp are stored.
 template <int P, bool MUSCLE, bool CPIC>
-__global__ void __launch_bounds__(P, GBM_P2G_THREADS_PER_SM / P) k_g2p2g(P2GArgs a) {
+__global__ void __launch_bounds__(P, kP2GCtasPerSM<P>) k_g2p2g(P2GArgs a) {
     __shared__ VelTile VT;
     __shared__ Tile T;
     __shared__ Stash<P> SH;
