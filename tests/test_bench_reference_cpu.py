@@ -1,5 +1,5 @@
 """bench.py's reference arm runs on the host alone (the C restatement on every host thread)
-and prints the JSON line the driver reads: the same metric and config as the GPU arm, with
+and prints one JSON line: the same metric and config as the GPU arm, with
 `impl`, `cpu_baseline` and a zero-copy `e2e`."""
 
 import json

@@ -64,7 +64,7 @@ def _errs(g, o, sel):
 
 
 def test_elastic_cube_vs_fp64():
-    """Config 1 at full size: 32,768 particles, 65^3 grid, dt 1e-4, 100 substeps."""
+    """The elastic cube at full size: 32,768 particles, 65^3 grid, dt 1e-4, 100 substeps."""
     d = W.elastic_cube()
     _, g = _run([d], 100)
     o = _oracle(d, 100)
@@ -78,7 +78,7 @@ def test_elastic_cube_vs_fp64():
 
 
 def test_mixed_500k_vs_fp64_per_material():
-    """Config 2 at full size: 500,000 particles (Liquid, Sand, Snow, ElastoPlastic), 129^3 grid,
+    """The mixed scene at full size: 500,000 particles (Liquid, Sand, Snow, ElastoPlastic), 129^3 grid,
     dt 5e-5, 100 substeps.  Also reports, per material, how many particles came within 1e-5 of
     their return mapping's branch switch in the float64 run, and the error among them and
     among the rest (the float32 error is not concentrated near the switches)."""
