@@ -1491,59 +1491,60 @@ __device__ __forceinline__ bool gather(const VelTile& VT, const Ws& w, const mpm
             wxd[k] = wx[k] * ((float)k - fx[0]);
         }
         if constexpr (kF32x2Gather<P>) {
-            // the same sums on lane pairs (x, y) and (z, w); the tile's w is 0
+            // the same sums on lane pairs: (x, y) of every sum, and for z the pairs (s0, s1),
+            // (a0, az), (vp, c2), whose two lanes take the same node value: the tile's w holds
+            // a copy of z (k_grid_op stores (vx, vy, vz, vz)), so (g.z, g.w) is that pair as loaded
             const float2 z2 = make_float2(0.f, 0.f);
-            float2 vp[2] = {z2, z2}, c0[2] = {z2, z2}, c1[2] = {z2, z2}, c2[2] = {z2, z2};
+            float2 vp = z2, c0 = z2, c1 = z2, c2 = z2, vc2z = z2;
+            float c0z = 0.f, c1z = 0.f;
+            const float2 wzp[3] = {make_float2(wz[0], wzd[0]), make_float2(wz[1], wzd[1]), make_float2(wz[2], wzd[2])};
 #pragma unroll kOuterUnroll
             for (int i = 0; i < 3; ++i) {
-                float2 a0[2] = {z2, z2}, ay[2] = {z2, z2}, az[2] = {z2, z2};
+                float2 a0 = z2, ay = z2, az = z2, a0azz = z2;
+                float ayz = 0.f;
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    float2 s0[2] = {z2, z2}, s1[2] = {z2, z2};
+                    float2 s0 = z2, s1 = z2, s01z = z2;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const float4 g = VT.v[vidx(lx + i, ly + j, lz + k)];
-                        const float2 gp[2] = {make_float2(g.x, g.y), make_float2(g.z, g.w)};
-                        const float2 wk = dup2(wz[k]), wdk = dup2(wzd[k]);
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            s0[h] = fma2(wk, gp[h], s0[h]);
-                            s1[h] = fma2(wdk, gp[h], s1[h]);
-                        }
+                        const float2 gxy = make_float2(g.x, g.y);
+                        s0 = fma2(dup2(wz[k]), gxy, s0);
+                        s1 = fma2(dup2(wzd[k]), gxy, s1);
+                        s01z = fma2(wzp[k], make_float2(g.z, g.w), s01z);
                     }
                     const float2 wj = dup2(wy[j]), wdj = dup2(wyd[j]);
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        a0[h] = fma2(wj, s0[h], a0[h]);
-                        ay[h] = fma2(wdj, s0[h], ay[h]);
-                        az[h] = fma2(wj, s1[h], az[h]);
-                    }
+                    a0 = fma2(wj, s0, a0);
+                    ay = fma2(wdj, s0, ay);
+                    az = fma2(wj, s1, az);
+                    a0azz = fma2(wj, s01z, a0azz);
+                    ayz = fmaf(wyd[j], s01z.x, ayz);
                 }
                 const float2 wi = dup2(sel3(wx, i)), wdi = dup2(sel3(wxd, i));
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    vp[h] = fma2(wi, a0[h], vp[h]);
-                    c0[h] = fma2(wdi, a0[h], c0[h]);
-                    c1[h] = fma2(wi, ay[h], c1[h]);
-                    c2[h] = fma2(wi, az[h], c2[h]);
-                }
+                vp = fma2(wi, a0, vp);
+                c0 = fma2(wdi, a0, c0);
+                c1 = fma2(wi, ay, c1);
+                c2 = fma2(wi, az, c2);
+                vc2z = fma2(wi, a0azz, vc2z);
+                c0z = fmaf(sel3(wxd, i), a0azz.x, c0z);
+                c1z = fmaf(sel3(wx, i), ayz, c1z);
             }
-            nv[0] = vp[0].x;
-            nv[1] = vp[0].y;
-            nv[2] = vp[1].x;
+            nv[0] = vp.x;
+            nv[1] = vp.y;
+            nv[2] = vc2z.x;
             const float2 cs = dup2(I.c_scale);
-            c0[0] = __fmul2_rn(c0[0], cs);
-            c1[0] = __fmul2_rn(c1[0], cs);
-            c2[0] = __fmul2_rn(c2[0], cs);
-            nC[0] = c0[0].x;
-            nC[1] = c1[0].x;
-            nC[2] = c2[0].x;
-            nC[3] = c0[0].y;
-            nC[4] = c1[0].y;
-            nC[5] = c2[0].y;
-            nC[6] = c0[1].x * I.c_scale;
-            nC[7] = c1[1].x * I.c_scale;
-            nC[8] = c2[1].x * I.c_scale;
+            c0 = __fmul2_rn(c0, cs);
+            c1 = __fmul2_rn(c1, cs);
+            c2 = __fmul2_rn(c2, cs);
+            nC[0] = c0.x;
+            nC[1] = c1.x;
+            nC[2] = c2.x;
+            nC[3] = c0.y;
+            nC[4] = c1.y;
+            nC[5] = c2.y;
+            nC[6] = c0z * I.c_scale;
+            nC[7] = c1z * I.c_scale;
+            nC[8] = vc2z.y * I.c_scale;
         } else {
 #pragma unroll kOuterUnroll
         for (int i = 0; i < 3; ++i) {
@@ -2042,7 +2043,7 @@ __global__ void __launch_bounds__(256, 4) k_grid_op(mpm_problem prob, const mpm_
             vy = bc_vel(py, vy, I.bnd_lo[1], I.bnd_hi[1]);
             vz = bc_vel(pz, vz, I.bnd_lo[2], I.bnd_hi[2]);
         }
-        w.gv[g] = make_float4(vx, vy, vz, 0.f);
+        w.gv[g] = make_float4(vx, vy, vz, vz);  // w: a copy of z for the packed gather
         w.mm[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ln == 0) w.flag[I.blk_base + lb] = 0u;
     }
