@@ -62,11 +62,11 @@ constexpr int kP2GCtasPerSM = (P <= 128 ? GBM_P2G_THREADS_PER_SM : GBM_P2G_THREA
 
 constexpr int kOuterUnroll = GBM_OUTER_UNROLL;
 // GBM_F32X2_WIDE: the same bits for the 256- and 512-particle work items, whose register
-// budget differs: there the packed gather costs spills (40 B against 16 B at 256 threads per
-// CTA) and measured slower on the 256-scene batch (7.21e9 against 7.35e9 particle-substeps/s
-// with the packed scatter alone)
+// budget differs (64 registers at 4 CTAs of 256 threads per SM).  With the z channel paired
+// with itself in the gather, both packed forms measured faster on the 256-scene batch
+// (8.03e9 against 7.91e9 particle-substeps/s with the packed scatter alone)
 #ifndef GBM_F32X2_WIDE
-#define GBM_F32X2_WIDE 1
+#define GBM_F32X2_WIDE 3
 #endif
 template <int P>
 constexpr bool kF32x2Scatter = ((P <= 128 ? GBM_F32X2 : GBM_F32X2_WIDE) & 1) != 0;
