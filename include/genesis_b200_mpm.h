@@ -295,7 +295,8 @@ int mpm_max_chunks(int32_t n_particles, int64_t n_blocks, int32_t chunk_particle
 int mpm_workspace_bytes(const mpm_problem* prob, uint64_t* out);
 
 /* Byte offsets, inside the workspace, of the grid arrays: momentum+mass as float4
- * (x, y, z, mass) per node and velocity as float4 (x, y, z, 0), block-major: node
+ * (x, y, z, mass) per node and velocity as float4 (x, y, z, z: a copy of z that the
+ * packed gather reads as a (z, z) pair), block-major: node
  * (i, j, k) of instance k lives at ((blk_base + ((i/4)*nblk_y + j/4)*nblk_z + k/4) * 64
  * + ((i%4)*4 + j%4)*4 + k%4).  The momentum/mass grid holds p2g's output between
  * mpm_p2g and mpm_grid_op (grid op clears it); velocity holds grid op's output. */
